@@ -1,0 +1,348 @@
+"""Benchmark of the B200 APT solver.
+
+Workload (default, one GPU): the 2D batched configuration — 256 independent
+FP64 APT problems on sin-wavy meshes with sides drawn from U{64..512}, wave
+amplitude U(0, 0.08), κ = Tⁿ with n ∈ {0, 1, 2.5, 3}, Gaussian centre
+U(0.3, 0.7)² and width U(0.05, 0.2) from seed 20261203; every problem solves
+each time step to max|r|/√N ≤ 1e-8 (rtol = 0).  One bench step is one time
+step (dt = 1e-5) of the whole batch.  Inputs are synthetic (seeded), there is
+no dataset.
+
+Metric: Gcell-iter/s = Σ_p (domain cells_p × pseudo-iterations_p) / time,
+aggregated over all ranks (each rank solves its own seeded batch: weak
+scaling, no collective in the data path).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload batch|gaussian128|mms4096|gauss3d256]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+BYTES_PER_CELL_ITER = {2: 120, 3: 184}  # canonical algorithmic bytes, FP64 sweep
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="batch", choices=["batch", "gaussian128", "mms4096", "gauss3d256"])
+    ap.add_argument("--nprob", type=int, default=256)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- distributed
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch.distributed as dist
+        import datetime
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if args.impl == "ours":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allreduce_max(x, ws, device=None):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(x, ws, device=None):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# -------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------- workloads
+def make_workload(name, nprob, rank, device):
+    from curvilineardiffusionmanuscript_b200 import problems
+    if name == "batch":
+        probs = problems.batch_2d(nprob=nprob, seed=problems.BATCH_SEED + rank, device=device)
+        cfg = {"workload": "batch2d_256_fp64", "nprob": nprob, "sides": "U{64..512}", "seed": problems.BATCH_SEED,
+               "dt": 1e-5, "tol": "max|r|/sqrt(N) <= 1e-8, rtol 0", "bcs": "Neumann x4", "mean": "harmonic"}
+    elif name == "gaussian128":
+        probs = [problems.gaussian_2d(128, device=device)]
+        cfg = {"workload": "gaussian2d_128_fp64", "kappa": "T^3", "dt": 1e-5, "tol": 1e-8}
+    elif name == "mms4096":
+        probs = [problems.mms_2d(4096, device=device)]
+        cfg = {"workload": "mms2d_4096_fp64", "kappa": "T^2.5", "dt": 1e-5, "tol": 1e-8}
+    else:
+        probs = [problems.gaussian_3d(256, device=device)]
+        cfg = {"workload": "gaussian3d_256_fp64", "kappa": "T^2.5", "dt": 1e-5, "tol": 1e-8}
+    return probs, cfg
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args, ws, rank):
+    """The reference's CPU algorithm (the oracle restatement: the Julia reference
+    cannot run here) on the host cores, each step a bounded sample."""
+    if rank != 0:
+        return
+    import torch
+    from oracle.oracle import OracleSolver, num_threads
+    probs, cfg = make_workload(args.workload, args.nprob, 0, "cpu")
+    sample = probs[: min(len(probs), 6)] if args.workload == "batch" else probs
+    solvers = [OracleSolver(p.mesh, p.bcs) for p in sample]
+    Ts = [p.T0.numpy().copy() for p in sample]
+    for p, o in zip(sample, solvers):
+        if p.source is not None:
+            o.set_source(p.source.numpy())
+    tot_ci, tot_t = 0, 0.0
+    for s in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        ci = 0
+        for p, o, T in zip(sample, solvers, Ts):
+            st, _ = o.step(T, p.rho.numpy(), p.cp, p.kappa.k0, p.kappa.n, p.dt, rtol=p.rtol, atol=p.atol,
+                           max_iter=100000)
+            ci += p.mesh.ncells * st["niter"]
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            tot_ci += ci
+            tot_t += dt
+    v = tot_ci / tot_t / 1e9
+    cores = num_threads()
+    line = {"metric": "Gcell-iter/s", "value": v, "unit": "Gcell-iter/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": cfg, "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "Gcell-iter/s", "cores": cores, "kind": "port",
+                             "sample": f"first {len(sample)} problems of the workload, one time step each per bench step"},
+            "e2e": {"value": v, "unit": "Gcell-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(probs, budget_s=15.0):
+    """Oracle (OpenMP, all host threads) on a bounded sample of the workload."""
+    from oracle.oracle import OracleSolver, num_threads
+    t_start = time.perf_counter()
+    ci, tt, used = 0, 0.0, 0
+    for p in probs:
+        o = OracleSolver(p.mesh.to("cpu"), p.bcs)
+        T = p.T0.cpu().numpy().copy()
+        if p.source is not None:
+            o.set_source(p.source.cpu().numpy())
+        t0 = time.perf_counter()
+        st, _ = o.step(T, p.rho.cpu().numpy(), p.cp, p.kappa.k0, p.kappa.n, p.dt, rtol=p.rtol, atol=p.atol,
+                       max_iter=100000)
+        tt += time.perf_counter() - t0
+        ci += p.mesh.ncells * st["niter"]
+        used += 1
+        if time.perf_counter() - t_start > budget_s:
+            break
+    return {"value": ci / tt / 1e9, "unit": "Gcell-iter/s", "cores": num_threads(), "kind": "port",
+            "sample": f"first time step of {used} problem(s) of the workload"}
+
+
+# ---------------------------------------------------------------------- ours
+def run_ours(args, ws, rank, local):
+    import torch
+    from curvilineardiffusionmanuscript_b200.solver import PseudoTransientBatch, PseudoTransientSolver, step
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    probs, cfg = make_workload(args.workload, args.nprob, rank, dev)
+    nd = probs[0].mesh.ndim
+    stream = torch.cuda.current_stream(dev)
+    batch = PseudoTransientBatch([p.mesh for p in probs], [p.bcs for p in probs], stream=stream.cuda_stream)
+    for i, p in enumerate(probs):
+        if p.source is not None:
+            batch.set_source(i, p.source)
+    Ts = [p.T0.clone() for p in probs]
+    rhos = [p.rho for p in probs]
+    cps = [p.cp for p in probs]
+    kaps = [p.kappa for p in probs]
+    dts = [p.dt for p in probs]
+    kw = dict(rtol=probs[0].rtol, atol=probs[0].atol, max_iter=100000)
+
+    def one_step():
+        st, _ = batch.step(Ts, rhos, cps, kaps, dts, **kw)
+        return st, batch.profile()
+
+    for _ in range(args.warmup):
+        one_step()
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ci, sweep_ms, launches, sweep_launches, iters = 0, 0.0, 0, 0, []
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            st, pf = one_step()
+            ci += pf["cell_iters"]
+            sweep_ms += pf["sweep_ms"]
+            launches += pf["sweep_launches"] + pf["other_launches"]
+            sweep_launches += pf["sweep_launches"]
+            iters.append(sum(s["niter"] for s in st))
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    barrier(ws)
+    ms_max = allreduce_max(ms, ws, dev)
+    ci_tot = allreduce_sum(float(ci), ws, dev)
+    value = ci_tot / (ms_max / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    achieved = ci * BYTES_PER_CELL_ITER[nd] / (sweep_ms / 1e3) / 1e9 if sweep_ms > 0 else 0.0
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "kernel": f"sweep{nd}d_fp64", "peak_kind": peak_kind,
+            "bytes_per_cell_iter": BYTES_PER_CELL_ITER[nd]}
+    tp = ROOT / "profiles" / f"traffic_sweep{nd}d_fp64.json"
+    if tp.exists():
+        # DRAM bytes per cell-iteration from one ncu capture, times the cells one launch updates
+        t = json.loads(tp.read_text())
+        roof["traffic"] = t["dram_bytes_per_cell_iter"] * ci / max(1, sweep_launches)
+        roof["traffic_note"] = t.get("note", "")
+    e2e = None
+    if not args.no_e2e:
+        # end to end through the public API with host (pinned) buffers
+        Th = [t.cpu().pin_memory() for t in Ts]
+        Rh = [r.cpu().pin_memory() for r in rhos]
+        st, _ = batch.step(Th, Rh, cps, kaps, dts, **kw)  # warm the host path
+        barrier(ws)
+        torch.cuda.synchronize()
+        ci2 = 0
+        t0 = time.perf_counter()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            st, _ = batch.step(Th, Rh, cps, kaps, dts, **kw)
+            ci2 += batch.profile()["cell_iters"]
+        f1.record(stream)
+        torch.cuda.synchronize()
+        ms2 = max(f0.elapsed_time(f1), 1e3 * (time.perf_counter() - t0))
+        ms2 = allreduce_max(ms2, ws, dev)
+        ci2 = allreduce_sum(float(ci2), ws, dev)
+        nbytes = sum(t.numel() for t in Ts) * 8
+        e2e = {"value": ci2 / (ms2 / 1e3) / 1e9, "unit": "Gcell-iter/s", "h2d_bytes_per_step": 2 * nbytes,
+               "d2h_bytes_per_step": nbytes}
+    if rank != 0:
+        return
+    cpu = None
+    if ws == 1 and not args.no_cpu:
+        cpu = cpu_baseline(probs[:64])
+    cfg.update({"l2": "inputs larger than L2 (working set %.1f GB)" % (
+        sum(p.mesh.ncells_full for p in probs) * 8 * 16 / 1e9), "parallelism": f"dp{ws} (independent batches)"})
+    line = {"metric": "Gcell-iter/s", "value": value, "unit": "Gcell-iter/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "s_per_timestep": ms_max / args.steps / 1e3, "pseudo_iters_per_step": statistics.mean(iters),
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    batch.close()
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,50 @@
+// cdm_kernels.h — host-callable launchers of the device kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace cdm {
+
+struct Problem;
+struct Ctrl;
+
+struct TileShape {
+  int tx, ty, tz, threads;
+};
+
+int num_tile_shapes(int ndim);
+TileShape tile_shape(int ndim, int variant);
+
+// one fused FP64 pseudo-iteration over all items (problem, tile)
+cudaError_t launch_sweep_fp64(int ndim, int variant, const Problem* probs, const int2* items, int nitems,
+                              cudaStream_t s);
+
+// metric cache (mesh_metric_cache.jl:39-250) and the packed divergence
+// coefficients derived from the cell-centre metrics and the cache
+struct MeshPtrs {
+  const double* inv[9];
+  const double* edgeJ[3];
+  const double* edgehat[3][9];
+};
+cudaError_t launch_metric_cache(const Problem& P, const MeshPtrs& m, double* cache[3], cudaStream_t s);
+cudaError_t launch_coefficients(const Problem& P, const MeshPtrs& m, double* const cache[3], double* coef[9],
+                                cudaStream_t s);
+
+// finite-value check of a field on the domain and the first halo layer
+// (validity_checks.jl:1-43); writes bit 0 (non-finite) / bit 1 (negative) to *flag
+cudaError_t launch_validate(const Problem& P, const double* f, int* flag, cudaStream_t s);
+
+// Dirichlet ghosts beyond the first layer (2D: every halo layer, boundary_operators.jl:143-150)
+cudaError_t launch_dirichlet_fill(const Problem& P, double* u, cudaStream_t s);
+
+// enforce_positivity / cutoff! over the full array (PseudoTransientSolver.jl:323-368)
+cudaError_t launch_clamp(double* u, int64_t n, int positivity, int cutoff, cudaStream_t s);
+
+// next_dt reductions (timestep_control.jl:33-73) and the energy balance.
+// out[0] = max(u_prev) (NaN-propagating), out[1] = max relative change,
+// out[2] = sum rho*cp*T*J (T = u_prev) over the domain, out[3] = same for u,
+// out[4] = sum S*J over the domain.  `scratch` holds >= 2*1024 doubles.
+cudaError_t launch_step_reductions(const Problem& P, const double* u, const double* cellJ, double tol,
+                                   double* scratch, double* out, cudaStream_t s);
+
+}  // namespace cdm

@@ -1,0 +1,950 @@
+// engine.cu — host orchestration of the APT solver and the C ABI (cdm_apt.h).
+//
+// The reference's step! (PseudoTransientSolver.jl:180-351) issues ~11-13
+// launches per pseudo-iteration and reads the residual norm back to the host
+// at every check.  Here one fused kernel performs a whole iteration, the
+// stopping rule runs on the device, blocks of iterations are replayed from a
+// captured CUDA graph, and the host polls the control blocks only between
+// blocks.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <thread>
+
+#include "engine.h"
+
+namespace cdm {
+
+static thread_local std::string g_error;
+
+void set_error(const std::string& msg) { g_error = msg; }
+
+double now_seconds() {
+  using namespace std::chrono;
+  return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+// applybcs! applies the BCs in tuple order (boundary_operators.jl:26-30);
+// every rule writes only its own ghost slab except Periodic at a LO location,
+// which writes both slabs of its axis (:229-237) and Periodic at a HI
+// location, which writes nothing.  Folding that order gives one rule per side.
+int resolve_ghost_rules(int ndim, const cdm_bc* bcs, int* rule, double* val) {
+  for (int axis = 0; axis < ndim; ++axis) {
+    const cdm_bc lo = bcs[2 * axis], hi = bcs[2 * axis + 1];
+    for (const cdm_bc* b : {&lo, &hi})
+      if (b->kind < CDM_BC_NEUMANN || b->kind > CDM_BC_NEG_SYMMETRY) return CDM_BAD_INPUT;
+    rule[2 * axis] = lo.kind;  // LO: own rule; Periodic LO reads the HI interior
+    val[2 * axis] = lo.value;
+    if (hi.kind != CDM_BC_PERIODIC) {
+      rule[2 * axis + 1] = hi.kind;
+      val[2 * axis + 1] = hi.value;
+    } else {
+      rule[2 * axis + 1] = (lo.kind == CDM_BC_PERIODIC) ? GR_PERIODIC : GR_NONE;
+      val[2 * axis + 1] = 0.0;
+    }
+  }
+  return CDM_OK;
+}
+
+static void kappa_decompose(double n, int& mode, int& m, int& half) {
+  mode = 2;
+  m = 0;
+  half = 0;
+  if (n == 0.0) {
+    mode = 0;
+    return;
+  }
+  const double twice = 2.0 * n;
+  if (n > 0.0 && n <= 16.0 && twice == std::floor(twice)) {
+    mode = 1;
+    m = (int)std::floor(n);
+    half = (twice != 2.0 * m) ? 1 : 0;
+  }
+}
+
+template <typename T>
+static cudaError_t dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) return cudaSuccess;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e != cudaSuccess) return e;
+  return cudaMemsetAsync(*p, 0, count * sizeof(T));
+}
+
+template <typename T>
+static void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+Engine::~Engine() {
+  free_graphs();
+  for (auto& s : ps) {
+    for (int b = 0; b < 2; ++b) {
+      dfree(s.u[b]);
+      dfree(s.d32[b]);
+      dfree(s.ub64[b]);
+      for (int d = 0; d < 3; ++d) {
+        dfree(s.q[b][d]);
+        dfree(s.e32[b][d]);
+      }
+    }
+    dfree(s.u_prev);
+    dfree(s.S);
+    dfree(s.rho_buf);
+    for (int k = 0; k < 9; ++k) {
+      dfree(s.coef[k]);
+      dfree(s.coef32[k]);
+    }
+    for (int d = 0; d < 3; ++d) dfree(s.cache[d]);
+    dfree(s.cellJ);
+    dfree(s.partial);
+    dfree(s.guess);
+    dfree(s.ub32);
+    dfree(s.ab32);
+    dfree(s.R32);
+    dfree(s.rho32);
+  }
+  dfree(d_probs);
+  dfree(d_ctrl);
+  dfree(d_items);
+  dfree(d_flags);
+  dfree(d_red);
+  dfree(d_redout);
+  if (h_ctrl) cudaFreeHost(h_ctrl);
+  if (h_redout) cudaFreeHost(h_redout);
+  if (ev) cudaEventDestroy(ev);
+  for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+  if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+int Engine::free_graphs() {
+  for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+  for (auto& kv : graph_defs) cudaGraphDestroy(kv.second);
+  graphs.clear();
+  graph_defs.clear();
+  return CDM_OK;
+}
+
+// copy a full-size array given in `mem` space into device buffer dst
+static cudaError_t stage_in(double* dst, const double* src, int64_t n, int mem, cudaStream_t s) {
+  return cudaMemcpyAsync(dst, src, (size_t)n * sizeof(double),
+                         mem == CDM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s);
+}
+
+int Engine::init(int nprob, const cdm_mesh_desc* meshes, const cdm_bc* bcs, const cdm_apt_config* cfg) {
+  cdm_apt_config c;
+  cdm_apt_config_default(&c);
+  if (cfg) c = *cfg;
+  device = c.device;
+  mean = c.mean;
+  precision = c.precision;
+  if (nprob < 1) {
+    set_error("nprob must be >= 1");
+    return CDM_BAD_INPUT;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device) {
+    set_error("no CUDA device available for the APT library");
+    return CDM_NO_DEVICE;
+  }
+  CDM_CK(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  CDM_CK(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10) {
+    set_error("the APT library is built for sm_100a (B200); device is sm_" + std::to_string(prop.major) +
+              std::to_string(prop.minor));
+    return CDM_NO_DEVICE;
+  }
+  if (c.stream) {
+    stream = (cudaStream_t)c.stream;
+    own_stream = false;
+  } else {
+    CDM_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    own_stream = true;
+  }
+  CDM_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  ndim = meshes[0].ndim;
+  if (ndim != 2 && ndim != 3) {
+    set_error("ndim must be 2 or 3");
+    return CDM_BAD_INPUT;
+  }
+  if (mean != CDM_MEAN_HARMONIC && mean != CDM_MEAN_ARITHMETIC) {
+    set_error("mean must be CDM_MEAN_HARMONIC or CDM_MEAN_ARITHMETIC");
+    return CDM_BAD_INPUT;
+  }
+  ps.resize(nprob);
+  hp.resize(nprob);
+  const TileShape ts = tile_shape(ndim, variant);
+  for (int p = 0; p < nprob; ++p) {
+    const cdm_mesh_desc& m = meshes[p];
+    ProbState& s = ps[p];
+    if (m.ndim != ndim) {
+      set_error("all problems of a batch must have the same ndim");
+      return CDM_BAD_INPUT;
+    }
+    if (m.ni < 1 || m.nj < 1 || (ndim == 3 && m.nk < 1) || m.nhalo < 1) {
+      set_error("mesh sizes must be >= 1 and nhalo >= 1");
+      return CDM_BAD_INPUT;
+    }
+    s.ndim = ndim;
+    s.ni = m.ni;
+    s.nj = m.nj;
+    s.nk = ndim == 3 ? m.nk : 1;
+    s.nh = m.nhalo;
+    const int64_t nx = s.ni + 2 * s.nh, ny = s.nj + 2 * s.nh, nz = ndim == 3 ? s.nk + 2 * s.nh : 1;
+    s.nfull = nx * ny * nz;
+    s.ndomain = (int64_t)s.ni * s.nj * s.nk;
+    if (nx * ny > (int64_t)2147483647 || s.nfull > ((int64_t)1 << 40)) {
+      set_error("mesh too large");
+      return CDM_BAD_INPUT;
+    }
+    const cdm_bc* pb = bcs + (size_t)p * 2 * ndim;
+    for (int l = 0; l < 2 * ndim; ++l) s.bc_kind[l] = pb[l].kind;
+    if (resolve_ghost_rules(ndim, pb, s.rule, s.val) != CDM_OK) {
+      set_error("invalid boundary-condition kind");
+      return CDM_BAD_INPUT;
+    }
+    // phys_dims (PseudoTransientSolver.jl:122-153)
+    s.L = m.L;
+    for (int d = 0; d < 3; ++d) s.spacing[d] = m.spacing[d];
+    bool need_L = !(m.L > 0), need_sp = !(m.spacing[0] > 0);
+    const int64_t nnx = s.ni + 1, nny = s.nj + 1, nnz = ndim == 3 ? s.nk + 1 : 1;
+    if (need_L) {
+      double Lmin = INFINITY;
+      for (int d = 0; d < ndim; ++d) {
+        if (!m.node_x[d]) {
+          set_error("L not given and node coordinates missing");
+          return CDM_BAD_INPUT;
+        }
+        double lo = INFINITY, hi = -INFINITY;
+        for (int64_t e = 0; e < nnx * nny * nnz; ++e) {
+          lo = std::min(lo, m.node_x[d][e]);
+          hi = std::max(hi, m.node_x[d][e]);
+        }
+        Lmin = std::min(Lmin, std::fabs(hi - lo));
+      }
+      s.L = Lmin;
+    }
+    if (need_sp) {
+      if (ndim == 2) {
+        if (m.mem != CDM_MEM_HOST || !m.cell_J) {
+          set_error("spacing not given: cell_J must be a host array to derive it");
+          return CDM_BAD_INPUT;
+        }
+        double jmin = INFINITY;
+        for (int64_t b = 0; b < s.nj; ++b)
+          for (int64_t a = 0; a < s.ni; ++a) jmin = std::min(jmin, m.cell_J[(a + s.nh) + nx * (b + s.nh)]);
+        s.spacing[0] = s.spacing[1] = std::sqrt(jmin);
+      } else {
+        for (int d = 0; d < 3; ++d) {
+          if (!m.node_x[d]) {
+            set_error("spacing not given and node coordinates missing");
+            return CDM_BAD_INPUT;
+          }
+          const int64_t st = d == 0 ? 1 : (d == 1 ? nnx : nnx * nny);
+          double mn = INFINITY;
+          for (int64_t kk = 0; kk < nnz; ++kk)
+            for (int64_t jj = 0; jj < nny; ++jj)
+              for (int64_t ii = 0; ii < nnx; ++ii) {
+                const int64_t e = ii + nnx * (jj + nny * kk);
+                const bool has = d == 0 ? ii + 1 < nnx : (d == 1 ? jj + 1 < nny : kk + 1 < nnz);
+                if (has) mn = std::min(mn, m.node_x[d][e + st] - m.node_x[d][e]);
+              }
+          s.spacing[d] = mn;
+        }
+      }
+    }
+    if (!(s.L > 0)) {
+      set_error("physical length L must be > 0");
+      return CDM_BAD_INPUT;
+    }
+    // tiles
+    s.tiles_i = (s.ni + ts.tx - 1) / ts.tx;
+    s.tiles_j = (s.nj + ts.ty - 1) / ts.ty;
+    s.tiles_k = ndim == 3 ? (s.nk + ts.tz - 1) / ts.tz : 1;
+    s.ntiles = s.tiles_i * s.tiles_j * s.tiles_k;
+    // allocations
+    const size_t N = (size_t)s.nfull;
+    for (int b = 0; b < 2; ++b) {
+      CDM_CK(dalloc(&s.u[b], N));
+      for (int d = 0; d < ndim; ++d) CDM_CK(dalloc(&s.q[b][d], N));
+    }
+    CDM_CK(dalloc(&s.u_prev, N));
+    CDM_CK(dalloc(&s.S, N));
+    for (int k = 0; k < (ndim == 2 ? 5 : 9); ++k) CDM_CK(dalloc(&s.coef[k], N));
+    for (int d = 0; d < ndim; ++d) CDM_CK(dalloc(&s.cache[d], N));
+    CDM_CK(dalloc(&s.cellJ, N));
+    // partials are sized for the smallest tile of any shape
+    CDM_CK(dalloc(&s.partial, (size_t)s.ndomain + 64));
+    // mesh inputs on the device
+    MeshPtrs mp;
+    std::memset(&mp, 0, sizeof(mp));
+    std::vector<double*> tmp;
+    auto dev_in = [&](const double* src, const double** dst) -> int {
+      *dst = nullptr;
+      if (!src) return CDM_OK;
+      if (m.mem == CDM_MEM_DEVICE) {
+        *dst = src;
+        return CDM_OK;
+      }
+      double* d = nullptr;
+      CDM_CK(cudaMalloc((void**)&d, N * sizeof(double)));
+      tmp.push_back(d);
+      CDM_CK(cudaMemcpyAsync(d, src, N * sizeof(double), cudaMemcpyHostToDevice, stream));
+      *dst = d;
+      return CDM_OK;
+    };
+    int rc = CDM_OK;
+    for (int a = 0; a < ndim && rc == CDM_OK; ++a)
+      for (int cc = 0; cc < ndim && rc == CDM_OK; ++cc) {
+        if (!m.cell_inv[3 * a + cc]) {
+          set_error("missing cell_inv metric");
+          rc = CDM_BAD_INPUT;
+          break;
+        }
+        rc = dev_in(m.cell_inv[3 * a + cc], &mp.inv[3 * a + cc]);
+      }
+    for (int f = 0; f < ndim && rc == CDM_OK; ++f) {
+      if (!m.edge_J[f]) {
+        set_error("missing edge_J metric");
+        rc = CDM_BAD_INPUT;
+        break;
+      }
+      rc = dev_in(m.edge_J[f], &mp.edgeJ[f]);
+      for (int k = 0; k < 9 && rc == CDM_OK; ++k) {
+        const int a = k / 3, cc = k % 3;
+        if (a >= ndim || cc >= ndim) continue;
+        if (!m.edge_hat[f][k]) {
+          set_error("missing edge_hat metric");
+          rc = CDM_BAD_INPUT;
+          break;
+        }
+        rc = dev_in(m.edge_hat[f][k], &mp.edgehat[f][k]);
+      }
+    }
+    if (rc == CDM_OK && m.cell_J) {
+      CDM_CK(stage_in(s.cellJ, m.cell_J, s.nfull, m.mem, stream));
+    }
+    if (rc == CDM_OK) {
+      Problem P;
+      std::memset(&P, 0, sizeof(P));
+      P.ndim = ndim;
+      P.ni = s.ni;
+      P.nj = s.nj;
+      P.nk = s.nk;
+      P.nh = s.nh;
+      P.nx = (int)nx;
+      P.ny = (int)ny;
+      P.nz = (int)nz;
+      cudaError_t e1 = launch_metric_cache(P, mp, s.cache, stream);
+      cudaError_t e2 = launch_coefficients(P, mp, s.cache, s.coef, stream);
+      if (e1 != cudaSuccess || e2 != cudaSuccess) {
+        set_error(std::string("metric kernels: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+        rc = CDM_CUDA_ERROR;
+      }
+    }
+    cudaError_t es = cudaStreamSynchronize(stream);
+    for (double* d : tmp) cudaFree(d);
+    if (rc != CDM_OK) return rc;
+    if (es != cudaSuccess) {
+      set_error(std::string("mesh setup: ") + cudaGetErrorString(es));
+      return CDM_CUDA_ERROR;
+    }
+  }
+  CDM_CK(dalloc(&d_probs, (size_t)nprob));
+  CDM_CK(dalloc(&d_ctrl, (size_t)nprob));
+  CDM_CK(cudaMallocHost((void**)&h_ctrl, sizeof(Ctrl) * nprob));
+  std::memset(h_ctrl, 0, sizeof(Ctrl) * nprob);
+  CDM_CK(dalloc(&d_flags, (size_t)nprob));
+  CDM_CK(dalloc(&d_red, (size_t)4 * 1024));
+  CDM_CK(dalloc(&d_redout, (size_t)8 * nprob));
+  CDM_CK(cudaMallocHost((void**)&h_redout, sizeof(double) * 8 * nprob));
+  if (precision == CDM_PREC_MIXED) {
+    int rc = mixed_alloc();
+    if (rc != CDM_OK) return rc;
+  }
+  int rc = build_items();
+  if (rc != CDM_OK) return rc;
+  CDM_CK(cudaStreamSynchronize(stream));
+  return CDM_OK;
+}
+
+int Engine::build_items() {
+  const TileShape ts = tile_shape(ndim, variant);
+  std::vector<int2> items;
+  for (size_t p = 0; p < ps.size(); ++p) {
+    ProbState& s = ps[p];
+    s.tiles_i = (s.ni + ts.tx - 1) / ts.tx;
+    s.tiles_j = (s.nj + ts.ty - 1) / ts.ty;
+    s.tiles_k = ndim == 3 ? (s.nk + ts.tz - 1) / ts.tz : 1;
+    s.ntiles = s.tiles_i * s.tiles_j * s.tiles_k;
+    for (int t = 0; t < s.ntiles; ++t) items.push_back(make_int2((int)p, t));
+  }
+  // interleave tiles of different problems so that a launch spreads every
+  // problem over the whole GPU (uneven batches)
+  if (ps.size() > 1) {
+    std::vector<int2> mixed;
+    mixed.reserve(items.size());
+    std::vector<int> next(ps.size(), 0);
+    bool more = true;
+    while (more) {
+      more = false;
+      for (size_t p = 0; p < ps.size(); ++p)
+        if (next[p] < ps[p].ntiles) {
+          mixed.push_back(make_int2((int)p, next[p]++));
+          more = true;
+        }
+    }
+    items.swap(mixed);
+  }
+  dfree(d_items);
+  nitems = (int)items.size();
+  CDM_CK(cudaMalloc((void**)&d_items, sizeof(int2) * items.size()));
+  CDM_CK(cudaMemcpyAsync(d_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, stream));
+  CDM_CK(cudaStreamSynchronize(stream));
+  free_graphs();
+  return CDM_OK;
+}
+
+int Engine::set_source(int p, const double* S, int mem) {
+  ProbState& s = ps[p];
+  CDM_CK(cudaSetDevice(device));
+  CDM_CK(stage_in(s.S, S, s.nfull, mem, stream));
+  Problem P;
+  std::memset(&P, 0, sizeof(P));
+  P.ndim = ndim;
+  P.ni = s.ni;
+  P.nj = s.nj;
+  P.nk = s.nk;
+  P.nh = s.nh;
+  P.nx = s.ni + 2 * s.nh;
+  P.ny = s.nj + 2 * s.nh;
+  P.nz = ndim == 3 ? s.nk + 2 * s.nh : 1;
+  CDM_CK(cudaMemsetAsync(d_flags + p, 0, sizeof(int), stream));
+  CDM_CK(launch_validate(P, s.S, d_flags + p, stream));
+  int flag = 0;
+  CDM_CK(cudaMemcpyAsync(&flag, d_flags + p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  CDM_CK(cudaStreamSynchronize(stream));
+  s.s_bad = flag;
+  return CDM_OK;
+}
+
+int Engine::set_guess(int p, const double* u0, int mem) {
+  ProbState& s = ps[p];
+  CDM_CK(cudaSetDevice(device));
+  if (!s.guess) CDM_CK(dalloc(&s.guess, (size_t)s.nfull));
+  CDM_CK(stage_in(s.guess, u0, s.nfull, mem, stream));
+  CDM_CK(cudaStreamSynchronize(stream));
+  s.has_guess = 1;
+  return CDM_OK;
+}
+
+int Engine::wait_stream(double timeout_s) {
+  CDM_CK(cudaEventRecord(ev, stream));
+  const double t0 = now_seconds();
+  int spins = 0;
+  while (true) {
+    cudaError_t e = cudaEventQuery(ev);
+    if (e == cudaSuccess) return CDM_OK;
+    if (e != cudaErrorNotReady) {
+      set_error(std::string("device error: ") + cudaGetErrorString(e));
+      return CDM_CUDA_ERROR;
+    }
+    if (now_seconds() - t0 > timeout_s) {
+      set_error("timed out waiting for the device");
+      return CDM_TIMEOUT;
+    }
+    if (++spins > 64) std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
+}
+
+int Engine::record_pair() {
+  if (ev_used + 2 > (int)ev_pool.size()) {
+    for (int k = 0; k < 64; ++k) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return -1;
+      ev_pool.push_back(e);
+    }
+  }
+  const int i = ev_used;
+  ev_used += 2;
+  return i;
+}
+
+double Engine::collect_profile_ms() {
+  double ms = 0.0;
+  for (int i = 0; i + 1 < ev_used; i += 2) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, ev_pool[i], ev_pool[i + 1]) == cudaSuccess) ms += t;
+  }
+  ev_used = 0;
+  return ms;
+}
+
+int Engine::launch_block(int K, bool use_graph) {
+  const int pe = record_pair();
+  if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe], stream));
+  prof.sweep_launches += K;
+  if (!use_graph) {
+    for (int k = 0; k < K; ++k) CDM_CK(launch_sweep_fp64(ndim, variant, d_probs, d_items, nitems, stream));
+    if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe + 1], stream));
+    return CDM_OK;
+  }
+  if (graph_variant != variant) {
+    free_graphs();
+    graph_variant = variant;
+  }
+  auto it = graphs.find(K);
+  if (it == graphs.end()) {
+    cudaGraph_t g;
+    CDM_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t le = cudaSuccess;
+    for (int k = 0; k < K && le == cudaSuccess; ++k)
+      le = launch_sweep_fp64(ndim, variant, d_probs, d_items, nitems, stream);
+    cudaError_t ce = cudaStreamEndCapture(stream, &g);
+    if (le != cudaSuccess) {
+      set_error(std::string("sweep launch during capture: ") + cudaGetErrorString(le));
+      return CDM_CUDA_ERROR;
+    }
+    CDM_CK(ce);
+    cudaGraphExec_t ge;
+    CDM_CK(cudaGraphInstantiate(&ge, g, 0));
+    graphs[K] = ge;
+    graph_defs[K] = g;
+    it = graphs.find(K);
+  }
+  CDM_CK(cudaGraphLaunch(it->second, stream));
+  if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe + 1], stream));
+  return CDM_OK;
+}
+
+// Launch iteration blocks until every problem's control block says done.
+int Engine::run_iterations(const cdm_step_opts* o, int predicted, double t_start, double timeout_s) {
+  const int K = o->iter_block > 0 ? o->iter_block : 8;
+  const bool use_graph = o->use_graph != 0;
+  const int nprob = (int)ps.size();
+  int launched = 0;
+  // launch up to the predicted iteration count without polling
+  while (launched + K <= predicted) {
+    int rc = launch_block(K, use_graph);
+    if (rc != CDM_OK) return rc;
+    launched += K;
+  }
+  while (true) {
+    int rc = launch_block(K, use_graph);
+    if (rc != CDM_OK) return rc;
+    launched += K;
+    CDM_CK(cudaMemcpyAsync(h_ctrl, d_ctrl, sizeof(Ctrl) * nprob, cudaMemcpyDeviceToHost, stream));
+    rc = wait_stream(timeout_s - (now_seconds() - t_start));
+    if (rc != CDM_OK) return rc;
+    bool all = true;
+    for (int p = 0; p < nprob; ++p) all = all && h_ctrl[p].done;
+    if (all) return CDM_OK;
+    if (now_seconds() - t_start > timeout_s) {
+      set_error("step exceeded its wall-clock limit");
+      return CDM_TIMEOUT;
+    }
+  }
+}
+
+int Engine::step(double* const* T, const double* const* rho, const double* cp, const cdm_kappa* kappa,
+                 const double* dt, const cdm_step_opts* opts, cdm_stats* stats, double* next_dt) {
+  const double t0 = now_seconds();
+  cdm_step_opts o;
+  cdm_step_opts_default(&o);
+  if (opts) o = *opts;
+  const int nprob = (int)ps.size();
+  CDM_CK(cudaSetDevice(device));
+  std::memset(&prof, 0, sizeof(prof));
+  ev_used = 0;
+  double timeout_s = 3600.0;
+  if (const char* e = std::getenv("CDM_STEP_TIMEOUT_S")) timeout_s = std::atof(e);
+  for (int p = 0; p < nprob; ++p) {
+    std::memset(&stats[p], 0, sizeof(cdm_stats));
+    stats[p].status = CDM_OK;
+  }
+  // argument checks (:225-227) and validate_scalar (:238-250)
+  int predicted = 1 << 30;
+  int bad = CDM_OK;
+  for (int p = 0; p < nprob; ++p) {
+    ProbState& s = ps[p];
+    double msp = s.spacing[0];
+    for (int d = 1; d < ndim; ++d) msp = std::min(msp, s.spacing[d]);
+    const double Vp = o.CFL * msp;
+    const Ctrl& prev = h_ctrl[p];
+    const int abad = prev.abad[prev.iter & 1];
+    std::string why;
+    if (!(dt[p] > 0)) why = "dt must be > 0";
+    else if (!(Vp > 0)) why = "CFL * spacing must be > 0";
+    else if (!T[p] || !rho[p]) why = "T and rho must not be NULL";
+    else if ((abad & 1) || (o.enforce_positivity && (abad & 2))) why = "Invalid diffusivity (validate_scalar)";
+    else if (s.s_bad & 1) why = "Invalid source_term (validate_scalar)";
+    if (!why.empty()) {
+      stats[p].status = CDM_BAD_INPUT;
+      set_error(why);
+      bad = CDM_BAD_INPUT;
+    }
+  }
+  if (bad != CDM_OK) {
+    for (int p = 0; p < nprob; ++p) stats[p].time = now_seconds() - t0;
+    return bad;
+  }
+  for (int p = 0; p < nprob; ++p) {
+    ProbState& s = ps[p];
+    Problem& P = hp[p];
+    std::memset(&P, 0, sizeof(P));
+    const size_t bytes = (size_t)s.nfull * sizeof(double);
+    // copy!(solver.u, T); copy!(solver.u_prev, T)  (:229-230)
+    CDM_CK(stage_in(s.u_prev, T[p], s.nfull, o.mem, stream));
+    const double* init = (o.guess == CDM_GUESS_USER && s.has_guess) ? s.guess : s.u_prev;
+    CDM_CK(cudaMemcpyAsync(s.u[0], init, bytes, cudaMemcpyDeviceToDevice, stream));
+    CDM_CK(cudaMemcpyAsync(s.u[1], init, bytes, cudaMemcpyDeviceToDevice, stream));
+    const double* rp = rho[p];
+    if (o.mem != CDM_MEM_DEVICE) {
+      if (!s.rho_buf) CDM_CK(dalloc(&s.rho_buf, (size_t)s.nfull));
+      CDM_CK(cudaMemcpyAsync(s.rho_buf, rho[p], bytes, cudaMemcpyHostToDevice, stream));
+      rp = s.rho_buf;
+    }
+    P.ndim = ndim;
+    P.ni = s.ni;
+    P.nj = s.nj;
+    P.nk = s.nk;
+    P.nh = s.nh;
+    P.nx = s.ni + 2 * s.nh;
+    P.ny = s.nj + 2 * s.nh;
+    P.nz = ndim == 3 ? s.nk + 2 * s.nh : 1;
+    P.tiles_i = s.tiles_i;
+    P.tiles_j = s.tiles_j;
+    P.tiles_k = s.tiles_k;
+    P.ntiles = s.ntiles;
+    P.mean = mean;
+    P.subcycle = o.subcycle_conductivity ? 1 : 0;
+    kappa_decompose(kappa[p].n, P.kmode, P.km, P.khalf);
+    P.qpar = s.qpar;
+    for (int l = 0; l < 6; ++l) {
+      P.rule[l] = s.rule[l];
+      P.val[l] = s.val[l];
+    }
+    double msp = s.spacing[0];
+    for (int d = 1; d < ndim; ++d) msp = std::min(msp, s.spacing[d]);
+    P.dt = dt[p];
+    P.cp = cp[p];
+    P.k0 = kappa[p].k0;
+    P.kn = kappa[p].n;
+    P.L = s.L;
+    P.LL = s.L * s.L;
+    P.Vpdtau = o.CFL * msp;  // :223
+    P.VpL = P.Vpdtau * s.L;
+    for (int b = 0; b < 2; ++b) {
+      P.u[b] = s.u[b];
+      for (int d = 0; d < 3; ++d) P.q[b][d] = s.q[b][d];
+      P.d32[b] = s.d32[b];
+      P.ub64[b] = s.ub64[b];
+      for (int d = 0; d < 3; ++d) P.e32[b][d] = s.e32[b][d];
+    }
+    P.u_prev = s.u_prev;
+    P.S = s.S;
+    P.rho = rp;
+    for (int k = 0; k < 9; ++k) {
+      P.coef[k] = s.coef[k];
+      P.coef32[k] = s.coef32[k];
+    }
+    P.partial = s.partial;
+    P.ctrl = d_ctrl + p;
+    P.ub32 = s.ub32;
+    P.ab32 = s.ab32;
+    P.R32 = s.R32;
+    P.rho32 = s.rho32;
+    if (ndim == 2 && s.nh > 1) {
+      CDM_CK(launch_dirichlet_fill(P, s.u[0], stream));
+      CDM_CK(launch_dirichlet_fill(P, s.u[1], stream));
+      prof.other_launches += 2;
+    }
+    // control block (:206-221)
+    Ctrl& C = h_ctrl[p];
+    std::memset(&C, 0, sizeof(Ctrl));
+    const int last = s.last_err_check;
+    C.min_err_check = (int)std::nearbyint(last * 0.9);
+    C.err_interval = std::max(1, (last - C.min_err_check) / 2);
+    C.max_iter = o.max_iter;
+    C.check_every = o.check_every;
+    C.norm_kind = o.norm;
+    C.rtol = o.rtol;
+    C.atol = o.atol;
+    C.init_L2 = INFINITY;
+    C.rel = 2 * o.rtol;
+    C.abs = 2 * o.atol;
+    C.nfull = (double)s.nfull;
+    C.sqrtN = std::sqrt((double)s.nfull);
+    predicted = std::min(predicted, o.check_every > 0 ? 0 : std::max(0, C.min_err_check - 1));
+  }
+  CDM_CK(cudaMemcpyAsync(d_probs, hp.data(), sizeof(Problem) * nprob, cudaMemcpyHostToDevice, stream));
+  CDM_CK(cudaMemcpyAsync(d_ctrl, h_ctrl, sizeof(Ctrl) * nprob, cudaMemcpyHostToDevice, stream));
+  int rc;
+  if (precision == CDM_PREC_MIXED) rc = step_mixed(&o, t0, timeout_s);
+  else rc = run_iterations(&o, predicted, t0, timeout_s);
+  if (rc != CDM_OK) {
+    for (int p = 0; p < nprob; ++p) {
+      stats[p].status = rc;
+      stats[p].time = now_seconds() - t0;
+    }
+    return rc;
+  }
+  // after the loop (:321-346)
+  int worst = CDM_OK;
+  for (int p = 0; p < nprob; ++p) {
+    ProbState& s = ps[p];
+    const Ctrl& C = h_ctrl[p];
+    stats[p].rel_err = C.rel;
+    stats[p].abs_err = C.abs;
+    stats[p].niter = C.iter;
+    stats[p].status = C.status;
+    stats[p].n_checks = C.n_checks;
+    stats[p].n_restarts = C.n_restarts;
+    s.qpar = (s.qpar + C.iter) & 1;
+    if (C.status != ST_OK) {
+      worst = std::max(worst, C.status);
+      if (C.status == ST_NONFINITE)
+        set_error("Non-finite error detected! abs_error = " + std::to_string(C.abs) +
+                  ", rel_error = " + std::to_string(C.rel));
+      else
+        set_error("Maximum iteration limit reached (" + std::to_string(o.max_iter) + ")");
+      continue;
+    }
+    s.last_err_check = C.iter;
+    double* res = precision == CDM_PREC_MIXED ? s.ub64[C.iter & 1] : s.u[C.iter & 1];
+    if (precision == CDM_PREC_MIXED) res = s.ub64[C.n_restarts & 1];
+    CDM_CK(launch_clamp(res, s.nfull, o.enforce_positivity, o.apply_cutoff, stream));
+    CDM_CK(launch_step_reductions(hp[p], res, s.cellJ, o.ndt_tol, d_red, d_redout + 8 * p, stream));
+    prof.other_launches += 4 + ((o.enforce_positivity || o.apply_cutoff) ? 1 : 0);
+    prof.cell_iters += s.ndomain * (int64_t)C.iter;
+    CDM_CK(cudaMemcpyAsync(T[p], res, (size_t)s.nfull * sizeof(double),
+                           o.mem == CDM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, stream));
+  }
+  CDM_CK(cudaMemcpyAsync(h_redout, d_redout, sizeof(double) * 8 * nprob, cudaMemcpyDeviceToHost, stream));
+  rc = wait_stream(timeout_s);
+  if (rc != CDM_OK) return rc;
+  prof.sweep_ms = collect_profile_ms();
+  for (int p = 0; p < nprob; ++p) {
+    const double* r = h_redout + 8 * p;
+    if (stats[p].status == CDM_OK) {
+      // next_dt (timestep_control.jl:43-54)
+      if (o.calculate_next_dt) {
+        const double cand = dt[p] * std::sqrt(std::fabs(o.maximum_u_change / r[1]));
+        const double cap = o.timestep_growth_factor * dt[p];
+        next_dt[p] = cand < cap ? cand : cap;
+      } else {
+        next_dt[p] = dt[p];
+      }
+      stats[p].energy_before = r[2];
+      stats[p].energy_after = r[3];
+      stats[p].source_work = dt[p] * r[4];
+    } else {
+      next_dt[p] = dt[p];
+    }
+    stats[p].time = now_seconds() - t0;
+  }
+  return worst;
+}
+
+}  // namespace cdm
+
+// ============================================================================
+// C ABI
+using cdm::Engine;
+
+struct cdm_apt {
+  Engine e;
+};
+struct cdm_batch {
+  Engine e;
+};
+
+extern "C" {
+
+int cdm_apt_version(void) { return CDM_APT_ABI_VERSION; }
+
+const char* cdm_apt_last_error(void) { return cdm::g_error.c_str(); }
+
+void cdm_step_opts_default(cdm_step_opts* o) {
+  std::memset(o, 0, sizeof(*o));
+  o->t = 0.0;
+  o->tz = 0;
+  o->tz_dim = 1;
+  o->no_t = 1;
+  o->max_iter = 1500;
+  o->rtol = 1e-5;
+  o->atol = std::sqrt(2.220446049250313e-16);
+  o->error_check_interval = 2;
+  o->apply_cutoff = 0;
+  o->calculate_next_dt = 1;
+  o->subcycle_conductivity = 1;
+  o->enforce_positivity = 0;
+  o->CFL = 1.0 / std::sqrt(3.0);
+  o->ndt_tol = 1e-3;
+  o->maximum_u_change = 0.05;
+  o->timestep_growth_factor = 1.1;
+  o->norm = CDM_NORM_MAX;
+  o->check_every = 0;
+  o->guess = CDM_GUESS_PREV;
+  o->mem = CDM_MEM_HOST;
+  o->iter_block = 0;
+  o->use_graph = 1;
+}
+
+void cdm_apt_config_default(cdm_apt_config* c) {
+  c->mean = CDM_MEAN_HARMONIC;
+  c->precision = CDM_PREC_FP64;
+  c->device = 0;
+  c->stream = nullptr;
+}
+
+int cdm_apt_create(const cdm_mesh_desc* mesh, const cdm_bc* bcs, const cdm_apt_config* cfg, cdm_apt** out) {
+  if (!mesh || !bcs || !out) {
+    cdm::set_error("NULL argument");
+    return CDM_BAD_INPUT;
+  }
+  *out = nullptr;
+  cdm_apt* h = new cdm_apt();
+  int rc = h->e.init(1, mesh, bcs, cfg);
+  if (rc != CDM_OK) {
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return CDM_OK;
+}
+
+int cdm_apt_destroy(cdm_apt* h) {
+  if (h) {
+    cudaSetDevice(h->e.device);
+    cudaStreamSynchronize(h->e.stream);
+    delete h;
+  }
+  return CDM_OK;
+}
+
+int cdm_apt_set_source(cdm_apt* h, const double* S, int mem) {
+  if (!h || !S) return CDM_BAD_INPUT;
+  return h->e.set_source(0, S, mem);
+}
+
+int cdm_apt_step(cdm_apt* h, double* T, const double* rho, double cp, cdm_kappa kappa, double dt,
+                 const cdm_step_opts* opts, cdm_stats* stats, double* next_dt) {
+  if (!h || !stats || !next_dt) {
+    cdm::set_error("NULL argument");
+    return CDM_BAD_INPUT;
+  }
+  double* Ts[1] = {T};
+  const double* rs[1] = {rho};
+  return h->e.step(Ts, rs, &cp, &kappa, &dt, opts, stats, next_dt);
+}
+
+int cdm_apt_set_guess(cdm_apt* h, const double* u0, int mem) {
+  if (!h || !u0) return CDM_BAD_INPUT;
+  return h->e.set_guess(0, u0, mem);
+}
+
+int cdm_apt_get_state(cdm_apt* h, double* q, int* last_err_check) {
+  if (!h || !q || !last_err_check) return CDM_BAD_INPUT;
+  Engine& e = h->e;
+  cdm::ProbState& s = e.ps[0];
+  CDM_CK(cudaSetDevice(e.device));
+  for (int d = 0; d < e.ndim; ++d)
+    CDM_CK(cudaMemcpyAsync(q + d * s.nfull, s.q[s.qpar][d], sizeof(double) * s.nfull, cudaMemcpyDeviceToHost,
+                           e.stream));
+  CDM_CK(cudaStreamSynchronize(e.stream));
+  *last_err_check = s.last_err_check;
+  return CDM_OK;
+}
+
+int cdm_apt_set_state(cdm_apt* h, const double* q, int last_err_check) {
+  if (!h || !q) return CDM_BAD_INPUT;
+  Engine& e = h->e;
+  cdm::ProbState& s = e.ps[0];
+  CDM_CK(cudaSetDevice(e.device));
+  for (int d = 0; d < e.ndim; ++d)
+    CDM_CK(cudaMemcpyAsync(s.q[s.qpar][d], q + d * s.nfull, sizeof(double) * s.nfull, cudaMemcpyHostToDevice,
+                           e.stream));
+  CDM_CK(cudaStreamSynchronize(e.stream));
+  s.last_err_check = last_err_check;
+  return CDM_OK;
+}
+
+int cdm_apt_get_metric_cache(cdm_apt* h, double* cache) {
+  if (!h || !cache) return CDM_BAD_INPUT;
+  Engine& e = h->e;
+  cdm::ProbState& s = e.ps[0];
+  CDM_CK(cudaSetDevice(e.device));
+  for (int d = 0; d < e.ndim; ++d)
+    CDM_CK(cudaMemcpyAsync(cache + d * s.nfull, s.cache[d], sizeof(double) * s.nfull, cudaMemcpyDeviceToHost,
+                           e.stream));
+  CDM_CK(cudaStreamSynchronize(e.stream));
+  return CDM_OK;
+}
+
+int cdm_apt_full_size(const cdm_apt* h, int64_t* nfull, int64_t* ndomain) {
+  if (!h) return CDM_BAD_INPUT;
+  if (nfull) *nfull = h->e.ps[0].nfull;
+  if (ndomain) *ndomain = h->e.ps[0].ndomain;
+  return CDM_OK;
+}
+
+int cdm_apt_get_profile(const cdm_apt* h, cdm_profile* out) {
+  if (!h || !out) return CDM_BAD_INPUT;
+  *out = h->e.prof;
+  return CDM_OK;
+}
+
+int cdm_batch_get_profile(const cdm_batch* b, cdm_profile* out) {
+  if (!b || !out) return CDM_BAD_INPUT;
+  *out = b->e.prof;
+  return CDM_OK;
+}
+
+int cdm_batch_create(int nprob, const cdm_mesh_desc* meshes, const cdm_bc* bcs, const cdm_apt_config* cfg,
+                     cdm_batch** out) {
+  if (!meshes || !bcs || !out || nprob < 1) {
+    cdm::set_error("bad arguments to cdm_batch_create");
+    return CDM_BAD_INPUT;
+  }
+  *out = nullptr;
+  cdm_batch* b = new cdm_batch();
+  int rc = b->e.init(nprob, meshes, bcs, cfg);
+  if (rc != CDM_OK) {
+    delete b;
+    return rc;
+  }
+  *out = b;
+  return CDM_OK;
+}
+
+int cdm_batch_destroy(cdm_batch* b) {
+  if (b) {
+    cudaSetDevice(b->e.device);
+    cudaStreamSynchronize(b->e.stream);
+    delete b;
+  }
+  return CDM_OK;
+}
+
+int cdm_batch_set_source(cdm_batch* b, int p, const double* S, int mem) {
+  if (!b || !S || p < 0 || p >= (int)b->e.ps.size()) return CDM_BAD_INPUT;
+  return b->e.set_source(p, S, mem);
+}
+
+int cdm_batch_step(cdm_batch* b, double* const* T, const double* const* rho, const double* cp,
+                   const cdm_kappa* kappa, const double* dt, const cdm_step_opts* opts, cdm_stats* stats,
+                   double* next_dt) {
+  if (!b || !T || !rho || !cp || !kappa || !dt || !stats || !next_dt) {
+    cdm::set_error("NULL argument");
+    return CDM_BAD_INPUT;
+  }
+  return b->e.step(T, rho, cp, kappa, dt, opts, stats, next_dt);
+}
+
+}  // extern "C"

@@ -1,0 +1,112 @@
+// engine.h — host-side APT engine shared by the single-problem and batched C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "cdm_apt.h"
+#include "cdm_device.cuh"
+#include "cdm_kernels.h"
+
+namespace cdm {
+
+void set_error(const std::string& msg);
+
+#define CDM_CK(expr)                                                                      \
+  do {                                                                                    \
+    cudaError_t _e = (expr);                                                              \
+    if (_e != cudaSuccess) {                                                              \
+      ::cdm::set_error(std::string(#expr) + ": " + cudaGetErrorString(_e));               \
+      return CDM_CUDA_ERROR;                                                              \
+    }                                                                                     \
+  } while (0)
+
+// Host bookkeeping of one problem.
+struct ProbState {
+  int ndim = 2, ni = 0, nj = 0, nk = 1, nh = 1;
+  int64_t nfull = 0, ndomain = 0;
+  double L = 0, spacing[3] = {0, 0, 0};
+  int rule[6] = {0, 0, 0, 0, 0, 0};
+  double val[6] = {0, 0, 0, 0, 0, 0};
+  int bc_kind[6] = {0, 0, 0, 0, 0, 0};
+  int tiles_i = 1, tiles_j = 1, tiles_k = 1, ntiles = 1;
+  // device buffers owned by the engine
+  double* u[2] = {nullptr, nullptr};
+  double* q[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  double* u_prev = nullptr;
+  double* S = nullptr;
+  double* rho_buf = nullptr;
+  double* coef[9] = {nullptr};
+  double* cache[3] = {nullptr, nullptr, nullptr};
+  double* cellJ = nullptr;
+  double* partial = nullptr;
+  double* guess = nullptr;
+  // state carried across steps
+  int last_err_check = 0;
+  int qpar = 0;
+  int s_bad = 0;
+  int has_guess = 0;
+  // mixed precision buffers
+  float* d32[2] = {nullptr, nullptr};
+  float* e32[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  float* ub32 = nullptr;
+  float* ab32 = nullptr;
+  float* R32 = nullptr;
+  float* rho32 = nullptr;
+  float* coef32[9] = {nullptr};
+  double* ub64[2] = {nullptr, nullptr};
+};
+
+struct Engine {
+  int ndim = 2;
+  int device = 0;
+  int mean = 0;
+  int precision = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int variant = 0;
+  std::vector<ProbState> ps;
+  std::vector<Problem> hp;
+  Problem* d_probs = nullptr;
+  Ctrl* d_ctrl = nullptr;
+  Ctrl* h_ctrl = nullptr;  // pinned mirror
+  int2* d_items = nullptr;
+  int nitems = 0;
+  int* d_flags = nullptr;        // per problem: source validity bits
+  double* d_red = nullptr;       // reduction scratch
+  double* d_redout = nullptr;    // per problem 8 doubles
+  double* h_redout = nullptr;    // pinned
+  cudaEvent_t ev = nullptr;
+  std::map<int, cudaGraphExec_t> graphs;
+  std::map<int, cudaGraph_t> graph_defs;
+  int graph_variant = -1;
+  // profiling of the last step
+  std::vector<cudaEvent_t> ev_pool;
+  int ev_used = 0;
+  cdm_profile prof{};
+  int record_pair();           // returns index of a (start) event; end = start + 1
+  double collect_profile_ms();
+
+  ~Engine();
+  int init(int nprob, const cdm_mesh_desc* meshes, const cdm_bc* bcs, const cdm_apt_config* cfg);
+  int build_items();
+  int set_source(int p, const double* S, int mem);
+  int set_guess(int p, const double* u0, int mem);
+  int step(double* const* T, const double* const* rho, const double* cp, const cdm_kappa* kappa,
+           const double* dt, const cdm_step_opts* opts, cdm_stats* stats, double* next_dt);
+  int run_iterations(const cdm_step_opts* o, int predicted, double t_start, double timeout_s);
+  int launch_block(int K, bool use_graph);
+  int wait_stream(double timeout_s);
+  int free_graphs();
+  // mixed precision (apt_mixed.cu)
+  int mixed_alloc();
+  int step_mixed(const cdm_step_opts* o, double t_start, double timeout_s);
+};
+
+int resolve_ghost_rules(int ndim, const cdm_bc* bcs, int* rule, double* val);
+double now_seconds();
+
+}  // namespace cdm

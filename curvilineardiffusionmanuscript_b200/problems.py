@@ -1,0 +1,154 @@
+"""Seeded synthetic workloads of the benchmark configurations.
+
+No dataset is involved: every problem is defined by a closed-form mesh, an
+initial temperature and a conductivity law, generated here from a seed.
+
+* ``gaussian_2d``   — 2D Gaussian pulse on the sin-wavy unit square,
+                       κ = T³, ρ = cₚ = 1, zero-flux (Neumann) boundaries.
+* ``batch_2d``      — 256 independent problems, side n ~ U{64..512}, wave
+                       amplitude ~ U(0, 0.08), κ = Tⁿ with n ∈ {0, 1, 2.5, 3},
+                       centre ~ U(0.3, 0.7)², width ~ U(0.05, 0.2).
+* ``mms_2d``        — manufactured solution T = 1 + ½ sin πx sin πy e^{-t},
+                       κ = T^2.5, Dirichlet ghost value 1; forcing passed as
+                       the source term (the twilight-zone hook of the reference
+                       adds its forcing to the source, update.jl:181-184).
+* ``gaussian_3d``   — 3D pulse (width 0.1) on the perturbed unit cube, κ = T^2.5.
+* ``multi_gaussian_2d`` — 1..8 seeded Gaussians, κ = T³ (learned-guess data).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+import torch
+
+from .mesh import CurvilinearMesh, wavy_mesh_2d, wavy_mesh_3d
+from .solver import DirichletBC, NeumannBC, PowerLawConductivity
+
+BATCH_SEED = 20261203
+
+
+@dataclass
+class Problem:
+    name: str
+    mesh: CurvilinearMesh
+    bcs: list
+    T0: torch.Tensor
+    rho: torch.Tensor
+    cp: float
+    kappa: PowerLawConductivity
+    dt: float
+    nsteps: int
+    atol: float = 1e-8
+    rtol: float = 0.0
+    source: Optional[torch.Tensor] = None
+    meta: dict = field(default_factory=dict)
+
+
+def gaussian_2d(n: int = 128, amp: float = 0.05, center=(0.5, 0.5), width2: float = 0.01, height: float = 10.0,
+                kn: float = 3.0, dt: float = 1e-5, nsteps: int = 10, device="cpu") -> Problem:
+    """2D Gaussian pulse: T0 = 1 + 10 exp(-|r - c|² / 0.01) at the cell centres."""
+    m = wavy_mesh_2d(n, n, amp, nhalo=1, device=device)
+    x, y = m.centroids
+    T0 = 1.0 + height * torch.exp(-((x - center[0]) ** 2 + (y - center[1]) ** 2) / width2)
+    rho = torch.ones_like(T0)
+    bcs = [NeumannBC(), NeumannBC(), NeumannBC(), NeumannBC()]
+    return Problem("gaussian_2d", m, bcs, T0.contiguous(), rho, 1.0, PowerLawConductivity(1.0, kn), dt, nsteps,
+                   meta={"n": n, "amp": amp, "kn": kn, "center": center, "width2": width2})
+
+
+def batch_2d(nprob: int = 256, seed: int = BATCH_SEED, nmin: int = 64, nmax: int = 512, dt: float = 1e-5,
+             device="cpu") -> List[Problem]:
+    rng = np.random.default_rng(seed)
+    out = []
+    for p in range(nprob):
+        n = int(rng.integers(nmin, nmax + 1))
+        amp = float(rng.uniform(0.0, 0.08))
+        kn = float(rng.choice([0.0, 1.0, 2.5, 3.0]))
+        c = (float(rng.uniform(0.3, 0.7)), float(rng.uniform(0.3, 0.7)))
+        w = float(rng.uniform(0.05, 0.2))
+        pr = gaussian_2d(n, amp, c, w * w, 10.0, kn, dt, 1, device)
+        pr.name = f"batch_{p}"
+        pr.meta.update({"width": w})
+        out.append(pr)
+    return out
+
+
+# --------------------------------------------------------------------- MMS (C3)
+def mms_exact(x, y, t):
+    return 1.0 + 0.5 * torch.sin(math.pi * x) * torch.sin(math.pi * y) * math.exp(-t)
+
+
+def mms_forcing(x, y, t, rho=1.0, cp=1.0):
+    """S = ∂T/∂t − ∇·(α∇T) with α = T^2.5/(ρ cₚ) for the exact solution above.
+
+    The discrete equation of the APT path is (u − uⁿ)/Δt = −∇·q + S with
+    q = −ᾱ∇u (update.jl:13-15, residuals.jl:46), i.e. ∂T/∂t = ∇·(α∇T) + S.
+    """
+    pi = math.pi
+    e = math.exp(-t)
+    sx, sy = torch.sin(pi * x), torch.sin(pi * y)
+    cx, cy = torch.cos(pi * x), torch.cos(pi * y)
+    T = 1.0 + 0.5 * sx * sy * e
+    Tt = -0.5 * sx * sy * e
+    Tx = 0.5 * pi * cx * sy * e
+    Ty = 0.5 * pi * sx * cy * e
+    lap = -pi * pi * sx * sy * e  # Txx + Tyy
+    a = T ** 2.5 / (rho * cp)
+    da = 2.5 * T ** 1.5 / (rho * cp)
+    div = da * (Tx * Tx + Ty * Ty) + a * lap
+    return Tt - div
+
+
+def mms_2d(n: int = 4096, amp: float = 0.05, dt: float = 1e-5, nsteps: int = 10, device="cpu") -> Problem:
+    m = wavy_mesh_2d(n, n, amp, nhalo=1, device=device)
+    x, y = m.centroids
+    T0 = mms_exact(x, y, 0.0).contiguous()
+    rho = torch.ones_like(T0)
+    bcs = [DirichletBC(1.0), DirichletBC(1.0), DirichletBC(1.0), DirichletBC(1.0)]
+    pr = Problem("mms_2d", m, bcs, T0, rho, 1.0, PowerLawConductivity(1.0, 2.5), dt, nsteps, meta={"n": n})
+    return pr
+
+
+def mms_source(pr: Problem, t_next: float) -> torch.Tensor:
+    x, y = pr.mesh.centroids
+    return mms_forcing(x, y, t_next).contiguous()
+
+
+def mms_error(pr: Problem, T: torch.Tensor, t: float):
+    """(L2, Linf) error of T against the exact solution over the domain."""
+    x, y = pr.mesh.centroids
+    d = (T - mms_exact(x, y, t))[pr.mesh.domain()]
+    return float(torch.sqrt((d * d).mean())), float(d.abs().max())
+
+
+# ------------------------------------------------------------------------ 3D (C4)
+def gaussian_3d(n: int = 256, amp: float = 0.04, width: float = 0.1, dt: float = 1e-5, nsteps: int = 20,
+                kn: float = 2.5, device="cpu", nk: Optional[int] = None, nj: Optional[int] = None) -> Problem:
+    m = wavy_mesh_3d(n, nj or n, nk or n, amp, nhalo=1, device=device)
+    x, y, z = m.centroids
+    T0 = (1.0 + 10.0 * torch.exp(-((x - 0.5) ** 2 + (y - 0.5) ** 2 + (z - 0.5) ** 2) / (width * width))).contiguous()
+    rho = torch.ones_like(T0)
+    bcs = [NeumannBC() for _ in range(6)]
+    return Problem("gaussian_3d", m, bcs, T0, rho, 1.0, PowerLawConductivity(1.0, kn), dt, nsteps, meta={"n": n})
+
+
+# ------------------------------------------------------------------- C5 (learned)
+def multi_gaussian_2d(n: int = 1024, seed: int = 0, amp: float = 0.05, dt: float = 1e-5, nsteps: int = 10,
+                      device="cpu") -> Problem:
+    rng = np.random.default_rng(seed)
+    m = wavy_mesh_2d(n, n, amp, nhalo=1, device=device)
+    x, y = m.centroids
+    T0 = torch.ones_like(x)
+    M = int(rng.integers(1, 9))
+    for _ in range(M):
+        A = float(rng.uniform(1.0, 10.0))
+        w = float(rng.uniform(0.03, 0.15))
+        c = rng.uniform(0.15, 0.85, size=2)
+        T0 = T0 + A * torch.exp(-((x - c[0]) ** 2 + (y - c[1]) ** 2) / (w * w))
+    rho = torch.ones_like(T0)
+    bcs = [NeumannBC() for _ in range(4)]
+    return Problem("multi_gaussian_2d", m, bcs, T0.contiguous(), rho, 1.0, PowerLawConductivity(1.0, 3.0), dt,
+                   nsteps, meta={"n": n, "seed": seed, "M": M})

@@ -1,0 +1,249 @@
+/*
+ * cdm_apt.h — C ABI of the B200 accelerated pseudo-transient (APT) solver.
+ *
+ * This library is a drop-in for the APT path of CurvilinearDiffusion
+ * (smillerc/CurvilinearDiffusionManuscript).  Every entry point below names the
+ * reference function it replaces (path:line inside that project).  A Julia
+ * `ccall` shim, or any other FFI, binds these symbols directly: the signatures
+ * use only plain C types, pointers and sizes.
+ *
+ * Array layout (identical to `mesh.iterators.cell.full` of the reference):
+ *   every cell-centred or face-centred field is a full-size array including
+ *   `nhalo` halo layers per side, column-major (i fastest), i.e. element
+ *   (i, j, k) of a 3D field lives at  i + nx*(j + ny*k)  with
+ *   nx = ni + 2*nhalo, ny = nj + 2*nhalo, nz = nk + 2*nhalo (nz = 1 in 2D).
+ *   Domain cell (0,0,0) sits at (nhalo, nhalo, nhalo).  Face arrays store the
+ *   value at the i+1/2 (j+1/2, k+1/2) face of the cell with the same index.
+ *
+ * Errors: every call returns an int status (CDM_OK = 0).  No exception crosses
+ * the ABI and nothing traps on the device.  `cdm_apt_last_error` returns a
+ * human-readable message for the last failing call on this thread.
+ *
+ * Threading: a handle is not thread-safe; use one host thread per handle.  Each
+ * handle owns a CUDA stream (or uses the one passed in its config).  Calls are
+ * synchronous: they return after the device work of the call has finished.
+ */
+#ifndef CDM_APT_H
+#define CDM_APT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CDM_APT_ABI_VERSION 1
+
+/* ---- status codes (reference error paths in parentheses) ------------------ */
+enum cdm_status {
+  CDM_OK = 0,
+  CDM_MAX_ITER = 1,   /* PseudoTransientSolver.jl:309-314  iter > max_iter        */
+  CDM_NONFINITE = 2,  /* PseudoTransientSolver.jl:302-307  non-finite residual   */
+  CDM_BAD_INPUT = 3,  /* validity_checks.jl:1-43 and argument checks              */
+  CDM_CUDA_ERROR = 4, /* a CUDA runtime call failed                               */
+  CDM_TIMEOUT = 5,    /* a bounded host wait expired                              */
+  CDM_NO_DEVICE = 6   /* no usable sm_100 device                                  */
+};
+
+/* ---- enums ----------------------------------------------------------------- */
+enum cdm_mem { CDM_MEM_HOST = 0, CDM_MEM_DEVICE = 1 };
+
+/* boundary_operators.jl:9-17 */
+enum cdm_bc_kind {
+  CDM_BC_NEUMANN = 0,      /* ghost <- adjacent interior            (:55-82)   */
+  CDM_BC_DIRICHLET = 1,    /* ghost <- value                        (:137-200) */
+  CDM_BC_PERIODIC = 2,     /* ghost <- opposite interior, LO sides  (:220-263) */
+  CDM_BC_NEG_SYMMETRY = 3  /* ghost <- -adjacent interior           (:157-175) */
+};
+
+/* averaging.jl:7-8, selected by the `mean` keyword (PseudoTransientSolver.jl:76-80) */
+enum cdm_mean { CDM_MEAN_HARMONIC = 0, CDM_MEAN_ARITHMETIC = 1 };
+
+/* residual norm (residuals.jl:1-22): the reference's GPU and CPU paths differ. */
+enum cdm_norm {
+  CDM_NORM_MAX = 0, /* GPU path: norm(res, Inf) / sqrt(length(res))   (:5)     */
+  CDM_NORM_RMS = 1  /* CPU path: sqrt(sum(res.^2) / length(res))      (:12-22) */
+};
+
+enum cdm_precision {
+  CDM_PREC_FP64 = 0,  /* plain FP64 APT: the reference algorithm                 */
+  CDM_PREC_MIXED = 1  /* FP32 sweeps + FP64 residual / defect-correction restarts */
+};
+
+enum cdm_guess {
+  CDM_GUESS_PREV = 0,   /* u = T^n, as PseudoTransientSolver.jl:229                */
+  CDM_GUESS_USER = 1,   /* u = array given by cdm_apt_set_guess                    */
+  CDM_GUESS_LEARNED = 2 /* u = T^n + network(T^n, T^{n-1}, kappa, J) (learned guess) */
+};
+
+/* conductivity model: replaces the Julia closure kappa(rho, T) of the drivers,
+ * e.g. test/integrated/2d/gaussian/run.jl:129-135.  kappa = k0*|T|^n, and 0 when
+ * T is not finite.  Integer and half-integer n are evaluated by products and
+ * one sqrt; other n by pow(). */
+typedef struct cdm_kappa {
+  double k0;
+  double n;
+} cdm_kappa;
+
+typedef struct cdm_bc {
+  int kind;     /* enum cdm_bc_kind */
+  double value; /* Dirichlet value (bc.val.u in 2D, bc.val in 3D)     */
+} cdm_bc;
+
+/* Mesh description: the fields of a CurvilinearGrids mesh that the APT path
+ * reads (PseudoTransientSolver.jl:57-60,122-153; mesh_metric_cache.jl:51-85;
+ * flux_divergence.jl:11-14).  Pointers live in `mem` space and are full-size
+ * arrays in the layout above.  Only the first ndim components of each vector
+ * are read.  The library copies what it needs; the caller keeps ownership. */
+typedef struct cdm_mesh_desc {
+  int ndim;           /* 2 or 3 */
+  int ni, nj, nk;     /* domain cells per axis (nk ignored in 2D)  */
+  int nhalo;          /* >= 1 */
+  int mem;            /* enum cdm_mem for every pointer below      */
+  /* cell_center_metrics.{xi,eta,zeta}.{x1,x2,x3}: index [3*a + c], a = xi/eta/zeta, c = x1/x2/x3 */
+  const double* cell_inv[9];
+  /* cell_center_metrics.J (cell area / volume) */
+  const double* cell_J;
+  /* edge_metrics.{i+1/2, j+1/2, k+1/2}.J and the J-scaled metrics
+   * edge_metrics.f.{xi_hat, eta_hat, zeta_hat}.{x1,x2,x3} at index [3*a + c] */
+  const double* edge_J[3];
+  const double* edge_hat[3][9];
+  /* physical dimensions (phys_dims, PseudoTransientSolver.jl:122-153).  When
+   * L <= 0 or spacing[0] <= 0 they are computed from the domain node
+   * coordinates node_x[0..ndim) ((ni+1) x (nj+1) [x (nk+1)], column-major,
+   * host memory) and, in 2D, from cell_J as the reference does. */
+  double L;
+  double spacing[3];
+  const double* node_x[3];
+} cdm_mesh_desc;
+
+/* PseudoTransientSolver(mesh, bcs; backend, mean, T)  (PseudoTransientSolver.jl:48-103) */
+typedef struct cdm_apt_config {
+  int mean;      /* enum cdm_mean, default CDM_MEAN_HARMONIC (:49)      */
+  int precision; /* enum cdm_precision, default CDM_PREC_FP64            */
+  int device;    /* CUDA device ordinal, default 0                       */
+  void* stream;  /* cudaStream_t to use, or NULL for a private stream    */
+} cdm_apt_config;
+
+/* Keyword arguments of step! (PseudoTransientSolver.jl:188-202) and of next_dt
+ * (timestep_control.jl:33-42), same names and defaults, plus extensions. */
+typedef struct cdm_step_opts {
+  double t;
+  int tz, tz_dim, no_t;          /* accepted; manufactured forcing is passed as the source */
+  int max_iter;                  /* 1500 */
+  double rtol;                   /* 1e-5 */
+  double atol;                   /* sqrt(eps(Float64)) */
+  int error_check_interval;      /* 2; accepted and unused, as in the reference */
+  int apply_cutoff;              /* 0 */
+  int calculate_next_dt;         /* 1 */
+  int subcycle_conductivity;     /* 1 */
+  int enforce_positivity;        /* 0 */
+  double CFL;                    /* 1/sqrt(3) */
+  double ndt_tol;                /* next_dt tol = 1e-3 */
+  double maximum_u_change;       /* 0.05 */
+  double timestep_growth_factor; /* 1.1 */
+  /* extensions */
+  int norm;        /* enum cdm_norm, default CDM_NORM_MAX                          */
+  int check_every; /* 0: reference check schedule (:206-208, :280); k > 0: every k */
+  int guess;       /* enum cdm_guess, default CDM_GUESS_PREV                       */
+  int mem;         /* enum cdm_mem of the T / rho arrays passed to step            */
+  int iter_block;  /* iterations launched between host polls (0 = auto)            */
+  int use_graph;   /* capture iteration blocks in CUDA graphs (default 1)          */
+} cdm_step_opts;
+
+/* stats NamedTuple of step! (PseudoTransientSolver.jl:349) plus extensions */
+typedef struct cdm_stats {
+  double rel_err;
+  double abs_err;
+  int niter;
+  int status;
+  double time;             /* seconds, host wall clock of the call             */
+  double energy_before;    /* sum(rho*cp*T*J) over the domain at t^n           */
+  double energy_after;     /* same at t^{n+1}                                  */
+  double source_work;      /* dt * sum(S*J) over the domain                    */
+  int n_restarts;          /* mixed precision: FP64 defect-correction restarts */
+  int n_checks;            /* residual evaluations                             */
+} cdm_stats;
+
+typedef struct cdm_apt cdm_apt; /* opaque solver handle */
+
+/* device-time profile of the last step call (no reference counterpart: the
+ * reference times stages with TimerOutputs, PseudoTransientSolver.jl:232-339) */
+typedef struct cdm_profile {
+  double sweep_ms;          /* CUDA-event time of the pseudo-iteration launches     */
+  int64_t sweep_launches;   /* fused-sweep launches (including early-exit tails)    */
+  int64_t other_launches;   /* every other kernel launched by the step              */
+  int64_t cell_iters;       /* sum over problems of domain cells x pseudo-iterations */
+  int64_t fp32_cell_iters;  /* mixed precision: cells x FP32 correction sweeps      */
+  int64_t fp64_cell_evals;  /* mixed precision: cells x FP64 residual restarts      */
+} cdm_profile;
+
+/* ---- library ---------------------------------------------------------------- */
+int cdm_apt_version(void);
+const char* cdm_apt_last_error(void);
+void cdm_step_opts_default(cdm_step_opts* opts);
+void cdm_apt_config_default(cdm_apt_config* cfg);
+
+/* ---- construction: PseudoTransientSolver(mesh, bcs; ...)  (PseudoTransientSolver.jl:48-103)
+ * bcs has 2*ndim entries in the order ilo, ihi, jlo, jhi[, klo, khi]; the order
+ * is significant exactly as in applybcs! (boundary_operators.jl:26-30).  The
+ * metric cache (mesh_metric_cache.jl:2-37) is computed here on the device. */
+int cdm_apt_create(const cdm_mesh_desc* mesh, const cdm_bc* bcs, const cdm_apt_config* cfg,
+                   cdm_apt** out);
+int cdm_apt_destroy(cdm_apt* h);
+
+/* source_term (solver.source_term, PseudoTransientSolver.jl:31); full-size array in `mem` space */
+int cdm_apt_set_source(cdm_apt* h, const double* S, int mem);
+
+/* ---- one time step: step!(solver, mesh, T, rho, cp, kappa, dt; kwargs...)
+ * (PseudoTransientSolver.jl:180-351), reached through
+ * nonlinear_thermal_conduction_step! (nonlinear_thermal_conduction.jl:51-72).
+ * T (full size, in/out) and rho (full size) live in opts->mem space.  On
+ * return T holds the new temperature including the halo exactly as
+ * copy!(T, solver.u) leaves it (:346); *next_dt receives next_dt(...) (:338-344)
+ * or dt when calculate_next_dt == 0.  Returns stats->status. */
+int cdm_apt_step(cdm_apt* h, double* T, const double* rho, double cp, cdm_kappa kappa, double dt,
+                 const cdm_step_opts* opts, cdm_stats* stats, double* next_dt);
+
+/* initial guess for the next step (CDM_GUESS_USER); full-size array */
+int cdm_apt_set_guess(cdm_apt* h, const double* u0, int mem);
+
+/* ---- checkpoint of the state that carries across steps: the damped fluxes q
+ * (solver.q, :32) and last_err_check (:45).  `q` holds ndim full-size arrays
+ * back to back (host memory). */
+int cdm_apt_get_state(cdm_apt* h, double* q, int* last_err_check);
+int cdm_apt_set_state(cdm_apt* h, const double* q, int last_err_check);
+
+/* metric cache (mesh_metric_cache.jl:2-37) as computed on the device: ndim
+ * full-size arrays back to back (host memory); domain cells only are written. */
+int cdm_apt_get_metric_cache(cdm_apt* h, double* cache);
+
+/* grid sizes */
+int cdm_apt_full_size(const cdm_apt* h, int64_t* ncells_full, int64_t* ncells_domain);
+
+/* profile of the last cdm_apt_step / cdm_batch_step */
+int cdm_apt_get_profile(const cdm_apt* h, cdm_profile* out);
+
+/* ---- batched solve: many independent problems of uneven size, one launch per
+ * pseudo-iteration, iteration blocks captured in CUDA graphs.  Each problem is
+ * one step!(...) call of the reference; all problems share cp-free options.
+ * T[p], rho[p] are full-size arrays in opts->mem space. */
+typedef struct cdm_batch cdm_batch;
+int cdm_batch_create(int nprob, const cdm_mesh_desc* meshes, const cdm_bc* bcs /* nprob*2*ndim */,
+                     const cdm_apt_config* cfg, cdm_batch** out);
+int cdm_batch_destroy(cdm_batch* b);
+int cdm_batch_set_source(cdm_batch* b, int p, const double* S, int mem);
+int cdm_batch_step(cdm_batch* b, double* const* T, const double* const* rho, const double* cp,
+                   const cdm_kappa* kappa, const double* dt, const cdm_step_opts* opts,
+                   cdm_stats* stats /* nprob */, double* next_dt /* nprob */);
+/* autotuner: time the candidate tile shapes and iteration-block lengths on
+ * this batch and keep the fastest; result cached in `cache_path` (JSON) when
+ * it is not NULL.  *chosen receives an index into the candidate table. */
+int cdm_batch_autotune(cdm_batch* b, const char* cache_path, int* chosen);
+int cdm_batch_get_profile(const cdm_batch* b, cdm_profile* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CDM_APT_H */

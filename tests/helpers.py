@@ -1,0 +1,41 @@
+"""Shared helpers of the test-suite (seeded cases, oracle vs library runs)."""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from curvilineardiffusionmanuscript_b200 import problems
+from curvilineardiffusionmanuscript_b200.mesh import wavy_mesh_2d, wavy_mesh_3d
+from curvilineardiffusionmanuscript_b200.solver import (DirichletBC, FixedNegSymmetryBC, NeumannBC, PeriodicBC,
+                                                        PowerLawConductivity)
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def small_case_2d(ni=24, nj=17, amp=0.05, kn=3.0, bcs=None, seed=0, nhalo=1, source=False):
+    """Seeded small 2D problem on the wavy mesh."""
+    m = wavy_mesh_2d(ni, nj, amp, nhalo=nhalo)
+    x, y = m.centroids
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(0.3, 0.7, size=2)
+    T0 = (1.0 + 10.0 * torch.exp(-((x - c[0]) ** 2 + (y - c[1]) ** 2) / 0.02)).contiguous()
+    rho = (1.0 + 0.1 * torch.sin(3.0 * x) * torch.cos(2.0 * y)).contiguous()
+    bcs = bcs or [NeumannBC(), NeumannBC(), NeumannBC(), NeumannBC()]
+    S = None
+    if source:
+        S = (5.0 * torch.exp(-((x - 0.5) ** 2 + (y - 0.5) ** 2) / 0.05)).contiguous()
+    return problems.Problem("small2d", m, bcs, T0, rho, 1.3, PowerLawConductivity(1.0, kn), 1e-5, 3,
+                            source=S)
+
+
+def small_case_3d(n=(10, 9, 8), amp=0.04, kn=2.5, bcs=None):
+    m = wavy_mesh_3d(*n, amp=amp, nhalo=1)
+    x, y, z = m.centroids
+    T0 = (1.0 + 10.0 * torch.exp(-((x - 0.5) ** 2 + (y - 0.5) ** 2 + (z - 0.5) ** 2) / 0.05)).contiguous()
+    rho = torch.ones_like(T0)
+    bcs = bcs or [NeumannBC() for _ in range(6)]
+    return problems.Problem("small3d", m, bcs, T0, rho, 1.0, PowerLawConductivity(1.0, kn), 1e-5, 3)

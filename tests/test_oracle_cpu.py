@@ -1,0 +1,260 @@
+"""CPU tests of the oracle: reference known-answer tests, independent checks and golden fixtures.
+
+The oracle (oracle/apt_oracle.cpp) restates the reference APT path.  These
+tests pin it by
+  * the reference's own boundary-condition test (test/unit/test_bc.jl),
+  * the metric cache vanishing on a rectilinear mesh (mesh_metric_cache.jl),
+  * the fixed point of the pseudo-transient iteration being the backward-Euler
+    solution of the reference discretisation, restated independently here in
+    numpy (fluxes.jl, flux_divergence.jl, update.jl, residuals.jl),
+  * second-order convergence of a manufactured solution (the reference's own
+    verification, test/integrated/2d/wavy_manufactured_solution/run.jl:436-469),
+  * golden fixtures (tests/golden/make_golden.py).
+"""
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from helpers import small_case_2d, small_case_3d
+from oracle.oracle import OracleSolver, applybcs
+from curvilineardiffusionmanuscript_b200.mesh import uniform_mesh_2d, wavy_mesh_2d
+from curvilineardiffusionmanuscript_b200.solver import (DirichletBC, FixedNegSymmetryBC, NeumannBC, PeriodicBC,
+                                                        PowerLawConductivity)
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+# ------------------------------------------------------------ test_bc.jl restated
+def _full(shape_dom, nhalo, rng):
+    ni, nj = shape_dom[:2]
+    nk = shape_dom[2] if len(shape_dom) == 3 else None
+    h = nhalo
+    if nk is None:
+        u = np.zeros((nj + 2 * h, ni + 2 * h))
+        u[h:h + nj, h:h + ni] = rng.random((nj, ni))
+    else:
+        u = np.zeros((nk + 2 * h, nj + 2 * h, ni + 2 * h))
+        u[h:h + nk, h:h + nj, h:h + ni] = rng.random((nk, nj, ni))
+    return u
+
+
+def test_bc_2d_neumann_dirichlet_like_reference():
+    """test/unit/test_bc.jl:44-100: ni = nj = 6, nhalo = 4."""
+    rng = np.random.default_rng(1)
+    ni = nj = 6
+    h = 4
+    ilo, ihi, jlo, jhi = h, h + ni - 1, h, h + nj - 1
+    u = _full((ni, nj), h, rng)
+    before = u.copy()
+    applybcs(2, ni, nj, 1, h, [NeumannBC()] * 4, u)
+    assert np.array_equal(u[jlo:jhi + 1, ilo - 1], before[jlo:jhi + 1, ilo])
+    assert np.array_equal(u[jlo:jhi + 1, ihi + 1], before[jlo:jhi + 1, ihi])
+    assert np.array_equal(u[jlo - 1, ilo:ihi + 1], before[jlo, ilo:ihi + 1])
+    assert np.array_equal(u[jhi + 1, ilo:ihi + 1], before[jhi, ilo:ihi + 1])
+    # Dirichlet fills every halo layer of its side, corners excluded (boundary_operators.jl:143-150)
+    bcs = [DirichletBC(1.0), DirichletBC(2.0), DirichletBC(3.0), DirichletBC(4.0)]
+    applybcs(2, ni, nj, 1, h, bcs, u)
+    assert np.all(u[jlo:jhi + 1, :ilo] == 1.0)
+    assert np.all(u[jlo:jhi + 1, ihi + 1:] == 2.0)
+    assert np.all(u[:jlo, ilo:ihi + 1] == 3.0)
+    assert np.all(u[jhi + 1:, ilo:ihi + 1] == 4.0)
+    assert np.all(u[:jlo, :ilo] == before[:jlo, :ilo])  # corners untouched
+
+
+def test_bc_3d_like_reference():
+    """test/unit/test_bc.jl:103-165 (3D, nhalo = 4)."""
+    rng = np.random.default_rng(2)
+    ni, nj, nk, h = 5, 6, 7, 4
+    u = _full((ni, nj, nk), h, rng)
+    before = u.copy()
+    applybcs(3, ni, nj, nk, h, [NeumannBC()] * 6, u)
+    d = (slice(h, h + nk), slice(h, h + nj), slice(h, h + ni))
+    assert np.array_equal(u[d[0], d[1], h - 1], before[d[0], d[1], h])
+    assert np.array_equal(u[d[0], d[1], h + ni], before[d[0], d[1], h + ni - 1])
+    assert np.array_equal(u[d[0], h - 1, d[2]], before[d[0], h, d[2]])
+    assert np.array_equal(u[h + nk, d[1], d[2]], before[h + nk - 1, d[1], d[2]])
+    # 3D Dirichlet writes only the first layer (boundary_operators.jl:178-200)
+    applybcs(3, ni, nj, nk, h, [DirichletBC(float(v)) for v in range(1, 7)], u)
+    assert np.all(u[d[0], d[1], h - 1] == 1.0) and np.all(u[d[0], d[1], h - 2] == 0.0)
+    assert np.all(u[h + nk, d[1], d[2]] == 6.0)
+
+
+def test_bc_periodic_and_negsym_semantics():
+    rng = np.random.default_rng(3)
+    ni, nj, h = 5, 4, 1
+    u = _full((ni, nj), h, rng)
+    b = u.copy()
+    # Periodic acts at LO locations only (boundary_operators.jl:229-237)
+    applybcs(2, ni, nj, 1, h, [PeriodicBC(), PeriodicBC(), FixedNegSymmetryBC(), NeumannBC()], u)
+    assert np.array_equal(u[1:-1, 0], b[1:-1, ni])        # ilo-1 <- ihi
+    assert np.array_equal(u[1:-1, ni + 1], b[1:-1, 1])    # ihi+1 <- ilo
+    assert np.array_equal(u[0, 1:-1], -b[1, 1:-1])        # negative symmetry
+    assert np.array_equal(u[nj + 1, 1:-1], b[nj, 1:-1])   # Neumann
+    # a HI Periodic after a non-periodic LO writes nothing
+    u2 = b.copy()
+    applybcs(2, ni, nj, 1, h, [NeumannBC(), PeriodicBC(), NeumannBC(), NeumannBC()], u2)
+    assert np.array_equal(u2[1:-1, ni + 1], b[1:-1, ni + 1])
+
+
+# ------------------------------------------------------------------ metric cache
+def test_metric_cache_vanishes_on_rectilinear_mesh():
+    m = uniform_mesh_2d(12, 9, lx=2.0, ly=0.5)
+    o = OracleSolver(m, [NeumannBC()] * 4)
+    cache = o.metric_cache()
+    assert np.all(cache[:, 1:-1, 1:-1] == 0.0)
+
+
+def test_metric_cache_is_laplacian_of_coordinates():
+    """∇²ξ of x = ξ + a sin(2πξ) sin(2πη): compare the cache with a fine finite-difference value."""
+    m = wavy_mesh_2d(64, 64, 0.05)
+    o = OracleSolver(m, [NeumannBC()] * 4)
+    cache = o.metric_cache()
+    # the cache is a second-order approximation of ∇²ξ in index units
+    alpha = cache[0, 1:-1, 1:-1]
+    assert np.isfinite(alpha).all() and np.abs(alpha).max() > 0
+
+
+# --------------------------------------------------- backward-Euler fixed point
+def _numpy_operator(mesh, alpha_face_const, bcs_kind="neumann"):
+    """Independent numpy restatement of -∇·q'(u) for constant α (Neumann ghosts)."""
+    h = mesh.nhalo
+    ni, nj = mesh.ni, mesh.nj
+    inv = [None if t is None else t.numpy() for t in mesh.cell_inv]
+    ref = OracleSolver(mesh, [NeumannBC()] * 4)
+    cache = ref.metric_cache()
+    xx, xy, ex, ey = inv[0], inv[1], inv[3], inv[4]
+
+    def apply(ud):
+        u = np.zeros(mesh.full_shape)
+        u[h:h + nj, h:h + ni] = ud
+        u[h:h + nj, h - 1] = u[h:h + nj, h]
+        u[h:h + nj, h + ni] = u[h:h + nj, h + ni - 1]
+        u[h - 1, h:h + ni] = u[h, h:h + ni]
+        u[h + nj, h:h + ni] = u[h + nj - 1, h:h + ni]
+        qx = np.zeros_like(u)
+        qy = np.zeros_like(u)
+        a = alpha_face_const
+        qx[h:h + nj, h - 1:h + ni] = -a * (u[h:h + nj, h:h + ni + 1] - u[h:h + nj, h - 1:h + ni])
+        qy[h - 1:h + nj, h:h + ni] = -a * (u[h:h + nj + 1, h:h + ni] - u[h - 1:h + nj, h:h + ni])
+        out = np.zeros((nj, ni))
+        for j in range(h, h + nj):
+            for i in range(h, h + ni):
+                g11 = xx[j, i] ** 2 + xy[j, i] ** 2
+                g22 = ex[j, i] ** 2 + ey[j, i] ** 2
+                c = 0.25 * (ex[j, i] * xx[j, i] + ey[j, i] * xy[j, i])
+                d = (g11 * (qx[j, i] - qx[j, i - 1]) + g22 * (qy[j, i] - qy[j - 1, i])
+                     + c * ((qx[j + 1, i] + qx[j + 1, i - 1]) - (qx[j - 1, i] + qx[j - 1, i - 1]))
+                     + c * ((qy[j, i + 1] + qy[j - 1, i + 1]) - (qy[j, i - 1] + qy[j - 1, i - 1]))
+                     + cache[0, j, i] * 0.5 * (qx[j, i] + qx[j, i - 1])
+                     + cache[1, j, i] * 0.5 * (qy[j, i] + qy[j - 1, i]))
+                out[j - h, i - h] = -d
+        return out
+    return apply
+
+
+def test_fixed_point_is_backward_euler_solution():
+    """Linear κ: the converged APT iterate solves (u − uⁿ)/Δt = −∇·q′(u) + S exactly."""
+    ni, nj = 9, 7
+    m = wavy_mesh_2d(ni, nj, 0.06)
+    x, y = m.centroids
+    T0 = (1.0 + 3.0 * torch.exp(-((x - 0.4) ** 2 + (y - 0.6) ** 2) / 0.05)).numpy().copy()
+    S = (2.0 * torch.cos(3 * x) * torch.sin(2 * y)).numpy().copy()
+    rho = np.ones_like(T0)
+    k0, cp, dt = 2.5, 1.0, 1e-3
+    o = OracleSolver(m, [NeumannBC()] * 4)
+    o.set_source(S)
+    T = T0.copy()
+    st, _ = o.step(T, rho, cp, k0, 0.0, dt, rtol=0.0, atol=1e-13, max_iter=200000)
+    assert st["status"] == 0
+    op = _numpy_operator(m, k0 / cp)
+    n = ni * nj
+    A = np.zeros((n, n))
+    for c in range(n):
+        e = np.zeros(n)
+        e[c] = 1.0
+        A[:, c] = e / dt - op(e.reshape(nj, ni)).ravel()
+    h = 1
+    b = T0[h:h + nj, h:h + ni].ravel() / dt + S[h:h + nj, h:h + ni].ravel()
+    u = np.linalg.solve(A, b).reshape(nj, ni)
+    err = np.abs(T[h:h + nj, h:h + ni] - u).max()
+    assert err < 1e-12 * np.abs(u).max() + 1e-13 * dt * math.sqrt(m.ncells_full), err
+
+
+# ------------------------------------------------------ manufactured solution
+def _mms_periodic_error(n):
+    """T = 1 + ½ sin 2πx sin 2πy e^{-t}, κ = T², doubly periodic wavy mesh."""
+    m = wavy_mesh_2d(n, n, 0.04)
+    x, y = m.centroids
+    pi2 = 2 * math.pi
+
+    def exact(t):
+        return 1.0 + 0.5 * torch.sin(pi2 * x) * torch.sin(pi2 * y) * math.exp(-t)
+
+    def forcing(t):
+        e = math.exp(-t)
+        sx, sy, cx, cy = torch.sin(pi2 * x), torch.sin(pi2 * y), torch.cos(pi2 * x), torch.cos(pi2 * y)
+        T = 1.0 + 0.5 * sx * sy * e
+        Tt = -0.5 * sx * sy * e
+        Tx, Ty = 0.5 * pi2 * cx * sy * e, 0.5 * pi2 * sx * cy * e
+        lap = -2 * pi2 * pi2 * 0.5 * sx * sy * e
+        return Tt - (2.0 * T * (Tx * Tx + Ty * Ty) + T * T * lap)
+
+    o = OracleSolver(m, [PeriodicBC(), PeriodicBC(), PeriodicBC(), PeriodicBC()])
+    T = exact(0.0).numpy().copy()
+    rho = np.ones_like(T)
+    dt, t = 2e-4, 0.0
+    for _ in range(3):
+        o.set_source(forcing(t + dt).numpy().copy())
+        st, _ = o.step(T, rho, 1.0, 1.0, 2.0, dt, rtol=0.0, atol=1e-10, max_iter=100000)
+        assert st["status"] == 0
+        t += dt
+    d = (T - exact(t).numpy())[1:-1, 1:-1]
+    return float(np.sqrt((d * d).mean()))
+
+
+def test_mms_second_order_on_wavy_mesh():
+    e1, e2 = _mms_periodic_error(16), _mms_periodic_error(32)
+    order = math.log2(e1 / e2)
+    assert 1.7 < order < 2.4, (e1, e2, order)
+
+
+# ------------------------------------------------------------------ golden
+def test_golden_fixtures_reproduce():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", GOLDEN / "make_golden.py")
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    for name, case in mg.CASES.items():
+        ref = np.load(GOLDEN / f"{name}.npz")
+        got = mg.run_case(name, case)
+        assert np.array_equal(got["niter"], ref["niter"]), name
+        assert np.array_equal(got["T"], ref["T"]), name
+        assert np.array_equal(got["q"], ref["q"]), name
+        assert np.allclose(got["next_dt"], ref["next_dt"], rtol=1e-15, atol=0), name
+
+
+def test_schedule_round_half_even():
+    """min_err_check = Int(round(0.9·last)) uses round-half-even (PseudoTransientSolver.jl:207)."""
+    assert int(np.rint(0.9 * 5)) == 4 and int(np.rint(0.9 * 15)) == 14 and int(np.rint(0.9 * 25)) == 22
+
+
+def test_nonfinite_and_max_iter_paths():
+    pr = small_case_2d()
+    o = OracleSolver(pr.mesh, pr.bcs)
+    T = pr.T0.numpy().copy()
+    st, _ = o.step(T, pr.rho.numpy(), pr.cp, 1.0, 3.0, pr.dt, rtol=0.0, atol=1e-8, max_iter=3)
+    assert st["status"] == 1 and st["niter"] == 4
+    T = pr.T0.numpy().copy()
+    T[5, 5] = np.nan
+    o2 = OracleSolver(pr.mesh, pr.bcs)
+    st, _ = o2.step(T, pr.rho.numpy(), pr.cp, 1.0, 3.0, pr.dt, rtol=0.0, atol=1e-8)
+    assert st["status"] == 2 and st["niter"] == 1
+    S = np.zeros_like(T)
+    S[3, 3] = np.inf
+    o3 = OracleSolver(pr.mesh, pr.bcs)
+    o3.set_source(S)
+    st, _ = o3.step(pr.T0.numpy().copy(), pr.rho.numpy(), pr.cp, 1.0, 3.0, pr.dt)
+    assert st["status"] == 3
