@@ -40,7 +40,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batch", choices=["batch", "gaussian128", "mms4096", "gauss3d256"])
+    ap.add_argument("--workload", default="batch",
+                    choices=["batch", "gaussian128", "gaussian2048", "mms4096", "gauss3d256", "gauss3d128"])
     ap.add_argument("--nprob", type=int, default=256)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -159,10 +160,16 @@ def make_workload(name, nprob, rank, device):
     if name == "batch":
         probs = problems.batch_2d(nprob=nprob, seed=problems.BATCH_SEED + rank, device=device)
         cfg = {"workload": "batch2d_256_fp64", "nprob": nprob, "sides": "U{64..512}", "seed": problems.BATCH_SEED,
-               "dt": 1e-5, "tol": "max|r|/sqrt(N) <= 1e-8, rtol 0", "bcs": "Neumann x4", "mean": "harmonic"}
+               "dt": 1e-5, "tol": "rel <= 1e-8 or max|r|/sqrt(N) <= 1e-8", "bcs": "Neumann x4", "mean": "harmonic"}
     elif name == "gaussian128":
         probs = [problems.gaussian_2d(128, device=device)]
         cfg = {"workload": "gaussian2d_128_fp64", "kappa": "T^3", "dt": 1e-5, "tol": 1e-8}
+    elif name == "gaussian2048":
+        probs = [problems.gaussian_2d(2048, device=device)]
+        cfg = {"workload": "gaussian2d_2048_fp64", "kappa": "T^3", "dt": 1e-5, "tol": 1e-8}
+    elif name == "gauss3d128":
+        probs = [problems.gaussian_3d(128, device=device)]
+        cfg = {"workload": "gaussian3d_128_fp64", "kappa": "T^2.5", "dt": 1e-5, "tol": 1e-8}
     elif name == "mms4096":
         probs = [problems.mms_2d(4096, device=device)]
         cfg = {"workload": "mms2d_4096_fp64", "kappa": "T^2.5", "dt": 1e-5, "tol": 1e-8}

@@ -41,8 +41,12 @@ class Problem:
     kappa: PowerLawConductivity
     dt: float
     nsteps: int
+    # "1e-8 residual": the reference's stopping rule rel <= rtol || abs <= atol
+    # (PseudoTransientSolver.jl:316) with both at 1e-8.  An absolute 1e-8 alone
+    # in the max-norm/sqrt(N) sits below the FP64 round-off floor
+    # (about 4·α·|∇ξ|²·ulp(T) per cell) for some configured problems.
     atol: float = 1e-8
-    rtol: float = 0.0
+    rtol: float = 1e-8
     source: Optional[torch.Tensor] = None
     meta: dict = field(default_factory=dict)
 
