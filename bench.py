@@ -4,7 +4,7 @@ Workload (default, one GPU): the 2D batched configuration — 256 independent
 FP64 APT problems on sin-wavy meshes with sides drawn from U{64..512}, wave
 amplitude U(0, 0.08), κ = Tⁿ with n ∈ {0, 1, 2.5, 3}, Gaussian centre
 U(0.3, 0.7)² and width U(0.05, 0.2) from seed 20261203; every problem solves
-each time step to max|r|/√N ≤ 1e-8 (rtol = 0).  One bench step is one time
+each time step to rel ≤ 1e-8 or max|r|/√N ≤ 1e-8.  One bench step is one time
 step (dt = 1e-5) of the whole batch.  Inputs are synthetic (seeded), there is
 no dataset.
 
