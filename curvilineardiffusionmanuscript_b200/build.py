@@ -26,6 +26,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", f"-I{ROOT / '
 # translation unit -> extra flags
 UNITS = {
     "apt_sweep_fp64.cu": ["-fmad=false"],
+    "apt_march2d.cu": ["-fmad=false"],
     "apt_aux.cu": ["-fmad=false"],
     "engine.cu": ["-fmad=false"],
     "apt_mixed.cu": [],

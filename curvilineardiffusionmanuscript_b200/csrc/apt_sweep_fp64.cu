@@ -25,6 +25,7 @@
 // q' and r are never stored.
 #include "cdm_device.cuh"
 #include "cdm_kernels.h"
+#include "cdm_finish.cuh"
 
 namespace cdm {
 
@@ -86,93 +87,6 @@ __device__ __forceinline__ void stage_cell(const Problem& P, const double* __res
   us = uval; as = al; ts = t; ds = d;
   if (!isfinite(al)) bad |= 1;
   if (al < 0.0) bad |= 2;
-}
-
-// block-wide reduction of the residual partial and the last-block finish
-template <int NT>
-__device__ __forceinline__ void finish_iteration(const Problem& P, Ctrl* C, int tile, int iter,
-                                                 bool check, double local, bool local_nan, int bad,
-                                                 double* s_red, int* s_flag) {
-  const int tid = threadIdx.x;
-  const int lane = tid & 31, warp = tid >> 5;
-  const bool rms = C->norm_kind == 1;
-  // validity bits of the diffusivity of this iteration (validate_scalar, next step)
-  const int anybad = __syncthreads_or(bad);
-  if (tid == 0 && anybad) atomicOr(&C->abad[iter & 1], anybad);
-  if (check) {
-    const int anynan = __syncthreads_or(local_nan ? 1 : 0);
-    double v = local;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double w = __shfl_xor_sync(0xffffffffu, v, o);
-      v = rms ? v + w : fmax(v, w);
-    }
-    if (lane == 0) s_red[warp] = v;
-    __syncthreads();
-    if (tid == 0) {
-      double r = s_red[0];
-      for (int w = 1; w < NT / 32; ++w) r = rms ? r + s_red[w] : fmax(r, s_red[w]);
-      if (anynan && !rms) r = __longlong_as_double(0x7ff8000000000000ll);
-      P.partial[tile] = r;
-    }
-  }
-  // arrival; the last block of this problem finishes the iteration
-  if (tid == 0) {
-    __threadfence();
-    const unsigned prev = atomicAdd(&C->arrive, 1u);
-    *s_flag = (prev == (unsigned)P.ntiles - 1u);
-  }
-  __syncthreads();
-  if (!*s_flag) return;
-  __threadfence();
-  double L2 = 0.0;
-  if (check) {
-    // deterministic: fixed partition of partials over threads, fixed tree
-    double v = rms ? 0.0 : 0.0;
-    bool nan = false;
-    for (int t = tid; t < P.ntiles; t += NT) {
-      const double w = ld_cg_double(&P.partial[t]);
-      if (w != w) nan = true;
-      v = rms ? v + w : fmax(v, w);
-    }
-    const int anynan = __syncthreads_or(nan ? 1 : 0);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double w = __shfl_xor_sync(0xffffffffu, v, o);
-      v = rms ? v + w : fmax(v, w);
-    }
-    if (lane == 0) s_red[warp] = v;
-    __syncthreads();
-    if (tid == 0) {
-      double r = s_red[0];
-      for (int w = 1; w < NT / 32; ++w) r = rms ? r + s_red[w] : fmax(r, s_red[w]);
-      if (anynan) r = __longlong_as_double(0x7ff8000000000000ll);
-      L2 = rms ? sqrt(r / C->nfull) : r / C->sqrtN;
-    }
-  }
-  if (tid == 0) {
-    // PseudoTransientSolver.jl:284-318
-    if (check) {
-      C->n_checks += 1;
-      if (iter == 1) C->init_L2 = L2;
-      C->rel = L2 / C->init_L2;
-      C->abs = L2;
-    }
-    const double rel = C->rel, ab = C->abs;
-    if (!isfinite(rel) || !isfinite(ab)) {
-      C->status = ST_NONFINITE;
-      C->done = 1;
-    } else if (iter > C->max_iter) {
-      C->status = ST_MAX_ITER;
-      C->done = 1;
-    } else if (rel <= C->rtol || ab <= C->atol) {
-      C->done = 1;
-    }
-    C->abad[(iter + 1) & 1] = 0;
-    C->arrive = 0u;
-    __threadfence();
-    C->iter = iter;
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -501,10 +415,10 @@ __global__ void __launch_bounds__(NT) sweep3d_fp64(const Problem* __restrict__ p
 // ---------------------------------------------------------------------------
 // tile shape table (the autotuner picks among these)
 static const TileShape kShapes2D[] = {
-    {32, 16, 1, 256}, {32, 8, 1, 256}, {64, 8, 1, 256}, {16, 16, 1, 256},
+    {128, 0, 0, 128, 1}, {64, 0, 0, 64, 1}, {32, 16, 1, 256, 0}, {32, 8, 1, 256, 0},
 };
 static const TileShape kShapes3D[] = {
-    {32, 4, 4, 256}, {16, 8, 4, 256},
+    {32, 4, 4, 256, 0}, {16, 8, 4, 256, 0},
 };
 
 int num_tile_shapes(int ndim) { return ndim == 2 ? 4 : 2; }
@@ -529,10 +443,10 @@ cudaError_t launch_sweep_fp64(int ndim, int variant, const Problem* probs, const
   if (nitems <= 0) return cudaSuccess;
   if (ndim == 2) {
     switch (variant) {
-      case 0: sweep2d_fp64<32, 16, 256><<<nitems, 256, 0, s>>>(probs, items); break;
-      case 1: sweep2d_fp64<32, 8, 256><<<nitems, 256, 0, s>>>(probs, items); break;
-      case 2: sweep2d_fp64<64, 8, 256><<<nitems, 256, 0, s>>>(probs, items); break;
-      default: sweep2d_fp64<16, 16, 256><<<nitems, 256, 0, s>>>(probs, items); break;
+      case 0: return launch_march2d_fp64(0, probs, items, nitems, s);
+      case 1: return launch_march2d_fp64(1, probs, items, nitems, s);
+      case 2: sweep2d_fp64<32, 16, 256><<<nitems, 256, 0, s>>>(probs, items); break;
+      default: sweep2d_fp64<32, 8, 256><<<nitems, 256, 0, s>>>(probs, items); break;
     }
     return cudaGetLastError();
   }

@@ -51,6 +51,7 @@ struct Problem {
   int ndim, ni, nj, nk, nh;
   int nx, ny, nz;                   // full sizes
   int tiles_i, tiles_j, tiles_k, ntiles;
+  int strip_h;                      // row-marching kernels: rows per strip
   int mean;                         // 0 harmonic, 1 arithmetic
   int subcycle;                     // subcycle_conductivity
   int kmode, km, khalf;             // conductivity exponent decomposition

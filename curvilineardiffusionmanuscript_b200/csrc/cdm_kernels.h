@@ -10,10 +10,13 @@ struct Ctrl;
 
 struct TileShape {
   int tx, ty, tz, threads;
+  int march;  // 1: row-marching kernel, tx = threads per block (tx-2 owned columns)
 };
 
 int num_tile_shapes(int ndim);
 TileShape tile_shape(int ndim, int variant);
+
+cudaError_t launch_march2d_fp64(int variant, const Problem* probs, const int2* items, int nitems, cudaStream_t s);
 
 // one fused FP64 pseudo-iteration over all items (problem, tile)
 cudaError_t launch_sweep_fp64(int ndim, int variant, const Problem* probs, const int2* items, int nitems,

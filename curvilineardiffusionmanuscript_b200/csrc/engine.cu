@@ -178,7 +178,6 @@ int Engine::init(int nprob, const cdm_mesh_desc* meshes, const cdm_bc* bcs, cons
   }
   ps.resize(nprob);
   hp.resize(nprob);
-  const TileShape ts = tile_shape(ndim, variant);
   for (int p = 0; p < nprob; ++p) {
     const cdm_mesh_desc& m = meshes[p];
     ProbState& s = ps[p];
@@ -262,11 +261,6 @@ int Engine::init(int nprob, const cdm_mesh_desc* meshes, const cdm_bc* bcs, cons
       set_error("physical length L must be > 0");
       return CDM_BAD_INPUT;
     }
-    // tiles
-    s.tiles_i = (s.ni + ts.tx - 1) / ts.tx;
-    s.tiles_j = (s.nj + ts.ty - 1) / ts.ty;
-    s.tiles_k = ndim == 3 ? (s.nk + ts.tz - 1) / ts.tz : 1;
-    s.ntiles = s.tiles_i * s.tiles_j * s.tiles_k;
     // allocations
     const size_t N = (size_t)s.nfull;
     for (int b = 0; b < 2; ++b) {
@@ -376,11 +370,30 @@ int Engine::init(int nprob, const cdm_mesh_desc* meshes, const cdm_bc* bcs, cons
 int Engine::build_items() {
   const TileShape ts = tile_shape(ndim, variant);
   std::vector<int2> items;
-  for (size_t p = 0; p < ps.size(); ++p) {
+  const int nprob = (int)ps.size();
+  for (int p = 0; p < nprob; ++p) {
     ProbState& s = ps[p];
-    s.tiles_i = (s.ni + ts.tx - 1) / ts.tx;
-    s.tiles_j = (s.nj + ts.ty - 1) / ts.ty;
-    s.tiles_k = ndim == 3 ? (s.nk + ts.tz - 1) / ts.tz : 1;
+    if (ts.march) {
+      // column blocks of tx-2 owned columns; strips of rows sized so that a
+      // single problem fills several waves of 148 SMs
+      const int ow = ts.tx - 2;
+      s.tiles_i = (s.ni + ow - 1) / ow;
+      int h = 64;
+      if (nprob == 1) {
+        const int target = 148 * 24;
+        int nstrips = (target + s.tiles_i - 1) / s.tiles_i;
+        nstrips = std::max(1, std::min(nstrips, (s.nj + 31) / 32));
+        h = (s.nj + nstrips - 1) / nstrips;
+      }
+      s.strip_h = std::max(1, std::min(h, s.nj));
+      s.tiles_j = (s.nj + s.strip_h - 1) / s.strip_h;
+      s.tiles_k = 1;
+    } else {
+      s.tiles_i = (s.ni + ts.tx - 1) / ts.tx;
+      s.tiles_j = (s.nj + ts.ty - 1) / ts.ty;
+      s.tiles_k = ndim == 3 ? (s.nk + ts.tz - 1) / ts.tz : 1;
+      s.strip_h = 0;
+    }
     s.ntiles = s.tiles_i * s.tiles_j * s.tiles_k;
     for (int t = 0; t < s.ntiles; ++t) items.push_back(make_int2((int)p, t));
   }
@@ -621,6 +634,7 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
     P.tiles_j = s.tiles_j;
     P.tiles_k = s.tiles_k;
     P.ntiles = s.ntiles;
+    P.strip_h = s.strip_h;
     P.mean = mean;
     P.subcycle = o.subcycle_conductivity ? 1 : 0;
     kappa_decompose(kappa[p].n, P.kmode, P.km, P.khalf);

@@ -32,7 +32,7 @@ struct ProbState {
   int rule[6] = {0, 0, 0, 0, 0, 0};
   double val[6] = {0, 0, 0, 0, 0, 0};
   int bc_kind[6] = {0, 0, 0, 0, 0, 0};
-  int tiles_i = 1, tiles_j = 1, tiles_k = 1, ntiles = 1;
+  int tiles_i = 1, tiles_j = 1, tiles_k = 1, ntiles = 1, strip_h = 1;
   // device buffers owned by the engine
   double* u[2] = {nullptr, nullptr};
   double* q[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
