@@ -27,6 +27,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", f"-I{ROOT / '
 UNITS = {
     "apt_sweep_fp64.cu": ["-fmad=false"],
     "apt_march2d.cu": ["-fmad=false"],
+    "apt_march2d_fast.cu": [],
     "apt_aux.cu": ["-fmad=false"],
     "engine.cu": ["-fmad=false"],
     "apt_mixed.cu": [],

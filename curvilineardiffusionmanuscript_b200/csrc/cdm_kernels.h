@@ -17,10 +17,13 @@ int num_tile_shapes(int ndim);
 TileShape tile_shape(int ndim, int variant);
 
 cudaError_t launch_march2d_fp64(int variant, const Problem* probs, const int2* items, int nitems, cudaStream_t s);
+cudaError_t launch_march2d_fast(int variant, const Problem* probs, const int2* items, int nitems, cudaStream_t s);
 
 // one fused FP64 pseudo-iteration over all items (problem, tile)
-cudaError_t launch_sweep_fp64(int ndim, int variant, const Problem* probs, const int2* items, int nitems,
-                              cudaStream_t s);
+// exact = 1: operation-for-operation reference arithmetic (bit-identical to the
+// CPU restatement); exact = 0: reciprocal form (last-bit differences)
+cudaError_t launch_sweep_fp64(int ndim, int variant, int exact, const Problem* probs, const int2* items,
+                              int nitems, cudaStream_t s);
 
 // metric cache (mesh_metric_cache.jl:39-250) and the packed divergence
 // coefficients derived from the cell-centre metrics and the cache

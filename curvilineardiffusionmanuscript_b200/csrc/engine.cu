@@ -503,7 +503,7 @@ int Engine::launch_block(int K, bool use_graph) {
   if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe], stream));
   prof.sweep_launches += K;
   if (!use_graph) {
-    for (int k = 0; k < K; ++k) CDM_CK(launch_sweep_fp64(ndim, variant, d_probs, d_items, nitems, stream));
+    for (int k = 0; k < K; ++k) CDM_CK(launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT, d_probs, d_items, nitems, stream));
     if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe + 1], stream));
     return CDM_OK;
   }
@@ -517,7 +517,7 @@ int Engine::launch_block(int K, bool use_graph) {
     CDM_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t le = cudaSuccess;
     for (int k = 0; k < K && le == cudaSuccess; ++k)
-      le = launch_sweep_fp64(ndim, variant, d_probs, d_items, nitems, stream);
+      le = launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT, d_probs, d_items, nitems, stream);
     cudaError_t ce = cudaStreamEndCapture(stream, &g);
     if (le != cudaSuccess) {
       set_error(std::string("sweep launch during capture: ") + cudaGetErrorString(le));

@@ -186,7 +186,8 @@ class PseudoTransientSolver:
         self.bcs = bc_list(bcs)
         cfg = L.default_config()
         cfg.mean = L.CDM_MEAN_HARMONIC if mean == "harmonic" else L.CDM_MEAN_ARITHMETIC
-        cfg.precision = {"fp64": L.CDM_PREC_FP64, "mixed": L.CDM_PREC_MIXED}[precision]
+        cfg.precision = {"fp64": L.CDM_PREC_FP64, "mixed": L.CDM_PREC_MIXED,
+                         "fp64_exact": L.CDM_PREC_FP64_EXACT}[precision]
         cfg.device = device
         cfg.stream = stream
         desc, keep = mesh_desc(mesh)
@@ -281,7 +282,7 @@ class PseudoTransientBatch:
     pseudo-iteration (CUDA-graph replays of the fused sweep)."""
 
     def __init__(self, meshes: Sequence[CurvilinearMesh], bcs_list, mean="harmonic", device=0,
-                 stream: Optional[int] = None):
+                 stream: Optional[int] = None, precision: str = "fp64"):
         self._lib = L.load()
         self.meshes = list(meshes)
         n = len(self.meshes)
@@ -301,6 +302,8 @@ class PseudoTransientBatch:
         cfg.mean = L.CDM_MEAN_HARMONIC if mean == "harmonic" else L.CDM_MEAN_ARITHMETIC
         cfg.device = device
         cfg.stream = stream
+        cfg.precision = {"fp64": L.CDM_PREC_FP64, "mixed": L.CDM_PREC_MIXED,
+                         "fp64_exact": L.CDM_PREC_FP64_EXACT}[precision]
         h = C.c_void_p()
         rc = self._lib.cdm_batch_create(n, descs, bcs, C.byref(cfg), C.byref(h))
         del keep

@@ -67,8 +67,12 @@ enum cdm_norm {
 };
 
 enum cdm_precision {
-  CDM_PREC_FP64 = 0,  /* plain FP64 APT: the reference algorithm                 */
-  CDM_PREC_MIXED = 1  /* FP32 sweeps + FP64 residual / defect-correction restarts */
+  CDM_PREC_FP64 = 0,       /* plain FP64 APT, divisions in reciprocal form (last-bit
+                              differences from the reference's expressions)          */
+  CDM_PREC_MIXED = 1,      /* FP32 sweeps + FP64 residual / defect-correction restarts */
+  CDM_PREC_FP64_EXACT = 2  /* plain FP64 APT evaluating the reference's expressions
+                              operation for operation (bit-identical to the CPU
+                              restatement of the reference)                          */
 };
 
 enum cdm_guess {
