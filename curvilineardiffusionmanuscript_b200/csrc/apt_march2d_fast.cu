@@ -2,8 +2,8 @@
 //
 // The same discrete iteration as apt_march2d.cu (and the reference's step!,
 // PseudoTransientSolver.jl:253-319), with the divisions of the reference's
-// expressions rewritten algebraically so that a cell needs four reciprocals
-// and a face two, instead of 4 + 3 per face + 3 IEEE divisions:
+// expressions rewritten algebraically so that a cell needs three or four
+// reciprocals and a face two, instead of 4 + 3 per face + 3 IEEE divisions:
 //
 //   α⁻¹ = ρcₚ/κ,  Re = π + √(π² + (L²/Δt)·ρ·α⁻¹),  dτ = Vp·L·α⁻¹·Re⁻¹,
 //   θ = (L/Vp)·Re⁻¹,  θ⁻¹ = (Vp/L)·Re,           (iteration_parameters.jl:2-15)
@@ -14,9 +14,15 @@
 //
 // Reciprocals come from the hardware approximation refined by two Newton–
 // Raphson steps (y ← y + y(1 − b·y)), accurate to about one ulp, and
-// multiply-adds are contracted.  Results therefore differ from the
-// operation-for-operation path in the last bits only (checked against the
-// CPU oracle at a relative L2 of 1e-10 with equal iteration counts).
+// multiply-adds are contracted, so results differ from the operation-for-
+// operation path in the last bits only (checked against the CPU oracle at a
+// relative L2 of 1e-10 with equal iteration counts).
+//
+// Organisation (see apt_march2d.cu): a block of TX threads owns TX-2 columns
+// and marches up a strip of rows.  Each thread keeps the values of its own
+// column (u, update factors, the fluxes of its faces) in registers; only the
+// values its neighbours need go through shared memory.  Blocks that touch no
+// domain boundary run a branch-free instantiation without ghost logic.
 #include "cdm_device.cuh"
 #include "cdm_finish.cuh"
 #include "cdm_kernels.h"
@@ -25,19 +31,17 @@ namespace cdm {
 
 namespace {
 
-// Newton–Raphson refinement of the hardware reciprocal approximation
-// (each step doubles the number of correct bits); exact IEEE division is
-// used for zero, subnormal, huge and non-finite arguments.
+// Newton–Raphson refinement of the hardware reciprocal approximation; the
+// approximation's own result is kept for 0 and ±inf arguments (1/0 = inf,
+// 1/inf = 0), where the refinement would produce NaN.
 __device__ __forceinline__ double rcp_nr(double b) {
-  const double ab = fabs(b);
-  if (!(ab > 1e-290 && ab < 1e290)) return 1.0 / b;
-  double y;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
-  double e = fma(-b, y, 1.0);
-  y = fma(y, e, y);
+  double y0;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(b));
+  double e = fma(-b, y0, 1.0);
+  double y = fma(y0, e, y0);
   e = fma(-b, y, 1.0);
   y = fma(y, e, y);
-  return y;
+  return (y0 == 0.0 || fabs(y0) == __longlong_as_double(0x7ff0000000000000ll)) ? y0 : y;
 }
 
 __device__ __forceinline__ double pow_fast(double x, int mode, int m, int half, double n) {
@@ -54,25 +58,26 @@ __device__ __forceinline__ double pow_fast(double x, int mode, int m, int half, 
   return pow(x, n);
 }
 
+template <int TX>
+struct FastSmem {
+  double U[3][TX], IA[3][TX], IT[3][TX];  // u, α⁻¹ (or α), θ⁻¹ (or θ) for the i-1 neighbour
+  double QX[3][TX], PX[3][TX];           // new damped / undamped i+1/2 fluxes
+  double QY[2][TX], PY[2][TX];           // new damped / undamped j+1/2 fluxes
+  double red[TX / 32];
+  int flag;
+};
+
+struct Cell {
+  double u, ia, it, g, f;
+};
+
 }  // namespace
 
-template <int TX>
-__global__ void __launch_bounds__(TX, 5) march2d_fast(const Problem* __restrict__ probs,
-                                                      const int2* __restrict__ items) {
+template <int TX, bool EDGE, bool HARM>
+__device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, int iter, bool check,
+                                          FastSmem<TX>& sm) {
   constexpr int OW = TX - 2;
-  __shared__ double sU[3][TX], sA[3][TX], sT[3][TX], sG[3][TX], sF[3][TX];
-  __shared__ double sQX[3][TX], sQY[2][TX], sPX[3][TX], sPY[2][TX];
-  __shared__ double s_red[TX / 32];
-  __shared__ int s_flag;
-
-  const int2 item = items[blockIdx.x];
-  const Problem& P = probs[item.x];
-  Ctrl* C = P.ctrl;
-  if (ld_cg_int(&C->done)) return;
-  const int iter = ld_cg_int(&C->iter) + 1;
-  const bool check = is_check_iter(C, iter);
   const int tid = threadIdx.x;
-  const int tile = item.y;
   const int cb = tile % P.tiles_i, sj = tile / P.tiles_i;
   const int ni = P.ni, nj = P.nj, nx = P.nx, nh = P.nh;
   const int i0 = cb * OW;
@@ -88,58 +93,77 @@ __global__ void __launch_bounds__(TX, 5) march2d_fast(const Problem* __restrict_
   double* __restrict__ qyout = P.q[qin ^ 1][1];
   const double* __restrict__ uprev = P.u_prev;
   const double* __restrict__ rho = P.rho;
+  const double* __restrict__ Sg = P.S;
+  const double* __restrict__ G11 = P.coef[0];
+  const double* __restrict__ G22 = P.coef[1];
+  const double* __restrict__ C12 = P.coef[2];
+  const double* __restrict__ CA = P.coef[3];
+  const double* __restrict__ CB = P.coef[4];
   const bool alpha_from_u = P.subcycle || iter == 1;
-  const bool harmonic = P.mean == 0;
   const bool rms = C->norm_kind == 1;
   const double dt = P.dt, cp = P.cp, k0 = P.k0;
   const double inv_dt = 1.0 / dt;
   const double LLdt = P.LL / dt, VpL = P.VpL, LoVp = P.L / P.Vpdtau, VpoL = P.Vpdtau / P.L;
   const int kmode = P.kmode, km = P.km, khalf = P.khalf;
   const double kn = P.kn;
-  const bool colIn = a >= 0 && a < ni;
+  const bool colIn = EDGE ? (a >= 0 && a < ni) : true;
   const bool owner = tid >= 1 && tid <= OW && colIn;
-  const bool qx_col = a >= -1 && a <= ni - 1 && tid < TX - 1;
-  const bool qx_own = qx_col && (owner || a == -1);
-  const int col = a + nh;  // full-array column of this thread
+  const bool qx_col = EDGE ? (a >= -1 && a <= ni - 1 && tid < TX - 1) : (tid < TX - 1);
+  const bool qx_own = qx_col && (owner || (EDGE && a == -1));
+  const int col = a + nh;
 
-  // ghost rule of this thread's column (i sides) resolved once
-  int cside = -1;
-  if (a == -1) cside = 0;
-  else if (a == ni) cside = 1;
-  int csrc_col = col;
+  // ghost rule of this thread's column (i sides), resolved once
+  int cside = -1, csrc_col = col;
   bool cneg = false, cconst = false;
   double cval = 0.0;
-  if (cside >= 0) {
-    const int rule = P.rule[cside];
-    const bool lo = cside == 0;
-    if (rule == GR_DIRICHLET) {
-      cconst = true;
-      cval = P.val[cside];
-    } else {
-      int p = rule == GR_NONE ? (lo ? -1 : ni) : (rule == GR_PERIODIC ? (lo ? ni - 1 : 0) : (lo ? 0 : ni - 1));
-      csrc_col = p + nh;
-      cneg = rule == GR_NEGSYM;
+  if (EDGE) {
+    if (a == -1) cside = 0;
+    else if (a == ni) cside = 1;
+    if (cside >= 0) {
+      const int rule = P.rule[cside];
+      const bool lo = cside == 0;
+      if (rule == GR_DIRICHLET) {
+        cconst = true;
+        cval = P.val[cside];
+      } else {
+        const int p = rule == GR_NONE ? (lo ? -1 : ni) : (rule == GR_PERIODIC ? (lo ? ni - 1 : 0) : (lo ? 0 : ni - 1));
+        csrc_col = p + nh;
+        cneg = rule == GR_NEGSYM;
+      }
     }
   }
 
-  // u-source of cell (a, r): offset, constant or inactive
-  struct Src {
-    int off;  // >= 0 offset; -1 constant; -2 inactive
+  struct Pre {
+    double u, ua, rho, qx, qy;
+    int off;  // >= 0 source offset, -1 constant (value in u), -2 inactive
     bool neg;
-    double cv;
   };
-  auto src_of = [&](int r) -> Src {
-    Src s{-2, false, 0.0};
+  // issue the loads of row r (u with its ghost source, rho, old fluxes)
+  auto prefetch = [&](int r, Pre& L) {
+    const int ro = col + nx * (r + nh);
+    L.neg = false;
+    L.ua = 0.0;
+    if (!EDGE) {
+      L.off = ro;
+      L.u = uin[ro];
+      if (!alpha_from_u) L.ua = uprev[ro];
+      L.rho = rho[ro];
+      L.qx = qx_col ? qxin[ro] : 0.0;
+      L.qy = qyin[ro - nx];
+      return;
+    }
+    int off = -2;
+    double cv = 0.0;
     const bool rIn = r >= 0 && r < nj;
     if (rIn) {
-      if (colIn) s.off = col + nx * (r + nh);
+      if (colIn) off = ro;
       else if (cside >= 0) {
         if (cconst) {
-          s.off = -1;
-          s.cv = cval;
+          off = -1;
+          cv = cval;
         } else {
-          s.off = csrc_col + nx * (r + nh);
-          s.neg = cneg;
+          off = csrc_col + nx * (r + nh);
+          L.neg = cneg;
         }
       }
     } else if (colIn && (r == -1 || r == nj)) {
@@ -147,80 +171,67 @@ __global__ void __launch_bounds__(TX, 5) march2d_fast(const Problem* __restrict_
       const int rule = P.rule[side];
       const bool lo = side == 2;
       if (rule == GR_DIRICHLET) {
-        s.off = -1;
-        s.cv = P.val[side];
+        off = -1;
+        cv = P.val[side];
       } else {
         const int p = rule == GR_NONE ? (lo ? -1 : nj) : (rule == GR_PERIODIC ? (lo ? nj - 1 : 0) : (lo ? 0 : nj - 1));
-        s.off = col + nx * (p + nh);
-        s.neg = rule == GR_NEGSYM;
+        off = col + nx * (p + nh);
+        L.neg = rule == GR_NEGSYM;
       }
     }
-    return s;
-  };
-
-  struct Pre {
-    double u, ua, rho, qx, qy;
-    Src s;
-  };
-  auto prefetch = [&](int r, Pre& L) {
-    L.s = src_of(r);
-    L.u = 0.0;
-    L.ua = 0.0;
+    L.off = off;
+    L.u = cv;
     L.rho = 1.0;
-    const int ro = col + nx * (r + nh);
-    if (L.s.off >= 0) {
-      L.u = uin[L.s.off];
-      if (!alpha_from_u) L.ua = uprev[L.s.off];
+    if (off >= 0) {
+      L.u = uin[off];
+      if (!alpha_from_u) L.ua = uprev[off];
+    } else if (off == -1) {
+      L.ua = cv;
     }
-    if (L.s.off != -2) L.rho = rho[ro];
-    L.qx = (qx_col && r >= 0 && r < nj) ? qxin[ro] : 0.0;
+    if (off != -2) L.rho = rho[ro];
+    L.qx = (qx_col && rIn) ? qxin[ro] : 0.0;
     L.qy = (colIn && r >= 0 && r <= nj) ? qyin[ro - nx] : 0.0;
   };
 
   int bad = 0;
-  auto stage = [&](int r, int s, const Pre& L) {
-    double us = 0.0, ia = 0.0, it = 0.0, g = 0.0, f = 0.0;
-    if (L.s.off != -2) {
-      us = L.s.off == -1 ? L.s.cv : (L.s.neg ? -L.u : L.u);
-      double src = us;
-      if (!alpha_from_u) src = L.s.off == -1 ? L.s.cv : (L.s.neg ? -L.ua : L.ua);
-      const double kap = isfinite(src) ? k0 * pow_fast(fabs(src), kmode, km, khalf, kn) : 0.0;
-      const double rc = L.rho * cp;
-      const double inva = rc * rcp_nr(kap);    // α⁻¹
-      const double al = harmonic ? 0.0 : kap * rcp_nr(rc);  // α for the arithmetic mean
-      const double Re = kPi + sqrt(kPi * kPi + LLdt * L.rho * inva);
-      const double iRe = rcp_nr(Re);
-      double dtau = VpL * inva * iRe;
-      double th = LoVp * iRe;
-      dtau = isfinite(dtau) ? dtau : 0.0;
-      th = isfinite(th) ? th : 0.0;
-      const double id = rcp_nr(dt + dtau);
-      g = dt * id;
-      f = dtau * dt * id;
-      if (harmonic) {
-        ia = inva;
-        it = VpoL * Re;
-      } else {
-        ia = al;
-        it = th;
-      }
-      const bool track = (tid >= 1 && tid <= OW) || cside >= 0;
-      if (track && r >= j0 - (j0 == 0) && r < j1 + (j1 == nj)) {
-        // α = κ/(ρcₚ) is finite iff κ and ρcₚ are finite and ρcₚ ≠ 0; negative iff signs differ
-        if (!(isfinite(kap) && isfinite(rc) && rc != 0.0)) bad |= 1;
-        if (kap != 0.0 && ((kap < 0.0) != (rc < 0.0))) bad |= 2;
-      }
+  // diffusivity, pseudo-time parameters and update factors of cell (a, r)
+  auto stage = [&](int r, const Pre& L) -> Cell {
+    Cell c{0.0, 0.0, 0.0, 0.0, 0.0};
+    if (EDGE && L.off == -2) return c;
+    const double us = L.neg ? -L.u : L.u;
+    const double src = alpha_from_u ? us : (L.neg ? -L.ua : L.ua);
+    const double kap = isfinite(src) ? k0 * pow_fast(fabs(src), kmode, km, khalf, kn) : 0.0;
+    const double rc = L.rho * cp;
+    const double inva = rc * rcp_nr(kap);
+    const double Re = kPi + sqrt(kPi * kPi + LLdt * L.rho * inva);
+    const double iRe = rcp_nr(Re);
+    double dtau = VpL * inva * iRe;
+    double th = LoVp * iRe;
+    dtau = isfinite(dtau) ? dtau : 0.0;
+    th = isfinite(th) ? th : 0.0;
+    const double id = rcp_nr(dt + dtau);
+    c.u = us;
+    c.g = dt * id;
+    c.f = dtau * dt * id;
+    if (HARM) {
+      c.ia = inva;
+      c.it = VpoL * Re;
+    } else {
+      c.ia = kap * rcp_nr(rc);
+      c.it = th;
     }
-    sU[s][tid] = us;
-    sA[s][tid] = ia;
-    sT[s][tid] = it;
-    sG[s][tid] = g;
-    sF[s][tid] = f;
+    // validity of α = κ/(ρcₚ) on owned cells and first-layer ghosts
+    const bool track = (tid >= 1 && tid <= OW) || (EDGE && cside >= 0);
+    if (track && r >= j0 - (EDGE && j0 == 0) && r < j1 + (EDGE && j1 == nj)) {
+      if (!(isfinite(kap) && isfinite(rc) && rc != 0.0)) bad |= 1;
+      if (kap != 0.0 && ((kap < 0.0) != (rc < 0.0))) bad |= 2;
+    }
+    return c;
   };
 
-  auto flux = [&](double ia0, double ia1, double it0, double it1, double du, double qold, double& qp) {
+  auto flux = [&](double ia0, double ia1, double it0, double it1, double du, double qold, double& qp) -> double {
     double an, qn;
-    if (harmonic) {
+    if (HARM) {
       an = 2.0 * rcp_nr(ia0 + ia1);
       const double St = it0 + it1;
       // θ̄ = 0 when a cell has θ = 0 (θ⁻¹ infinite): q ← −ᾱΔu
@@ -233,41 +244,54 @@ __global__ void __launch_bounds__(TX, 5) march2d_fast(const Problem* __restrict_
     qp = -an * du;
     return qn;
   };
-  auto face_x = [&](int r, int s, double qold) {
-    double qn = 0.0, qp = 0.0;
-    if (qx_col && r >= 0 && r < nj)
-      qn = flux(sA[s][tid], sA[s][tid + 1], sT[s][tid], sT[s][tid + 1], sU[s][tid + 1] - sU[s][tid], qold, qp);
-    sQX[s][tid] = qn;
-    sPX[s][tid] = qp;
-  };
-  auto face_y = [&](int r, int s0, int s1, int sy, double qold) {
-    double qn = 0.0, qp = 0.0;
-    if (colIn && r >= -1 && r <= nj - 1)
-      qn = flux(sA[s0][tid], sA[s1][tid], sT[s0][tid], sT[s1][tid], sU[s1][tid] - sU[s0][tid], qold, qp);
-    sQY[sy][tid] = qn;
-    sPY[sy][tid] = qp;
+  // i+1/2 face of row r between this column and the next (neighbour from shared memory)
+  auto face_x = [&](int r, int s, const Cell& c, double qold, double& qp) -> double {
+    double qn = 0.0;
+    qp = 0.0;
+    if (qx_col && (!EDGE || (r >= 0 && r < nj)))
+      qn = flux(c.ia, sm.IA[s][tid + 1], c.it, sm.IT[s][tid + 1], sm.U[s][tid + 1] - c.u, qold, qp);
     return qn;
   };
+  // j+1/2 face between rows r and r+1 of this column (registers only)
+  auto face_y = [&](int r, const Cell& lo, const Cell& hi, double qold, double& qp) -> double {
+    double qn = 0.0;
+    qp = 0.0;
+    if (colIn && (!EDGE || (r >= -1 && r <= nj - 1))) qn = flux(lo.ia, hi.ia, lo.it, hi.it, hi.u - lo.u, qold, qp);
+    return qn;
+  };
+  auto publish = [&](int s, const Cell& c) {
+    sm.U[s][tid] = c.u;
+    sm.IA[s][tid] = c.ia;
+    sm.IT[s][tid] = c.it;
+  };
 
-  // rotating slots: row r lives in slot sl[(r - j0 + 1) % 3]; handled by rotation
-  int sm = 0, s0 = 1, sp = 2;  // slots of rows j-1, j, j+1 when processing row j
-  int ym = 0, y0 = 1;          // slots of face rows j-1 and j
+  int s_m = 0, s_0 = 1, s_p = 2;  // slots of rows j-1, j, j+1
+  int y_m = 0, y_0 = 1;           // slots of face rows j-1, j
   Pre L0, L1, Ln;
   prefetch(j0 - 1, L0);
   prefetch(j0, L1);
-  stage(j0 - 1, sm, L0);
-  stage(j0, s0, L1);
-  __syncthreads();
-  face_x(j0 - 1, sm, L0.qx);
-  face_x(j0, s0, L1.qx);
-  {
-    const double qn = face_y(j0 - 1, sm, s0, ym, L1.qy);
-    if (j0 == 0 && owner) {
-      qyout[col + nx * (nh - 1)] = qn;
-      uout[col + nx * (nh - 1)] = sU[sm][tid];
-    }
-  }
   prefetch(j0 + 1, Ln);
+  Cell cm = stage(j0 - 1, L0);
+  Cell c0 = stage(j0, L1);
+  publish(s_m, cm);
+  publish(s_0, c0);
+  __syncthreads();
+  double px_m, px_0, py_m;
+  const double qx_m = face_x(j0 - 1, s_m, cm, L0.qx, px_m);
+  const double qx_0 = face_x(j0, s_0, c0, L1.qx, px_0);
+  const double qy_m = face_y(j0 - 1, cm, c0, L1.qy, py_m);
+  sm.QX[s_m][tid] = qx_m;
+  sm.PX[s_m][tid] = px_m;
+  sm.QX[s_0][tid] = qx_0;
+  sm.PX[s_0][tid] = px_0;
+  sm.QY[y_m][tid] = qy_m;
+  sm.PY[y_m][tid] = py_m;
+  if (EDGE && j0 == 0 && owner) {
+    qyout[col + nx * (nh - 1)] = qy_m;
+    uout[col + nx * (nh - 1)] = cm.u;  // row -1 ghost after applybcs!
+  }
+  // own-column fluxes in registers: x faces of rows j-1 and j, y face of row j-1
+  double rqx_m = qx_m, rqx_0 = qx_0, rpx_m = px_m, rpx_0 = px_0, rqy_m = qy_m, rpy_m = py_m;
 
   double local = 0.0;
   bool local_nan = false;
@@ -275,38 +299,44 @@ __global__ void __launch_bounds__(TX, 5) march2d_fast(const Problem* __restrict_
     const Pre Lc = Ln;
     if (j + 1 < j1) prefetch(j + 2, Ln);
     const int o = col + nx * (j + nh);
-    double G11 = 0, G22 = 0, C12 = 0, CA = 0, CB = 0, UP = 0, SS = 0;
+    double g11 = 0, g22 = 0, c12 = 0, ca = 0, cbv = 0, up = 0, S = 0;
     if (owner) {
-      G11 = P.coef[0][o];
-      G22 = P.coef[1][o];
-      C12 = P.coef[2][o];
-      CA = P.coef[3][o];
-      CB = P.coef[4][o];
-      UP = uprev[o];
-      SS = P.S[o];
+      g11 = G11[o];
+      g22 = G22[o];
+      c12 = C12[o];
+      ca = CA[o];
+      cbv = CB[o];
+      up = uprev[o];
+      S = Sg[o];
     }
-    stage(j + 1, sp, Lc);
+    const Cell cp1 = stage(j + 1, Lc);
+    publish(s_p, cp1);
     __syncthreads();
-    face_x(j + 1, sp, Lc.qx);
-    const double qyn = face_y(j, s0, sp, y0, Lc.qy);
+    double px_p1, py_0n;
+    const double qx_p1 = face_x(j + 1, s_p, cp1, Lc.qx, px_p1);
+    const double qy_0n = face_y(j, c0, cp1, Lc.qy, py_0n);
+    sm.QX[s_p][tid] = qx_p1;
+    sm.PX[s_p][tid] = px_p1;
+    sm.QY[y_0][tid] = qy_0n;
+    sm.PY[y_0][tid] = py_0n;
     __syncthreads();
     if (owner) {
       const int x = tid;
-      const double dq = G11 * (sQX[s0][x] - sQX[s0][x - 1]) + G22 * (sQY[y0][x] - sQY[ym][x]) +
-                        C12 * ((sQX[sp][x] + sQX[sp][x - 1]) - (sQX[sm][x] + sQX[sm][x - 1])) +
-                        C12 * ((sQY[y0][x + 1] + sQY[ym][x + 1]) - (sQY[y0][x - 1] + sQY[ym][x - 1])) +
-                        CA * (0.5 * (sQX[s0][x] + sQX[s0][x - 1])) + CB * (0.5 * (sQY[y0][x] + sQY[ym][x]));
-      const double un = sG[s0][x] * sU[s0][x] + sF[s0][x] * (UP * inv_dt - dq + SS);
+      const double dq = g11 * (rqx_0 - sm.QX[s_0][x - 1]) + g22 * (qy_0n - rqy_m) +
+                        c12 * ((qx_p1 + sm.QX[s_p][x - 1]) - (rqx_m + sm.QX[s_m][x - 1])) +
+                        c12 * ((sm.QY[y_0][x + 1] + sm.QY[y_m][x + 1]) - (sm.QY[y_0][x - 1] + sm.QY[y_m][x - 1])) +
+                        ca * (0.5 * (rqx_0 + sm.QX[s_0][x - 1])) + cbv * (0.5 * (qy_0n + rqy_m));
+      const double un = c0.g * c0.u + c0.f * (up * inv_dt - dq + S);
       uout[o] = un;
-      qyout[o] = qyn;
+      qyout[o] = qy_0n;
       if (check) {
-        const double dqp = G11 * (sPX[s0][x] - sPX[s0][x - 1]) + G22 * (sPY[y0][x] - sPY[ym][x]) +
-                           C12 * ((sPX[sp][x] + sPX[sp][x - 1]) - (sPX[sm][x] + sPX[sm][x - 1])) +
-                           C12 * ((sPY[y0][x + 1] + sPY[ym][x + 1]) - (sPY[y0][x - 1] + sPY[ym][x - 1])) +
-                           CA * (0.5 * (sPX[s0][x] + sPX[s0][x - 1])) + CB * (0.5 * (sPY[y0][x] + sPY[ym][x]));
-        double du = un - UP;
-        if (isapprox_eps(un, UP)) du = 0.0;
-        const double r = -du * inv_dt - dqp + SS;
+        const double dqp = g11 * (rpx_0 - sm.PX[s_0][x - 1]) + g22 * (py_0n - rpy_m) +
+                           c12 * ((px_p1 + sm.PX[s_p][x - 1]) - (rpx_m + sm.PX[s_m][x - 1])) +
+                           c12 * ((sm.PY[y_0][x + 1] + sm.PY[y_m][x + 1]) - (sm.PY[y_0][x - 1] + sm.PY[y_m][x - 1])) +
+                           ca * (0.5 * (rpx_0 + sm.PX[s_0][x - 1])) + cbv * (0.5 * (py_0n + rpy_m));
+        double du = un - up;
+        if (isapprox_eps(un, up)) du = 0.0;
+        const double r = -du * inv_dt - dqp + S;
         if (rms) local += r * r;
         else {
           const double ar = fabs(r);
@@ -314,26 +344,67 @@ __global__ void __launch_bounds__(TX, 5) march2d_fast(const Problem* __restrict_
           else local = fmax(local, ar);
         }
       }
-      if (j == nj - 1) uout[o + nx] = sU[sp][x];
+      if (EDGE && j == nj - 1) uout[o + nx] = cp1.u;
     }
-    if (qx_own) qxout[o] = sQX[s0][tid];
-    if (cside >= 0) uout[o] = sU[s0][tid];
-    // rotate the windows: rows (j, j+1, j+2) -> slots (s0, sp, sm)
-    const int t = sm;
-    sm = s0;
-    s0 = sp;
-    sp = t;
-    const int u = ym;
-    ym = y0;
-    y0 = u;
+    if (qx_own) qxout[o] = rqx_0;
+    if (EDGE && cside >= 0) uout[o] = c0.u;
+    // rotate: rows (j, j+1) become (j-1, j)
+    c0 = cp1;
+    rqx_m = rqx_0;
+    rqx_0 = qx_p1;
+    rpx_m = rpx_0;
+    rpx_0 = px_p1;
+    rqy_m = qy_0n;
+    rpy_m = py_0n;
+    const int t = s_m;
+    s_m = s_0;
+    s_0 = s_p;
+    s_p = t;
+    const int u2 = y_m;
+    y_m = y_0;
+    y_0 = u2;
   }
-  finish_iteration<TX>(P, C, tile, iter, check, local, local_nan, bad, s_red, &s_flag);
+  finish_iteration<TX>(P, C, tile, iter, check, local, local_nan, bad, sm.red, &sm.flag);
 }
 
-cudaError_t launch_march2d_fast(int variant, const Problem* probs, const int2* items, int nitems, cudaStream_t s) {
-  if (nitems <= 0) return cudaSuccess;
-  if (variant == 0) march2d_fast<128><<<nitems, 128, 0, s>>>(probs, items);
-  else march2d_fast<64><<<nitems, 64, 0, s>>>(probs, items);
+// EDGE: blocks that touch a domain boundary (ghost logic); HARM: harmonic face means
+template <int TX, bool EDGE, bool HARM>
+__global__ void __launch_bounds__(TX, EDGE ? 4 : 5) march2d_fast(const Problem* __restrict__ probs,
+                                                                 const int2* __restrict__ items) {
+  __shared__ FastSmem<TX> sm;
+  const int2 item = items[blockIdx.x];
+  const Problem& P = probs[item.x];
+  Ctrl* C = P.ctrl;
+  if (ld_cg_int(&C->done)) return;
+  const int iter = ld_cg_int(&C->iter) + 1;
+  const bool check = is_check_iter(C, iter);
+  fast_body<TX, EDGE, HARM>(P, C, item.y, iter, check, sm);
+}
+
+// Is tile `tile` of a problem free of domain-boundary logic (no ghost column,
+// no ghost row in its staged rows)?  Shared by the host item builder.
+bool march_tile_interior(int ni, int nj, int tiles_i, int strip_h, int tx, int tile) {
+  const int ow = tx - 2;
+  const int cb = tile % tiles_i, sj = tile / tiles_i;
+  const int i0 = cb * ow, j0 = sj * strip_h, j1 = (j0 + strip_h < nj) ? j0 + strip_h : nj;
+  return cb > 0 && i0 + tx - 2 < ni && j0 > 0 && j1 < nj;
+}
+
+template <int TX, bool HARM>
+static void launch_pair(const Problem* probs, const int2* items, int n_edge, int n_int, cudaStream_t s) {
+  if (n_edge > 0) march2d_fast<TX, true, HARM><<<n_edge, TX, 0, s>>>(probs, items);
+  if (n_int > 0) march2d_fast<TX, false, HARM><<<n_int, TX, 0, s>>>(probs, items + n_edge);
+}
+
+cudaError_t launch_march2d_fast(int variant, int harmonic, const Problem* probs, const int2* items, int n_edge,
+                                int n_int, cudaStream_t s) {
+  if (variant == 0) {
+    if (harmonic) launch_pair<128, true>(probs, items, n_edge, n_int, s);
+    else launch_pair<128, false>(probs, items, n_edge, n_int, s);
+  } else {
+    if (harmonic) launch_pair<64, true>(probs, items, n_edge, n_int, s);
+    else launch_pair<64, false>(probs, items, n_edge, n_int, s);
+  }
   return cudaGetLastError();
 }
 

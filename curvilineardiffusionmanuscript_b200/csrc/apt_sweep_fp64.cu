@@ -438,13 +438,15 @@ static cudaError_t launch3(const Problem* probs, const int2* items, int nitems, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_sweep_fp64(int ndim, int variant, int exact, const Problem* probs, const int2* items,
-                              int nitems, cudaStream_t s) {
+cudaError_t launch_sweep_fp64(int ndim, int variant, int exact, int harmonic, const Problem* probs,
+                              const int2* items, int nitems, int n_edge, cudaStream_t s) {
   if (nitems <= 0) return cudaSuccess;
   if (ndim == 2) {
     switch (variant) {
-      case 0: return exact ? launch_march2d_fp64(0, probs, items, nitems, s) : launch_march2d_fast(0, probs, items, nitems, s);
-      case 1: return exact ? launch_march2d_fp64(1, probs, items, nitems, s) : launch_march2d_fast(1, probs, items, nitems, s);
+      case 0:
+      case 1:
+        if (exact) return launch_march2d_fp64(variant, probs, items, nitems, s);
+        return launch_march2d_fast(variant, harmonic, probs, items, n_edge, nitems - n_edge, s);
       case 2: sweep2d_fp64<32, 16, 256><<<nitems, 256, 0, s>>>(probs, items); break;
       default: sweep2d_fp64<32, 8, 256><<<nitems, 256, 0, s>>>(probs, items); break;
     }

@@ -414,6 +414,18 @@ int Engine::build_items() {
     }
     items.swap(mixed);
   }
+  // the fast 2D kernel runs boundary tiles and interior tiles as two launches
+  n_edge = (int)items.size();
+  if (ts.march) {
+    std::vector<int2> edge, inner;
+    for (const int2& it : items) {
+      const ProbState& s = ps[it.x];
+      (march_tile_interior(s.ni, s.nj, s.tiles_i, s.strip_h, ts.tx, it.y) ? inner : edge).push_back(it);
+    }
+    n_edge = (int)edge.size();
+    items.assign(edge.begin(), edge.end());
+    items.insert(items.end(), inner.begin(), inner.end());
+  }
   dfree(d_items);
   nitems = (int)items.size();
   CDM_CK(cudaMalloc((void**)&d_items, sizeof(int2) * items.size()));
@@ -503,7 +515,7 @@ int Engine::launch_block(int K, bool use_graph) {
   if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe], stream));
   prof.sweep_launches += K;
   if (!use_graph) {
-    for (int k = 0; k < K; ++k) CDM_CK(launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT, d_probs, d_items, nitems, stream));
+    for (int k = 0; k < K; ++k) CDM_CK(launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT, mean == CDM_MEAN_HARMONIC, d_probs, d_items, nitems, n_edge, stream));
     if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe + 1], stream));
     return CDM_OK;
   }
@@ -517,7 +529,7 @@ int Engine::launch_block(int K, bool use_graph) {
     CDM_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t le = cudaSuccess;
     for (int k = 0; k < K && le == cudaSuccess; ++k)
-      le = launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT, d_probs, d_items, nitems, stream);
+      le = launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT, mean == CDM_MEAN_HARMONIC, d_probs, d_items, nitems, n_edge, stream);
     cudaError_t ce = cudaStreamEndCapture(stream, &g);
     if (le != cudaSuccess) {
       set_error(std::string("sweep launch during capture: ") + cudaGetErrorString(le));
