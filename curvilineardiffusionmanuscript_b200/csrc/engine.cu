@@ -112,6 +112,7 @@ Engine::~Engine() {
   dfree(d_ctrl);
   dfree(d_items);
   dfree(d_flags);
+  dfree(d_counters);
   dfree(d_red);
   dfree(d_redout);
   if (h_ctrl) cudaFreeHost(h_ctrl);
@@ -354,6 +355,7 @@ int Engine::init(int nprob, const cdm_mesh_desc* meshes, const cdm_bc* bcs, cons
   CDM_CK(cudaMallocHost((void**)&h_ctrl, sizeof(Ctrl) * nprob));
   std::memset(h_ctrl, 0, sizeof(Ctrl) * nprob);
   CDM_CK(dalloc(&d_flags, (size_t)nprob));
+  CDM_CK(dalloc(&d_counters, (size_t)2));
   CDM_CK(dalloc(&d_red, (size_t)4 * 1024));
   CDM_CK(dalloc(&d_redout, (size_t)8 * nprob));
   CDM_CK(cudaMallocHost((void**)&h_redout, sizeof(double) * 8 * nprob));
@@ -413,18 +415,6 @@ int Engine::build_items() {
         }
     }
     items.swap(mixed);
-  }
-  // the fast 2D kernel runs boundary tiles and interior tiles as two launches
-  n_edge = (int)items.size();
-  if (ts.march) {
-    std::vector<int2> edge, inner;
-    for (const int2& it : items) {
-      const ProbState& s = ps[it.x];
-      (march_tile_interior(s.ni, s.nj, s.tiles_i, s.strip_h, ts.tx, it.y) ? inner : edge).push_back(it);
-    }
-    n_edge = (int)edge.size();
-    items.assign(edge.begin(), edge.end());
-    items.insert(items.end(), inner.begin(), inner.end());
   }
   dfree(d_items);
   nitems = (int)items.size();
@@ -515,7 +505,7 @@ int Engine::launch_block(int K, bool use_graph) {
   if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe], stream));
   prof.sweep_launches += K;
   if (!use_graph) {
-    for (int k = 0; k < K; ++k) CDM_CK(launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT, mean == CDM_MEAN_HARMONIC, d_probs, d_items, nitems, n_edge, stream));
+    for (int k = 0; k < K; ++k) CDM_CK(launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT, mean == CDM_MEAN_HARMONIC, d_probs, d_items, nitems, d_counters, stream));
     if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe + 1], stream));
     return CDM_OK;
   }
@@ -529,7 +519,7 @@ int Engine::launch_block(int K, bool use_graph) {
     CDM_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t le = cudaSuccess;
     for (int k = 0; k < K && le == cudaSuccess; ++k)
-      le = launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT, mean == CDM_MEAN_HARMONIC, d_probs, d_items, nitems, n_edge, stream);
+      le = launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT, mean == CDM_MEAN_HARMONIC, d_probs, d_items, nitems, d_counters, stream);
     cudaError_t ce = cudaStreamEndCapture(stream, &g);
     if (le != cudaSuccess) {
       set_error(std::string("sweep launch during capture: ") + cudaGetErrorString(le));
@@ -709,6 +699,7 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
     predicted = std::min(predicted, o.check_every > 0 ? 0 : std::max(0, C.min_err_check - 1));
   }
   CDM_CK(cudaMemcpyAsync(d_probs, hp.data(), sizeof(Problem) * nprob, cudaMemcpyHostToDevice, stream));
+  CDM_CK(cudaMemsetAsync(d_counters, 0, 2 * sizeof(unsigned int), stream));
   CDM_CK(cudaMemcpyAsync(d_ctrl, h_ctrl, sizeof(Ctrl) * nprob, cudaMemcpyHostToDevice, stream));
   int rc;
   if (precision == CDM_PREC_MIXED) rc = step_mixed(&o, t0, timeout_s);

@@ -75,7 +75,7 @@ struct Engine {
   Ctrl* h_ctrl = nullptr;  // pinned mirror
   int2* d_items = nullptr;
   int nitems = 0;
-  int n_edge = 0;  // items [0, n_edge) touch a domain boundary
+  unsigned int* d_counters = nullptr;  // tile tickets of the persistent sweep
   int* d_flags = nullptr;        // per problem: source validity bits
   double* d_red = nullptr;       // reduction scratch
   double* d_redout = nullptr;    // per problem 8 doubles

@@ -57,7 +57,7 @@ def assert_parity(out, exact=True):
         assert abs(ndg - ndo) <= 1e-14 * abs(ndo), (s, ndo, ndg)
         # near convergence the residual is a difference of large terms, so its
         # last digits follow the rounding of the path (fast form: a few percent)
-        assert abs(sg["abs_err"] - so["abs_err"]) <= (1e-12 if exact else 0.1) * abs(so["abs_err"]) + 1e-300
+        assert abs(sg["abs_err"] - so["abs_err"]) <= (1e-12 if exact else 1e-3) * abs(so["abs_err"]) + 1e-300
         if exact:
             assert np.array_equal(Tg, To), (s, np.abs(Tg - To).max())
 
@@ -234,9 +234,16 @@ def test_batch_matches_individual_oracle_runs():
 
 
 # --------------------------------------------------------------- fast FP64 form
+# The fast form is compared at the workload's stopping rule (rel <= 1e-8 or
+# abs <= 1e-8), where the residual is far above round-off: an absolute 1e-8
+# alone stops within a few ulps of the FP64 floor of these problems, where the
+# iteration at which the noise dips below the threshold is not reproducible.
+FAST = dict(precision="fp64", rtol=1e-8, atol=1e-8)
+
+
 @pytest.mark.parametrize("mean", ["harmonic", "arithmetic"])
 def test_fast_gaussian_128_ten_steps(mean):
-    _, _, out = run_pair(problems.gaussian_2d(128), precision="fp64", mean=mean)
+    _, _, out = run_pair(problems.gaussian_2d(128), mean=mean, **FAST)
     assert_parity(out, exact=False)
 
 
@@ -246,7 +253,7 @@ def test_fast_gaussian_128_ten_steps(mean):
     [NeumannBC(), PeriodicBC(), NeumannBC(), NeumannBC()],
 ])
 def test_fast_boundary_conditions(bcs):
-    _, _, out = run_pair(small_case_2d(ni=29, nj=19, bcs=bcs, source=True), precision="fp64", apply_cutoff=True)
+    _, _, out = run_pair(small_case_2d(ni=29, nj=19, bcs=bcs, source=True), apply_cutoff=True, **FAST)
     assert_parity(out, exact=False)
 
 
@@ -255,7 +262,7 @@ def test_fast_no_subcycle_multi_halo():
     # exceeds the stable pseudo-step across the thin cells; both paths report NONFINITE)
     pr = small_case_2d(ni=300, nj=260, nhalo=2, kn=2.5, bcs=[DirichletBC(1.2), DirichletBC(0.8), NeumannBC(),
                                                             NeumannBC()])
-    _, _, out = run_pair(pr, precision="fp64", subcycle_conductivity=False)
+    _, _, out = run_pair(pr, subcycle_conductivity=False, **FAST)
     assert_parity(out, exact=False)
 
 
