@@ -2,17 +2,15 @@
 //
 // The same discrete iteration as apt_march2d.cu (and the reference's step!,
 // PseudoTransientSolver.jl:253-319), with the divisions of the reference's
-// expressions rewritten algebraically so that a cell needs three reciprocals
-// and a square root and a face two reciprocals, instead of 4 + 3 per face + 3
-// IEEE divisions:
+// expressions rewritten algebraically so that a cell needs three or four
+// reciprocals and a face two, instead of 4 + 3 per face + 3 IEEE divisions:
 //
-//   α⁻¹ = ρcₚ/κ,  Re = π + √(π² + (L²/Δt)·ρ·α⁻¹)            (iteration_parameters.jl:2-15)
-//   dτ = Vp·L/(αRe),  θ = L/(Vp·Re),  θ⁻¹ = (Vp/L)·Re
-//   D = Δt·κ·Re + Vp·L·ρcₚ:   Δt/(Δt + dτ) = Δt·κ·Re/D,  dτΔt/(Δt + dτ) = Vp·L·Δt·ρcₚ/D
-//   harmonic face means  ᾱ = 2/(α⁻¹ₐ + α⁻¹_b),  θ̄ = 2/S_θ with S_θ = θ⁻¹ₐ + θ⁻¹_b
-//   q ← (qθ̄ − ᾱΔu)/(1 + θ̄) = (2q − ᾱΔu·S_θ)/(S_θ + 2)                  (fluxes.jl:5-16)
+//   α⁻¹ = ρcₚ/κ,  Re = π + √(π² + (L²/Δt)·ρ·α⁻¹),  dτ = Vp·L·α⁻¹·Re⁻¹,
+//   θ = (L/Vp)·Re⁻¹,  θ⁻¹ = (Vp/L)·Re,           (iteration_parameters.jl:2-15)
+//   harmonic face means  ᾱ = 2/(α⁻¹ₐ + α⁻¹_b),  θ̄ = 2/S_θ with S_θ = θ⁻¹ₐ + θ⁻¹_b,
+//   q ← (qθ̄ − ᾱΔu)/(1 + θ̄) = (2q − ᾱΔu·S_θ)/(S_θ + 2)          (fluxes.jl:5-16)
 //   u ← (u + dτ(uⁿ/Δt − ∇·q + S))/(1 + dτ/Δt)
-//     = u·Δt/(Δt + dτ) + dτΔt/(Δt + dτ)·(uⁿ·Δt⁻¹ − ∇·q + S)              (update.jl:13-15)
+//     = u·Δt/(Δt + dτ) + dτΔt/(Δt + dτ)·(uⁿ·Δt⁻¹ − ∇·q + S)      (update.jl:13-15)
 //
 // Reciprocals come from the hardware approximation refined by two Newton–
 // Raphson steps (y ← y + y(1 − b·y)), accurate to about one ulp, and
@@ -20,16 +18,14 @@
 // operation path in the last bits only (checked against the CPU oracle at a
 // relative L2 of 1e-10 with equal iteration counts).
 //
-// Organisation: a block of TX threads owns TX-2 columns of a strip of rows and
-// marches up it (see apt_march2d.cu); each thread keeps its own column's values
-// in registers and publishes only what its neighbours read.  Ghost cells are
-// handled by per-thread and per-row source offsets, so every tile runs the same
-// code.  Blocks are persistent: the grid fills the GPU once and each block
-// claims strips from a ticket counter until the launch's strips are exhausted,
-// so the last wave is at most one strip long.  The row loop is unrolled by four
-// with four shared-memory row slots, which makes every slot index a constant.
-#include <type_traits>
-
+// Organisation (see apt_march2d.cu): a block of TX threads owns TX-2 columns
+// and marches up a strip of rows.  Each thread keeps the values of its own
+// column (u, update factors, the fluxes of its faces) in registers; only the
+// values its neighbours need go through shared memory.  Strips that touch no
+// domain boundary run a branch-free instantiation without ghost logic, in a
+// persistent launch whose blocks claim strips from a ticket counter (the last
+// wave is one strip long); boundary strips run the general instantiation in a
+// concurrent launch on a side stream.
 #include "cdm_device.cuh"
 #include "cdm_finish.cuh"
 #include "cdm_kernels.h"
@@ -51,6 +47,10 @@ __device__ __forceinline__ double rcp_nr(double b) {
   return (y0 == 0.0 || fabs(y0) == __longlong_as_double(0x7ff0000000000000ll)) ? y0 : y;
 }
 
+// general exponents go through pow() out of line, keeping its temporaries out
+// of the sweep's register budget
+__device__ __noinline__ double pow_general(double x, double n) { return pow(x, n); }
+
 __device__ __forceinline__ double pow_fast(double x, int mode, int m, int half, double n) {
   if (mode == 0) return 1.0;
   if (mode == 1) {
@@ -62,13 +62,13 @@ __device__ __forceinline__ double pow_fast(double x, int mode, int m, int half, 
     if (half) p = (m >= 1) ? p * sqrt(x) : sqrt(x);
     return p;
   }
-  return pow(x, n);
+  return pow_general(x, n);
 }
 
 template <int TX>
 struct FastSmem {
-  double U[4][TX], IA[4][TX], IT[4][TX];  // u, α⁻¹ (or α), θ⁻¹ (or θ): read by the i-1 neighbour
-  double QX[4][TX], PX[4][TX];           // new damped / undamped i+1/2 fluxes
+  double U[3][TX], IA[3][TX], IT[3][TX];  // u, α⁻¹ (or α), θ⁻¹ (or θ) for the i-1 neighbour
+  double QX[3][TX], PX[3][TX];           // new damped / undamped i+1/2 fluxes
   double QY[2][TX], PY[2][TX];           // new damped / undamped j+1/2 fluxes
   double red[TX / 32];
   int flag;
@@ -79,34 +79,11 @@ struct Cell {
   double u, ia, it, g, f;
 };
 
-struct Pre {
-  double u, ua, rho, qx, qy;
-  bool act;
-};
-
-// ghost source of one boundary side: the row/column the rule reads, or a constant
-struct SideSrc {
-  int pos;   // position along the axis read by the rule
-  bool cst;  // Dirichlet
-  bool neg;  // negative symmetry
-  double val;
-};
-
-__device__ __forceinline__ SideSrc side_src(const Problem& P, int side, int n) {
-  SideSrc s;
-  const int rule = P.rule[side];
-  const bool lo = (side & 1) == 0;
-  s.cst = rule == GR_DIRICHLET;
-  s.neg = rule == GR_NEGSYM;
-  s.val = P.val[side];
-  s.pos = rule == GR_NONE ? (lo ? -1 : n) : (rule == GR_PERIODIC ? (lo ? n - 1 : 0) : (lo ? 0 : n - 1));
-  return s;
-}
-
 }  // namespace
 
-template <int TX, bool HARM>
-__device__ __forceinline__ void strip(const Problem& P, Ctrl* C, int tile, int iter, bool check, FastSmem<TX>& sm) {
+template <int TX, bool EDGE, bool HARM>
+__device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, int iter, bool check,
+                                          FastSmem<TX>& sm) {
   constexpr int OW = TX - 2;
   const int tid = threadIdx.x;
   const int cb = tile % P.tiles_i, sj = tile / P.tiles_i;
@@ -135,59 +112,92 @@ __device__ __forceinline__ void strip(const Problem& P, Ctrl* C, int tile, int i
   const double dt = P.dt, cp = P.cp, k0 = P.k0;
   const double inv_dt = 1.0 / dt;
   const double LLdt = P.LL / dt, VpL = P.VpL, LoVp = P.L / P.Vpdtau, VpoL = P.Vpdtau / P.L;
-  const double VpLdt = VpL * dt;
   const int kmode = P.kmode, km = P.km, khalf = P.khalf;
   const double kn = P.kn;
-
-  // column of this thread: domain, ghost (i side) or outside
-  const bool colIn = a >= 0 && a < ni;
-  const bool colGhost = a == -1 || a == ni;
+  const bool colIn = EDGE ? (a >= 0 && a < ni) : true;
   const bool owner = tid >= 1 && tid <= OW && colIn;
-  const bool qx_col = a >= -1 && a <= ni - 1 && tid < TX - 1;
-  const bool qx_own = qx_col && (owner || a == -1);
+  const bool qx_col = EDGE ? (a >= -1 && a <= ni - 1 && tid < TX - 1) : (tid < TX - 1);
+  const bool qx_own = qx_col && (owner || (EDGE && a == -1));
   const int col = a + nh;
-  int src_col = col;  // column the u value is read from
-  bool col_cst = false, col_neg = false;
-  double col_val = 0.0;
-  if (colGhost) {
-    const SideSrc s = side_src(P, a < 0 ? 0 : 1, ni);
-    src_col = s.pos + nh;
-    col_cst = s.cst;
-    col_neg = s.neg;
-    col_val = s.val;
-  }
-  // ghost rows (j sides)
-  const SideSrc rlo = side_src(P, 2, nj), rhi = side_src(P, 3, nj);
 
-  auto prefetch = [&](int r, Pre& L) {
-    const int ro = col + nx * (r + nh);
-    const bool rowIn = r >= 0 && r < nj;
-    const bool rowGhost = r == -1 || r == nj;
-    L.act = (colIn && (rowIn || rowGhost)) || (colGhost && rowIn);
-    int srow = r;
-    bool cst = col_cst, neg = col_neg;
-    double cv = col_val;
-    if (rowGhost) {
-      const SideSrc& s = r < 0 ? rlo : rhi;
-      srow = s.pos;
-      cst = s.cst;
-      neg = s.neg;
-      cv = s.val;
-    }
-    const int so = src_col + nx * (srow + nh);
-    double u = cv, ua = cv;
-    if (L.act && !cst) {
-      u = uin[so];
-      ua = alpha_from_u ? u : uprev[so];
-      if (neg) {
-        u = -u;
-        ua = -ua;
+  // ghost rule of this thread's column (i sides), resolved once
+  int cside = -1, csrc_col = col;
+  bool cneg = false, cconst = false;
+  double cval = 0.0;
+  if (EDGE) {
+    if (a == -1) cside = 0;
+    else if (a == ni) cside = 1;
+    if (cside >= 0) {
+      const int rule = P.rule[cside];
+      const bool lo = cside == 0;
+      if (rule == GR_DIRICHLET) {
+        cconst = true;
+        cval = P.val[cside];
+      } else {
+        const int p = rule == GR_NONE ? (lo ? -1 : ni) : (rule == GR_PERIODIC ? (lo ? ni - 1 : 0) : (lo ? 0 : ni - 1));
+        csrc_col = p + nh;
+        cneg = rule == GR_NEGSYM;
       }
     }
-    L.u = u;
-    L.ua = ua;
-    L.rho = L.act ? rho[ro] : 1.0;
-    L.qx = (qx_col && rowIn) ? qxin[ro] : 0.0;
+  }
+
+  struct Pre {
+    double u, ua, rho, qx, qy;
+    int off;  // >= 0 source offset, -1 constant (value in u), -2 inactive
+    bool neg;
+  };
+  // issue the loads of row r (u with its ghost source, rho, old fluxes)
+  auto prefetch = [&](int r, Pre& L) {
+    const int ro = col + nx * (r + nh);
+    L.neg = false;
+    L.ua = 0.0;
+    if (!EDGE) {
+      L.off = ro;
+      L.u = uin[ro];
+      if (!alpha_from_u) L.ua = uprev[ro];
+      L.rho = rho[ro];
+      L.qx = qx_col ? qxin[ro] : 0.0;
+      L.qy = qyin[ro - nx];
+      return;
+    }
+    int off = -2;
+    double cv = 0.0;
+    const bool rIn = r >= 0 && r < nj;
+    if (rIn) {
+      if (colIn) off = ro;
+      else if (cside >= 0) {
+        if (cconst) {
+          off = -1;
+          cv = cval;
+        } else {
+          off = csrc_col + nx * (r + nh);
+          L.neg = cneg;
+        }
+      }
+    } else if (colIn && (r == -1 || r == nj)) {
+      const int side = r < 0 ? 2 : 3;
+      const int rule = P.rule[side];
+      const bool lo = side == 2;
+      if (rule == GR_DIRICHLET) {
+        off = -1;
+        cv = P.val[side];
+      } else {
+        const int p = rule == GR_NONE ? (lo ? -1 : nj) : (rule == GR_PERIODIC ? (lo ? nj - 1 : 0) : (lo ? 0 : nj - 1));
+        off = col + nx * (p + nh);
+        L.neg = rule == GR_NEGSYM;
+      }
+    }
+    L.off = off;
+    L.u = cv;
+    L.rho = 1.0;
+    if (off >= 0) {
+      L.u = uin[off];
+      if (!alpha_from_u) L.ua = uprev[off];
+    } else if (off == -1) {
+      L.ua = cv;
+    }
+    if (off != -2) L.rho = rho[ro];
+    L.qx = (qx_col && rIn) ? qxin[ro] : 0.0;
     L.qy = (colIn && r >= 0 && r <= nj) ? qyin[ro - nx] : 0.0;
   };
 
@@ -195,30 +205,32 @@ __device__ __forceinline__ void strip(const Problem& P, Ctrl* C, int tile, int i
   // diffusivity, pseudo-time parameters and update factors of cell (a, r)
   auto stage = [&](int r, const Pre& L) -> Cell {
     Cell c{0.0, 0.0, 0.0, 0.0, 0.0};
-    if (!L.act) return c;
-    const double src = alpha_from_u ? L.u : L.ua;
+    if (EDGE && L.off == -2) return c;
+    const double us = L.neg ? -L.u : L.u;
+    const double src = alpha_from_u ? us : (L.neg ? -L.ua : L.ua);
     const double kap = isfinite(src) ? k0 * pow_fast(fabs(src), kmode, km, khalf, kn) : 0.0;
     const double rc = L.rho * cp;
     const double inva = rc * rcp_nr(kap);
     const double Re = kPi + sqrt(kPi * kPi + LLdt * L.rho * inva);
-    const double kRe = dt * kap * Re;
-    const double iD = rcp_nr(kRe + VpL * rc);
-    c.u = L.u;
-    // dτ = Vp·L/(α·Re); where dτ is not finite the reference masks it to 0
-    const bool dt_ok = isfinite(VpL * inva * rcp_nr(Re));
-    c.g = dt_ok ? kRe * iD : 1.0;
-    c.f = dt_ok ? VpLdt * rc * iD : 0.0;
+    const double iRe = rcp_nr(Re);
+    double dtau = VpL * inva * iRe;
+    double th = LoVp * iRe;
+    dtau = isfinite(dtau) ? dtau : 0.0;
+    th = isfinite(th) ? th : 0.0;
+    const double id = rcp_nr(dt + dtau);
+    c.u = us;
+    c.g = dt * id;
+    c.f = dtau * dt * id;
     if (HARM) {
       c.ia = inva;
       c.it = VpoL * Re;
     } else {
-      const double th = LoVp * rcp_nr(Re);
       c.ia = kap * rcp_nr(rc);
-      c.it = isfinite(th) ? th : 0.0;
+      c.it = th;
     }
     // validity of α = κ/(ρcₚ) on owned cells and first-layer ghosts
-    const bool track = (tid >= 1 && tid <= OW) || colGhost;
-    if (track && r >= j0 - (j0 == 0) && r < j1 + (j1 == nj)) {
+    const bool track = (tid >= 1 && tid <= OW) || (EDGE && cside >= 0);
+    if (track && r >= j0 - (EDGE && j0 == 0) && r < j1 + (EDGE && j1 == nj)) {
       if (!(isfinite(kap) && isfinite(rc) && rc != 0.0)) bad |= 1;
       if (kap != 0.0 && ((kap < 0.0) != (rc < 0.0))) bad |= 2;
     }
@@ -240,45 +252,58 @@ __device__ __forceinline__ void strip(const Problem& P, Ctrl* C, int tile, int i
     qp = -an * du;
     return qn;
   };
+  // i+1/2 face of row r between this column and the next (neighbour from shared memory)
+  auto face_x = [&](int r, int s, const Cell& c, double qold, double& qp) -> double {
+    double qn = 0.0;
+    qp = 0.0;
+    if (qx_col && (!EDGE || (r >= 0 && r < nj)))
+      qn = flux(c.ia, sm.IA[s][tid + 1], c.it, sm.IT[s][tid + 1], sm.U[s][tid + 1] - c.u, qold, qp);
+    return qn;
+  };
+  // j+1/2 face between rows r and r+1 of this column (registers only)
+  auto face_y = [&](int r, const Cell& lo, const Cell& hi, double qold, double& qp) -> double {
+    double qn = 0.0;
+    qp = 0.0;
+    if (colIn && (!EDGE || (r >= -1 && r <= nj - 1))) qn = flux(lo.ia, hi.ia, lo.it, hi.it, hi.u - lo.u, qold, qp);
+    return qn;
+  };
+  auto publish = [&](int s, const Cell& c) {
+    sm.U[s][tid] = c.u;
+    sm.IA[s][tid] = c.ia;
+    sm.IT[s][tid] = c.it;
+  };
+
+  int s_m = 0, s_0 = 1, s_p = 2;  // slots of rows j-1, j, j+1
+  int y_m = 0, y_0 = 1;           // slots of face rows j-1, j
+  Pre L0, L1, Ln;
+  prefetch(j0 - 1, L0);
+  prefetch(j0, L1);
+  prefetch(j0 + 1, Ln);
+  Cell cm = stage(j0 - 1, L0);
+  Cell c0 = stage(j0, L1);
+  publish(s_m, cm);
+  publish(s_0, c0);
+  __syncthreads();
+  double px_m, px_0, py_m;
+  const double qx_m = face_x(j0 - 1, s_m, cm, L0.qx, px_m);
+  const double qx_0 = face_x(j0, s_0, c0, L1.qx, px_0);
+  const double qy_m = face_y(j0 - 1, cm, c0, L1.qy, py_m);
+  sm.QX[s_m][tid] = qx_m;
+  sm.PX[s_m][tid] = px_m;
+  sm.QX[s_0][tid] = qx_0;
+  sm.PX[s_0][tid] = px_0;
+  sm.QY[y_m][tid] = qy_m;
+  sm.PY[y_m][tid] = py_m;
+  if (EDGE && j0 == 0 && owner) {
+    qyout[col + nx * (nh - 1)] = qy_m;
+    uout[col + nx * (nh - 1)] = cm.u;  // row -1 ghost after applybcs!
+  }
+  // own-column fluxes in registers: x faces of rows j-1 and j, y face of row j-1
+  double rqx_m = qx_m, rqx_0 = qx_0, rpx_m = px_m, rpx_0 = px_0, rqy_m = qy_m, rpy_m = py_m;
 
   double local = 0.0;
   bool local_nan = false;
-
-  // prologue: rows j0-1 and j0 (slots 3 and 0), x faces of both, y face j0-1 (slot 1)
-  Pre Lm, L0, Ln;
-  prefetch(j0 - 1, Lm);
-  prefetch(j0, L0);
-  prefetch(j0 + 1, Ln);
-  const Cell cm = stage(j0 - 1, Lm);
-  Cell c0 = stage(j0, L0);
-  sm.U[3][tid] = cm.u;
-  sm.IA[3][tid] = cm.ia;
-  sm.IT[3][tid] = cm.it;
-  sm.U[0][tid] = c0.u;
-  sm.IA[0][tid] = c0.ia;
-  sm.IT[0][tid] = c0.it;
-  __syncthreads();
-  double rqx_m = 0.0, rpx_m = 0.0, rqx_0 = 0.0, rpx_0 = 0.0, rqy_m = 0.0, rpy_m = 0.0;
-  if (qx_col && j0 - 1 >= 0)
-    rqx_m = flux(cm.ia, sm.IA[3][tid + 1], cm.it, sm.IT[3][tid + 1], sm.U[3][tid + 1] - cm.u, Lm.qx, rpx_m);
-  if (qx_col)
-    rqx_0 = flux(c0.ia, sm.IA[0][tid + 1], c0.it, sm.IT[0][tid + 1], sm.U[0][tid + 1] - c0.u, L0.qx, rpx_0);
-  if (colIn) rqy_m = flux(cm.ia, c0.ia, cm.it, c0.it, c0.u - cm.u, L0.qy, rpy_m);
-  sm.QX[3][tid] = rqx_m;
-  sm.PX[3][tid] = rpx_m;
-  sm.QX[0][tid] = rqx_0;
-  sm.PX[0][tid] = rpx_0;
-  sm.QY[1][tid] = rqy_m;
-  sm.PY[1][tid] = rpy_m;
-  if (j0 == 0 && owner) {
-    qyout[col + nx * (nh - 1)] = rqy_m;
-    uout[col + nx * (nh - 1)] = cm.u;  // row -1 ghost after applybcs!
-  }
-
-  // one output row j with constant slots: SM, S0, SP rows j-1, j, j+1; YM, Y0 face rows j-1, j
-  auto row = [&](int j, auto SMc, auto S0c, auto SPc, auto YMc, auto Y0c) {
-    constexpr int SMi = decltype(SMc)::value, S0i = decltype(S0c)::value, SPi = decltype(SPc)::value;
-    constexpr int YMi = decltype(YMc)::value, Y0i = decltype(Y0c)::value;
+  for (int j = j0; j < j1; ++j) {
     const Pre Lc = Ln;
     if (j + 1 < j1) prefetch(j + 2, Ln);
     const int o = col + nx * (j + nh);
@@ -293,34 +318,30 @@ __device__ __forceinline__ void strip(const Problem& P, Ctrl* C, int tile, int i
       S = Sg[o];
     }
     const Cell cp1 = stage(j + 1, Lc);
-    sm.U[SPi][tid] = cp1.u;
-    sm.IA[SPi][tid] = cp1.ia;
-    sm.IT[SPi][tid] = cp1.it;
+    publish(s_p, cp1);
     __syncthreads();
-    double px_p1 = 0.0, py_0n = 0.0, qx_p1 = 0.0, qy_0n = 0.0;
-    if (qx_col && j + 1 < nj)
-      qx_p1 = flux(cp1.ia, sm.IA[SPi][tid + 1], cp1.it, sm.IT[SPi][tid + 1], sm.U[SPi][tid + 1] - cp1.u, Lc.qx,
-                   px_p1);
-    if (colIn) qy_0n = flux(c0.ia, cp1.ia, c0.it, cp1.it, cp1.u - c0.u, Lc.qy, py_0n);
-    sm.QX[SPi][tid] = qx_p1;
-    sm.PX[SPi][tid] = px_p1;
-    sm.QY[Y0i][tid] = qy_0n;
-    sm.PY[Y0i][tid] = py_0n;
+    double px_p1, py_0n;
+    const double qx_p1 = face_x(j + 1, s_p, cp1, Lc.qx, px_p1);
+    const double qy_0n = face_y(j, c0, cp1, Lc.qy, py_0n);
+    sm.QX[s_p][tid] = qx_p1;
+    sm.PX[s_p][tid] = px_p1;
+    sm.QY[y_0][tid] = qy_0n;
+    sm.PY[y_0][tid] = py_0n;
     __syncthreads();
     if (owner) {
       const int x = tid;
-      const double dq = g11 * (rqx_0 - sm.QX[S0i][x - 1]) + g22 * (qy_0n - rqy_m) +
-                        c12 * ((qx_p1 + sm.QX[SPi][x - 1]) - (rqx_m + sm.QX[SMi][x - 1])) +
-                        c12 * ((sm.QY[Y0i][x + 1] + sm.QY[YMi][x + 1]) - (sm.QY[Y0i][x - 1] + sm.QY[YMi][x - 1])) +
-                        ca * (0.5 * (rqx_0 + sm.QX[S0i][x - 1])) + cbv * (0.5 * (qy_0n + rqy_m));
+      const double dq = g11 * (rqx_0 - sm.QX[s_0][x - 1]) + g22 * (qy_0n - rqy_m) +
+                        c12 * ((qx_p1 + sm.QX[s_p][x - 1]) - (rqx_m + sm.QX[s_m][x - 1])) +
+                        c12 * ((sm.QY[y_0][x + 1] + sm.QY[y_m][x + 1]) - (sm.QY[y_0][x - 1] + sm.QY[y_m][x - 1])) +
+                        ca * (0.5 * (rqx_0 + sm.QX[s_0][x - 1])) + cbv * (0.5 * (qy_0n + rqy_m));
       const double un = c0.g * c0.u + c0.f * (up * inv_dt - dq + S);
       uout[o] = un;
       qyout[o] = qy_0n;
       if (check) {
-        const double dqp = g11 * (rpx_0 - sm.PX[S0i][x - 1]) + g22 * (py_0n - rpy_m) +
-                           c12 * ((px_p1 + sm.PX[SPi][x - 1]) - (rpx_m + sm.PX[SMi][x - 1])) +
-                           c12 * ((sm.PY[Y0i][x + 1] + sm.PY[YMi][x + 1]) - (sm.PY[Y0i][x - 1] + sm.PY[YMi][x - 1])) +
-                           ca * (0.5 * (rpx_0 + sm.PX[S0i][x - 1])) + cbv * (0.5 * (py_0n + rpy_m));
+        const double dqp = g11 * (rpx_0 - sm.PX[s_0][x - 1]) + g22 * (py_0n - rpy_m) +
+                           c12 * ((px_p1 + sm.PX[s_p][x - 1]) - (rpx_m + sm.PX[s_m][x - 1])) +
+                           c12 * ((sm.PY[y_0][x + 1] + sm.PY[y_m][x + 1]) - (sm.PY[y_0][x - 1] + sm.PY[y_m][x - 1])) +
+                           ca * (0.5 * (rpx_0 + sm.PX[s_0][x - 1])) + cbv * (0.5 * (py_0n + rpy_m));
         double du = un - up;
         if (isapprox_eps(un, up)) du = 0.0;
         const double r = -du * inv_dt - dqp + S;
@@ -331,10 +352,11 @@ __device__ __forceinline__ void strip(const Problem& P, Ctrl* C, int tile, int i
           else local = fmax(local, ar);
         }
       }
-      if (j == nj - 1) uout[o + nx] = cp1.u;
+      if (EDGE && j == nj - 1) uout[o + nx] = cp1.u;
     }
     if (qx_own) qxout[o] = rqx_0;
-    if (colGhost) uout[o] = c0.u;
+    if (EDGE && cside >= 0) uout[o] = c0.u;
+    // rotate: rows (j, j+1) become (j-1, j)
     c0 = cp1;
     rqx_m = rqx_0;
     rqx_0 = qx_p1;
@@ -342,32 +364,37 @@ __device__ __forceinline__ void strip(const Problem& P, Ctrl* C, int tile, int i
     rpx_0 = px_p1;
     rqy_m = qy_0n;
     rpy_m = py_0n;
-  };
-  using I0 = std::integral_constant<int, 0>;
-  using I1 = std::integral_constant<int, 1>;
-  using I2 = std::integral_constant<int, 2>;
-  using I3 = std::integral_constant<int, 3>;
-  // row j0 + k uses slots ((k+3)&3, k&3, (k+1)&3) and face slots ((k+1)&1, k&1)
-  int j = j0;
-  for (; j + 4 <= j1; j += 4) {
-    row(j, I3{}, I0{}, I1{}, I1{}, I0{});
-    row(j + 1, I0{}, I1{}, I2{}, I0{}, I1{});
-    row(j + 2, I1{}, I2{}, I3{}, I1{}, I0{});
-    row(j + 3, I2{}, I3{}, I0{}, I0{}, I1{});
+    const int t = s_m;
+    s_m = s_0;
+    s_0 = s_p;
+    s_p = t;
+    const int u2 = y_m;
+    y_m = y_0;
+    y_0 = u2;
   }
-  const int rem = j1 - j;
-  if (rem > 0) row(j, I3{}, I0{}, I1{}, I1{}, I0{});
-  if (rem > 1) row(j + 1, I0{}, I1{}, I2{}, I0{}, I1{});
-  if (rem > 2) row(j + 2, I1{}, I2{}, I3{}, I1{}, I0{});
   finish_iteration<TX>(P, C, tile, iter, check, local, local_nan, bad, sm.red, &sm.flag);
 }
 
-// Persistent launch: blocks claim items from counters[0] until `nitems` are
-// taken; the last block to leave resets the counters for the next launch.
+// Boundary strips: one block per strip.
 template <int TX, bool HARM>
-__global__ void __launch_bounds__(TX, 4) march2d_fast(const Problem* __restrict__ probs,
-                                                      const int2* __restrict__ items, int nitems,
-                                                      unsigned int* counters) {
+__global__ void __launch_bounds__(TX, 4) march2d_fast_edge(const Problem* __restrict__ probs,
+                                                           const int2* __restrict__ items) {
+  __shared__ FastSmem<TX> sm;
+  const int2 item = items[blockIdx.x];
+  const Problem& P = probs[item.x];
+  Ctrl* C = P.ctrl;
+  if (ld_cg_int(&C->done)) return;
+  const int iter = ld_cg_int(&C->iter) + 1;
+  const bool check = is_check_iter(C, iter);
+  fast_body<TX, true, HARM>(P, C, item.y, iter, check, sm);
+}
+
+// Interior strips: persistent blocks claim strips from counters[0] until
+// `nitems` are taken; the last block to leave resets the counters.
+template <int TX, bool HARM>
+__global__ void __launch_bounds__(TX, 5) march2d_fast_inner(const Problem* __restrict__ probs,
+                                                            const int2* __restrict__ items, int nitems,
+                                                            unsigned int* counters) {
   __shared__ FastSmem<TX> sm;
   while (true) {
     if (threadIdx.x == 0) sm.ticket = (int)atomicAdd(&counters[0], 1u);
@@ -381,7 +408,7 @@ __global__ void __launch_bounds__(TX, 4) march2d_fast(const Problem* __restrict_
     if (ld_cg_int(&C->done)) continue;
     const int iter = ld_cg_int(&C->iter) + 1;
     const bool check = is_check_iter(C, iter);
-    strip<TX, HARM>(P, C, item.y, iter, check, sm);
+    fast_body<TX, false, HARM>(P, C, item.y, iter, check, sm);
     __syncthreads();
   }
   if (threadIdx.x == 0) {
@@ -395,34 +422,56 @@ __global__ void __launch_bounds__(TX, 4) march2d_fast(const Problem* __restrict_
   }
 }
 
-template <int TX>
-static int fast_grid(int nitems) {
-  static int per_sm = -1;
-  static int nsm = 0;
+// Is tile `tile` of a problem free of domain-boundary logic (no ghost column,
+// no ghost row in its staged rows)?  Used by the host item builder.
+bool march_tile_interior(int ni, int nj, int tiles_i, int strip_h, int tx, int tile) {
+  const int ow = tx - 2;
+  const int cb = tile % tiles_i, sj = tile / tiles_i;
+  const int i0 = cb * ow, j0 = sj * strip_h, j1 = (j0 + strip_h < nj) ? j0 + strip_h : nj;
+  return cb > 0 && i0 + tx - 2 < ni && j0 > 0 && j1 < nj;
+}
+
+template <int TX, bool HARM>
+static int inner_grid(int nitems) {
+  static int per_sm = -1, nsm = 0;
   if (per_sm < 0) {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, march2d_fast<TX, true>, TX, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, march2d_fast_inner<TX, HARM>, TX, 0);
     if (per_sm < 1) per_sm = 1;
   }
   const int g = nsm * per_sm;
   return nitems < g ? nitems : g;
 }
 
-cudaError_t launch_march2d_fast(int variant, int harmonic, const Problem* probs, const int2* items, int nitems,
-                                unsigned int* counters, cudaStream_t s) {
-  if (nitems <= 0) return cudaSuccess;
-  if (variant == 0) {
-    const int g = fast_grid<128>(nitems);
-    if (harmonic) march2d_fast<128, true><<<g, 128, 0, s>>>(probs, items, nitems, counters);
-    else march2d_fast<128, false><<<g, 128, 0, s>>>(probs, items, nitems, counters);
-  } else {
-    const int g = fast_grid<64>(nitems);
-    if (harmonic) march2d_fast<64, true><<<g, 64, 0, s>>>(probs, items, nitems, counters);
-    else march2d_fast<64, false><<<g, 64, 0, s>>>(probs, items, nitems, counters);
+template <int TX, bool HARM>
+static cudaError_t launch_pair(const Problem* probs, const int2* items, int n_edge, int n_int,
+                               unsigned int* counters, const SweepStreams& ss) {
+  const bool fork = n_edge > 0 && n_int > 0 && ss.side != nullptr;
+  cudaError_t e = cudaSuccess;
+  if (fork) {
+    if ((e = cudaEventRecord(ss.ev_fork, ss.main)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(ss.side, ss.ev_fork, 0)) != cudaSuccess) return e;
+  }
+  if (n_edge > 0) march2d_fast_edge<TX, HARM><<<n_edge, TX, 0, fork ? ss.side : ss.main>>>(probs, items);
+  if (n_int > 0)
+    march2d_fast_inner<TX, HARM><<<inner_grid<TX, HARM>(n_int), TX, 0, ss.main>>>(probs, items + n_edge, n_int,
+                                                                                   counters);
+  if (fork) {
+    if ((e = cudaEventRecord(ss.ev_join, ss.side)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(ss.main, ss.ev_join, 0)) != cudaSuccess) return e;
   }
   return cudaGetLastError();
+}
+
+cudaError_t launch_march2d_fast(int variant, int harmonic, const Problem* probs, const int2* items, int n_edge,
+                                int n_int, unsigned int* counters, const SweepStreams& ss) {
+  if (variant == 0)
+    return harmonic ? launch_pair<128, true>(probs, items, n_edge, n_int, counters, ss)
+                    : launch_pair<128, false>(probs, items, n_edge, n_int, counters, ss);
+  return harmonic ? launch_pair<64, true>(probs, items, n_edge, n_int, counters, ss)
+                  : launch_pair<64, false>(probs, items, n_edge, n_int, counters, ss);
 }
 
 }  // namespace cdm

@@ -439,14 +439,16 @@ static cudaError_t launch3(const Problem* probs, const int2* items, int nitems, 
 }
 
 cudaError_t launch_sweep_fp64(int ndim, int variant, int exact, int harmonic, const Problem* probs,
-                              const int2* items, int nitems, unsigned int* counters, cudaStream_t s) {
+                              const int2* items, int nitems, int n_edge, unsigned int* counters,
+                              const SweepStreams& ss) {
   if (nitems <= 0) return cudaSuccess;
+  cudaStream_t s = ss.main;
   if (ndim == 2) {
     switch (variant) {
       case 0:
       case 1:
         if (exact) return launch_march2d_fp64(variant, probs, items, nitems, s);
-        return launch_march2d_fast(variant, harmonic, probs, items, nitems, counters, s);
+        return launch_march2d_fast(variant, harmonic, probs, items, n_edge, nitems - n_edge, counters, ss);
       case 2: sweep2d_fp64<32, 16, 256><<<nitems, 256, 0, s>>>(probs, items); break;
       default: sweep2d_fp64<32, 8, 256><<<nitems, 256, 0, s>>>(probs, items); break;
     }

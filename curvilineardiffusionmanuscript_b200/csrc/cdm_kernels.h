@@ -17,15 +17,26 @@ int num_tile_shapes(int ndim);
 TileShape tile_shape(int ndim, int variant);
 
 cudaError_t launch_march2d_fp64(int variant, const Problem* probs, const int2* items, int nitems, cudaStream_t s);
-// fast 2D kernel: persistent blocks claim items through counters[0..1] (zero between launches)
-cudaError_t launch_march2d_fast(int variant, int harmonic, const Problem* probs, const int2* items, int nitems,
-                                unsigned int* counters, cudaStream_t s);
+// streams of a sweep launch: boundary strips may run on `side`, concurrently
+// with the interior strips on `main` (fork/join through the two events)
+struct SweepStreams {
+  cudaStream_t main;
+  cudaStream_t side;
+  cudaEvent_t ev_fork, ev_join;
+};
+
+// fast 2D kernel: items[0, n_edge) are boundary strips, items[n_edge, n_edge + n_int)
+// interior strips claimed by persistent blocks through counters[0..1] (zero between launches)
+cudaError_t launch_march2d_fast(int variant, int harmonic, const Problem* probs, const int2* items, int n_edge,
+                                int n_int, unsigned int* counters, const SweepStreams& ss);
+bool march_tile_interior(int ni, int nj, int tiles_i, int strip_h, int tx, int tile);
 
 // one fused FP64 pseudo-iteration over all items (problem, tile)
 // exact = 1: operation-for-operation reference arithmetic (bit-identical to the
 // CPU restatement); exact = 0: reciprocal form (last-bit differences)
 cudaError_t launch_sweep_fp64(int ndim, int variant, int exact, int harmonic, const Problem* probs,
-                              const int2* items, int nitems, unsigned int* counters, cudaStream_t s);
+                              const int2* items, int nitems, int n_edge, unsigned int* counters,
+                              const SweepStreams& ss);
 
 // metric cache (mesh_metric_cache.jl:39-250) and the packed divergence
 // coefficients derived from the cell-centre metrics and the cache

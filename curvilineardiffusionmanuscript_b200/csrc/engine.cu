@@ -119,6 +119,9 @@ Engine::~Engine() {
   if (h_redout) cudaFreeHost(h_redout);
   if (ev) cudaEventDestroy(ev);
   for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+  if (ev_fork) cudaEventDestroy(ev_fork);
+  if (ev_join) cudaEventDestroy(ev_join);
+  if (side_stream) cudaStreamDestroy(side_stream);
   if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -168,6 +171,9 @@ int Engine::init(int nprob, const cdm_mesh_desc* meshes, const cdm_bc* bcs, cons
     own_stream = true;
   }
   CDM_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  CDM_CK(cudaStreamCreateWithFlags(&side_stream, cudaStreamNonBlocking));
+  CDM_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+  CDM_CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
   ndim = meshes[0].ndim;
   if (ndim != 2 && ndim != 3) {
     set_error("ndim must be 2 or 3");
@@ -416,6 +422,18 @@ int Engine::build_items() {
     }
     items.swap(mixed);
   }
+  // the fast 2D kernel runs boundary strips and interior strips as two launches
+  n_edge = (int)items.size();
+  if (ts.march && precision != CDM_PREC_FP64_EXACT) {
+    std::vector<int2> edge, inner;
+    for (const int2& it : items) {
+      const ProbState& s = ps[it.x];
+      (march_tile_interior(s.ni, s.nj, s.tiles_i, s.strip_h, ts.tx, it.y) ? inner : edge).push_back(it);
+    }
+    n_edge = (int)edge.size();
+    items.assign(edge.begin(), edge.end());
+    items.insert(items.end(), inner.begin(), inner.end());
+  }
   dfree(d_items);
   nitems = (int)items.size();
   CDM_CK(cudaMalloc((void**)&d_items, sizeof(int2) * items.size()));
@@ -477,6 +495,15 @@ int Engine::wait_stream(double timeout_s) {
   }
 }
 
+SweepStreams Engine::sweep_streams() const {
+  SweepStreams ss;
+  ss.main = stream;
+  ss.side = side_stream;
+  ss.ev_fork = ev_fork;
+  ss.ev_join = ev_join;
+  return ss;
+}
+
 int Engine::record_pair() {
   if (ev_used + 2 > (int)ev_pool.size()) {
     for (int k = 0; k < 64; ++k) {
@@ -505,7 +532,7 @@ int Engine::launch_block(int K, bool use_graph) {
   if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe], stream));
   prof.sweep_launches += K;
   if (!use_graph) {
-    for (int k = 0; k < K; ++k) CDM_CK(launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT, mean == CDM_MEAN_HARMONIC, d_probs, d_items, nitems, d_counters, stream));
+    for (int k = 0; k < K; ++k) CDM_CK(launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT, mean == CDM_MEAN_HARMONIC, d_probs, d_items, nitems, n_edge, d_counters, sweep_streams()));
     if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe + 1], stream));
     return CDM_OK;
   }
@@ -519,7 +546,7 @@ int Engine::launch_block(int K, bool use_graph) {
     CDM_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t le = cudaSuccess;
     for (int k = 0; k < K && le == cudaSuccess; ++k)
-      le = launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT, mean == CDM_MEAN_HARMONIC, d_probs, d_items, nitems, d_counters, stream);
+      le = launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT, mean == CDM_MEAN_HARMONIC, d_probs, d_items, nitems, n_edge, d_counters, sweep_streams());
     cudaError_t ce = cudaStreamEndCapture(stream, &g);
     if (le != cudaSuccess) {
       set_error(std::string("sweep launch during capture: ") + cudaGetErrorString(le));

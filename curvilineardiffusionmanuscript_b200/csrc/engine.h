@@ -76,6 +76,10 @@ struct Engine {
   int2* d_items = nullptr;
   int nitems = 0;
   unsigned int* d_counters = nullptr;  // tile tickets of the persistent sweep
+  int n_edge = 0;                      // items [0, n_edge) touch a domain boundary
+  cudaStream_t side_stream = nullptr;  // boundary strips run here, concurrently
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  SweepStreams sweep_streams() const;
   int* d_flags = nullptr;        // per problem: source validity bits
   double* d_red = nullptr;       // reduction scratch
   double* d_redout = nullptr;    // per problem 8 doubles
