@@ -1,16 +1,634 @@
-// apt_mixed.cu — FP32 correction sweeps with FP64 residual and defect-correction restarts.
+// apt_mixed.cu — FP32 correction sweeps with FP64 residual and defect-correction
+// restarts (2D).
+//
+// The pseudo-transient iteration of step! (PseudoTransientSolver.jl:253-319)
+// is run in increment form around an FP64 base state u_b:
+//
+//   u = u_b + δ,   q = q′(u_b) + e,                       δ, e in FP32
+//   e ← (e·θ̄ + Δq′)/(1 + θ̄),  Δq′ = q′(u) − q′(u_b) = −(ᾱ·Δδ + Δᾱ·Δu_b)   (fluxes.jl:5-16)
+//   δ ← δ + dτΔt/(Δt + dτ)·(R_b − δ/Δt − ∇·e)                              (update.jl:13-15)
+//
+// with R_b = −(u_b − uⁿ)/Δt − ∇·q′(u_b) + S the FP64 residual of the base
+// (residuals.jl:24-47), rounded to FP32.  Every term an FP32 sweep evaluates
+// is proportional to the correction, so its rounding error is relative to the
+// correction and not to u: the increments of the diffusivity use
+// Δα = α_b((1 + δ/u_b)ⁿ − 1) and the exact increment of the harmonic mean,
+//   H(a+Δa, b+Δb) − H(a, b) = 2(b²Δa + a²Δb + ΔaΔb(a+b)) / ((a+b)(a+b+Δa+Δb)).
+// The pseudo-time parameters (θ, dτ) only set the path of the iteration and
+// are computed from u in FP32.
+//
+// A restart folds δ into u_b in FP64, recomputes R_b and its max-norm on the
+// device (the convergence check of :280-318, evaluated in FP64), and clears δ
+// and e.  An inner cycle ends when the FP32 correction residual has dropped to
+// a fraction of max|R_b| (FP32 resolves about 1e-6 of it) or below the
+// stopping tolerance.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "cdm_device.cuh"
+#include "cdm_finish.cuh"
 #include "engine.h"
 
 namespace cdm {
 
-int Engine::mixed_alloc() {
-  set_error("mixed precision is not available in this build");
-  return CDM_BAD_INPUT;
+namespace {
+
+__device__ __forceinline__ int off2m(const Problem& P, int a, int b) { return (a + P.nh) + P.nx * (b + P.nh); }
+
+// ghost source (offset) of cell (a, b) for the side rules; -1 constant, -2 inactive
+__device__ __forceinline__ int ghost_src(const Problem& P, int a, int b, bool& cst, bool& neg, double& val) {
+  cst = false;
+  neg = false;
+  val = 0.0;
+  const bool ca = a >= 0 && a < P.ni, cb = b >= 0 && b < P.nj;
+  if (ca && cb) return off2m(P, a, b);
+  int side;
+  if (cb && (a == -1 || a == P.ni)) side = a < 0 ? 0 : 1;
+  else if (ca && (b == -1 || b == P.nj)) side = b < 0 ? 2 : 3;
+  else return -2;
+  const int rule = P.rule[side];
+  const bool lo = (side & 1) == 0;
+  const int n = side < 2 ? P.ni : P.nj;
+  if (rule == GR_DIRICHLET) {
+    cst = true;
+    val = P.val[side];
+    return -1;
+  }
+  const int p = rule == GR_NONE ? (lo ? -1 : n) : (rule == GR_PERIODIC ? (lo ? n - 1 : 0) : (lo ? 0 : n - 1));
+  neg = rule == GR_NEGSYM;
+  return side < 2 ? off2m(P, p, b) : off2m(P, a, p);
 }
 
-int Engine::step_mixed(const cdm_step_opts*, double, double) {
-  set_error("mixed precision is not available in this build");
-  return CDM_BAD_INPUT;
+__device__ __forceinline__ double pow_m64(double x, int mode, int m, int half, double n) {
+  if (mode == 0) return 1.0;
+  if (mode == 1) {
+    double p = 1.0;
+    if (m >= 1) {
+      p = x;
+      for (int e = 1; e < m; ++e) p *= x;
+    }
+    if (half) p = (m >= 1) ? p * sqrt(x) : sqrt(x);
+    return p;
+  }
+  return pow(x, n);
+}
+
+__device__ __forceinline__ float pow_m32(float x, int mode, int m, int half, float n) {
+  if (mode == 0) return 1.0f;
+  if (mode == 1) {
+    float p = 1.0f;
+    if (m >= 1) {
+      p = x;
+      for (int e = 1; e < m; ++e) p *= x;
+    }
+    if (half) p = (m >= 1) ? p * sqrtf(x) : sqrtf(x);
+    return p;
+  }
+  return powf(x, n);
+}
+
+// max-norm reduction of a block, last block of the launch publishes the result
+template <int NT>
+__device__ void reduce_and_publish(const Problem& P, Ctrl* C, int tile, double local, bool nan, double* s_red,
+                                   int* s_flag, bool restart) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int anynan = __syncthreads_or(nan ? 1 : 0);
+  double v = local;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if (lane == 0) s_red[warp] = v;
+  __syncthreads();
+  if (tid == 0) {
+    double r = s_red[0];
+    for (int w = 1; w < NT / 32; ++w) r = fmax(r, s_red[w]);
+    if (anynan) r = __longlong_as_double(0x7ff8000000000000ll);
+    P.partial[tile] = r;
+    __threadfence();
+    const unsigned prev = atomicAdd(&C->arrive, 1u);
+    *s_flag = (prev == (unsigned)P.ntiles - 1u);
+  }
+  __syncthreads();
+  if (!*s_flag) return;
+  __threadfence();
+  double m = 0.0;
+  bool bad = false;
+  for (int t = tid; t < P.ntiles; t += NT) {
+    const double w = ld_cg_double(&P.partial[t]);
+    if (w != w) bad = true;
+    else m = fmax(m, w);
+  }
+  const int anybad = __syncthreads_or(bad ? 1 : 0);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) s_red[warp] = m;
+  __syncthreads();
+  if (tid == 0) {
+    for (int w = 1; w < NT / 32; ++w) m = fmax(m, s_red[w]);
+    if (anybad) m = __longlong_as_double(0x7ff8000000000000ll);
+    C->arrive = 0u;
+    if (restart) {
+      C->restart_L2 = m;
+      C->restart_nan = anybad;
+    } else {
+      C->inner_L2 = m;
+      if (!(m > C->inner_target) || anybad) C->inner_done = 1;  // NaN ends the cycle too
+    }
+    __threadfence();
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// FP64 restart: u = u_b + δ on the domain, ghosts by the side rules, the FP64
+// residual R(u) with the undamped fluxes (residuals.jl:24-47), its max-norm,
+// and the FP32 copies the sweeps read.  One block per 32x16 tile.
+constexpr int RTX = 32, RTY = 16, RNT = 256;
+
+__global__ void __launch_bounds__(RNT) mixed_restart2d(const Problem* __restrict__ probs, const double* __restrict__ ub_in,
+                                                       const float* __restrict__ d_in, double* __restrict__ ub_out,
+                                                       float* __restrict__ ub32, float* __restrict__ R32) {
+  constexpr int RX = RTX + 2, RY = RTY + 2;
+  __shared__ double s_u[RY][RX], s_a[RY][RX];
+  __shared__ double s_qx[RY][RTX + 1], s_qy[RTY + 1][RX];
+  __shared__ double s_red[RNT / 32];
+  __shared__ int s_flag;
+  const Problem& P = probs[0];
+  Ctrl* C = P.ctrl;
+  const int tile = blockIdx.x;
+  const int ti = tile % P.tiles_j, tj = tile / P.tiles_j;  // restart tiling: tiles_j columns of RTX
+  const int i0 = ti * RTX, j0 = tj * RTY;
+  const int tid = threadIdx.x;
+  const int ni = P.ni, nj = P.nj;
+  const double dt = P.dt;
+  for (int r = tid; r < RX * RY; r += RNT) {
+    const int rb = r / RX, ra = r - rb * RX;
+    const int a = i0 - 1 + ra, b = j0 - 1 + rb;
+    bool cst, neg;
+    double val;
+    const int so = ghost_src(P, a, b, cst, neg, val);
+    double u = 0.0, al = 0.0;
+    if (so != -2) {
+      if (cst) u = val;
+      else {
+        u = ub_in[so] + (d_in ? (double)d_in[so] : 0.0);
+        if (neg) u = -u;
+      }
+      const double rh = P.rho[off2m(P, a, b)];
+      const double kap = isfinite(u) ? P.k0 * pow_m64(fabs(u), P.kmode, P.km, P.khalf, P.kn) : 0.0;
+      al = kap / (rh * P.cp);
+      // the new base state, ghosts included (copy!(T, u) returns them)
+      const bool own = (ra >= 1 && ra <= RTX && rb >= 1 && rb <= RTY) ||
+                       ((a == -1 || a == ni) && rb >= 1 && rb <= RTY) || ((b == -1 || b == nj) && ra >= 1 && ra <= RTX);
+      if (own) {
+        const int o = off2m(P, a, b);
+        ub_out[o] = u;
+        ub32[o] = (float)u;
+      }
+    }
+    s_u[rb][ra] = u;
+    s_a[rb][ra] = al;
+  }
+  __syncthreads();
+  for (int f = tid; f < RY * (RTX + 1); f += RNT) {
+    const int fb = f / (RTX + 1), fa = f - fb * (RTX + 1);
+    const int a = i0 - 1 + fa, b = j0 - 1 + fb;
+    double q = 0.0;
+    if (a >= -1 && a <= ni - 1 && b >= 0 && b <= nj - 1)
+      q = -face_mean(P.mean, s_a[fb][fa], s_a[fb][fa + 1]) * (s_u[fb][fa + 1] - s_u[fb][fa]);
+    s_qx[fb][fa] = q;
+  }
+  for (int f = tid; f < (RTY + 1) * RX; f += RNT) {
+    const int fb = f / RX, fa = f - fb * RX;
+    const int a = i0 - 1 + fa, b = j0 - 1 + fb;
+    double q = 0.0;
+    if (a >= 0 && a <= ni - 1 && b >= -1 && b <= nj - 1)
+      q = -face_mean(P.mean, s_a[fb][fa], s_a[fb + 1][fa]) * (s_u[fb + 1][fa] - s_u[fb][fa]);
+    s_qy[fb][fa] = q;
+  }
+  __syncthreads();
+  double local = 0.0;
+  bool nan = false;
+  for (int e = tid; e < RTX * RTY; e += RNT) {
+    const int cb = e / RTX, ca = e - cb * RTX;
+    const int a = i0 + ca, b = j0 + cb;
+    if (a >= ni || b >= nj) continue;
+    const int o = off2m(P, a, b);
+    const int x = ca + 1, y = cb + 1;
+    const double dq = P.coef[0][o] * (s_qx[y][x] - s_qx[y][x - 1]) + P.coef[1][o] * (s_qy[y][x] - s_qy[y - 1][x]) +
+                      P.coef[2][o] * ((s_qx[y + 1][x] + s_qx[y + 1][x - 1]) - (s_qx[y - 1][x] + s_qx[y - 1][x - 1])) +
+                      P.coef[2][o] * ((s_qy[y][x + 1] + s_qy[y - 1][x + 1]) - (s_qy[y][x - 1] + s_qy[y - 1][x - 1])) +
+                      P.coef[3][o] * (0.5 * (s_qx[y][x] + s_qx[y][x - 1])) +
+                      P.coef[4][o] * (0.5 * (s_qy[y][x] + s_qy[y - 1][x]));
+    const double u = s_u[y][x], up = P.u_prev[o];
+    double du = u - up;
+    if (isapprox_eps(u, up)) du = 0.0;
+    const double r = -du / dt - dq + P.S[o];
+    R32[o] = (float)r;
+    const double ar = fabs(r);
+    if (ar != ar) nan = true;
+    else local = fmax(local, ar);
+  }
+  reduce_and_publish<RNT>(P, C, tile, local, nan, s_red, &s_flag, true);
+}
+
+// ---------------------------------------------------------------------------
+// FP32 correction sweep, row-marching (see apt_march2d_fast.cu for the layout):
+// a block of TX threads owns TX-2 columns of a strip of rows.
+template <int TX>
+struct MixSmem {
+  float D[3][TX], UB[3][TX], AB[3][TX], DA[3][TX], IT[3][TX];
+  float EX[3][TX], PX[3][TX], EY[2][TX], PY[2][TX];
+  double red[TX / 32];
+  int flag;
+};
+
+struct MCell {
+  float d, ub, ab, da, it, f;
+};
+
+template <int TX, bool HARM>
+__global__ void __launch_bounds__(TX) mixed_sweep2d(const Problem* __restrict__ probs, const int2* __restrict__ items) {
+  constexpr int OW = TX - 2;
+  __shared__ MixSmem<TX> sm;
+  const int2 item = items[blockIdx.x];
+  const Problem& P = probs[item.x];
+  Ctrl* C = P.ctrl;
+  if (ld_cg_int(&C->inner_done) || ld_cg_int(&C->done)) return;
+  const int k = ld_cg_int(&C->inner_iter) + 1;  // inner iteration of this cycle
+  const bool check = (k % C->inner_check_every) == 0;
+  const int tid = threadIdx.x;
+  const int tile = item.y;
+  const int cbk = tile % P.tiles_i, sj = tile / P.tiles_i;
+  const int ni = P.ni, nj = P.nj, nx = P.nx, nh = P.nh;
+  const int i0 = cbk * OW, a = i0 - 1 + tid;
+  const int j0 = sj * P.strip_h, j1 = min(j0 + P.strip_h, nj);
+  const float* __restrict__ din = P.d32[(k - 1) & 1];
+  float* __restrict__ dout = P.d32[k & 1];
+  const float* __restrict__ exin = P.e32[(k - 1) & 1][0];
+  const float* __restrict__ eyin = P.e32[(k - 1) & 1][1];
+  float* __restrict__ exout = P.e32[k & 1][0];
+  float* __restrict__ eyout = P.e32[k & 1][1];
+  const float* __restrict__ ub = P.ub32;
+  const float* __restrict__ Rb = P.R32;
+  const float* __restrict__ rho = P.rho32;
+  const float dt = (float)P.dt, inv_dt = (float)(1.0 / P.dt), cp = (float)P.cp, k0 = (float)P.k0;
+  const float LLdt = (float)(P.LL / P.dt), VpL = (float)P.VpL, VpoL = (float)(P.Vpdtau / P.L);
+  const float LoVp = (float)(P.L / P.Vpdtau), VpLdt = (float)(P.VpL * P.dt);
+  const float kn = (float)P.kn;
+  const int kmode = P.kmode, km = P.km, khalf = P.khalf;
+  const float pi = 3.14159265358979f;
+  const bool colIn = a >= 0 && a < ni;
+  const bool colGhost = a == -1 || a == ni;
+  const bool owner = tid >= 1 && tid <= OW && colIn;
+  const bool qx_col = a >= -1 && a <= ni - 1 && tid < TX - 1;
+  const bool qx_own = qx_col && (owner || a == -1);
+  const int col = a + nh;
+
+  // stage cell (a, r): correction with its ghost rule, base state, diffusivities
+  auto stage = [&](int r) -> MCell {
+    MCell c{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    bool cst, neg;
+    double val;
+    const int so = ghost_src(P, a, r, cst, neg, val);
+    if (so == -2) return c;
+    const int o = col + nx * (r + nh);
+    c.d = cst ? 0.f : (neg ? -din[so] : din[so]);  // Dirichlet ghosts carry no correction
+    c.ub = ub[o];                                    // ghost values of u_b written by the restart
+    const float rh = rho[o];
+    const float rc = rh * cp;
+    const float irc = __frcp_rn(rc);
+    const float u = c.ub + c.d;
+    const float kb = k0 * pow_m32(fabsf(c.ub), kmode, km, khalf, kn);
+    c.ab = kb * irc;
+    // Δα = α_b((1 + δ/u_b)ⁿ − 1), accurate relative to the increment
+    float da = 0.f;
+    if (kmode != 0) {
+      const float x = c.d * __frcp_rn(c.ub);
+      da = (fabsf(c.ub) > 1e-30f && isfinite(x)) ? c.ab * expm1f(kn * log1pf(x))
+                                                  : k0 * pow_m32(fabsf(u), kmode, km, khalf, kn) * irc - c.ab;
+    }
+    c.da = da;
+    const float al = c.ab + da;  // α(u) for the pseudo-time parameters
+    const float kap = al * rc;
+    const float Re = pi + sqrtf(pi * pi + LLdt * rh * __frcp_rn(al));
+    const float iD = __frcp_rn(dt * kap * Re + VpL * rc);
+    const float dtau = VpL * __frcp_rn(al * Re);
+    c.f = isfinite(dtau) ? VpLdt * rc * iD : 0.f;
+    if (HARM) c.it = VpoL * Re;
+    else {
+      const float th = LoVp * __frcp_rn(Re);
+      c.it = isfinite(th) ? th : 0.f;
+    }
+    return c;
+  };
+  // new flux correction of a face between cells c0 and c1
+  auto face = [&](const MCell& c0, float d1, float ub1, float ab1, float da1, float it1, float eold,
+                  float& dqp) -> float {
+    float abar, dabar, en;
+    if (HARM) {
+      const float s = c0.ab + ab1;
+      const float is = __frcp_rn(s);
+      abar = 2.f * c0.ab * ab1 * is;
+      dabar = 2.f * (ab1 * ab1 * c0.da + c0.ab * c0.ab * da1 + c0.da * da1 * s) * is * __frcp_rn(s + c0.da + da1);
+      const float St = c0.it + it1;
+      dqp = -((abar + dabar) * (d1 - c0.d) + dabar * (ub1 - c0.ub));
+      en = isfinite(St) ? (2.f * eold + dqp * St) * __frcp_rn(St + 2.f) : dqp;
+    } else {
+      abar = 0.5f * (c0.ab + ab1);
+      dabar = 0.5f * (c0.da + da1);
+      const float tn = 0.5f * (c0.it + it1);
+      dqp = -((abar + dabar) * (d1 - c0.d) + dabar * (ub1 - c0.ub));
+      en = (eold * tn + dqp) * __frcp_rn(1.f + tn);
+    }
+    return en;
+  };
+  auto publish = [&](int s, const MCell& c) {
+    sm.D[s][tid] = c.d;
+    sm.UB[s][tid] = c.ub;
+    sm.AB[s][tid] = c.ab;
+    sm.DA[s][tid] = c.da;
+    sm.IT[s][tid] = c.it;
+  };
+  auto face_x = [&](int r, int s, const MCell& c, float& dqp) -> float {
+    dqp = 0.f;
+    if (!(qx_col && r >= 0 && r < nj)) return 0.f;
+    const int o = col + nx * (r + nh);
+    return face(c, sm.D[s][tid + 1], sm.UB[s][tid + 1], sm.AB[s][tid + 1], sm.DA[s][tid + 1], sm.IT[s][tid + 1],
+                exin[o], dqp);
+  };
+  auto face_y = [&](int r, const MCell& lo, const MCell& hi, float& dqp) -> float {
+    dqp = 0.f;
+    if (!(colIn && r >= -1 && r <= nj - 1)) return 0.f;
+    const int o = col + nx * (r + nh);
+    return face(lo, hi.d, hi.ub, hi.ab, hi.da, hi.it, eyin[o], dqp);
+  };
+
+  int s_m = 0, s_0 = 1, s_p = 2, y_m = 0, y_0 = 1;
+  MCell cm = stage(j0 - 1), c0 = stage(j0);
+  publish(s_m, cm);
+  publish(s_0, c0);
+  __syncthreads();
+  float px_m, px_0, py_m;
+  float rqx_m = face_x(j0 - 1, s_m, cm, px_m);
+  float rqx_0 = face_x(j0, s_0, c0, px_0);
+  float rqy_m = face_y(j0 - 1, cm, c0, py_m);
+  sm.EX[s_m][tid] = rqx_m;
+  sm.PX[s_m][tid] = px_m;
+  sm.EX[s_0][tid] = rqx_0;
+  sm.PX[s_0][tid] = px_0;
+  sm.EY[y_m][tid] = rqy_m;
+  sm.PY[y_m][tid] = py_m;
+  if (j0 == 0 && owner) eyout[col + nx * (nh - 1)] = rqy_m;
+  float rpx_m = px_m, rpx_0 = px_0, rpy_m = py_m;
+  double local = 0.0;
+  bool nan = false;
+  for (int j = j0; j < j1; ++j) {
+    const int o = col + nx * (j + nh);
+    float g11 = 0, g22 = 0, c12 = 0, ca = 0, cbv = 0, R = 0;
+    if (owner) {
+      g11 = P.coef32[0][o];
+      g22 = P.coef32[1][o];
+      c12 = P.coef32[2][o];
+      ca = P.coef32[3][o];
+      cbv = P.coef32[4][o];
+      R = Rb[o];
+    }
+    const MCell cp1 = stage(j + 1);
+    publish(s_p, cp1);
+    __syncthreads();
+    float px_p1, py_0n;
+    const float qx_p1 = face_x(j + 1, s_p, cp1, px_p1);
+    const float qy_0n = face_y(j, c0, cp1, py_0n);
+    sm.EX[s_p][tid] = qx_p1;
+    sm.PX[s_p][tid] = px_p1;
+    sm.EY[y_0][tid] = qy_0n;
+    sm.PY[y_0][tid] = py_0n;
+    __syncthreads();
+    if (owner) {
+      const int x = tid;
+      const float dq = g11 * (rqx_0 - sm.EX[s_0][x - 1]) + g22 * (qy_0n - rqy_m) +
+                       c12 * ((qx_p1 + sm.EX[s_p][x - 1]) - (rqx_m + sm.EX[s_m][x - 1])) +
+                       c12 * ((sm.EY[y_0][x + 1] + sm.EY[y_m][x + 1]) - (sm.EY[y_0][x - 1] + sm.EY[y_m][x - 1])) +
+                       ca * (0.5f * (rqx_0 + sm.EX[s_0][x - 1])) + cbv * (0.5f * (qy_0n + rqy_m));
+      const float dn = c0.d + c0.f * (R - c0.d * inv_dt - dq);
+      dout[o] = dn;
+      eyout[o] = qy_0n;
+      if (check) {
+        const float dqp = g11 * (rpx_0 - sm.PX[s_0][x - 1]) + g22 * (py_0n - rpy_m) +
+                          c12 * ((px_p1 + sm.PX[s_p][x - 1]) - (rpx_m + sm.PX[s_m][x - 1])) +
+                          c12 * ((sm.PY[y_0][x + 1] + sm.PY[y_m][x + 1]) - (sm.PY[y_0][x - 1] + sm.PY[y_m][x - 1])) +
+                          ca * (0.5f * (rpx_0 + sm.PX[s_0][x - 1])) + cbv * (0.5f * (py_0n + rpy_m));
+        const float r = R - dn * inv_dt - dqp;
+        const float ar = fabsf(r);
+        if (ar != ar) nan = true;
+        else local = fmax(local, (double)ar);
+      }
+    }
+    if (qx_own) exout[o] = rqx_0;
+    c0 = cp1;
+    rqx_m = rqx_0;
+    rqx_0 = qx_p1;
+    rpx_m = rpx_0;
+    rpx_0 = px_p1;
+    rqy_m = qy_0n;
+    rpy_m = py_0n;
+    const int t = s_m;
+    s_m = s_0;
+    s_0 = s_p;
+    s_p = t;
+    const int u2 = y_m;
+    y_m = y_0;
+    y_0 = u2;
+  }
+  (void)cm;
+  // arrival; the last block advances the inner counters and, on check
+  // iterations, publishes max|r| and the end of the cycle
+  if (check) {
+    reduce_and_publish<TX>(P, C, tile, local, nan, sm.red, &sm.flag, false);
+    if (threadIdx.x == 0 && sm.flag) {
+      C->inner_iter = k;
+      C->iter += 1;
+      __threadfence();
+    }
+  } else {
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const unsigned prev = atomicAdd(&C->arrive, 1u);
+      if (prev == (unsigned)P.ntiles - 1u) {
+        C->arrive = 0u;
+        C->inner_iter = k;
+        C->iter += 1;
+        __threadfence();
+      }
+    }
+  }
+}
+
+// FP32 copies of the metric coefficients and of rho
+__global__ void to_f32(const double* __restrict__ src, float* __restrict__ dst, int64_t n) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+    dst[e] = (float)src[e];
+}
+
+// ---------------------------------------------------------------------------
+// host side
+int Engine::mixed_alloc() {
+  if (ndim != 2 || ps.size() != 1) {
+    set_error("mixed precision is available for single 2D problems");
+    return CDM_BAD_INPUT;
+  }
+  ProbState& s = ps[0];
+  const size_t N = (size_t)s.nfull;
+  auto fa = [&](float** p) -> cudaError_t {
+    cudaError_t e = cudaMalloc((void**)p, N * sizeof(float));
+    if (e != cudaSuccess) return e;
+    return cudaMemsetAsync(*p, 0, N * sizeof(float), stream);
+  };
+  for (int b = 0; b < 2; ++b) {
+    CDM_CK(fa(&s.d32[b]));
+    for (int d = 0; d < 2; ++d) CDM_CK(fa(&s.e32[b][d]));
+    CDM_CK(cudaMalloc((void**)&s.ub64[b], N * sizeof(double)));
+  }
+  CDM_CK(fa(&s.ub32));
+  CDM_CK(fa(&s.R32));
+  CDM_CK(fa(&s.rho32));
+  for (int k = 0; k < 5; ++k) {
+    CDM_CK(fa(&s.coef32[k]));
+    to_f32<<<1184, 256, 0, stream>>>(s.coef[k], s.coef32[k], (int64_t)N);
+    CDM_CK(cudaGetLastError());
+  }
+  return CDM_OK;
+}
+
+int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s) {
+  ProbState& s = ps[0];
+  Problem& P = hp[0];
+  const size_t N = (size_t)s.nfull;
+  // restart tiling: tiles_j column tiles x rows of RTY
+  const int rti = (s.ni + RTX - 1) / RTX, rtj = (s.nj + RTY - 1) / RTY;
+  // the FP32 sweep uses the strips of the 2D row-marching layout (variant 0)
+  to_f32<<<1184, 256, 0, stream>>>(P.rho, s.rho32, (int64_t)N);
+  CDM_CK(cudaGetLastError());
+  Ctrl& Ch = h_ctrl[0];
+  const double tolmax_abs = o->atol * Ch.sqrtN;  // abs tolerance in max|R| units
+  int restarts = 0, iters = 0;
+  double init_L2 = INFINITY, rel = 2 * o->rtol, ab = 2 * o->atol;
+  auto upload = [&]() -> int {
+    CDM_CK(cudaMemcpyAsync(d_probs, hp.data(), sizeof(Problem), cudaMemcpyHostToDevice, stream));
+    CDM_CK(cudaMemcpyAsync(d_ctrl, &Ch, sizeof(Ctrl), cudaMemcpyHostToDevice, stream));
+    return CDM_OK;
+  };
+  auto poll = [&]() -> int {
+    CDM_CK(cudaMemcpyAsync(&Ch, d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, stream));
+    return wait_stream(timeout_s - (now_seconds() - t_start));
+  };
+  // restart r: u_b(r) = u_b(r-1) + δ (δ absent for r = 0), R_b, max|R_b|
+  auto restart = [&](const float* d) -> int {
+    const double* in = restarts == 0 ? s.u[0] : s.ub64[(restarts - 1) & 1];
+    double* out = s.ub64[restarts & 1];
+    P.tiles_j = rti;
+    P.ntiles = rti * rtj;
+    int rc = upload();
+    if (rc != CDM_OK) return rc;
+    mixed_restart2d<<<rti * rtj, RNT, 0, stream>>>(d_probs, in, d, out, s.ub32, s.R32);
+    CDM_CK(cudaGetLastError());
+    prof.other_launches += 1;
+    prof.fp64_cell_evals += s.ndomain;
+    rc = poll();
+    if (rc != CDM_OK) return rc;
+    P.tiles_j = s.tiles_j;
+    P.ntiles = s.ntiles;
+    ++restarts;
+    // clear the correction and its fluxes for the next cycle
+    for (int b = 0; b < 2; ++b) {
+      CDM_CK(cudaMemsetAsync(s.d32[b], 0, N * sizeof(float), stream));
+      for (int d = 0; d < 2; ++d) CDM_CK(cudaMemsetAsync(s.e32[b][d], 0, N * sizeof(float), stream));
+    }
+    return CDM_OK;
+  };
+  // a convergence check on the FP64 residual of the current base (:284-318)
+  auto check = [&](bool first) -> int {
+    const double L2 = Ch.restart_nan ? NAN : Ch.restart_L2 / Ch.sqrtN;
+    Ch.n_checks += 1;
+    if (first) init_L2 = L2;
+    rel = L2 / init_L2;
+    ab = L2;
+    if (!std::isfinite(rel) || !std::isfinite(ab)) return ST_NONFINITE;
+    if (iters > o->max_iter) return ST_MAX_ITER;
+    if (rel <= o->rtol || ab <= o->atol) return 0;
+    return -1;  // continue
+  };
+  auto sweeps = [&](int n) -> int {
+    P.qpar = 0;
+    int rc = upload();
+    if (rc != CDM_OK) return rc;
+    int done = 0;
+    while (done < n) {
+      const int K = std::min(8, n - done);
+      const int pe = record_pair();
+      if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe], stream));
+      for (int k = 0; k < K; ++k) {
+        if (mean == CDM_MEAN_HARMONIC) mixed_sweep2d<128, true><<<nitems, 128, 0, stream>>>(d_probs, d_items);
+        else mixed_sweep2d<128, false><<<nitems, 128, 0, stream>>>(d_probs, d_items);
+        CDM_CK(cudaGetLastError());
+      }
+      if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe + 1], stream));
+      prof.sweep_launches += K;
+      done += K;
+      rc = poll();
+      if (rc != CDM_OK) return rc;
+      if (Ch.inner_done) break;
+    }
+    return CDM_OK;
+  };
+
+  Ch.iter = 0;
+  Ch.inner_iter = 0;
+  Ch.inner_done = 0;
+  Ch.inner_check_every = 4;
+  Ch.n_checks = 0;
+  int rc = restart(nullptr);
+  if (rc != CDM_OK) return rc;
+  if (Ch.restart_nan) {
+    Ch.status = ST_NONFINITE;
+    Ch.done = 1;
+    return CDM_OK;
+  }
+  int st = -1;
+  bool first = true;
+  const int cap_inner = std::max(64, std::min(o->max_iter, 4096));
+  while (st < 0) {
+    // first cycle: one sweep, so that the first check is at iteration 1 as in the reference
+    const double Rmax = Ch.restart_L2;
+    double target = 1e-4 * Rmax;
+    double floor_t = tolmax_abs;
+    if (!first && std::isfinite(init_L2)) floor_t = std::min(floor_t, o->rtol * init_L2 * Ch.sqrtN);
+    target = std::max(target, 0.25 * floor_t);
+    Ch.inner_target = target;
+    Ch.inner_done = 0;
+    Ch.inner_iter = 0;
+    const int n = first ? 1 : cap_inner;
+    rc = sweeps(n);
+    if (rc != CDM_OK) return rc;
+    iters = Ch.iter;
+    const int cur = Ch.inner_iter;
+    rc = restart(s.d32[cur & 1]);
+    if (rc != CDM_OK) return rc;
+    st = check(first);
+    first = false;
+    if (Ch.inner_iter >= cap_inner && st < 0 && iters > o->max_iter) st = ST_MAX_ITER;
+  }
+  Ch.rel = rel;
+  Ch.abs = ab;
+  Ch.status = st;
+  Ch.done = 1;
+  Ch.n_restarts = restarts;
+  Ch.iter = iters;
+  prof.fp32_cell_iters += s.ndomain * (int64_t)iters;
+  return CDM_OK;
 }
 
 }  // namespace cdm

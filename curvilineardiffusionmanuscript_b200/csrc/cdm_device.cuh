@@ -42,8 +42,13 @@ struct Ctrl {
   // mixed precision bookkeeping
   int n_restarts;
   int inner_iter;       // FP32 sweeps since the last restart
-  double restart_L2;    // FP64 residual norm at the last restart
-  double inner_L2;      // FP32 correction residual at the last inner check
+  double restart_L2;    // FP64 residual max|R| at the last restart (not normalised)
+  double inner_L2;      // FP32 correction residual max|r| at the last inner check
+  double inner_target;  // inner cycle ends when max|r| <= inner_target
+  int inner_done;       // set on the device when the inner target is met
+  int inner_check_every;
+  int restart_nan;
+  int pad2;
 };
 
 // Kernel-facing description of one problem (one mesh, one step! call).

@@ -749,7 +749,7 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
     stats[p].status = C.status;
     stats[p].n_checks = C.n_checks;
     stats[p].n_restarts = C.n_restarts;
-    s.qpar = (s.qpar + C.iter) & 1;
+    if (precision != CDM_PREC_MIXED) s.qpar = (s.qpar + C.iter) & 1;
     if (C.status != ST_OK) {
       worst = std::max(worst, C.status);
       if (C.status == ST_NONFINITE)
@@ -760,8 +760,8 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
       continue;
     }
     s.last_err_check = C.iter;
-    double* res = precision == CDM_PREC_MIXED ? s.ub64[C.iter & 1] : s.u[C.iter & 1];
-    if (precision == CDM_PREC_MIXED) res = s.ub64[C.n_restarts & 1];
+    // result: the last ping-pong iterate (FP64 path) or the last restart's base (mixed)
+    double* res = precision == CDM_PREC_MIXED ? s.ub64[(C.n_restarts - 1) & 1] : s.u[C.iter & 1];
     CDM_CK(launch_clamp(res, s.nfull, o.enforce_positivity, o.apply_cutoff, stream));
     CDM_CK(launch_step_reductions(hp[p], res, s.cellJ, o.ndt_tol, d_red, d_redout + 8 * p, stream));
     prof.other_launches += 4 + ((o.enforce_positivity || o.apply_cutoff) ? 1 : 0);
