@@ -23,6 +23,8 @@
 // a fraction of max|R_b| (FP32 resolves about 1e-6 of it) or below the
 // stopping tolerance.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -89,6 +91,30 @@ __device__ __forceinline__ float pow_m32(float x, int mode, int m, int half, flo
   return powf(x, n);
 }
 
+// (|1 + x|)ⁿ − 1, accurate relative to x for small x and defined for every x
+// (the reference's κ uses |T|ⁿ): binomial Horner form for integer n, plus
+// √(1+y) − 1 = y/(√(1+y) + 1) for the half of half-integer n, log1p/expm1 otherwise
+__device__ __forceinline__ float incr_pow(float x, int mode, int m, int half, float n) {
+  if (mode == 0) return 0.f;
+  const float y = x >= -1.f ? x : -2.f - x;
+  if (mode == 2) return expm1f(n * log1pf(y));
+  float r = 0.f;  // (1+y)^m - 1
+  if (m >= 1) {
+    float c = (float)m, p = 0.f;  // Horner over binomial coefficients C(m,k), k = m..1
+    float coef[17];
+    coef[0] = 1.f;
+    for (int k = 1; k <= m; ++k) coef[k] = coef[k - 1] * (float)(m - k + 1) / (float)k;
+    for (int k = m; k >= 1; --k) p = p * y + coef[k];
+    r = p * y;
+    (void)c;
+  }
+  if (half) {
+    const float sq = sqrtf(1.f + y);
+    r = r * sq + y / (sq + 1.f);
+  }
+  return r;
+}
+
 // max-norm reduction of a block, last block of the launch publishes the result
 template <int NT>
 __device__ void reduce_and_publish(const Problem& P, Ctrl* C, int tile, double local, bool nan, double* s_red,
@@ -147,11 +173,15 @@ __device__ void reduce_and_publish(const Problem& P, Ctrl* C, int tile, double l
 // and the FP32 copies the sweeps read.  One block per 32x16 tile.
 constexpr int RTX = 32, RTY = 16, RNT = 256;
 
+// The damped-flux memory carries over: the total damped flux q′(u_b) + e is
+// kept, so e ← e + q′(u_old) − q′(u_new) on the faces the tile owns.
 __global__ void __launch_bounds__(RNT) mixed_restart2d(const Problem* __restrict__ probs, const double* __restrict__ ub_in,
                                                        const float* __restrict__ d_in, double* __restrict__ ub_out,
-                                                       float* __restrict__ ub32, float* __restrict__ R32) {
+                                                       float* __restrict__ ub32, float* __restrict__ R32,
+                                                       const float* __restrict__ ex_in, const float* __restrict__ ey_in,
+                                                       float* __restrict__ ex_out, float* __restrict__ ey_out) {
   constexpr int RX = RTX + 2, RY = RTY + 2;
-  __shared__ double s_u[RY][RX], s_a[RY][RX];
+  __shared__ double s_u[RY][RX], s_a[RY][RX], s_uo[RY][RX], s_ao[RY][RX];
   __shared__ double s_qx[RY][RTX + 1], s_qy[RTY + 1][RX];
   __shared__ double s_red[RNT / 32];
   __shared__ int s_flag;
@@ -169,16 +199,24 @@ __global__ void __launch_bounds__(RNT) mixed_restart2d(const Problem* __restrict
     bool cst, neg;
     double val;
     const int so = ghost_src(P, a, b, cst, neg, val);
-    double u = 0.0, al = 0.0;
+    double u = 0.0, al = 0.0, uo = 0.0, alo = 0.0;
     if (so != -2) {
-      if (cst) u = val;
+      if (cst) u = uo = val;
       else {
-        u = ub_in[so] + (d_in ? (double)d_in[so] : 0.0);
-        if (neg) u = -u;
+        uo = ub_in[so];
+        u = uo + (d_in ? (double)d_in[so] : 0.0);
+        if (neg) {
+          u = -u;
+          uo = -uo;
+        }
       }
       const double rh = P.rho[off2m(P, a, b)];
       const double kap = isfinite(u) ? P.k0 * pow_m64(fabs(u), P.kmode, P.km, P.khalf, P.kn) : 0.0;
       al = kap / (rh * P.cp);
+      if (ex_in) {
+        const double ko = isfinite(uo) ? P.k0 * pow_m64(fabs(uo), P.kmode, P.km, P.khalf, P.kn) : 0.0;
+        alo = ko / (rh * P.cp);
+      }
       // the new base state, ghosts included (copy!(T, u) returns them)
       const bool own = (ra >= 1 && ra <= RTX && rb >= 1 && rb <= RTY) ||
                        ((a == -1 || a == ni) && rb >= 1 && rb <= RTY) || ((b == -1 || b == nj) && ra >= 1 && ra <= RTX);
@@ -190,22 +228,36 @@ __global__ void __launch_bounds__(RNT) mixed_restart2d(const Problem* __restrict
     }
     s_u[rb][ra] = u;
     s_a[rb][ra] = al;
+    s_uo[rb][ra] = uo;
+    s_ao[rb][ra] = alo;
   }
   __syncthreads();
   for (int f = tid; f < RY * (RTX + 1); f += RNT) {
     const int fb = f / (RTX + 1), fa = f - fb * (RTX + 1);
     const int a = i0 - 1 + fa, b = j0 - 1 + fb;
     double q = 0.0;
-    if (a >= -1 && a <= ni - 1 && b >= 0 && b <= nj - 1)
+    if (a >= -1 && a <= ni - 1 && b >= 0 && b <= nj - 1) {
       q = -face_mean(P.mean, s_a[fb][fa], s_a[fb][fa + 1]) * (s_u[fb][fa + 1] - s_u[fb][fa]);
+      if (ex_in && fb >= 1 && fb <= RTY && (fa >= 1 || a == -1)) {
+        const double qo = -face_mean(P.mean, s_ao[fb][fa], s_ao[fb][fa + 1]) * (s_uo[fb][fa + 1] - s_uo[fb][fa]);
+        const int o = off2m(P, a, b);
+        ex_out[o] = (float)((double)ex_in[o] + (qo - q));
+      }
+    }
     s_qx[fb][fa] = q;
   }
   for (int f = tid; f < (RTY + 1) * RX; f += RNT) {
     const int fb = f / RX, fa = f - fb * RX;
     const int a = i0 - 1 + fa, b = j0 - 1 + fb;
     double q = 0.0;
-    if (a >= 0 && a <= ni - 1 && b >= -1 && b <= nj - 1)
+    if (a >= 0 && a <= ni - 1 && b >= -1 && b <= nj - 1) {
       q = -face_mean(P.mean, s_a[fb][fa], s_a[fb + 1][fa]) * (s_u[fb + 1][fa] - s_u[fb][fa]);
+      if (ex_in && fa >= 1 && fa <= RTX && (fb >= 1 || b == -1)) {
+        const double qo = -face_mean(P.mean, s_ao[fb][fa], s_ao[fb + 1][fa]) * (s_uo[fb + 1][fa] - s_uo[fb][fa]);
+        const int o = off2m(P, a, b);
+        ey_out[o] = (float)((double)ey_in[o] + (qo - q));
+      }
+    }
     s_qy[fb][fa] = q;
   }
   __syncthreads();
@@ -307,7 +359,7 @@ __global__ void __launch_bounds__(TX) mixed_sweep2d(const Problem* __restrict__ 
     float da = 0.f;
     if (kmode != 0) {
       const float x = c.d * __frcp_rn(c.ub);
-      da = (fabsf(c.ub) > 1e-30f && isfinite(x)) ? c.ab * expm1f(kn * log1pf(x))
+      da = (fabsf(c.ub) > 1e-30f && isfinite(x)) ? c.ab * incr_pow(x, kmode, km, khalf, kn)
                                                   : k0 * pow_m32(fabsf(u), kmode, km, khalf, kn) * irc - c.ab;
     }
     c.da = da;
@@ -512,6 +564,10 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
   // the FP32 sweep uses the strips of the 2D row-marching layout (variant 0)
   to_f32<<<1184, 256, 0, stream>>>(P.rho, s.rho32, (int64_t)N);
   CDM_CK(cudaGetLastError());
+  // the bases start as T everywhere (corners and outer halo layers are never rewritten)
+  for (int b = 0; b < 2; ++b)
+    CDM_CK(cudaMemcpyAsync(s.ub64[b], s.u[0], N * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+  const bool debug = std::getenv("CDM_DEBUG_MIXED") != nullptr;
   Ctrl& Ch = h_ctrl[0];
   const double tolmax_abs = o->atol * Ch.sqrtN;  // abs tolerance in max|R| units
   int restarts = 0, iters = 0;
@@ -526,14 +582,28 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
     return wait_stream(timeout_s - (now_seconds() - t_start));
   };
   // restart r: u_b(r) = u_b(r-1) + δ (δ absent for r = 0), R_b, max|R_b|
-  auto restart = [&](const float* d) -> int {
+  // ecur: parity of the flux-correction buffer the last sweep wrote (-1: none)
+  auto restart = [&](const float* d, int ecur) -> int {
     const double* in = restarts == 0 ? s.u[0] : s.ub64[(restarts - 1) & 1];
     double* out = s.ub64[restarts & 1];
     P.tiles_j = rti;
     P.ntiles = rti * rtj;
     int rc = upload();
     if (rc != CDM_OK) return rc;
-    mixed_restart2d<<<rti * rtj, RNT, 0, stream>>>(d_probs, in, d, out, s.ub32, s.R32);
+    // the carried flux correction lands in buffer 0, read by the next cycle's first sweep;
+    // when the last sweep wrote buffer 1 it is first moved to buffer 0 in place
+    const float* exi = nullptr;
+    const float* eyi = nullptr;
+    if (ecur >= 0) {
+      if (ecur == 1) {
+        CDM_CK(cudaMemcpyAsync(s.e32[0][0], s.e32[1][0], N * sizeof(float), cudaMemcpyDeviceToDevice, stream));
+        CDM_CK(cudaMemcpyAsync(s.e32[0][1], s.e32[1][1], N * sizeof(float), cudaMemcpyDeviceToDevice, stream));
+      }
+      exi = s.e32[0][0];
+      eyi = s.e32[0][1];
+    }
+    mixed_restart2d<<<rti * rtj, RNT, 0, stream>>>(d_probs, in, d, out, s.ub32, s.R32, exi, eyi, s.e32[0][0],
+                                                   s.e32[0][1]);
     CDM_CK(cudaGetLastError());
     prof.other_launches += 1;
     prof.fp64_cell_evals += s.ndomain;
@@ -542,11 +612,11 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
     P.tiles_j = s.tiles_j;
     P.ntiles = s.ntiles;
     ++restarts;
-    // clear the correction and its fluxes for the next cycle
-    for (int b = 0; b < 2; ++b) {
-      CDM_CK(cudaMemsetAsync(s.d32[b], 0, N * sizeof(float), stream));
-      for (int d = 0; d < 2; ++d) CDM_CK(cudaMemsetAsync(s.e32[b][d], 0, N * sizeof(float), stream));
-    }
+    // clear the correction for the next cycle (the flux correction carries over)
+    for (int b = 0; b < 2; ++b) CDM_CK(cudaMemsetAsync(s.d32[b], 0, N * sizeof(float), stream));
+    if (ecur < 0)
+      for (int b = 0; b < 2; ++b)
+        for (int d = 0; d < 2; ++d) CDM_CK(cudaMemsetAsync(s.e32[b][d], 0, N * sizeof(float), stream));
     return CDM_OK;
   };
   // a convergence check on the FP64 residual of the current base (:284-318)
@@ -590,7 +660,7 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
   Ch.inner_done = 0;
   Ch.inner_check_every = 4;
   Ch.n_checks = 0;
-  int rc = restart(nullptr);
+  int rc = restart(nullptr, -1);
   if (rc != CDM_OK) return rc;
   if (Ch.restart_nan) {
     Ch.status = ST_NONFINITE;
@@ -615,9 +685,12 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
     if (rc != CDM_OK) return rc;
     iters = Ch.iter;
     const int cur = Ch.inner_iter;
-    rc = restart(s.d32[cur & 1]);
+    rc = restart(s.d32[cur & 1], cur & 1);
     if (rc != CDM_OK) return rc;
     st = check(first);
+    if (debug)
+      std::fprintf(stderr, "[mixed] cycle %d: inner %d (target %.3e, last inner %.3e) restart max|R| %.3e rel %.3e st %d\n",
+                   restarts - 1, cur, target, Ch.inner_L2, Ch.restart_L2, rel, st);
     first = false;
     if (Ch.inner_iter >= cap_inner && st < 0 && iters > o->max_iter) st = ST_MAX_ITER;
   }
