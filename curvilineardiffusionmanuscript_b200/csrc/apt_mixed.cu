@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "cdm_device.cuh"
 #include "cdm_finish.cuh"
@@ -158,8 +159,16 @@ __device__ void reduce_and_publish(const Problem& P, Ctrl* C, int tile, double l
       C->restart_L2 = m;
       C->restart_nan = anybad;
     } else {
+      // the cycle ends at the target, on NaN, or when FP32 stops making progress
+      // (no 5% improvement of the best max|r| over 12 consecutive checks)
       C->inner_L2 = m;
-      if (!(m > C->inner_target) || anybad) C->inner_done = 1;  // NaN ends the cycle too
+      if (m < 0.95 * C->inner_best) {
+        C->inner_best = m;
+        C->inner_stall = 0;
+      } else {
+        C->inner_stall += 1;
+      }
+      if (!(m > C->inner_target) || anybad || C->inner_stall >= 12) C->inner_done = 1;
     }
     __threadfence();
   }
@@ -173,13 +182,30 @@ __device__ void reduce_and_publish(const Problem& P, Ctrl* C, int tile, double l
 // and the FP32 copies the sweeps read.  One block per 32x16 tile.
 constexpr int RTX = 32, RTY = 16, RNT = 256;
 
-// The damped-flux memory carries over: the total damped flux q′(u_b) + e is
-// kept, so e ← e + q′(u_old) − q′(u_new) on the faces the tile owns.
-__global__ void __launch_bounds__(RNT) mixed_restart2d(const Problem* __restrict__ probs, const double* __restrict__ ub_in,
-                                                       const float* __restrict__ d_in, double* __restrict__ ub_out,
-                                                       float* __restrict__ ub32, float* __restrict__ R32,
-                                                       const float* __restrict__ ex_in, const float* __restrict__ ey_in,
-                                                       float* __restrict__ ex_out, float* __restrict__ ey_out) {
+// The damped flux of the pseudo-time iteration carries over: its total
+// q′(u_b) + e is kept, so e ← e + q′(u_old) − q′(u_new) on the faces the tile
+// owns.  At the first restart of a step the total is the solver's FP64 flux
+// state q (carried across steps as in the reference, PseudoTransientSolver.jl:
+// 32): e ← q − q′(u).  Every restart also writes the current total damped flux
+// q′(u_old) + e back to the FP64 state.
+struct RestartIO {
+  const double* ub_in;
+  const float* d_in;       // correction to fold in (NULL at the first restart)
+  double* ub_out;
+  float* ub32;
+  float* R32;
+  const float* e_in[2];    // flux correction of the last sweep (NULL at the first restart)
+  const double* q_in[2];   // FP64 damped-flux state (first restart)
+  float* e_out[2];
+  double* q_out[2];        // FP64 damped-flux state (written at every restart)
+};
+
+__global__ void __launch_bounds__(RNT) mixed_restart2d(const Problem* __restrict__ probs, RestartIO io) {
+  const double* __restrict__ ub_in = io.ub_in;
+  const float* __restrict__ d_in = io.d_in;
+  double* __restrict__ ub_out = io.ub_out;
+  float* __restrict__ ub32 = io.ub32;
+  float* __restrict__ R32 = io.R32;
   constexpr int RX = RTX + 2, RY = RTY + 2;
   __shared__ double s_u[RY][RX], s_a[RY][RX], s_uo[RY][RX], s_ao[RY][RX];
   __shared__ double s_qx[RY][RTX + 1], s_qy[RTY + 1][RX];
@@ -213,7 +239,7 @@ __global__ void __launch_bounds__(RNT) mixed_restart2d(const Problem* __restrict
       const double rh = P.rho[off2m(P, a, b)];
       const double kap = isfinite(u) ? P.k0 * pow_m64(fabs(u), P.kmode, P.km, P.khalf, P.kn) : 0.0;
       al = kap / (rh * P.cp);
-      if (ex_in) {
+      if (io.e_in[0]) {
         const double ko = isfinite(uo) ? P.k0 * pow_m64(fabs(uo), P.kmode, P.km, P.khalf, P.kn) : 0.0;
         alo = ko / (rh * P.cp);
       }
@@ -238,10 +264,17 @@ __global__ void __launch_bounds__(RNT) mixed_restart2d(const Problem* __restrict
     double q = 0.0;
     if (a >= -1 && a <= ni - 1 && b >= 0 && b <= nj - 1) {
       q = -face_mean(P.mean, s_a[fb][fa], s_a[fb][fa + 1]) * (s_u[fb][fa + 1] - s_u[fb][fa]);
-      if (ex_in && fb >= 1 && fb <= RTY && (fa >= 1 || a == -1)) {
-        const double qo = -face_mean(P.mean, s_ao[fb][fa], s_ao[fb][fa + 1]) * (s_uo[fb][fa + 1] - s_uo[fb][fa]);
+      if (fb >= 1 && fb <= RTY && (fa >= 1 || a == -1)) {
         const int o = off2m(P, a, b);
-        ex_out[o] = (float)((double)ex_in[o] + (qo - q));
+        double total;  // damped flux of the iteration so far
+        if (io.e_in[0]) {
+          const double qo = -face_mean(P.mean, s_ao[fb][fa], s_ao[fb][fa + 1]) * (s_uo[fb][fa + 1] - s_uo[fb][fa]);
+          total = qo + (double)io.e_in[0][o];
+        } else {
+          total = io.q_in[0][o];
+        }
+        io.e_out[0][o] = (float)(total - q);
+        io.q_out[0][o] = total;
       }
     }
     s_qx[fb][fa] = q;
@@ -252,10 +285,17 @@ __global__ void __launch_bounds__(RNT) mixed_restart2d(const Problem* __restrict
     double q = 0.0;
     if (a >= 0 && a <= ni - 1 && b >= -1 && b <= nj - 1) {
       q = -face_mean(P.mean, s_a[fb][fa], s_a[fb + 1][fa]) * (s_u[fb + 1][fa] - s_u[fb][fa]);
-      if (ex_in && fa >= 1 && fa <= RTX && (fb >= 1 || b == -1)) {
-        const double qo = -face_mean(P.mean, s_ao[fb][fa], s_ao[fb + 1][fa]) * (s_uo[fb + 1][fa] - s_uo[fb][fa]);
+      if (fa >= 1 && fa <= RTX && (fb >= 1 || b == -1)) {
         const int o = off2m(P, a, b);
-        ey_out[o] = (float)((double)ey_in[o] + (qo - q));
+        double total;
+        if (io.e_in[1]) {
+          const double qo = -face_mean(P.mean, s_ao[fb][fa], s_ao[fb + 1][fa]) * (s_uo[fb + 1][fa] - s_uo[fb][fa]);
+          total = qo + (double)io.e_in[1][o];
+        } else {
+          total = io.q_in[1][o];
+        }
+        io.e_out[1][o] = (float)(total - q);
+        io.q_out[1][o] = total;
       }
     }
     s_qy[fb][fa] = q;
@@ -567,8 +607,8 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
   // the bases start as T everywhere (corners and outer halo layers are never rewritten)
   for (int b = 0; b < 2; ++b)
     CDM_CK(cudaMemcpyAsync(s.ub64[b], s.u[0], N * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-  const bool debug = std::getenv("CDM_DEBUG_MIXED") != nullptr;
   Ctrl& Ch = h_ctrl[0];
+  const bool debug = std::getenv("CDM_DEBUG_MIXED") != nullptr;
   const double tolmax_abs = o->atol * Ch.sqrtN;  // abs tolerance in max|R| units
   int restarts = 0, iters = 0;
   double init_L2 = INFINITY, rel = 2 * o->rtol, ab = 2 * o->atol;
@@ -590,20 +630,21 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
     P.ntiles = rti * rtj;
     int rc = upload();
     if (rc != CDM_OK) return rc;
-    // the carried flux correction lands in buffer 0, read by the next cycle's first sweep;
-    // when the last sweep wrote buffer 1 it is first moved to buffer 0 in place
-    const float* exi = nullptr;
-    const float* eyi = nullptr;
-    if (ecur >= 0) {
-      if (ecur == 1) {
-        CDM_CK(cudaMemcpyAsync(s.e32[0][0], s.e32[1][0], N * sizeof(float), cudaMemcpyDeviceToDevice, stream));
-        CDM_CK(cudaMemcpyAsync(s.e32[0][1], s.e32[1][1], N * sizeof(float), cudaMemcpyDeviceToDevice, stream));
-      }
-      exi = s.e32[0][0];
-      eyi = s.e32[0][1];
+    // the carried flux correction lands in buffer 0, read by the next cycle's
+    // first sweep; when the last sweep wrote buffer 1 it is read from there
+    RestartIO io;
+    io.ub_in = in;
+    io.d_in = d;
+    io.ub_out = out;
+    io.ub32 = s.ub32;
+    io.R32 = s.R32;
+    for (int c = 0; c < 2; ++c) {
+      io.e_in[c] = ecur >= 0 ? s.e32[ecur][c] : nullptr;
+      io.q_in[c] = s.q[s.qpar][c];
+      io.e_out[c] = s.e32[0][c];
+      io.q_out[c] = s.q[s.qpar][c];
     }
-    mixed_restart2d<<<rti * rtj, RNT, 0, stream>>>(d_probs, in, d, out, s.ub32, s.R32, exi, eyi, s.e32[0][0],
-                                                   s.e32[0][1]);
+    mixed_restart2d<<<rti * rtj, RNT, 0, stream>>>(d_probs, io);
     CDM_CK(cudaGetLastError());
     prof.other_launches += 1;
     prof.fp64_cell_evals += s.ndomain;
@@ -614,9 +655,6 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
     ++restarts;
     // clear the correction for the next cycle (the flux correction carries over)
     for (int b = 0; b < 2; ++b) CDM_CK(cudaMemsetAsync(s.d32[b], 0, N * sizeof(float), stream));
-    if (ecur < 0)
-      for (int b = 0; b < 2; ++b)
-        for (int d = 0; d < 2; ++d) CDM_CK(cudaMemsetAsync(s.e32[b][d], 0, N * sizeof(float), stream));
     return CDM_OK;
   };
   // a convergence check on the FP64 residual of the current base (:284-318)
@@ -631,25 +669,49 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
     if (rel <= o->rtol || ab <= o->atol) return 0;
     return -1;  // continue
   };
+  // inner sweeps in blocks of 16 replayed from a captured graph; a sweep after
+  // the end of the cycle returns at once
   auto sweeps = [&](int n) -> int {
-    P.qpar = 0;
     int rc = upload();
     if (rc != CDM_OK) return rc;
-    int done = 0;
-    while (done < n) {
-      const int K = std::min(8, n - done);
-      const int pe = record_pair();
-      if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe], stream));
+    const int K = 16;
+    if (!mixed_graph) {
+      cudaGraph_t g;
+      CDM_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
       for (int k = 0; k < K; ++k) {
         if (mean == CDM_MEAN_HARMONIC) mixed_sweep2d<128, true><<<nitems, 128, 0, stream>>>(d_probs, d_items);
         else mixed_sweep2d<128, false><<<nitems, 128, 0, stream>>>(d_probs, d_items);
-        CDM_CK(cudaGetLastError());
+      }
+      cudaError_t le = cudaGetLastError();
+      cudaError_t ce = cudaStreamEndCapture(stream, &g);
+      CDM_CK(le);
+      CDM_CK(ce);
+      CDM_CK(cudaGraphInstantiate(&mixed_graph, g, 0));
+      cudaGraphDestroy(g);
+    }
+    int done = 0;
+    while (done < n) {
+      const int pe = record_pair();
+      if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe], stream));
+      if (n - done >= K) {
+        CDM_CK(cudaGraphLaunch(mixed_graph, stream));
+        done += K;
+        prof.sweep_launches += K;
+      } else {
+        for (int k = 0; k < n - done; ++k) {
+          if (mean == CDM_MEAN_HARMONIC) mixed_sweep2d<128, true><<<nitems, 128, 0, stream>>>(d_probs, d_items);
+          else mixed_sweep2d<128, false><<<nitems, 128, 0, stream>>>(d_probs, d_items);
+          CDM_CK(cudaGetLastError());
+        }
+        prof.sweep_launches += n - done;
+        done = n;
       }
       if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe + 1], stream));
-      prof.sweep_launches += K;
-      done += K;
       rc = poll();
       if (rc != CDM_OK) return rc;
+      if (debug)
+        std::fprintf(stderr, "   [mixed] k=%d inner max|r| %.3e best %.3e stall %d\n", Ch.inner_iter, Ch.inner_L2,
+                     Ch.inner_best, Ch.inner_stall);
       if (Ch.inner_done) break;
     }
     return CDM_OK;
@@ -673,13 +735,17 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
   while (st < 0) {
     // first cycle: one sweep, so that the first check is at iteration 1 as in the reference
     const double Rmax = Ch.restart_L2;
-    double target = 1e-4 * Rmax;
+    // either stopping criterion suffices (rel <= rtol || abs <= atol), so the
+    // cycle need not go below the larger of the two thresholds (in max|R| units)
+    double target = 1e-3 * Rmax;
     double floor_t = tolmax_abs;
-    if (!first && std::isfinite(init_L2)) floor_t = std::min(floor_t, o->rtol * init_L2 * Ch.sqrtN);
-    target = std::max(target, 0.25 * floor_t);
+    if (!first && std::isfinite(init_L2)) floor_t = std::max(floor_t, o->rtol * init_L2 * Ch.sqrtN);
+    target = std::max(target, 0.5 * floor_t);
     Ch.inner_target = target;
     Ch.inner_done = 0;
     Ch.inner_iter = 0;
+    Ch.inner_stall = 0;
+    Ch.inner_best = INFINITY;
     const int n = first ? 1 : cap_inner;
     rc = sweeps(n);
     if (rc != CDM_OK) return rc;

@@ -48,7 +48,8 @@ struct Ctrl {
   int inner_done;       // set on the device when the inner target is met
   int inner_check_every;
   int restart_nan;
-  int pad2;
+  int inner_stall;      // inner checks since the last new best
+  double inner_best;    // best max|r| of the cycle
 };
 
 // Kernel-facing description of one problem (one mesh, one step! call).

@@ -126,6 +126,8 @@ Engine::~Engine() {
 }
 
 int Engine::free_graphs() {
+  if (mixed_graph) cudaGraphExecDestroy(mixed_graph);
+  mixed_graph = nullptr;
   for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
   for (auto& kv : graph_defs) cudaGraphDestroy(kv.second);
   graphs.clear();
@@ -386,11 +388,13 @@ int Engine::build_items() {
       // single problem fills several waves of 148 SMs
       const int ow = ts.tx - 2;
       s.tiles_i = (s.ni + ow - 1) / ow;
+      // a single problem: about 24 strips per SM (several waves), no shorter
+      // than 8 rows (the two staged ring rows cost 2/h); a batch: 64-row strips
       int h = 64;
       if (nprob == 1) {
         const int target = 148 * 24;
         int nstrips = (target + s.tiles_i - 1) / s.tiles_i;
-        nstrips = std::max(1, std::min(nstrips, (s.nj + 31) / 32));
+        nstrips = std::max(1, std::min(nstrips, (s.nj + 7) / 8));
         h = (s.nj + nstrips - 1) / nstrips;
       }
       s.strip_h = std::max(1, std::min(h, s.nj));

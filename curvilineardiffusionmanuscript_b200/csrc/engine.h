@@ -80,6 +80,7 @@ struct Engine {
   cudaStream_t side_stream = nullptr;  // boundary strips run here, concurrently
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   SweepStreams sweep_streams() const;
+  cudaGraphExec_t mixed_graph = nullptr;  // 16 FP32 correction sweeps
   int* d_flags = nullptr;        // per problem: source validity bits
   double* d_red = nullptr;       // reduction scratch
   double* d_redout = nullptr;    // per problem 8 doubles

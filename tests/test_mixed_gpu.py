@@ -1,0 +1,92 @@
+"""GPU tests of the mixed-precision path: FP32 correction sweeps with FP64
+residual and defect-correction restarts.
+
+The FP32 path solves the same discrete equations to the same stopping rule, so
+its solution differs from the FP64 oracle's by the stopping tolerance, not by
+FP32 rounding: the stated bound is a relative L2 difference ≤ 1e-6 on the full
+array at rel ≤ 1e-8, and the manufactured-solution error equals the FP64 one.
+"""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from helpers import rel_l2, small_case_2d
+from oracle.oracle import OracleSolver
+from curvilineardiffusionmanuscript_b200 import problems
+from curvilineardiffusionmanuscript_b200.solver import (APTError, DirichletBC, NeumannBC, PeriodicBC,
+                                                        PseudoTransientSolver, step)
+
+pytestmark = pytest.mark.gpu
+KW = dict(rtol=1e-8, atol=1e-8, max_iter=100000)
+
+
+def run_mixed_vs_oracle(pr, nsteps, src=None, mean="harmonic"):
+    o = OracleSolver(pr.mesh, pr.bcs, mean=mean)
+    g = PseudoTransientSolver(pr.mesh, pr.bcs, precision="mixed", mean=mean)
+    To = pr.T0.numpy().copy()
+    Tg = pr.T0.clone().cuda()
+    rho = pr.rho.cuda()
+    t = 0.0
+    out = []
+    for _ in range(nsteps):
+        if src is not None:
+            S = src(t + pr.dt)
+            o.set_source(S.numpy())
+            g.set_source(S.cuda())
+        so, _ = o.step(To, pr.rho.numpy(), pr.cp, pr.kappa.k0, pr.kappa.n, pr.dt, **KW)
+        sg, _ = step(g, pr.mesh, Tg, rho, pr.cp, pr.kappa, pr.dt, **KW)
+        t += pr.dt
+        out.append((so, sg, To.copy(), Tg.cpu().numpy()))
+    return out
+
+
+def test_mixed_gaussian_128():
+    for so, sg, To, Tg in run_mixed_vs_oracle(problems.gaussian_2d(128), 4):
+        assert so["status"] == 0 and sg["status"] == 0
+        assert sg["rel_err"] <= 1e-8 or sg["abs_err"] <= 1e-8
+        assert sg["n_restarts"] >= 2
+        assert rel_l2(Tg, To) <= 1e-6, rel_l2(Tg, To)
+
+
+def test_mixed_mms_error_matches_fp64():
+    pr = problems.mms_2d(256)
+    out = run_mixed_vs_oracle(pr, 3, src=lambda t: problems.mms_source(pr, t))
+    so, sg, To, Tg = out[-1]
+    e_o = problems.mms_error(pr, torch.from_numpy(To), 3 * pr.dt)
+    e_g = problems.mms_error(pr, torch.from_numpy(Tg), 3 * pr.dt)
+    assert abs(e_g[0] - e_o[0]) <= 1e-6 * e_o[0] and abs(e_g[1] - e_o[1]) <= 1e-6 * e_o[1]
+    assert rel_l2(Tg, To) <= 1e-8
+
+
+@pytest.mark.parametrize("bcs", [[DirichletBC(1.5), NeumannBC(), PeriodicBC(), PeriodicBC()],
+                                 [NeumannBC(), NeumannBC(), DirichletBC(0.5), NeumannBC()]])
+def test_mixed_boundary_conditions(bcs):
+    pr = small_case_2d(ni=150, nj=140, bcs=bcs, source=True)
+    for so, sg, To, Tg in run_mixed_vs_oracle(pr, 2):
+        assert so["status"] == 0 and sg["status"] == 0
+        assert rel_l2(Tg, To) <= 1e-6
+
+
+def test_mixed_arithmetic_mean():
+    pr = small_case_2d(ni=120, nj=100, kn=2.5)
+    for so, sg, To, Tg in run_mixed_vs_oracle(pr, 2, mean="arithmetic"):
+        assert sg["status"] == 0 and rel_l2(Tg, To) <= 1e-6
+
+
+def test_mixed_state_carries_into_fp64():
+    """The damped-flux state written by the mixed path continues the FP64 iteration."""
+    pr = problems.gaussian_2d(96)
+    g = PseudoTransientSolver(pr.mesh, pr.bcs, precision="mixed")
+    T = pr.T0.clone().cuda()
+    step(g, pr.mesh, T, pr.rho.cuda(), pr.cp, pr.kappa, pr.dt, **KW)
+    q, last = g.get_state()
+    assert np.isfinite(q).all() and np.abs(q).max() > 0 and last > 0
+
+
+def test_mixed_rejects_batches_and_3d():
+    from curvilineardiffusionmanuscript_b200.mesh import wavy_mesh_3d
+    m = wavy_mesh_3d(8, 8, 8)
+    with pytest.raises(APTError):
+        PseudoTransientSolver(m, [NeumannBC()] * 6, precision="mixed")
