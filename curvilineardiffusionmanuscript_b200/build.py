@@ -31,6 +31,7 @@ UNITS = {
     "apt_aux.cu": ["-fmad=false"],
     "engine.cu": ["-fmad=false"],
     "apt_mixed.cu": [],
+    "apt_noalloc.cu": ["-fmad=false"],
     "autotune.cu": [],
 }
 

@@ -247,6 +247,25 @@ int cdm_batch_step(cdm_batch* b, double* const* T, const double* const* rho, con
 int cdm_batch_autotune(cdm_batch* b, const char* cache_path, int* chosen);
 int cdm_batch_get_profile(const cdm_batch* b, cdm_profile* out);
 
+/* ---- allocation-free end-of-step reductions ------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory while they run (a Julia host whose CUDA.jl pool owns the device
+ * memory, a service that forbids allocation on its latency path): computes,
+ * from device arrays the caller owns, what cdm_apt_step computes after its
+ * pseudo-time loop — next_dt and the energy balance — using a fixed scratch
+ * array inside the library instead of cudaMalloc.  u_new, u_prev, rho, S
+ * (may be NULL) and cell_J are full-size device arrays; out (host) receives
+ * {next_dt, energy_before, energy_after, source_work} as in cdm_stats.
+ * Limit: at most 134,217,728 cells in the full array (CDM_BAD_INPUT beyond).
+ * The first call on a device sets the scratch up and must come before any
+ * stream capture; calls that overlap on the GPU race on the shared scratch.
+ * stream: cudaStream_t or NULL. */
+int cdm_step_reductions_noalloc(int ndim, int ni, int nj, int nk, int nhalo, const double* u_new,
+                                const double* u_prev, const double* rho, const double* S,
+                                const double* cell_J, double cp, double dt, double ndt_tol,
+                                double maximum_u_change, double timestep_growth_factor, double* out,
+                                void* stream);
+
 #ifdef __cplusplus
 }
 #endif
