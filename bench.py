@@ -41,8 +41,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batch",
-                    choices=["batch", "gaussian128", "gaussian2048", "mms4096", "gauss3d256", "gauss3d128"])
+                    choices=["batch", "gaussian128", "gaussian2048", "mms4096", "mms1024", "multigauss1024",
+                             "gauss3d256", "gauss3d128"])
     ap.add_argument("--nprob", type=int, default=256)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64_exact", "mixed"])
+    ap.add_argument("--compare", action="store_true", help="single-problem s/timestep: fp64 vs mixed")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -172,7 +175,13 @@ def make_workload(name, nprob, rank, device):
         cfg = {"workload": "gaussian3d_128_fp64", "kappa": "T^2.5", "dt": 1e-5, "tol": 1e-8}
     elif name == "mms4096":
         probs = [problems.mms_2d(4096, device=device)]
-        cfg = {"workload": "mms2d_4096_fp64", "kappa": "T^2.5", "dt": 1e-5, "tol": 1e-8}
+        cfg = {"workload": "mms2d_4096", "kappa": "T^2.5", "dt": 1e-5, "tol": 1e-8}
+    elif name == "mms1024":
+        probs = [problems.mms_2d(1024, device=device)]
+        cfg = {"workload": "mms2d_1024", "kappa": "T^2.5", "dt": 1e-5, "tol": 1e-8}
+    elif name == "multigauss1024":
+        probs = [problems.multi_gaussian_2d(1024, seed=12345, device=device)]
+        cfg = {"workload": "multigauss2d_1024", "kappa": "T^3", "dt": 1e-5, "tol": 1e-8}
     else:
         probs = [problems.gaussian_3d(256, device=device)]
         cfg = {"workload": "gaussian3d_256_fp64", "kappa": "T^2.5", "dt": 1e-5, "tol": 1e-8}
@@ -337,8 +346,58 @@ def run_ours(args, ws, rank, local):
     batch.close()
 
 
+def time_single(pr, precision, steps, warmup, stream, guess=None):
+    """Seconds per time step of one problem (CUDA events on the solver's stream)."""
+    import torch
+    from curvilineardiffusionmanuscript_b200 import problems
+    from curvilineardiffusionmanuscript_b200.solver import PseudoTransientSolver, step
+    g = PseudoTransientSolver(pr.mesh, pr.bcs, precision=precision, stream=stream.cuda_stream)
+    T = pr.T0.clone()
+    t = 0.0
+    mms = pr.name == "mms_2d"
+    times, iters, restarts = [], [], []
+    for k in range(warmup + steps):
+        if mms:
+            g.set_source(problems.mms_source(pr, t + pr.dt))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st, _ = step(g, pr.mesh, T, pr.rho, pr.cp, pr.kappa, pr.dt, rtol=pr.rtol, atol=pr.atol, max_iter=100000)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t += pr.dt
+        if k >= warmup:
+            times.append(e0.elapsed_time(e1) / 1e3)
+            iters.append(st["niter"])
+            restarts.append(st["n_restarts"])
+    out = {"s_per_step": statistics.median(times), "iters": statistics.mean(iters),
+           "restarts": statistics.mean(restarts)}
+    if mms:
+        out["err_vs_exact"] = problems.mms_error(pr, T.cpu(), t)
+    g.close()
+    return out
+
+
+def run_compare(args):
+    import torch
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    res = {}
+    for wl in (["mms4096", "multigauss1024"] if args.workload == "batch" else [args.workload]):
+        r = {}
+        for prec in ("fp64", "mixed"):
+            probs, cfg = make_workload(wl, 1, 0, dev)
+            r[prec] = time_single(probs[0], prec, args.steps, args.warmup, stream)
+        r["speedup_mixed_vs_fp64"] = r["fp64"]["s_per_step"] / r["mixed"]["s_per_step"]
+        res[wl] = r
+    print(json.dumps({"compare": res}), flush=True)
+
+
 def main():
     args = parse()
+    if args.compare:
+        run_compare(args)
+        return
     ws, rank, local = dist_setup(args)
     try:
         if args.impl == "reference":
