@@ -373,7 +373,7 @@ def time_single(pr, precision, steps, warmup, stream, guess=None):
     out = {"s_per_step": statistics.median(times), "iters": statistics.mean(iters),
            "restarts": statistics.mean(restarts)}
     if mms:
-        out["err_vs_exact"] = problems.mms_error(pr, T.cpu(), t)
+        out["err_vs_exact"] = problems.mms_error(pr, T, t)
     g.close()
     return out
 
