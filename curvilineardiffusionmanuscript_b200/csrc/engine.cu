@@ -119,6 +119,7 @@ Engine::~Engine() {
   if (h_redout) cudaFreeHost(h_redout);
   if (ev) cudaEventDestroy(ev);
   for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+  if (ev_caller) cudaEventDestroy(ev_caller);
   if (ev_fork) cudaEventDestroy(ev_fork);
   if (ev_join) cudaEventDestroy(ev_join);
   if (side_stream) cudaStreamDestroy(side_stream);
@@ -173,6 +174,8 @@ int Engine::init(int nprob, const cdm_mesh_desc* meshes, const cdm_bc* bcs, cons
     own_stream = true;
   }
   CDM_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  CDM_CK(cudaEventCreateWithFlags(&ev_caller, cudaEventDisableTiming));
+  CDM_CK(fence_caller());
   CDM_CK(cudaStreamCreateWithFlags(&side_stream, cudaStreamNonBlocking));
   CDM_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
   CDM_CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
@@ -450,6 +453,7 @@ int Engine::build_items() {
 int Engine::set_source(int p, const double* S, int mem) {
   ProbState& s = ps[p];
   CDM_CK(cudaSetDevice(device));
+  CDM_CK(fence_caller());
   CDM_CK(stage_in(s.S, S, s.nfull, mem, stream));
   Problem P;
   std::memset(&P, 0, sizeof(P));
@@ -474,10 +478,18 @@ int Engine::set_guess(int p, const double* u0, int mem) {
   ProbState& s = ps[p];
   CDM_CK(cudaSetDevice(device));
   if (!s.guess) CDM_CK(dalloc(&s.guess, (size_t)s.nfull));
+  CDM_CK(fence_caller());
   CDM_CK(stage_in(s.guess, u0, s.nfull, mem, stream));
   CDM_CK(cudaStreamSynchronize(stream));
   s.has_guess = 1;
   return CDM_OK;
+}
+
+cudaError_t Engine::fence_caller() {
+  if (!own_stream) return cudaSuccess;
+  cudaError_t e = cudaEventRecord(ev_caller, cudaStreamLegacy);
+  if (e != cudaSuccess) return e;
+  return cudaStreamWaitEvent(stream, ev_caller, 0);
 }
 
 int Engine::wait_stream(double timeout_s) {
@@ -639,6 +651,8 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
     for (int p = 0; p < nprob; ++p) stats[p].time = now_seconds() - t0;
     return bad;
   }
+  // T and rho may still be written by the caller's kernels
+  CDM_CK(fence_caller());
   for (int p = 0; p < nprob; ++p) {
     ProbState& s = ps[p];
     Problem& P = hp[p];

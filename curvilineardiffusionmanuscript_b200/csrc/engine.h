@@ -106,6 +106,11 @@ struct Engine {
   int run_iterations(const cdm_step_opts* o, int predicted, double t_start, double timeout_s);
   int launch_block(int K, bool use_graph);
   int wait_stream(double timeout_s);
+  // Orders a private stream after the work the caller issued to the legacy
+  // default stream before this call, so that the caller's device arrays are
+  // complete when the library reads them.  A caller-supplied stream orders itself.
+  cudaError_t fence_caller();
+  cudaEvent_t ev_caller = nullptr;
   int free_graphs();
   // mixed precision (apt_mixed.cu)
   int mixed_alloc();

@@ -94,12 +94,22 @@ def _ptr(a) -> int:
     if isinstance(a, torch.Tensor):
         if a.dtype != torch.float64 or not a.is_contiguous():
             raise ValueError("arrays must be contiguous float64")
+        if a.is_cuda:
+            _order_after_torch(a.device)
         return a.data_ptr()
     if isinstance(a, np.ndarray):
         if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
             raise ValueError("arrays must be C-contiguous float64")
         return a.ctypes.data
     raise TypeError(f"unsupported array type {type(a)}")
+
+
+def _order_after_torch(device) -> None:
+    """The library orders its reads after the legacy default stream (torch's
+    default stream); work queued on another torch stream is waited for here."""
+    cur = torch.cuda.current_stream(device)
+    if cur.cuda_stream != 0:
+        cur.synchronize()
 
 
 def _mem(a) -> int:

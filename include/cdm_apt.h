@@ -22,6 +22,12 @@
  * Threading: a handle is not thread-safe; use one host thread per handle.  Each
  * handle owns a CUDA stream (or uses the one passed in its config).  Calls are
  * synchronous: they return after the device work of the call has finished.
+ *
+ * Stream order of device arguments: with a stream in the config, the library
+ * reads the caller's device arrays in that stream's order, so the caller issues
+ * the kernels that produce them there.  With a NULL stream, every call that
+ * reads caller device memory first waits for the work already issued to the
+ * legacy default stream; work on other streams must be finished by the caller.
  */
 #ifndef CDM_APT_H
 #define CDM_APT_H

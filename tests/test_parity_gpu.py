@@ -281,6 +281,48 @@ def test_fast_and_exact_agree_on_large_grid():
         assert rel_l2(Tf.cpu().numpy(), Te.cpu().numpy()) <= TOL
 
 
+def test_device_inputs_written_just_before_the_call():
+    """Solvers exist before their inputs: S, T and rho are produced by torch
+    kernels queued immediately before set_source / step on a 3000 x 3000 MMS
+    grid (long strips, many column blocks).  The library must read them only
+    after those kernels finish; fast and exact then agree to round-off."""
+    prd = problems.mms_2d(3000, device="cuda")
+    solvers = {p: PseudoTransientSolver(prd.mesh, prd.bcs, precision=p) for p in ("fp64", "fp64_exact")}
+    out = {}
+    for p, g in solvers.items():
+        S = problems.mms_source(prd, prd.dt)
+        g.set_source(S)
+        T = prd.T0.clone() * 1.0
+        rho = prd.rho * 1.0
+        st, _ = step(g, prd.mesh, T, rho, 1.0, prd.kappa, prd.dt, rtol=1e-8, atol=1e-8, max_iter=100000)
+        out[p] = (st["niter"], T.cpu().numpy())
+    assert out["fp64"][0] == out["fp64_exact"][0]
+    assert rel_l2(out["fp64"][1], out["fp64_exact"][1]) <= TOL
+
+
+def test_caller_stream_other_than_the_default():
+    """Inputs produced on a non-default torch stream are complete before the
+    library reads them."""
+    pr = problems.gaussian_2d(512)
+    side = torch.cuda.Stream()
+    g = PseudoTransientSolver(pr.mesh, pr.bcs, precision="fp64_exact")
+    ref = PseudoTransientSolver(pr.mesh, pr.bcs, precision="fp64_exact")
+    T0 = pr.T0.cuda()
+    rho0 = pr.rho.cuda()
+    torch.cuda.synchronize()
+    Tr = T0.clone()
+    sr, _ = step(ref, pr.mesh, Tr, rho0, pr.cp, pr.kappa, pr.dt, rtol=1e-8, atol=1e-8)
+    with torch.cuda.stream(side):
+        T = T0 * 1.0
+        for _ in range(20):
+            T = T * 1.0
+        rho = rho0 * 1.0
+        sg, _ = step(g, pr.mesh, T, rho, pr.cp, pr.kappa, pr.dt, rtol=1e-8, atol=1e-8)
+    torch.cuda.synchronize()
+    assert sg["niter"] == sr["niter"]
+    assert rel_l2(T.cpu().numpy(), Tr.cpu().numpy()) == 0.0
+
+
 def test_divergent_case_reports_nonfinite_like_the_reference():
     """A 300 x 70 mesh makes the reference iteration diverge; the library reports
     the same NONFINITE error at the same pseudo-iteration (exact form)."""
