@@ -280,6 +280,7 @@ def run_ours(args, ws, rank, local):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ci, sweep_ms, launches, sweep_launches, iters = 0, 0.0, 0, 0, []
     with ClockSampler(local) as clk:
+        torch.cuda.nvtx.range_push("bench_timed")
         e0.record(stream)
         for _ in range(args.steps):
             st, pf = one_step()
@@ -290,6 +291,7 @@ def run_ours(args, ws, rank, local):
             iters.append(sum(s["niter"] for s in st))
         e1.record(stream)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
     ms = e0.elapsed_time(e1)
     barrier(ws)
     ms_max = allreduce_max(ms, ws, dev)
@@ -300,12 +302,11 @@ def run_ours(args, ws, rank, local):
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": None, "kernel": f"sweep{nd}d_fp64", "peak_kind": peak_kind,
             "bytes_per_cell_iter": BYTES_PER_CELL_ITER[nd]}
-    tp = ROOT / "profiles" / f"traffic_sweep{nd}d_fp64.json"
-    if tp.exists():
-        # DRAM bytes per cell-iteration from one ncu capture, times the cells one launch updates
-        t = json.loads(tp.read_text())
-        roof["traffic"] = t["dram_bytes_per_cell_iter"] * ci / max(1, sweep_launches)
-        roof["traffic_note"] = t.get("note", "")
+    tb, tsrc = traffic_per_cell_iter(nd, args.workload)
+    if tb is not None:
+        # DRAM bytes per cell-iteration from one ncu capture, times the cells one sweep updates
+        roof["traffic"] = tb * ci / max(1, sweep_launches)
+        roof["traffic_source"] = tsrc
     e2e = None
     if not args.no_e2e:
         # end to end through the public API with host (pinned) buffers
@@ -344,6 +345,26 @@ def run_ours(args, ws, rank, local):
             "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     batch.close()
+
+
+TRAFFIC_SUMMARY = {2: {"batch": "sweep2d_fp64_batch.md"}, 3: {}}
+TRAFFIC_DEFAULT = {2: "sweep2d_fp64_gaussian2048.md", 3: "sweep3d_fp64_gauss3d.md"}
+
+
+def traffic_per_cell_iter(nd, workload):
+    """DRAM bytes per cell-iteration of the sweep, read from the committed ncu summary
+    (line `dram_bytes_per_cell_iter: X`): the capture of this workload where one
+    exists, else the 2048^2 (2D) / 3D capture, scaled by the cells a sweep updates."""
+    import re
+    for name in (TRAFFIC_SUMMARY[nd].get(workload), TRAFFIC_DEFAULT[nd]):
+        if not name:
+            continue
+        f = ROOT / "profiles" / name
+        if f.exists():
+            m = re.search(r"^dram_bytes_per_cell_iter:\s*([0-9.]+)", f.read_text(), re.M)
+            if m:
+                return float(m.group(1)), "profiles/" + name
+    return None, None
 
 
 def time_single(pr, precision, steps, warmup, stream, guess=None):

@@ -92,30 +92,6 @@ __device__ __forceinline__ float pow_m32(float x, int mode, int m, int half, flo
   return powf(x, n);
 }
 
-// (|1 + x|)ⁿ − 1, accurate relative to x for small x and defined for every x
-// (the reference's κ uses |T|ⁿ): binomial Horner form for integer n, plus
-// √(1+y) − 1 = y/(√(1+y) + 1) for the half of half-integer n, log1p/expm1 otherwise
-__device__ __forceinline__ float incr_pow(float x, int mode, int m, int half, float n) {
-  if (mode == 0) return 0.f;
-  const float y = x >= -1.f ? x : -2.f - x;
-  if (mode == 2) return expm1f(n * log1pf(y));
-  float r = 0.f;  // (1+y)^m - 1
-  if (m >= 1) {
-    float c = (float)m, p = 0.f;  // Horner over binomial coefficients C(m,k), k = m..1
-    float coef[17];
-    coef[0] = 1.f;
-    for (int k = 1; k <= m; ++k) coef[k] = coef[k - 1] * (float)(m - k + 1) / (float)k;
-    for (int k = m; k >= 1; --k) p = p * y + coef[k];
-    r = p * y;
-    (void)c;
-  }
-  if (half) {
-    const float sq = sqrtf(1.f + y);
-    r = r * sq + y / (sq + 1.f);
-  }
-  return r;
-}
-
 // max-norm reduction of a block, last block of the launch publishes the result
 template <int NT>
 __device__ void reduce_and_publish(const Problem& P, Ctrl* C, int tile, double local, bool nan, double* s_red,
@@ -193,6 +169,7 @@ struct RestartIO {
   const float* d_in;       // correction to fold in (NULL at the first restart)
   double* ub_out;
   float* ub32;
+  float* ab32;             // diffusivity of the new base state, rounded
   float* R32;
   const float* e_in[2];    // flux correction of the last sweep (NULL at the first restart)
   const double* q_in[2];   // FP64 damped-flux state (first restart)
@@ -205,6 +182,7 @@ __global__ void __launch_bounds__(RNT) mixed_restart2d(const Problem* __restrict
   const float* __restrict__ d_in = io.d_in;
   double* __restrict__ ub_out = io.ub_out;
   float* __restrict__ ub32 = io.ub32;
+  float* __restrict__ ab32 = io.ab32;
   float* __restrict__ R32 = io.R32;
   constexpr int RX = RTX + 2, RY = RTY + 2;
   __shared__ double s_u[RY][RX], s_a[RY][RX], s_uo[RY][RX], s_ao[RY][RX];
@@ -250,6 +228,7 @@ __global__ void __launch_bounds__(RNT) mixed_restart2d(const Problem* __restrict
         const int o = off2m(P, a, b);
         ub_out[o] = u;
         ub32[o] = (float)u;
+        ab32[o] = (float)al;
       }
     }
     s_u[rb][ra] = u;
@@ -327,32 +306,65 @@ __global__ void __launch_bounds__(RNT) mixed_restart2d(const Problem* __restrict
 }
 
 // ---------------------------------------------------------------------------
-// FP32 correction sweep, row-marching (see apt_march2d_fast.cu for the layout):
-// a block of TX threads owns TX-2 columns of a strip of rows.
+// FP32 correction sweep, row-marching (the layout of apt_march2d_fast.cu): a
+// block of TX threads owns TX-2 columns of a strip of rows, keeps its own
+// column in registers, passes neighbour values through shared memory and
+// issues the loads of the row after next before it computes the next row.
+// Boundary strips run the general instantiation (ghost rules) in one block per
+// strip on a side stream; interior strips run a branch-free instantiation in a
+// persistent launch whose blocks claim strips from a ticket counter.
+//
+// The FP32 arithmetic only moves the correction: reciprocals and square roots
+// use the hardware approximations (rcp/sqrt.approx, about one ulp), and the
+// restarts evaluate everything the stopping rule sees in FP64.
+__device__ __forceinline__ float rcp_a(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+__device__ __forceinline__ float sqrt_a(float x) {
+  float y;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// (|1 + x|)ⁿ − 1, accurate relative to x for small x and defined for every x
+// (the reference's κ uses |T|ⁿ): one step r ← r + y(1 + r) per integer power,
+// (1 + r)√(1+y) − 1 = r√(1+y) + y/(√(1+y) + 1) for the half of a half-integer
+// n, expm1(n·log1p(y)) otherwise
+__device__ __forceinline__ float incr_pow32(float x, int mode, int m, int half, float n) {
+  if (mode == 0) return 0.f;
+  const float y = x >= -1.f ? x : -2.f - x;
+  if (mode == 2) return expm1f(n * log1pf(y));
+  float r = 0.f;
+  for (int k = 0; k < m; ++k) r = fmaf(y, 1.f + r, r);
+  if (half) {
+    const float sq = sqrt_a(1.f + y);
+    r = fmaf(r, sq, y * rcp_a(sq + 1.f));
+  }
+  return r;
+}
+
 template <int TX>
 struct MixSmem {
   float D[3][TX], UB[3][TX], AB[3][TX], DA[3][TX], IT[3][TX];
   float EX[3][TX], PX[3][TX], EY[2][TX], PY[2][TX];
   double red[TX / 32];
   int flag;
+  int ticket;
 };
 
 struct MCell {
   float d, ub, ab, da, it, f;
 };
 
-template <int TX, bool HARM>
-__global__ void __launch_bounds__(TX) mixed_sweep2d(const Problem* __restrict__ probs, const int2* __restrict__ items) {
+template <int TX, bool EDGE, bool HARM>
+__device__ __forceinline__ void mixed_body(const Problem& P, Ctrl* C, int tile, int k, bool check,
+                                           MixSmem<TX>& sm) {
   constexpr int OW = TX - 2;
-  __shared__ MixSmem<TX> sm;
-  const int2 item = items[blockIdx.x];
-  const Problem& P = probs[item.x];
-  Ctrl* C = P.ctrl;
-  if (ld_cg_int(&C->inner_done) || ld_cg_int(&C->done)) return;
-  const int k = ld_cg_int(&C->inner_iter) + 1;  // inner iteration of this cycle
-  const bool check = (k % C->inner_check_every) == 0;
+  constexpr float kPiF = 3.14159265358979f;
   const int tid = threadIdx.x;
-  const int tile = item.y;
   const int cbk = tile % P.tiles_i, sj = tile / P.tiles_i;
   const int ni = P.ni, nj = P.nj, nx = P.nx, nh = P.nh;
   const int i0 = cbk * OW, a = i0 - 1 + tid;
@@ -364,76 +376,106 @@ __global__ void __launch_bounds__(TX) mixed_sweep2d(const Problem* __restrict__ 
   float* __restrict__ exout = P.e32[k & 1][0];
   float* __restrict__ eyout = P.e32[k & 1][1];
   const float* __restrict__ ub = P.ub32;
+  const float* __restrict__ abv = P.ab32;
   const float* __restrict__ Rb = P.R32;
   const float* __restrict__ rho = P.rho32;
+  const float* __restrict__ G11 = P.coef32[0];
+  const float* __restrict__ G22 = P.coef32[1];
+  const float* __restrict__ C12 = P.coef32[2];
+  const float* __restrict__ CA = P.coef32[3];
+  const float* __restrict__ CB = P.coef32[4];
   const float dt = (float)P.dt, inv_dt = (float)(1.0 / P.dt), cp = (float)P.cp, k0 = (float)P.k0;
   const float LLdt = (float)(P.LL / P.dt), VpL = (float)P.VpL, VpoL = (float)(P.Vpdtau / P.L);
   const float LoVp = (float)(P.L / P.Vpdtau), VpLdt = (float)(P.VpL * P.dt);
   const float kn = (float)P.kn;
   const int kmode = P.kmode, km = P.km, khalf = P.khalf;
-  const float pi = 3.14159265358979f;
-  const bool colIn = a >= 0 && a < ni;
-  const bool colGhost = a == -1 || a == ni;
+  const bool colIn = EDGE ? (a >= 0 && a < ni) : true;
   const bool owner = tid >= 1 && tid <= OW && colIn;
-  const bool qx_col = a >= -1 && a <= ni - 1 && tid < TX - 1;
-  const bool qx_own = qx_col && (owner || a == -1);
+  const bool qx_col = EDGE ? (a >= -1 && a <= ni - 1 && tid < TX - 1) : (tid < TX - 1);
+  const bool qx_own = qx_col && (owner || (EDGE && a == -1));
   const int col = a + nh;
 
-  // stage cell (a, r): correction with its ghost rule, base state, diffusivities
-  auto stage = [&](int r) -> MCell {
-    MCell c{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  struct Pre {
+    float d, ub, ab, rho, ex, ey;
+    bool on;
+  };
+  // loads of row r: the correction at the ghost source, the base state and
+  // diffusivity at the cell itself (the restart writes ghosts), old fluxes
+  auto prefetch = [&](int r, Pre& L) {
+    const int ro = col + nx * (r + nh);
+    if (!EDGE) {
+      L.on = true;
+      L.d = din[ro];
+      L.ub = ub[ro];
+      L.ab = abv[ro];
+      L.rho = rho[ro];
+      L.ex = qx_col ? exin[ro] : 0.f;
+      L.ey = eyin[ro - nx];
+      return;
+    }
     bool cst, neg;
     double val;
     const int so = ghost_src(P, a, r, cst, neg, val);
-    if (so == -2) return c;
-    const int o = col + nx * (r + nh);
-    c.d = cst ? 0.f : (neg ? -din[so] : din[so]);  // Dirichlet ghosts carry no correction
-    c.ub = ub[o];                                    // ghost values of u_b written by the restart
-    const float rh = rho[o];
-    const float rc = rh * cp;
-    const float irc = __frcp_rn(rc);
-    const float u = c.ub + c.d;
-    const float kb = k0 * pow_m32(fabsf(c.ub), kmode, km, khalf, kn);
-    c.ab = kb * irc;
-    // Δα = α_b((1 + δ/u_b)ⁿ − 1), accurate relative to the increment
+    L.on = so != -2;
+    L.d = 0.f;
+    L.ub = 0.f;
+    L.ab = 0.f;
+    L.rho = 1.f;
+    if (L.on) {
+      if (!cst) L.d = neg ? -din[so] : din[so];  // Dirichlet ghosts carry no correction
+      L.ub = ub[ro];
+      L.ab = abv[ro];
+      L.rho = rho[ro];
+    }
+    const bool rIn = r >= 0 && r < nj;
+    L.ex = (qx_col && rIn) ? exin[ro] : 0.f;
+    L.ey = (colIn && r >= 0 && r <= nj) ? eyin[ro - nx] : 0.f;
+  };
+  auto stage = [&](const Pre& L) -> MCell {
+    MCell c{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (EDGE && !L.on) return c;
+    c.d = L.d;
+    c.ub = L.ub;
+    c.ab = L.ab;
+    // Δα = α_b((1 + δ/u_b)ⁿ − 1)
     float da = 0.f;
     if (kmode != 0) {
-      const float x = c.d * __frcp_rn(c.ub);
-      da = (fabsf(c.ub) > 1e-30f && isfinite(x)) ? c.ab * incr_pow(x, kmode, km, khalf, kn)
-                                                  : k0 * pow_m32(fabsf(u), kmode, km, khalf, kn) * irc - c.ab;
+      const float x = c.d * rcp_a(c.ub);
+      if (fabsf(c.ub) > 1e-30f && fabsf(x) < 1e30f) da = c.ab * incr_pow32(x, kmode, km, khalf, kn);
+      else da = k0 * pow_m32(fabsf(c.ub + c.d), kmode, km, khalf, kn) * rcp_a(L.rho * cp) - c.ab;
     }
     c.da = da;
-    const float al = c.ab + da;  // α(u) for the pseudo-time parameters
-    const float kap = al * rc;
-    const float Re = pi + sqrtf(pi * pi + LLdt * rh * __frcp_rn(al));
-    const float iD = __frcp_rn(dt * kap * Re + VpL * rc);
-    const float dtau = VpL * __frcp_rn(al * Re);
-    c.f = isfinite(dtau) ? VpLdt * rc * iD : 0.f;
-    if (HARM) c.it = VpoL * Re;
-    else {
-      const float th = LoVp * __frcp_rn(Re);
-      c.it = isfinite(th) ? th : 0.f;
+    // pseudo-time parameters of α(u) = α_b + Δα (iteration_parameters.jl:2-15):
+    // dτΔt/(Δt + dτ) = VpLΔt/(αReΔt + VpL); dτ and θ are 0 where α = 0
+    const float al = c.ab + da;
+    if (al > 0.f) {
+      const float Re = kPiF + sqrt_a(kPiF * kPiF + LLdt * L.rho * rcp_a(al));
+      c.f = VpLdt * rcp_a(fmaf(al * Re, dt, VpL));
+      c.it = HARM ? VpoL * Re : LoVp * rcp_a(Re);
+    } else {
+      c.f = 0.f;
+      c.it = HARM ? __int_as_float(0x7f800000) : 0.f;
     }
     return c;
   };
-  // new flux correction of a face between cells c0 and c1
+  // new flux correction of a face between cells c0 and c1, and its undamped part
   auto face = [&](const MCell& c0, float d1, float ub1, float ab1, float da1, float it1, float eold,
                   float& dqp) -> float {
-    float abar, dabar, en;
+    float en;
     if (HARM) {
       const float s = c0.ab + ab1;
-      const float is = __frcp_rn(s);
-      abar = 2.f * c0.ab * ab1 * is;
-      dabar = 2.f * (ab1 * ab1 * c0.da + c0.ab * c0.ab * da1 + c0.da * da1 * s) * is * __frcp_rn(s + c0.da + da1);
+      const float is = rcp_a(s);
+      const float abar = 2.f * c0.ab * ab1 * is;
+      const float dabar = 2.f * (ab1 * ab1 * c0.da + c0.ab * c0.ab * da1 + c0.da * da1 * s) * is * rcp_a(s + c0.da + da1);
       const float St = c0.it + it1;
       dqp = -((abar + dabar) * (d1 - c0.d) + dabar * (ub1 - c0.ub));
-      en = isfinite(St) ? (2.f * eold + dqp * St) * __frcp_rn(St + 2.f) : dqp;
+      en = fabsf(St) < __int_as_float(0x7f800000) ? (2.f * eold + dqp * St) * rcp_a(St + 2.f) : dqp;
     } else {
-      abar = 0.5f * (c0.ab + ab1);
-      dabar = 0.5f * (c0.da + da1);
+      const float abar = 0.5f * (c0.ab + ab1);
+      const float dabar = 0.5f * (c0.da + da1);
       const float tn = 0.5f * (c0.it + it1);
       dqp = -((abar + dabar) * (d1 - c0.d) + dabar * (ub1 - c0.ub));
-      en = (eold * tn + dqp) * __frcp_rn(1.f + tn);
+      en = (eold * tn + dqp) * rcp_a(1.f + tn);
     }
     return en;
   };
@@ -444,56 +486,61 @@ __global__ void __launch_bounds__(TX) mixed_sweep2d(const Problem* __restrict__ 
     sm.DA[s][tid] = c.da;
     sm.IT[s][tid] = c.it;
   };
-  auto face_x = [&](int r, int s, const MCell& c, float& dqp) -> float {
+  auto face_x = [&](int r, int s, const MCell& c, float eold, float& dqp) -> float {
     dqp = 0.f;
-    if (!(qx_col && r >= 0 && r < nj)) return 0.f;
-    const int o = col + nx * (r + nh);
+    if (!(qx_col && (!EDGE || (r >= 0 && r < nj)))) return 0.f;
     return face(c, sm.D[s][tid + 1], sm.UB[s][tid + 1], sm.AB[s][tid + 1], sm.DA[s][tid + 1], sm.IT[s][tid + 1],
-                exin[o], dqp);
+                eold, dqp);
   };
-  auto face_y = [&](int r, const MCell& lo, const MCell& hi, float& dqp) -> float {
+  auto face_y = [&](int r, const MCell& lo, const MCell& hi, float eold, float& dqp) -> float {
     dqp = 0.f;
-    if (!(colIn && r >= -1 && r <= nj - 1)) return 0.f;
-    const int o = col + nx * (r + nh);
-    return face(lo, hi.d, hi.ub, hi.ab, hi.da, hi.it, eyin[o], dqp);
+    if (!(colIn && (!EDGE || (r >= -1 && r <= nj - 1)))) return 0.f;
+    return face(lo, hi.d, hi.ub, hi.ab, hi.da, hi.it, eold, dqp);
   };
 
   int s_m = 0, s_0 = 1, s_p = 2, y_m = 0, y_0 = 1;
-  MCell cm = stage(j0 - 1), c0 = stage(j0);
+  Pre L0, L1, Ln;
+  prefetch(j0 - 1, L0);
+  prefetch(j0, L1);
+  prefetch(j0 + 1, Ln);
+  const MCell cm = stage(L0);
+  MCell c0 = stage(L1);
   publish(s_m, cm);
   publish(s_0, c0);
   __syncthreads();
   float px_m, px_0, py_m;
-  float rqx_m = face_x(j0 - 1, s_m, cm, px_m);
-  float rqx_0 = face_x(j0, s_0, c0, px_0);
-  float rqy_m = face_y(j0 - 1, cm, c0, py_m);
+  float rqx_m = face_x(j0 - 1, s_m, cm, L0.ex, px_m);
+  float rqx_0 = face_x(j0, s_0, c0, L1.ex, px_0);
+  float rqy_m = face_y(j0 - 1, cm, c0, L1.ey, py_m);
   sm.EX[s_m][tid] = rqx_m;
   sm.PX[s_m][tid] = px_m;
   sm.EX[s_0][tid] = rqx_0;
   sm.PX[s_0][tid] = px_0;
   sm.EY[y_m][tid] = rqy_m;
   sm.PY[y_m][tid] = py_m;
-  if (j0 == 0 && owner) eyout[col + nx * (nh - 1)] = rqy_m;
+  if (EDGE && j0 == 0 && owner) eyout[col + nx * (nh - 1)] = rqy_m;
   float rpx_m = px_m, rpx_0 = px_0, rpy_m = py_m;
-  double local = 0.0;
+  float local = 0.f;
   bool nan = false;
   for (int j = j0; j < j1; ++j) {
+    const Pre Lc = Ln;
+    if (j + 1 < j1) prefetch(j + 2, Ln);
     const int o = col + nx * (j + nh);
     float g11 = 0, g22 = 0, c12 = 0, ca = 0, cbv = 0, R = 0;
     if (owner) {
-      g11 = P.coef32[0][o];
-      g22 = P.coef32[1][o];
-      c12 = P.coef32[2][o];
-      ca = P.coef32[3][o];
-      cbv = P.coef32[4][o];
+      g11 = G11[o];
+      g22 = G22[o];
+      c12 = C12[o];
+      ca = CA[o];
+      cbv = CB[o];
       R = Rb[o];
     }
-    const MCell cp1 = stage(j + 1);
+    const MCell cp1 = stage(Lc);
     publish(s_p, cp1);
     __syncthreads();
     float px_p1, py_0n;
-    const float qx_p1 = face_x(j + 1, s_p, cp1, px_p1);
-    const float qy_0n = face_y(j, c0, cp1, py_0n);
+    const float qx_p1 = face_x(j + 1, s_p, cp1, Lc.ex, px_p1);
+    const float qy_0n = face_y(j, c0, cp1, Lc.ey, py_0n);
     sm.EX[s_p][tid] = qx_p1;
     sm.PX[s_p][tid] = px_p1;
     sm.EY[y_0][tid] = qy_0n;
@@ -513,10 +560,9 @@ __global__ void __launch_bounds__(TX) mixed_sweep2d(const Problem* __restrict__ 
                           c12 * ((px_p1 + sm.PX[s_p][x - 1]) - (rpx_m + sm.PX[s_m][x - 1])) +
                           c12 * ((sm.PY[y_0][x + 1] + sm.PY[y_m][x + 1]) - (sm.PY[y_0][x - 1] + sm.PY[y_m][x - 1])) +
                           ca * (0.5f * (rpx_0 + sm.PX[s_0][x - 1])) + cbv * (0.5f * (py_0n + rpy_m));
-        const float r = R - dn * inv_dt - dqp;
-        const float ar = fabsf(r);
+        const float ar = fabsf(R - dn * inv_dt - dqp);
         if (ar != ar) nan = true;
-        else local = fmax(local, (double)ar);
+        else local = fmaxf(local, ar);
       }
     }
     if (qx_own) exout[o] = rqx_0;
@@ -535,28 +581,112 @@ __global__ void __launch_bounds__(TX) mixed_sweep2d(const Problem* __restrict__ 
     y_m = y_0;
     y_0 = u2;
   }
-  (void)cm;
   // arrival; the last block advances the inner counters and, on check
   // iterations, publishes max|r| and the end of the cycle
   if (check) {
-    reduce_and_publish<TX>(P, C, tile, local, nan, sm.red, &sm.flag, false);
+    reduce_and_publish<TX>(P, C, tile, (double)local, nan, sm.red, &sm.flag, false);
     if (threadIdx.x == 0 && sm.flag) {
       C->inner_iter = k;
       C->iter += 1;
       __threadfence();
     }
-  } else {
-    if (threadIdx.x == 0) {
+  } else if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned prev = atomicAdd(&C->arrive, 1u);
+    if (prev == (unsigned)P.ntiles - 1u) {
+      C->arrive = 0u;
+      C->inner_iter = k;
+      C->iter += 1;
       __threadfence();
-      const unsigned prev = atomicAdd(&C->arrive, 1u);
-      if (prev == (unsigned)P.ntiles - 1u) {
-        C->arrive = 0u;
-        C->inner_iter = k;
-        C->iter += 1;
-        __threadfence();
-      }
     }
   }
+}
+
+// Boundary strips: one block per strip.
+template <int TX, bool HARM>
+__global__ void __launch_bounds__(TX, 4) mixed_sweep2d_edge(const Problem* __restrict__ probs,
+                                                            const int2* __restrict__ items) {
+  __shared__ MixSmem<TX> sm;
+  const int2 item = items[blockIdx.x];
+  const Problem& P = probs[item.x];
+  Ctrl* C = P.ctrl;
+  if (ld_cg_int(&C->inner_done) || ld_cg_int(&C->done)) return;
+  const int k = ld_cg_int(&C->inner_iter) + 1;  // inner iteration of this cycle
+  mixed_body<TX, true, HARM>(P, C, item.y, k, (k % C->inner_check_every) == 0, sm);
+}
+
+// Interior strips: persistent blocks claim strips from counters[0] until
+// `nitems` are taken; the last block to leave resets the counters.
+template <int TX, bool HARM>
+__global__ void __launch_bounds__(TX, 6) mixed_sweep2d_inner(const Problem* __restrict__ probs,
+                                                             const int2* __restrict__ items, int nitems,
+                                                             unsigned int* counters) {
+  __shared__ MixSmem<TX> sm;
+  while (true) {
+    if (threadIdx.x == 0) sm.ticket = (int)atomicAdd(&counters[0], 1u);
+    __syncthreads();
+    const int t = sm.ticket;
+    __syncthreads();
+    if (t >= nitems) break;
+    const int2 item = items[t];
+    const Problem& P = probs[item.x];
+    Ctrl* C = P.ctrl;
+    if (ld_cg_int(&C->inner_done) || ld_cg_int(&C->done)) continue;
+    const int k = ld_cg_int(&C->inner_iter) + 1;
+    mixed_body<TX, false, HARM>(P, C, item.y, k, (k % C->inner_check_every) == 0, sm);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned prev = atomicAdd(&counters[1], 1u);
+    if (prev == gridDim.x - 1) {
+      counters[0] = 0u;
+      counters[1] = 0u;
+      __threadfence();
+    }
+  }
+}
+
+template <int TX, bool HARM>
+static int mixed_inner_grid(int nitems) {
+  static int per_sm = -1, nsm = 0;
+  if (per_sm < 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_sweep2d_inner<TX, HARM>, TX, 0);
+    if (per_sm < 1) per_sm = 1;
+  }
+  const int g = nsm * per_sm;
+  return nitems < g ? nitems : g;
+}
+
+// one FP32 sweep: boundary strips on the side stream, interior strips on the
+// main stream, joined before the next sweep
+template <int TX, bool HARM>
+static cudaError_t launch_mixed_pair(const Problem* probs, const int2* items, int n_edge, int n_int,
+                                     unsigned int* counters, const SweepStreams& ss) {
+  const bool fork = n_edge > 0 && n_int > 0 && ss.side != nullptr;
+  cudaError_t e = cudaSuccess;
+  if (fork) {
+    if ((e = cudaEventRecord(ss.ev_fork, ss.main)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(ss.side, ss.ev_fork, 0)) != cudaSuccess) return e;
+  }
+  if (n_edge > 0) mixed_sweep2d_edge<TX, HARM><<<n_edge, TX, 0, fork ? ss.side : ss.main>>>(probs, items);
+  if (n_int > 0)
+    mixed_sweep2d_inner<TX, HARM><<<mixed_inner_grid<TX, HARM>(n_int), TX, 0, ss.main>>>(probs, items + n_edge,
+                                                                                          n_int, counters);
+  if (fork) {
+    if ((e = cudaEventRecord(ss.ev_join, ss.side)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(ss.main, ss.ev_join, 0)) != cudaSuccess) return e;
+  }
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_mixed_sweep(bool harmonic, const Problem* probs, const int2* items, int n_edge, int n_int,
+                                      unsigned int* counters, const SweepStreams& ss) {
+  return harmonic ? launch_mixed_pair<128, true>(probs, items, n_edge, n_int, counters, ss)
+                  : launch_mixed_pair<128, false>(probs, items, n_edge, n_int, counters, ss);
 }
 
 // FP32 copies of the metric coefficients and of rho
@@ -585,6 +715,7 @@ int Engine::mixed_alloc() {
     CDM_CK(cudaMalloc((void**)&s.ub64[b], N * sizeof(double)));
   }
   CDM_CK(fa(&s.ub32));
+  CDM_CK(fa(&s.ab32));
   CDM_CK(fa(&s.R32));
   CDM_CK(fa(&s.rho32));
   for (int k = 0; k < 5; ++k) {
@@ -637,6 +768,7 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
     io.d_in = d;
     io.ub_out = out;
     io.ub32 = s.ub32;
+    io.ab32 = s.ab32;
     io.R32 = s.R32;
     for (int c = 0; c < 2; ++c) {
       io.e_in[c] = ecur >= 0 ? s.e32[ecur][c] : nullptr;
@@ -678,11 +810,10 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
     if (!mixed_graph) {
       cudaGraph_t g;
       CDM_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-      for (int k = 0; k < K; ++k) {
-        if (mean == CDM_MEAN_HARMONIC) mixed_sweep2d<128, true><<<nitems, 128, 0, stream>>>(d_probs, d_items);
-        else mixed_sweep2d<128, false><<<nitems, 128, 0, stream>>>(d_probs, d_items);
-      }
-      cudaError_t le = cudaGetLastError();
+      cudaError_t le = cudaSuccess;
+      for (int k = 0; k < K && le == cudaSuccess; ++k)
+        le = launch_mixed_sweep(mean == CDM_MEAN_HARMONIC, d_probs, d_items, n_edge, nitems - n_edge, d_counters,
+                                sweep_streams());
       cudaError_t ce = cudaStreamEndCapture(stream, &g);
       CDM_CK(le);
       CDM_CK(ce);
@@ -698,11 +829,9 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
         done += K;
         prof.sweep_launches += K;
       } else {
-        for (int k = 0; k < n - done; ++k) {
-          if (mean == CDM_MEAN_HARMONIC) mixed_sweep2d<128, true><<<nitems, 128, 0, stream>>>(d_probs, d_items);
-          else mixed_sweep2d<128, false><<<nitems, 128, 0, stream>>>(d_probs, d_items);
-          CDM_CK(cudaGetLastError());
-        }
+        for (int k = 0; k < n - done; ++k)
+          CDM_CK(launch_mixed_sweep(mean == CDM_MEAN_HARMONIC, d_probs, d_items, n_edge, nitems - n_edge, d_counters,
+                                    sweep_streams()));
         prof.sweep_launches += n - done;
         done = n;
       }
