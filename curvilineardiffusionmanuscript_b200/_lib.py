@@ -76,7 +76,19 @@ class Profile(C.Structure):
                 ("cell_iters", C.c_int64), ("fp32_cell_iters", C.c_int64), ("fp64_cell_evals", C.c_int64)]
 
 
-# every symbol declared in include/cdm_apt.h: name -> (restype, argtypes)
+class NetBatch(C.Structure):
+    """cdm_net_batch (include/cdm_net.h)."""
+    _fields_ = [
+        ("nsamp", C.c_int), ("tprev", C.POINTER(C.c_void_p)), ("tcur", C.POINTER(C.c_void_p)),
+        ("tnext", C.POINTER(C.c_void_p)), ("J", C.c_void_p), ("ox", C.POINTER(C.c_int)), ("oy", C.POINTER(C.c_int)),
+        ("crop", C.c_int), ("ni", C.c_int), ("nj", C.c_int), ("nhalo", C.c_int), ("k0", C.c_double),
+        ("kn", C.c_double), ("log_jmean", C.c_double),
+    ]
+
+
+PF = C.POINTER(C.c_float)
+
+# every symbol declared in include/cdm_apt.h and include/cdm_net.h: name -> (restype, argtypes)
 SIGNATURES = {
     "cdm_apt_version": (C.c_int, []),
     "cdm_apt_last_error": (C.c_char_p, []),
@@ -102,6 +114,18 @@ SIGNATURES = {
     "cdm_apt_get_profile": (C.c_int, [C.c_void_p, C.POINTER(Profile)]),
     "cdm_batch_get_profile": (C.c_int, [C.c_void_p, C.POINTER(Profile)]),
     "cdm_step_reductions_noalloc": (C.c_int, [C.c_int] * 5 + [C.c_void_p] * 5 + [C.c_double] * 5 + [PD, C.c_void_p]),
+    "cdm_net_create": (C.c_int, [C.c_int, C.c_uint64, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "cdm_net_destroy": (C.c_int, [C.c_void_p]),
+    "cdm_net_num_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "cdm_net_get_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "cdm_net_set_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "cdm_net_get_grads": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "cdm_net_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "cdm_net_backward": (C.c_int, [C.c_void_p, C.c_void_p, PF]),
+    "cdm_net_train_step": (C.c_int, [C.c_void_p, C.POINTER(NetBatch), C.c_float, PF]),
+    "cdm_net_predict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                  C.c_double, C.c_double, C.c_double, C.c_void_p]),
+    "cdm_apt_set_guess_net": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double]),
 }
 
 _lib = None

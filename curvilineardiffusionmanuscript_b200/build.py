@@ -33,6 +33,8 @@ UNITS = {
     "apt_mixed.cu": [],
     "apt_noalloc.cu": ["-fmad=false"],
     "autotune.cu": [],
+    "net_kernels.cu": [],
+    "net.cu": [],
 }
 
 

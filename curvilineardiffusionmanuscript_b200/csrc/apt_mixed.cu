@@ -306,6 +306,56 @@ __global__ void __launch_bounds__(RNT) mixed_restart2d(const Problem* __restrict
 }
 
 // ---------------------------------------------------------------------------
+// Damped flux consistent with a guessed start: at a converged step the damped
+// flux equals the plain one (q = q′(u) is the fixed point of fluxes.jl:5-16),
+// so a start from u₀ ≠ Tⁿ takes q = q′(u₀) = −ᾱ·Δu₀ on every face the sweeps
+// read, with α from u₀ (as at iteration 1) and ghosts by the side rules.
+__global__ void flux_init2d(Problem P, const double* __restrict__ u, double* __restrict__ qx,
+                            double* __restrict__ qy) {
+  const int64_t nfx = (int64_t)(P.ni + 1) * P.nj;  // x faces: a = -1..ni-1, b = 0..nj-1
+  const int64_t nfy = (int64_t)P.ni * (P.nj + 1);  // y faces: a = 0..ni-1, b = -1..nj-1
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nfx + nfy;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    int as[2], bs[2];
+    double* out;
+    if (e < nfx) {
+      as[0] = (int)(e % (P.ni + 1)) - 1;
+      bs[0] = (int)(e / (P.ni + 1));
+      as[1] = as[0] + 1;
+      bs[1] = bs[0];
+      out = qx;
+    } else {
+      const int64_t f = e - nfx;
+      as[0] = (int)(f % P.ni);
+      bs[0] = (int)(f / P.ni) - 1;
+      as[1] = as[0];
+      bs[1] = bs[0] + 1;
+      out = qy;
+    }
+    double uu[2], al[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      bool cst, neg;
+      double val;
+      const int so = ghost_src(P, as[k], bs[k], cst, neg, val);
+      double v = so >= 0 ? u[so] : val;
+      if (neg) v = -v;
+      uu[k] = v;
+      const double kap = isfinite(v) ? P.k0 * pow_m64(fabs(v), P.kmode, P.km, P.khalf, P.kn) : 0.0;
+      al[k] = kap / (P.rho[off2m(P, as[k], bs[k])] * P.cp);
+    }
+    out[off2m(P, as[0], bs[0])] = -face_mean(P.mean, al[0], al[1]) * (uu[1] - uu[0]);
+  }
+}
+
+cudaError_t launch_flux_init2d(const Problem& P, const double* u, double* qx, double* qy, cudaStream_t s) {
+  const int64_t n = (int64_t)(P.ni + 1) * P.nj + (int64_t)P.ni * (P.nj + 1);
+  const int64_t g = (n + 255) / 256;
+  flux_init2d<<<(int)(g < 148 * 16 ? g : 148 * 16), 256, 0, s>>>(P, u, qx, qy);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // FP32 correction sweep, row-marching (the layout of apt_march2d_fast.cu): a
 // block of TX threads owns TX-2 columns of a strip of rows, keeps its own
 // column in registers, passes neighbour values through shared memory and
@@ -793,7 +843,7 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
   auto check = [&](bool first) -> int {
     const double L2 = Ch.restart_nan ? NAN : Ch.restart_L2 / Ch.sqrtN;
     Ch.n_checks += 1;
-    if (first) init_L2 = L2;
+    if (first) init_L2 = Ch.init_fixed ? Ch.init_L2 : L2;
     rel = L2 / init_L2;
     ab = L2;
     if (!std::isfinite(rel) || !std::isfinite(ab)) return ST_NONFINITE;
@@ -868,7 +918,9 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
     // cycle need not go below the larger of the two thresholds (in max|R| units)
     double target = 1e-3 * Rmax;
     double floor_t = tolmax_abs;
-    if (!first && std::isfinite(init_L2)) floor_t = std::max(floor_t, o->rtol * init_L2 * Ch.sqrtN);
+    if (Ch.init_fixed && first) init_L2 = Ch.init_L2;
+    if ((!first || Ch.init_fixed) && std::isfinite(init_L2))
+      floor_t = std::max(floor_t, o->rtol * init_L2 * Ch.sqrtN);
     target = std::max(target, 0.5 * floor_t);
     Ch.inner_target = target;
     Ch.inner_done = 0;

@@ -36,7 +36,7 @@ struct Ctrl {
   unsigned int arrive;  // blocks of the current iteration that finished
   int n_checks;
   int abad[2];          // diffusivity validity bits of the last two iterations
-  int pad;
+  int init_fixed;       // 1: init_L2 was set before the loop (guessed start)
   double sqrtN;         // sqrt(length(res)) over the full array
   double nfull;
   // mixed precision bookkeeping

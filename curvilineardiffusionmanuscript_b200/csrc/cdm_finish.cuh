@@ -72,7 +72,7 @@ __device__ __forceinline__ void finish_iteration(const Problem& P, Ctrl* C, int 
     // PseudoTransientSolver.jl:284-318
     if (check) {
       C->n_checks += 1;
-      if (iter == 1) C->init_L2 = L2;
+      if (iter == 1 && !C->init_fixed) C->init_L2 = L2;
       C->rel = L2 / C->init_L2;
       C->abs = L2;
     }

@@ -103,6 +103,7 @@ Engine::~Engine() {
     dfree(s.cellJ);
     dfree(s.partial);
     dfree(s.guess);
+    dfree(s.t_hist);
     dfree(s.ub32);
     dfree(s.ab32);
     dfree(s.R32);
@@ -609,6 +610,63 @@ int Engine::run_iterations(const cdm_step_opts* o, int predicted, double t_start
   }
 }
 
+// Network prediction of this step's solution from (Tⁿ⁻¹, Tⁿ, κ, J): 1 when
+// s.guess holds it, 0 when the step starts from Tⁿ (no network, no previous
+// step, 3D, or sizes the network does not take), negative on error
+// (-1 CUDA error, otherwise minus the network's status).
+int Engine::learned_guess(int p, const cdm_kappa& kappa) {
+  ProbState& s = ps[p];
+  if (!guess_net || !s.has_hist || ndim != 2 || s.ni % 8 || s.nj % 8 || !s.cellJ) return 0;
+  if (!s.guess && dalloc(&s.guess, (size_t)s.nfull) != cudaSuccess) return -1;
+  if (cudaStreamSynchronize(stream) != cudaSuccess) return -1;  // Tⁿ staged
+  const int rc = cdm_net_predict(guess_net, s.t_hist, s.u_prev, s.cellJ, s.ni, s.nj, s.nh, kappa.k0, kappa.n,
+                                 log_jmean, s.guess);
+  if (rc != CDM_OK) return -rc;
+  prof.other_launches += 22;
+  return 1;
+}
+
+// A guessed start is stopped where the plain start would stop: the relative
+// criterion (:297) divides by the residual norm that the plain start (u = Tⁿ)
+// reaches at its first check.  One FP64 iteration from Tⁿ gives that norm;
+// then the control block is reset, the iterates are set to the guess and, in
+// 2D, the damped flux to the plain flux of the guess.
+int Engine::probe_plain_norm(const std::vector<int>& guessed, const std::vector<const double*>& init,
+                             double t_start, double timeout_s) {
+  const int nprob = (int)ps.size();
+  std::vector<Ctrl> c0(h_ctrl, h_ctrl + nprob);
+  int rc = launch_block(1, false);
+  if (rc != CDM_OK) return rc;
+  CDM_CK(cudaMemcpyAsync(h_ctrl, d_ctrl, sizeof(Ctrl) * nprob, cudaMemcpyDeviceToHost, stream));
+  rc = wait_stream(timeout_s - (now_seconds() - t_start));
+  if (rc != CDM_OK) return rc;
+  for (int p = 0; p < nprob; ++p) {
+    ProbState& s = ps[p];
+    const double ref = h_ctrl[p].init_L2;
+    h_ctrl[p] = c0[p];
+    if (guessed[p]) {
+      h_ctrl[p].init_L2 = ref;
+      h_ctrl[p].init_fixed = 1;
+    }
+    prof.cell_iters += s.ndomain;
+    const size_t bytes = (size_t)s.nfull * sizeof(double);
+    CDM_CK(cudaMemcpyAsync(s.u[0], init[p], bytes, cudaMemcpyDeviceToDevice, stream));
+    CDM_CK(cudaMemcpyAsync(s.u[1], init[p], bytes, cudaMemcpyDeviceToDevice, stream));
+    if (ndim == 2 && s.nh > 1) {
+      CDM_CK(launch_dirichlet_fill(hp[p], s.u[0], stream));
+      CDM_CK(launch_dirichlet_fill(hp[p], s.u[1], stream));
+      prof.other_launches += 2;
+    }
+    if (guessed[p] && ndim == 2) {
+      CDM_CK(launch_flux_init2d(hp[p], s.u[0], s.q[s.qpar][0], s.q[s.qpar][1], stream));
+      prof.other_launches += 1;
+    }
+  }
+  CDM_CK(cudaMemsetAsync(d_counters, 0, 2 * sizeof(unsigned int), stream));
+  CDM_CK(cudaMemcpyAsync(d_ctrl, h_ctrl, sizeof(Ctrl) * nprob, cudaMemcpyHostToDevice, stream));
+  return CDM_OK;
+}
+
 int Engine::step(double* const* T, const double* const* rho, const double* cp, const cdm_kappa* kappa,
                  const double* dt, const cdm_step_opts* opts, cdm_stats* stats, double* next_dt) {
   const double t0 = now_seconds();
@@ -653,6 +711,9 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
   }
   // T and rho may still be written by the caller's kernels
   CDM_CK(fence_caller());
+  std::vector<const double*> inits(nprob, nullptr);
+  std::vector<int> guessed(nprob, 0);
+  bool any_guess = false;
   for (int p = 0; p < nprob; ++p) {
     ProbState& s = ps[p];
     Problem& P = hp[p];
@@ -660,9 +721,21 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
     const size_t bytes = (size_t)s.nfull * sizeof(double);
     // copy!(solver.u, T); copy!(solver.u_prev, T)  (:229-230)
     CDM_CK(stage_in(s.u_prev, T[p], s.nfull, o.mem, stream));
-    const double* init = (o.guess == CDM_GUESS_USER && s.has_guess) ? s.guess : s.u_prev;
-    CDM_CK(cudaMemcpyAsync(s.u[0], init, bytes, cudaMemcpyDeviceToDevice, stream));
-    CDM_CK(cudaMemcpyAsync(s.u[1], init, bytes, cudaMemcpyDeviceToDevice, stream));
+    // the iteration starts from Tⁿ (:229), a user array, or the network's prediction
+    const double* init = s.u_prev;
+    if (o.guess == CDM_GUESS_USER && s.has_guess) {
+      init = s.guess;
+    } else if (o.guess == CDM_GUESS_LEARNED) {
+      const int lg = learned_guess(p, kappa[p]);
+      if (lg < 0) return lg == -1 ? CDM_CUDA_ERROR : -lg;
+      if (lg == 1) init = s.guess;
+    }
+    inits[p] = init;
+    guessed[p] = init != s.u_prev;
+    any_guess = any_guess || guessed[p];
+    // a guessed start first runs the plain start's first iteration (probe below)
+    CDM_CK(cudaMemcpyAsync(s.u[0], s.u_prev, bytes, cudaMemcpyDeviceToDevice, stream));
+    CDM_CK(cudaMemcpyAsync(s.u[1], s.u_prev, bytes, cudaMemcpyDeviceToDevice, stream));
     const double* rp = rho[p];
     if (o.mem != CDM_MEM_DEVICE) {
       if (!s.rho_buf) CDM_CK(dalloc(&s.rho_buf, (size_t)s.nfull));
@@ -746,9 +819,12 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
   CDM_CK(cudaMemcpyAsync(d_probs, hp.data(), sizeof(Problem) * nprob, cudaMemcpyHostToDevice, stream));
   CDM_CK(cudaMemsetAsync(d_counters, 0, 2 * sizeof(unsigned int), stream));
   CDM_CK(cudaMemcpyAsync(d_ctrl, h_ctrl, sizeof(Ctrl) * nprob, cudaMemcpyHostToDevice, stream));
-  int rc;
-  if (precision == CDM_PREC_MIXED) rc = step_mixed(&o, t0, timeout_s);
-  else rc = run_iterations(&o, predicted, t0, timeout_s);
+  int rc = CDM_OK;
+  if (any_guess) rc = probe_plain_norm(guessed, inits, t0, timeout_s);
+  if (rc == CDM_OK) {
+    if (precision == CDM_PREC_MIXED) rc = step_mixed(&o, t0, timeout_s);
+    else rc = run_iterations(&o, predicted, t0, timeout_s);
+  }
   if (rc != CDM_OK) {
     for (int p = 0; p < nprob; ++p) {
       stats[p].status = rc;
@@ -778,6 +854,13 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
       continue;
     }
     s.last_err_check = C.iter;
+    // Tⁿ becomes the previous step of the next call's learned guess
+    if (guess_net) {
+      if (!s.t_hist) CDM_CK(dalloc(&s.t_hist, (size_t)s.nfull));
+      CDM_CK(cudaMemcpyAsync(s.t_hist, s.u_prev, (size_t)s.nfull * sizeof(double), cudaMemcpyDeviceToDevice,
+                             stream));
+      s.has_hist = 1;
+    }
     // result: the last ping-pong iterate (FP64 path) or the last restart's base (mixed)
     double* res = precision == CDM_PREC_MIXED ? s.ub64[(C.n_restarts - 1) & 1] : s.u[C.iter & 1];
     CDM_CK(launch_clamp(res, s.nfull, o.enforce_positivity, o.apply_cutoff, stream));
@@ -909,6 +992,15 @@ int cdm_apt_step(cdm_apt* h, double* T, const double* rho, double cp, cdm_kappa 
 int cdm_apt_set_guess(cdm_apt* h, const double* u0, int mem) {
   if (!h || !u0) return CDM_BAD_INPUT;
   return h->e.set_guess(0, u0, mem);
+}
+
+int cdm_apt_set_guess_net(cdm_apt* h, cdm_net* net, double log_jmean) {
+  if (!h) return CDM_BAD_INPUT;
+  h->e.guess_net = net;
+  h->e.log_jmean = log_jmean;
+  if (!net)
+    for (auto& s : h->e.ps) s.has_hist = 0;
+  return CDM_OK;
 }
 
 int cdm_apt_get_state(cdm_apt* h, double* q, int* last_err_check) {

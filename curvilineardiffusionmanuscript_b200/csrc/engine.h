@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "cdm_apt.h"
+#include "cdm_net.h"
 #include "cdm_device.cuh"
 #include "cdm_kernels.h"
 
@@ -25,6 +26,8 @@ void set_error(const std::string& msg);
   } while (0)
 
 // Host bookkeeping of one problem.
+cudaError_t launch_flux_init2d(const Problem& P, const double* u, double* qx, double* qy, cudaStream_t s);
+
 struct ProbState {
   int ndim = 2, ni = 0, nj = 0, nk = 1, nh = 1;
   int64_t nfull = 0, ndomain = 0;
@@ -49,6 +52,8 @@ struct ProbState {
   int qpar = 0;
   int s_bad = 0;
   int has_guess = 0;
+  double* t_hist = nullptr;  // Tⁿ of the previous step (learned guess input)
+  int has_hist = 0;
   // mixed precision buffers
   float* d32[2] = {nullptr, nullptr};
   float* e32[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
@@ -65,6 +70,8 @@ struct Engine {
   int device = 0;
   int mean = 0;
   int precision = 0;
+  cdm_net* guess_net = nullptr;  // attached learned-guess network (not owned)
+  double log_jmean = 0.0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int variant = 0;
@@ -115,6 +122,9 @@ struct Engine {
   // mixed precision (apt_mixed.cu)
   int mixed_alloc();
   int step_mixed(const cdm_step_opts* o, double t_start, double timeout_s);
+  int learned_guess(int p, const cdm_kappa& kappa);
+  int probe_plain_norm(const std::vector<int>& guessed, const std::vector<const double*>& init, double t_start,
+                       double timeout_s);
 };
 
 int resolve_ghost_rules(int ndim, const cdm_bc* bcs, int* rule, double* val);

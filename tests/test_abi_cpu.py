@@ -49,8 +49,9 @@ def test_struct_layout_matches_header():
     src = r'''
 #include <stdio.h>
 #include "cdm_apt.h"
-int main(void){printf("%zu %zu %zu %zu %zu %zu\n", sizeof(cdm_mesh_desc), sizeof(cdm_step_opts),
- sizeof(cdm_stats), sizeof(cdm_apt_config), sizeof(cdm_bc), sizeof(cdm_kappa));return 0;}
+#include "cdm_net.h"
+int main(void){printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(cdm_mesh_desc), sizeof(cdm_step_opts),
+ sizeof(cdm_stats), sizeof(cdm_apt_config), sizeof(cdm_bc), sizeof(cdm_kappa), sizeof(cdm_net_batch));return 0;}
 '''
     with tempfile.TemporaryDirectory() as d:
         p = os.path.join(d, "s.c")
@@ -60,7 +61,7 @@ int main(void){printf("%zu %zu %zu %zu %zu %zu\n", sizeof(cdm_mesh_desc), sizeof
         sizes = [int(x) for x in subprocess.run([exe], capture_output=True, text=True).stdout.split()]
     from curvilineardiffusionmanuscript_b200 import _lib
     assert sizes == [C.sizeof(_lib.MeshDesc), C.sizeof(_lib.StepOpts), C.sizeof(_lib.Stats),
-                     C.sizeof(_lib.Config), C.sizeof(_lib.BC), C.sizeof(_lib.Kappa)]
+                     C.sizeof(_lib.Config), C.sizeof(_lib.BC), C.sizeof(_lib.Kappa), C.sizeof(_lib.NetBatch)]
 
 
 def test_create_without_device_reports_error():
@@ -71,4 +72,8 @@ def test_create_without_device_reports_error():
     from curvilineardiffusionmanuscript_b200 import APTError, NeumannBC, PseudoTransientSolver, wavy_mesh_2d
     with pytest.raises(APTError) as ei:
         PseudoTransientSolver(wavy_mesh_2d(8, 8), [NeumannBC()] * 4)
+    assert ei.value.status in (4, 6)
+    from curvilineardiffusionmanuscript_b200.learned import GuessNet
+    with pytest.raises(APTError) as ei:
+        GuessNet(seed=0)
     assert ei.value.status in (4, 6)
