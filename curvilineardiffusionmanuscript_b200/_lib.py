@@ -82,7 +82,7 @@ class NetBatch(C.Structure):
         ("nsamp", C.c_int), ("tprev", C.POINTER(C.c_void_p)), ("tcur", C.POINTER(C.c_void_p)),
         ("tnext", C.POINTER(C.c_void_p)), ("J", C.c_void_p), ("ox", C.POINTER(C.c_int)), ("oy", C.POINTER(C.c_int)),
         ("crop", C.c_int), ("ni", C.c_int), ("nj", C.c_int), ("nhalo", C.c_int), ("k0", C.c_double),
-        ("kn", C.c_double), ("log_jmean", C.c_double),
+        ("kn", C.c_double), ("log_jmean", C.c_double), ("dt", C.c_double), ("rho_cp", C.c_double),
     ]
 
 
@@ -117,6 +117,7 @@ SIGNATURES = {
     "cdm_net_create": (C.c_int, [C.c_int, C.c_uint64, C.c_void_p, C.POINTER(C.c_void_p)]),
     "cdm_net_destroy": (C.c_int, [C.c_void_p]),
     "cdm_net_num_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "cdm_net_set_guess_smoothing": (C.c_int, [C.c_void_p, C.c_int]),
     "cdm_net_get_params": (C.c_int, [C.c_void_p, C.c_void_p]),
     "cdm_net_set_params": (C.c_int, [C.c_void_p, C.c_void_p]),
     "cdm_net_get_grads": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -45,7 +45,10 @@ class Net {
   std::vector<void*> allocs;
   __nv_bfloat16 *X = nullptr, *A0, *S0, *U0, *D0, *P1, *S1, *U1, *D1, *P2, *S2, *U2, *D2, *P3, *B3;
   __nv_bfloat16 *gY = nullptr, *ga[4], *gb[4];
-  float *Y = nullptr, *target = nullptr, *d_loss = nullptr;
+  float *Y = nullptr, *target = nullptr, *weight = nullptr, *d_loss = nullptr;
+  float *sm0 = nullptr, *sm1 = nullptr;  // smoothing of the predicted correction
+  int smooth_passes = 8;
+  bool use_weight = false;
   // training batch scratch
   double* d_scale = nullptr;
   const double** d_ptrs = nullptr;  // tprev, tcur, tnext arrays (3 x cap)
@@ -166,6 +169,9 @@ class Net {
     CDM_CK(alloc(&gY, n0 * 16));
     CDM_CK(alloc(&Y, n0 * 16));
     CDM_CK(alloc(&target, n0));
+    CDM_CK(alloc(&weight, n0));
+    CDM_CK(alloc(&sm0, n0));
+    CDM_CK(alloc(&sm1, n0));
     CDM_CK(alloc(&A0, n[0] * c));
     CDM_CK(alloc(&S0, n[0] * c));
     CDM_CK(alloc(&U0, n[0] * c));
@@ -266,7 +272,7 @@ class Net {
     const int64_t npix = (int64_t)B * H * W;
     CDM_CK(cudaMemsetAsync(grads, 0, nparams * sizeof(float), stream));
     CDM_CK(cudaMemsetAsync(d_loss, 0, sizeof(float), stream));
-    CDM_CK(loss_grad(Y, target, gY, npix, d_loss, stream));
+    CDM_CK(loss_grad(Y, target, use_weight ? weight : nullptr, gY, npix, d_loss, stream));
     CDM_CK(wgrad(8, D0, gY, 0));
     CDM_CK(conv_bwd(8, gY, ga[0], 0, D0));                              // gD0
     CDM_CK(wgrad(7, U0, ga[0], 0));
@@ -354,6 +360,12 @@ int cdm_net_destroy(cdm_net* net) {
   return CDM_OK;
 }
 
+int cdm_net_set_guess_smoothing(cdm_net* net, int passes) {
+  if (!net || passes < 0 || passes > 1024) return CDM_BAD_INPUT;
+  net->n.smooth_passes = passes;
+  return CDM_OK;
+}
+
 int cdm_net_num_params(const cdm_net* net, int64_t* n) {
   if (!net || !n) return CDM_BAD_INPUT;
   *n = net->n.nparams;
@@ -413,6 +425,7 @@ int cdm_net_backward(cdm_net* net, const float* target, float* loss) {
   CDM_CK(cudaSetDevice(n.device));
   const size_t np = (size_t)n.B * n.H * n.W;
   CDM_CK(cudaMemcpyAsync(n.target, target, np * sizeof(float), cudaMemcpyDeviceToDevice, n.stream));
+  n.use_weight = false;
   int rc = n.backward();
   if (rc != CDM_OK) return rc;
   *loss = n.read_loss();
@@ -473,11 +486,15 @@ int cdm_net_train_step(cdm_net* net, const cdm_net_batch* bt, float lr, float* l
   fa.k0 = bt->k0;
   fa.kn = bt->kn;
   fa.log_jmean = bt->log_jmean;
+  fa.dt = bt->dt;
+  fa.rho_cp = bt->rho_cp > 0.0 ? bt->rho_cp : 1.0;
   fa.x = n.X;
   fa.target = n.target;
+  fa.weight = n.weight;
   CDM_CK(cdm::net::features(fa, n.stream));
   rc = n.forward();
   if (rc != CDM_OK) return rc;
+  n.use_weight = bt->dt > 0.0;
   rc = n.backward();
   if (rc != CDM_OK) return rc;
   rc = n.adam_step(lr);
@@ -523,8 +540,19 @@ int cdm_net_predict(cdm_net* net, const double* tprev, const double* tcur, const
   CDM_CK(cdm::net::features(fa, n.stream));
   rc = n.forward();
   if (rc != CDM_OK) return rc;
+  // the correction over linear extrapolation, smoothed: grid-scale noise of the
+  // bf16 activations would enter the step's residual amplified by the local
+  // diffusion number
+  const float* y = n.Y;
+  int ystride = 16;
+  for (int k = 0; k < n.smooth_passes; ++k) {
+    float* dst = (k & 1) ? n.sm1 : n.sm0;
+    CDM_CK(cdm::net::smooth3x3(y, ystride, dst, nj, ni, n.stream));
+    y = dst;
+    ystride = 1;
+  }
   CDM_CK(cudaMemcpyAsync(u0, tcur, (size_t)nx * ny * sizeof(double), cudaMemcpyDeviceToDevice, n.stream));
-  CDM_CK(cdm::net::apply_guess(tprev, tcur, n.Y, n.d_scale, u0, ni, nj, nx, nhalo, n.stream));
+  CDM_CK(cdm::net::apply_guess(tprev, tcur, y, ystride, n.d_scale, u0, ni, nj, nx, nhalo, n.stream));
   CDM_CK(cudaStreamSynchronize(n.stream));
   return CDM_OK;
 }

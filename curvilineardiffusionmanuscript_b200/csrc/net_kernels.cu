@@ -364,6 +364,12 @@ __global__ void features_kernel(FeatArgs a) {
     dst[0] = pack8(f);
     dst[1] = pack8(f + 8);
     if (a.target) a.target[e] = (float)(((a.tnext[b][o] - tc) - (tc - tp)) * is);
+    // A smooth error of the guess enters the step's residual amplified by about
+    // 1 + D(h/ℓ)² with D = κΔt/(ρcₚJ) the local diffusion number and ℓ its
+    // length scale; the loss weights each pixel by that factor at ℓ = 4 cells.
+    if (a.weight)
+      a.weight[e] = a.dt > 0.0 ? (float)(1.0 + kappa_of(tc, a.k0, a.kn) * a.dt / (a.rho_cp * a.J[o]) / 16.0)
+                               : 1.0f;
   }
 }
 
@@ -399,18 +405,21 @@ __global__ void finish_scale_kernel(double* acc, int nsamp, int64_t ncells) {
   }
 }
 
-// squared error of channel 0 and its gradient 2(y − t)/N (channels 1..15 zero)
+// (weighted) squared error of channel 0, w²(y − t)², and its gradient
+// 2w²(y − t)/N (channels 1..15 zero); w = 1 without weights
 __global__ void loss_grad_kernel(const float* __restrict__ y, const float* __restrict__ t,
-                                 __nv_bfloat16* __restrict__ gy, int64_t npix, float* loss_acc) {
+                                 const float* __restrict__ w, __nv_bfloat16* __restrict__ gy, int64_t npix,
+                                 float* loss_acc) {
   float l = 0.f;
   const float sc = 2.f / (float)npix;
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < npix; p += (int64_t)gridDim.x * blockDim.x) {
+    const float ww = w ? w[p] * w[p] : 1.f;
     const float d = y[p * 16] - t[p];
-    l += d * d;
+    l += ww * d * d;
     float f[16];
 #pragma unroll
     for (int k = 1; k < 16; ++k) f[k] = 0.f;
-    f[0] = sc * d;
+    f[0] = sc * ww * d;
     uint4* dst = reinterpret_cast<uint4*>(gy + p * 16);
     dst[0] = pack8(f);
     dst[1] = pack8(f + 8);
@@ -420,16 +429,36 @@ __global__ void loss_grad_kernel(const float* __restrict__ y, const float* __res
   if ((threadIdx.x & 31) == 0) atomicAdd(loss_acc, l);
 }
 
-// u0 = 2Tⁿ − Tⁿ⁻¹ + s·y on the domain (y: one image of ni x nj pixels, 16 channels)
+// out = ((1 2 1)ᵀ(1 2 1) / 16) * in on an H x W image, edge pixels replicated
+__global__ void smooth3x3_kernel(const float* __restrict__ in, int in_stride, float* __restrict__ out, int H,
+                                 int W) {
+  const int64_t n = (int64_t)H * W;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(e % W), y = (int)(e / W);
+    float s = 0.f;
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int yy = min(max(y + dy, 0), H - 1);
+#pragma unroll
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int xx = min(max(x + dx, 0), W - 1);
+        s += (float)((2 - (dx < 0 ? -dx : dx)) * (2 - (dy < 0 ? -dy : dy))) * in[((int64_t)yy * W + xx) * in_stride];
+      }
+    }
+    out[e] = s * (1.f / 16.f);
+  }
+}
+
+// u0 = 2Tⁿ − Tⁿ⁻¹ + s·y on the domain (y: one image of ni x nj pixels, y_stride floats apart)
 __global__ void apply_guess_kernel(const double* __restrict__ tprev, const double* __restrict__ tcur,
-                                   const float* __restrict__ y, const double* __restrict__ scale,
+                                   const float* __restrict__ y, int y_stride, const double* __restrict__ scale,
                                    double* __restrict__ u0, int ni, int nj, int nx, int nh) {
   const int64_t n = (int64_t)ni * nj;
   const double s = scale[0];
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
     const int i = (int)(e % ni), j = (int)(e / ni);
     const int64_t o = (int64_t)(i + nh) + (int64_t)nx * (j + nh);
-    u0[o] = (2.0 * tcur[o] - tprev[o]) + s * (double)y[e * 16];
+    u0[o] = (2.0 * tcur[o] - tprev[o]) + s * (double)y[e * y_stride];
   }
 }
 
@@ -562,15 +591,21 @@ cudaError_t finish_scale(double* acc, int nsamp, int64_t ncells, cudaStream_t s)
   return cudaGetLastError();
 }
 
-cudaError_t loss_grad(const float* y, const float* target, __nv_bfloat16* gy, int64_t npix, float* loss_acc,
-                      cudaStream_t s) {
-  loss_grad_kernel<<<grid_for(npix), 256, 0, s>>>(y, target, gy, npix, loss_acc);
+cudaError_t loss_grad(const float* y, const float* target, const float* weight, __nv_bfloat16* gy, int64_t npix,
+                      float* loss_acc, cudaStream_t s) {
+  loss_grad_kernel<<<grid_for(npix), 256, 0, s>>>(y, target, weight, gy, npix, loss_acc);
   return cudaGetLastError();
 }
 
-cudaError_t apply_guess(const double* tprev, const double* tcur, const float* y, const double* scale, double* u0,
-                        int ni, int nj, int nx, int nh, cudaStream_t s) {
-  apply_guess_kernel<<<grid_for((int64_t)ni * nj), 256, 0, s>>>(tprev, tcur, y, scale, u0, ni, nj, nx, nh);
+cudaError_t smooth3x3(const float* in, int in_stride, float* out, int H, int W, cudaStream_t s) {
+  smooth3x3_kernel<<<grid_for((int64_t)H * W), 256, 0, s>>>(in, in_stride, out, H, W);
+  return cudaGetLastError();
+}
+
+cudaError_t apply_guess(const double* tprev, const double* tcur, const float* y, int y_stride, const double* scale,
+                        double* u0, int ni, int nj, int nx, int nh, cudaStream_t s) {
+  apply_guess_kernel<<<grid_for((int64_t)ni * nj), 256, 0, s>>>(tprev, tcur, y, y_stride, scale, u0, ni, nj, nx,
+                                                                 nh);
   return cudaGetLastError();
 }
 

@@ -63,17 +63,20 @@ struct FeatArgs {
   int nx, nh;                  // full row length, halo width
   int B, H, W;                 // crop size
   double k0, kn, log_jmean;
+  double dt, rho_cp;           // loss weights when dt > 0 (see features_kernel)
   __nv_bfloat16* x;            // [B][H][W][16]
   float* target;               // [B][H][W] or NULL
+  float* weight;               // [B][H][W] or NULL
 };
 cudaError_t features(const FeatArgs& a, cudaStream_t s);
 cudaError_t delta_scale(const double* const* tprev, const double* const* tcur, int nsamp, int ni, int nj, int nx,
                         int nh, double* acc, cudaStream_t s);
 cudaError_t finish_scale(double* acc, int nsamp, int64_t ncells, cudaStream_t s);
-cudaError_t loss_grad(const float* y, const float* target, __nv_bfloat16* gy, int64_t npix, float* loss_acc,
-                      cudaStream_t s);
-cudaError_t apply_guess(const double* tprev, const double* tcur, const float* y, const double* scale, double* u0,
-                        int ni, int nj, int nx, int nh, cudaStream_t s);
+cudaError_t loss_grad(const float* y, const float* target, const float* weight, __nv_bfloat16* gy, int64_t npix,
+                      float* loss_acc, cudaStream_t s);
+cudaError_t smooth3x3(const float* in, int in_stride, float* out, int H, int W, cudaStream_t s);
+cudaError_t apply_guess(const double* tprev, const double* tcur, const float* y, int y_stride, const double* scale,
+                        double* u0, int ni, int nj, int nx, int nh, cudaStream_t s);
 
 // parameters: master fp32 W[9][cin][cout] → Wf bf16 [9][cout][cin], Wb bf16 [9][cin][cout] (flipped taps)
 cudaError_t prep_weights(const float* w, __nv_bfloat16* wf, __nv_bfloat16* wb, int cin, int cout, cudaStream_t s);

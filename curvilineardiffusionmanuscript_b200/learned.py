@@ -103,9 +103,15 @@ class GuessNet:
         self._ck(self._lib.cdm_net_backward(self._h, target.data_ptr(), C.byref(loss)))
         return loss.value
 
+    def set_smoothing(self, passes: int):
+        """3x3 binomial passes applied to the predicted correction (default 8)."""
+        self._ck(self._lib.cdm_net_set_guess_smoothing(self._h, int(passes)))
+
     def train_step(self, frames: Sequence[torch.Tensor], idx: Sequence[int], ox: Sequence[int],
-                   oy: Sequence[int], crop: int, mesh, k0: float, kn: float, lr: float, ljm: float) -> float:
-        """One Adam step on crops: sample b uses frames[idx[b] − 1, idx[b], idx[b] + 1]."""
+                   oy: Sequence[int], crop: int, mesh, k0: float, kn: float, lr: float, ljm: float,
+                   dt: float = 0.0, rho_cp: float = 1.0) -> float:
+        """One Adam step on crops: sample b uses frames[idx[b] − 1, idx[b], idx[b] + 1].
+        dt > 0 weights each pixel's error by 1 + κΔt/(16ρcₚJ)."""
         n = len(idx)
         torch.cuda.current_stream(frames[0].device).synchronize()
         P = C.c_void_p * n
@@ -117,7 +123,7 @@ class GuessNet:
         b = L.NetBatch(n, C.cast(tp, C.POINTER(C.c_void_p)), C.cast(tc, C.POINTER(C.c_void_p)),
                        C.cast(tn, C.POINTER(C.c_void_p)), mesh.cell_J.data_ptr(),
                        C.cast(ax, C.POINTER(C.c_int)), C.cast(ay, C.POINTER(C.c_int)),
-                       crop, mesh.ni, mesh.nj, mesh.nhalo, k0, kn, ljm)
+                       crop, mesh.ni, mesh.nj, mesh.nhalo, k0, kn, ljm, dt, rho_cp)
         loss = C.c_float(0.0)
         self._ck(self._lib.cdm_net_train_step(self._h, C.byref(b), lr, C.byref(loss)))
         return loss.value
@@ -160,8 +166,10 @@ def generate_trajectories(make_problem, seeds: Sequence[int], nsteps: int, preci
 
 
 def train(net: GuessNet, trajs: List[List[torch.Tensor]], mesh, k0: float, kn: float, steps: int,
-          batch: int = 16, crop: int = 128, lr: float = 1e-3, seed: int = 0, log_every: int = 0) -> List[float]:
-    """Adam on random crops of random (Tⁿ⁻¹, Tⁿ, Tⁿ⁺¹) triples; cosine learning-rate decay."""
+          batch: int = 16, crop: int = 128, lr: float = 1e-3, seed: int = 0, log_every: int = 0,
+          dt: float = 0.0, rho_cp: float = 1.0) -> List[float]:
+    """Adam on random crops of random (Tⁿ⁻¹, Tⁿ, Tⁿ⁺¹) triples; cosine learning-rate decay.
+    dt > 0 weights the loss by the local diffusion number (see cdm_net_batch)."""
     rng = np.random.default_rng(seed)
     ljm = log_jmean(mesh)
     triples = [(t, i) for t, fr in enumerate(trajs) for i in range(1, len(fr) - 1)]
@@ -178,7 +186,7 @@ def train(net: GuessNet, trajs: List[List[torch.Tensor]], mesh, k0: float, kn: f
         ox = rng.integers(0, mesh.ni - crop + 1, size=batch)
         oy = rng.integers(0, mesh.nj - crop + 1, size=batch)
         a = lr * 0.5 * (1.0 + math.cos(math.pi * s / max(1, steps)))
-        losses.append(net.train_step(frames, idx, ox, oy, crop, mesh, k0, kn, a, ljm))
+        losses.append(net.train_step(frames, idx, ox, oy, crop, mesh, k0, kn, a, ljm, dt, rho_cp))
         if log_every and (s % log_every == 0 or s == steps - 1):
             print(f"[train] step {s} loss {losses[-1]:.4e} lr {a:.2e}", flush=True)
     return losses

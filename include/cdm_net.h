@@ -11,7 +11,7 @@
  * weights and activations, FP32 accumulation on the tensor cores.
  *   inputs (16 channels, 4 used):  log|Tⁿ|, (Tⁿ − Tⁿ⁻¹)/s, ¼·log κ(Tⁿ), log J − log J̄
  *   output (16 channels, 1 used):  y = (Tⁿ⁺¹ − 2Tⁿ + Tⁿ⁻¹)/s
- *   guess:                         u₀ = 2Tⁿ − Tⁿ⁻¹ + s·y
+ *   guess:                         u₀ = 2Tⁿ − Tⁿ⁻¹ + s·smooth(y)
  * with s the RMS over the domain of Tⁿ − Tⁿ⁻¹.  Layers (3x3, "same"):
  *   L0a 16→32, L0b 32→32 (skip S0) | 2x2 mean pool | L1 (skip S1) | pool |
  *   L2 (skip S2) | pool | L3 | upsample+S2 | L4 | upsample+S1 | L5 |
@@ -66,10 +66,16 @@ typedef struct {
   int ni, nj, nhalo;           /* domain size and halo of the full arrays           */
   double k0, kn;               /* κ = k0·|T|^kn                                     */
   double log_jmean;            /* log of the mean cell Jacobian of the mesh         */
+  double dt;                   /* > 0: weight the loss by 1 + D/16, D = κΔt/(ρcₚJ)  */
+  double rho_cp;               /* ρcₚ of that weight (constant over the mesh)       */
 } cdm_net_batch;
 
 /* features → forward → loss → backward → Adam (β = 0.9, 0.999, ε = 1e-8) */
 int cdm_net_train_step(cdm_net* net, const cdm_net_batch* batch, float lr, float* loss);
+
+/* Passes (default 8) of the 3x3 binomial filter applied to the predicted
+ * correction s·y before it is added to 2Tⁿ − Tⁿ⁻¹; 0 turns it off. */
+int cdm_net_set_guess_smoothing(cdm_net* net, int passes);
 
 /* guess u0 (full array; halo copied from tcur) for the domain of ni x nj cells */
 int cdm_net_predict(cdm_net* net, const double* tprev, const double* tcur, const double* J, int ni, int nj,

@@ -124,3 +124,57 @@ def test_guessed_start_stops_where_the_plain_start_stops():
             else:
                 step(g2, pr.mesh, T2, pr.rho, pr.cp, pr.kappa, pr.dt, **kw)
             assert rel_l2(T2.cpu().numpy(), frames[k + 1].cpu().numpy()) <= 1e-8
+
+
+def run_steps(pr, nsteps, net=None, check_every=4):
+    g = PseudoTransientSolver(pr.mesh, pr.bcs)
+    guess = L.CDM_GUESS_PREV
+    if net is not None:
+        learned.attach(g, net)
+        guess = L.CDM_GUESS_LEARNED
+    T = pr.T0.clone()
+    iters = []
+    for _ in range(nsteps):
+        st, _ = step(g, pr.mesh, T, pr.rho, pr.cp, pr.kappa, pr.dt, rtol=1e-8, atol=1e-8, max_iter=100000,
+                     guess=guess, check_every=check_every)
+        iters.append(st["niter"])
+    g.close()
+    return T, iters
+
+
+def test_trained_guess_gain_over_the_plain_start():
+    """What training buys, on held-out seeds of the 256² multi-Gaussian problem:
+    the trained guess is at least 2x closer to the next step than the untrained
+    network's (linear extrapolation), and steps 2..6 started from it need fewer
+    pseudo-iterations than the plain start while ending at the same solution."""
+    n = 256
+    make = small_problem(n)
+    pr0 = make(0)
+    trajs = learned.generate_trajectories(make, seeds=list(range(100, 124)), nsteps=8)
+    net = learned.GuessNet(seed=1)
+    untrained = learned.GuessNet(seed=1)
+    losses = learned.train(net, trajs, pr0.mesh, pr0.kappa.k0, pr0.kappa.n, steps=2500, batch=16, crop=128,
+                           lr=2e-3)
+    assert np.mean(losses[-50:]) < 0.1 * np.mean(losses[:10])
+    ljm = learned.log_jmean(pr0.mesh)
+    total_plain = total_learned = 0
+    for seed in (901, 902):
+        pr = make(seed)
+        Tp, ip = run_steps(pr, 6)
+        Tl, il = run_steps(pr, 6, net)
+        assert il[0] == ip[0]  # step 1 has no previous step: both start from Tⁿ
+        total_plain += sum(ip[1:])
+        total_learned += sum(il[1:])
+        assert rel_l2(Tl.cpu().numpy(), Tp.cpu().numpy()) <= 1e-7
+        # guess accuracy on this seed's own trajectory
+        fr = learned.generate_trajectories(make, seeds=[seed], nsteps=3)[0]
+        h = pr.mesh.nhalo
+        dom = (slice(h, -h), slice(h, -h))
+        e_tr = e_un = 0.0
+        for k in (1, 2):
+            nxt = fr[k + 1][dom]
+            e_tr += float((net.predict(fr[k - 1], fr[k], pr.mesh, 1.0, 3.0, ljm)[dom] - nxt).norm())
+            e_un += float((untrained.predict(fr[k - 1], fr[k], pr.mesh, 1.0, 3.0, ljm)[dom] - nxt).norm())
+        assert e_tr <= 0.5 * e_un, (e_tr, e_un)
+    print(f"pseudo-iterations of steps 2..6: plain {total_plain}, learned {total_learned}")
+    assert total_learned < total_plain, (total_learned, total_plain)
