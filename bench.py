@@ -45,7 +45,10 @@ def parse():
                              "gauss3d256", "gauss3d128"])
     ap.add_argument("--nprob", type=int, default=256)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64_exact", "mixed"])
-    ap.add_argument("--compare", action="store_true", help="single-problem s/timestep: fp64 vs mixed")
+    ap.add_argument("--compare", action="store_true", help="single-problem s/timestep: fp64 vs mixed (vs learned)")
+    ap.add_argument("--learned-steps", type=int, default=2000, help="APT steps of guess-network training data")
+    ap.add_argument("--train-steps", type=int, default=3000, help="optimisation steps of the guess network")
+    ap.add_argument("--smooth", type=int, default=8, help="smoothing passes of the predicted correction")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -367,12 +370,18 @@ def traffic_per_cell_iter(nd, workload):
     return None, None
 
 
-def time_single(pr, precision, steps, warmup, stream, guess=None):
-    """Seconds per time step of one problem (CUDA events on the solver's stream)."""
+def time_single(pr, precision, steps, warmup, stream, net=None):
+    """Seconds per time step of one problem (CUDA events on the solver's stream).
+    With a guess network the steps after the first start from its prediction;
+    the prediction and the plain-start probe are inside the timed step."""
     import torch
-    from curvilineardiffusionmanuscript_b200 import problems
+    from curvilineardiffusionmanuscript_b200 import _lib, learned, problems
     from curvilineardiffusionmanuscript_b200.solver import PseudoTransientSolver, step
     g = PseudoTransientSolver(pr.mesh, pr.bcs, precision=precision, stream=stream.cuda_stream)
+    guess = _lib.CDM_GUESS_PREV
+    if net is not None:
+        learned.attach(g, net)
+        guess = _lib.CDM_GUESS_LEARNED
     T = pr.T0.clone()
     t = 0.0
     mms = pr.name == "mms_2d"
@@ -383,7 +392,8 @@ def time_single(pr, precision, steps, warmup, stream, guess=None):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        st, _ = step(g, pr.mesh, T, pr.rho, pr.cp, pr.kappa, pr.dt, rtol=pr.rtol, atol=pr.atol, max_iter=100000)
+        st, _ = step(g, pr.mesh, T, pr.rho, pr.cp, pr.kappa, pr.dt, rtol=pr.rtol, atol=pr.atol, max_iter=100000,
+                     guess=guess)
         e1.record(stream)
         torch.cuda.synchronize()
         t += pr.dt
@@ -399,6 +409,31 @@ def time_single(pr, precision, steps, warmup, stream, guess=None):
     return out
 
 
+def train_guess(n, nseeds, nsteps, train_steps):
+    """Guess network trained on APT trajectories of the multi-Gaussian problem
+    (seeds disjoint from the timed problem's)."""
+    import time as _t
+    import torch
+    from curvilineardiffusionmanuscript_b200 import learned, problems
+    make = lambda seed: problems.multi_gaussian_2d(n, seed=seed, device="cuda")
+    t0 = _t.time()
+    skipped = []
+    trajs = learned.generate_trajectories(make, seeds=list(range(1000, 1000 + nseeds)), nsteps=nsteps,
+                                          skipped=skipped)
+    t1 = _t.time()
+    net = learned.GuessNet(seed=1)
+    pr0 = make(1000)
+    losses = learned.train(net, trajs, pr0.mesh, pr0.kappa.k0, pr0.kappa.n, steps=train_steps, batch=16, crop=128,
+                           lr=2e-3)
+    torch.cuda.synchronize()
+    info = {"apt_steps": len(trajs) * nsteps, "seeds_diverged": len(skipped), "data_s": round(t1 - t0, 1), "train_s": round(_t.time() - t1, 1),
+            "train_steps": train_steps, "loss_first": float(sum(losses[:10]) / 10),
+            "loss_last": float(sum(losses[-50:]) / 50)}
+    del trajs
+    torch.cuda.empty_cache()
+    return net, info
+
+
 def run_compare(args):
     import torch
     dev = torch.device("cuda", 0)
@@ -410,6 +445,18 @@ def run_compare(args):
             probs, cfg = make_workload(wl, 1, 0, dev)
             r[prec] = time_single(probs[0], prec, args.steps, args.warmup, stream)
         r["speedup_mixed_vs_fp64"] = r["fp64"]["s_per_step"] / r["mixed"]["s_per_step"]
+        if wl.startswith("multigauss") and args.learned_steps > 0:
+            n = probs[0].mesh.ni
+            net, info = train_guess(n, args.learned_steps // 8, 8, args.train_steps)
+            net.set_smoothing(args.smooth)
+            info["smoothing_passes"] = args.smooth
+            r["training"] = info
+            for prec in ("fp64", "mixed"):
+                probs, cfg = make_workload(wl, 1, 0, dev)
+                r["learned_" + prec] = time_single(probs[0], prec, args.steps, args.warmup, stream, net=net)
+            r["speedup_learned_fp64_vs_fp64"] = r["fp64"]["s_per_step"] / r["learned_fp64"]["s_per_step"]
+            r["speedup_learned_mixed_vs_fp64"] = r["fp64"]["s_per_step"] / r["learned_mixed"]["s_per_step"]
+            net.close()
         res[wl] = r
     print(json.dumps({"compare": res}), flush=True)
 

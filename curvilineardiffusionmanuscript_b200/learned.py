@@ -147,20 +147,29 @@ def attach(solver: PseudoTransientSolver, net: Optional[GuessNet], mesh=None):
 
 
 def generate_trajectories(make_problem, seeds: Sequence[int], nsteps: int, precision: str = "fp64",
-                          rtol: float = 1e-8, atol: float = 1e-8,
-                          max_iter: int = 100000) -> List[List[torch.Tensor]]:
+                          rtol: float = 1e-8, atol: float = 1e-8, max_iter: int = 100000,
+                          skipped: Optional[list] = None) -> List[List[torch.Tensor]]:
     """APT trajectories (nsteps + 1 frames, full arrays on the GPU) of the problems
-    make_problem(seed) for each seed, advanced by the library's own solver."""
+    make_problem(seed) for each seed, advanced by the library's own solver.  A
+    seed whose APT iteration fails (the pseudo-transient iteration itself can
+    diverge on steep initial states, as the reference's does) is left out and
+    appended to `skipped`."""
     out = []
     for seed in seeds:
         pr = make_problem(seed)
         g = PseudoTransientSolver(pr.mesh, pr.bcs, precision=precision)
         T = pr.T0.clone()
         frames = [T.clone()]
-        for _ in range(nsteps):
-            step(g, pr.mesh, T, pr.rho, pr.cp, pr.kappa, pr.dt, rtol=rtol, atol=atol, max_iter=max_iter)
-            frames.append(T.clone())
-        g.close()
+        try:
+            for _ in range(nsteps):
+                step(g, pr.mesh, T, pr.rho, pr.cp, pr.kappa, pr.dt, rtol=rtol, atol=atol, max_iter=max_iter)
+                frames.append(T.clone())
+        except APTError:
+            if skipped is not None:
+                skipped.append(seed)
+            continue
+        finally:
+            g.close()
         out.append(frames)
     return out
 
