@@ -271,6 +271,9 @@ def run_ours(args, ws, rank, local):
     kaps = [p.kappa for p in probs]
     dts = [p.dt for p in probs]
     kw = dict(rtol=probs[0].rtol, atol=probs[0].atol, max_iter=100000)
+    # strip height and iteration-block length timed on this batch (set-up, outside the timed region)
+    tuned = batch.autotune(Ts, rhos, cps, kaps, dts, **kw)
+    cfg["autotune"] = dict(candidate=tuned, **batch.tuning())
 
     def one_step():
         st, _ = batch.step(Ts, rhos, cps, kaps, dts, **kw)

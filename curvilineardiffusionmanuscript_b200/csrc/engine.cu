@@ -395,7 +395,9 @@ int Engine::build_items() {
       // a single problem: about 24 strips per SM (several waves), no shorter
       // than 8 rows (the two staged ring rows cost 2/h); a batch: 64-row strips
       int h = 64;
-      if (nprob == 1) {
+      if (strip_h_override > 0) {
+        h = strip_h_override;
+      } else if (nprob == 1) {
         const int target = 148 * 24;
         int nstrips = (target + s.tiles_i - 1) / s.tiles_i;
         nstrips = std::max(1, std::min(nstrips, (s.nj + 7) / 8));
@@ -583,7 +585,7 @@ int Engine::launch_block(int K, bool use_graph) {
 
 // Launch iteration blocks until every problem's control block says done.
 int Engine::run_iterations(const cdm_step_opts* o, int predicted, double t_start, double timeout_s) {
-  const int K = o->iter_block > 0 ? o->iter_block : 8;
+  const int K = o->iter_block > 0 ? o->iter_block : tuned_iter_block;
   const bool use_graph = o->use_graph != 0;
   const int nprob = (int)ps.size();
   int launched = 0;

@@ -75,6 +75,8 @@ struct Engine {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int variant = 0;
+  int strip_h_override = 0;   // row-marching strip height chosen by the autotuner (0: heuristic)
+  int tuned_iter_block = 8;   // iterations per graph block when cdm_step_opts.iter_block is 0
   std::vector<ProbState> ps;
   std::vector<Problem> hp;
   Problem* d_probs = nullptr;
@@ -123,6 +125,8 @@ struct Engine {
   int mixed_alloc();
   int step_mixed(const cdm_step_opts* o, double t_start, double timeout_s);
   int learned_guess(int p, const cdm_kappa& kappa);
+  int autotune(double* const* T, const double* const* rho, const double* cp, const cdm_kappa* kappa,
+               const double* dt, const cdm_step_opts* opts, const char* cache_path, int* chosen);
   int probe_plain_norm(const std::vector<int>& guessed, const std::vector<const double*>& init, double t_start,
                        double timeout_s);
 };

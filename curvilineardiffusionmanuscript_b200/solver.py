@@ -343,12 +343,28 @@ class PseudoTransientBatch:
         if rc != L.CDM_OK:
             raise APTError(rc, L.last_error())
 
-    def autotune(self, cache_path: Optional[str] = None) -> int:
-        ch = C.c_int(0)
-        rc = self._lib.cdm_batch_autotune(self._h, cache_path.encode() if cache_path else None, C.byref(ch))
+    def autotune(self, Ts, rhos, cps, kappas, dts, cache_path: Optional[str] = None, **kwargs) -> int:
+        """Time one step per (strip height, iteration block) candidate on these
+        inputs and keep the fastest; Ts are not modified.  Returns the candidate index."""
+        n = self.n
+        o = step_opts(**kwargs)
+        o.mem = _mem(Ts[0])
+        Tp = (C.c_void_p * n)(*[_ptr(t) for t in Ts])
+        Rp = (C.c_void_p * n)(*[_ptr(r) for r in rhos])
+        cpa = (C.c_double * n)(*[float(c) for c in cps])
+        ka = (L.Kappa * n)(*[k.as_c() for k in kappas])
+        dta = (C.c_double * n)(*[float(d) for d in dts])
+        ch = C.c_int(-1)
+        rc = self._lib.cdm_batch_autotune(self._h, Tp, Rp, cpa, ka, dta, C.byref(o),
+                                          cache_path.encode() if cache_path else None, C.byref(ch))
         if rc != L.CDM_OK:
             raise APTError(rc, L.last_error())
         return ch.value
+
+    def tuning(self) -> dict:
+        h, k = C.c_int(0), C.c_int(0)
+        self._lib.cdm_batch_tuning(self._h, C.byref(h), C.byref(k))
+        return {"strip_h": h.value, "iter_block": k.value}
 
     def step(self, Ts, rhos, cps, kappas, dts, raise_on_error=True, **kwargs):
         n = self.n

@@ -247,10 +247,20 @@ int cdm_batch_set_source(cdm_batch* b, int p, const double* S, int mem);
 int cdm_batch_step(cdm_batch* b, double* const* T, const double* const* rho, const double* cp,
                    const cdm_kappa* kappa, const double* dt, const cdm_step_opts* opts,
                    cdm_stats* stats /* nprob */, double* next_dt /* nprob */);
-/* autotuner: time the candidate tile shapes and iteration-block lengths on
- * this batch and keep the fastest; result cached in `cache_path` (JSON) when
- * it is not NULL.  *chosen receives an index into the candidate table. */
-int cdm_batch_autotune(cdm_batch* b, const char* cache_path, int* chosen);
+/* Autotuner (no counterpart in the reference).  Times one complete step of
+ * this batch per candidate — row-marching strip height h ∈ {8, 16, 32, 64} x
+ * iteration-block length K ∈ {4, 8, 16} (graph-replayed iterations between
+ * host polls), candidate index 3·index(h) + index(K) — from the given inputs
+ * (arguments as cdm_batch_step; T is not modified and the solver state is
+ * restored after every trial) and keeps the fastest for later steps.  With
+ * cache_path not NULL the choice is read from / written to that JSON file,
+ * keyed by the batch's sizes, precision and mean.  *chosen = -1 when nothing
+ * is tuned (3D tile kernels).  cdm_step_opts.iter_block > 0 still overrides K. */
+int cdm_batch_autotune(cdm_batch* b, double* const* T, const double* const* rho, const double* cp,
+                       const cdm_kappa* kappa, const double* dt, const cdm_step_opts* opts,
+                       const char* cache_path, int* chosen);
+/* strip height (0 = built-in heuristic) and iteration-block length in use */
+int cdm_batch_tuning(const cdm_batch* b, int* strip_h, int* iter_block);
 int cdm_batch_get_profile(const cdm_batch* b, cdm_profile* out);
 
 /* ---- allocation-free end-of-step reductions ------------------------------

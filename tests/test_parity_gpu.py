@@ -233,6 +233,37 @@ def test_batch_matches_individual_oracle_runs():
         assert np.array_equal(T, Ts[p]), p
 
 
+def test_batch_autotune_changes_speed_not_results(tmp_path):
+    """The autotuner times every (strip height, iteration block) candidate on the
+    given inputs without changing them or the solver state; after tuning the
+    exact batch still equals the oracle bit for bit, and the choice is cached."""
+    probs = problems.batch_2d(nprob=6, nmin=20, nmax=70, seed=7)
+    b = PseudoTransientBatch([p.mesh for p in probs], [p.bcs for p in probs], precision="fp64_exact")
+    Ts = [p.T0.numpy().copy() for p in probs]
+    T0 = [t.copy() for t in Ts]
+    args = ([p.rho.numpy() for p in probs], [p.cp for p in probs], [p.kappa for p in probs], [p.dt for p in probs])
+    kw = dict(rtol=0.0, atol=1e-8, max_iter=50000)
+    cache = str(tmp_path / "tune.json")
+    c = b.autotune(Ts, *args, cache_path=cache, **kw)
+    assert 0 <= c < 12
+    assert all(np.array_equal(a, t) for a, t in zip(Ts, T0))
+    tun = b.tuning()
+    assert tun["strip_h"] == [8, 16, 32, 64][c // 3] and tun["iter_block"] == [4, 8, 16][c % 3]
+    for _ in range(2):
+        stats, _ = b.step(Ts, *args, **kw)
+    for p, pr in enumerate(probs):
+        o = OracleSolver(pr.mesh, pr.bcs)
+        T = pr.T0.numpy().copy()
+        for _ in range(2):
+            so, _ = o.step(T, pr.rho.numpy(), pr.cp, pr.kappa.k0, pr.kappa.n, pr.dt, **kw)
+        assert so["niter"] == stats[p]["niter"], p
+        assert np.array_equal(T, Ts[p]), p
+    # a second batch of the same sizes reads the cached choice
+    b2 = PseudoTransientBatch([p.mesh for p in probs], [p.bcs for p in probs], precision="fp64_exact")
+    assert b2.autotune([p.T0.numpy().copy() for p in probs], *args, cache_path=cache, **kw) == c
+    assert b2.tuning() == tun
+
+
 # --------------------------------------------------------------- fast FP64 form
 # The fast form is compared at the workload's stopping rule (rel <= 1e-8 or
 # abs <= 1e-8), where the residual is far above round-off: an absolute 1e-8
