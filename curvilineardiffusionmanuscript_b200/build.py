@@ -28,6 +28,7 @@ UNITS = {
     "apt_sweep_fp64.cu": ["-fmad=false"],
     "apt_march2d.cu": ["-fmad=false"],
     "apt_march2d_fast.cu": [],
+    "apt_march3d.cu": [],
     "apt_aux.cu": ["-fmad=false"],
     "engine.cu": ["-fmad=false"],
     "apt_mixed.cu": [],

@@ -28,42 +28,15 @@
 // concurrent launch on a side stream.
 #include "cdm_device.cuh"
 #include "cdm_finish.cuh"
+#include "cdm_fast.cuh"
 #include "cdm_kernels.h"
 
 namespace cdm {
 
 namespace {
 
-// Newton–Raphson refinement of the hardware reciprocal approximation; the
-// approximation's own result is kept for 0 and ±inf arguments (1/0 = inf,
-// 1/inf = 0), where the refinement would produce NaN.
-__device__ __forceinline__ double rcp_nr(double b) {
-  double y0;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(b));
-  double e = fma(-b, y0, 1.0);
-  double y = fma(y0, e, y0);
-  e = fma(-b, y, 1.0);
-  y = fma(y, e, y);
-  return (y0 == 0.0 || fabs(y0) == __longlong_as_double(0x7ff0000000000000ll)) ? y0 : y;
-}
-
-// general exponents go through pow() out of line, keeping its temporaries out
-// of the sweep's register budget
-__device__ __noinline__ double pow_general(double x, double n) { return pow(x, n); }
-
-__device__ __forceinline__ double pow_fast(double x, int mode, int m, int half, double n) {
-  if (mode == 0) return 1.0;
-  if (mode == 1) {
-    double p = 1.0;
-    if (m >= 1) {
-      p = x;
-      for (int e = 1; e < m; ++e) p *= x;
-    }
-    if (half) p = (m >= 1) ? p * sqrt(x) : sqrt(x);
-    return p;
-  }
-  return pow_general(x, n);
-}
+using fastmath::pow_fast;
+using fastmath::rcp_nr;
 
 template <int TX>
 struct FastSmem {

@@ -1,0 +1,334 @@
+// apt_march3d.cu — plane-marching FP64 APT pseudo-iteration in 3D, reciprocal form.
+//
+// The iteration of step! (PseudoTransientSolver.jl:253-319) with the 3D flux
+// divergence of flux_divergence.jl:119-239, in the reciprocal ("fast") form of
+// apt_march2d_fast.cu: the same discrete iteration as the operation-for-
+// operation tile kernel (sweep3d_fp64), last-bit differences only.
+//
+// Organisation: a block of 256 threads owns a 32 x 8 column of cells in (i, j)
+// and marches a strip of k-planes.  Each thread owns one (i, j) position and
+// keeps its own cell's update factors in registers; 84 threads also stage one
+// cell of the one-cell (i, j) ring.  Shared memory holds two staged cell planes
+// (u, α⁻¹ or α, θ⁻¹ or θ), three planes of i- and j-face fluxes and two planes
+// of k-face fluxes (damped, and undamped on check iterations): the divergence
+// of plane z reads the i/j fluxes of planes z-1, z, z+1 and the k fluxes below
+// and above it.  Every face is computed once per strip; the ring costs 1.33x
+// the owned cells per plane and nothing along k.  Ghost cells come from the
+// boundary rules of every side applied on the fly (boundary_operators.jl).
+#include "cdm_device.cuh"
+#include "cdm_fast.cuh"
+#include "cdm_finish.cuh"
+#include "cdm_kernels.h"
+
+namespace cdm {
+
+namespace {
+
+using fastmath::pow_fast;
+using fastmath::rcp_nr;
+
+constexpr int TX = 32, TY = 8, NT = TX * TY, RX = TX + 2, RY = TY + 2;
+constexpr int NRING = RX * RY - TX * TY;  // 84 ring cells per plane
+
+struct M3Smem {
+  double U[2][RY][RX], IA[2][RY][RX], IT[2][RY][RX];  // staged cells of planes z, z+1
+  double QI[3][RY][TX + 1], QJ[3][TY + 1][RX], QK[2][RY][RX];  // new damped fluxes
+  double PI[3][RY][TX + 1], PJ[3][TY + 1][RX], PK[2][RY][RX];  // undamped (check iterations)
+  double red[NT / 32];
+  int flag;
+};
+
+struct C3 {
+  double u, ia, it, g, f;
+};
+
+}  // namespace
+
+template <bool HARM>
+__global__ void __launch_bounds__(NT, 3) march3d_fast(const Problem* __restrict__ probs,
+                                                      const int2* __restrict__ items) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  M3Smem& sm = *reinterpret_cast<M3Smem*>(smem_raw);
+  const int2 item = items[blockIdx.x];
+  const Problem& P = probs[item.x];
+  Ctrl* C = P.ctrl;
+  if (ld_cg_int(&C->done)) return;
+  const int iter = ld_cg_int(&C->iter) + 1;
+  const bool check = is_check_iter(C, iter);
+  const int tid = threadIdx.x;
+  const int tile = item.y;
+  const int ti = tile % P.tiles_i, tj = (tile / P.tiles_i) % P.tiles_j, sk = tile / (P.tiles_i * P.tiles_j);
+  const int ni = P.ni, nj = P.nj, nk = P.nk;
+  const int i0 = ti * TX, j0 = tj * TY;
+  const int k0 = sk * P.strip_h, k1 = min(k0 + P.strip_h, nk);
+  const int pin = (iter - 1) & 1;
+  const double* __restrict__ uin = P.u[pin];
+  double* __restrict__ uout = P.u[pin ^ 1];
+  const int qin = (P.qpar + iter - 1) & 1;
+  const double* __restrict__ qiin = P.q[qin][0];
+  const double* __restrict__ qjin = P.q[qin][1];
+  const double* __restrict__ qkin = P.q[qin][2];
+  double* __restrict__ qiout = P.q[qin ^ 1][0];
+  double* __restrict__ qjout = P.q[qin ^ 1][1];
+  double* __restrict__ qkout = P.q[qin ^ 1][2];
+  const bool alpha_from_u = P.subcycle || iter == 1;
+  const bool rms = C->norm_kind == 1;
+  const double dt = P.dt, cp = P.cp, k0c = P.k0;
+  const double inv_dt = 1.0 / dt;
+  const double LLdt = P.LL / dt, VpL = P.VpL, LoVp = P.L / P.Vpdtau, VpoL = P.Vpdtau / P.L;
+  const int kmode = P.kmode, km = P.km, khalf = P.khalf;
+  const double kn = P.kn;
+
+  // own (i, j) position in ring coordinates, and this thread's ring cell
+  const int ox = tid % TX + 1, oy = tid / TX + 1;
+  const int oa = i0 + ox - 1, ob = j0 + oy - 1;
+  const bool own_in = oa < ni && ob < nj;
+  int rx = -1, ry = -1;
+  if (tid < NRING) {
+    if (tid < RX) {
+      rx = tid;
+      ry = 0;
+    } else if (tid < 2 * RX) {
+      rx = tid - RX;
+      ry = RY - 1;
+    } else {
+      const int t = tid - 2 * RX;  // 0 .. 2(RY-2)-1
+      rx = (t & 1) ? RX - 1 : 0;
+      ry = 1 + (t >> 1);
+    }
+  }
+  const int ra = i0 + rx - 1, rb = j0 + ry - 1;
+
+  int bad = 0;
+  // stage cell (a, b, c): u with its ghost rule, pseudo-time parameters and
+  // update factors (iteration_parameters.jl:2-15 in reciprocal form)
+  auto stage = [&](int a, int b, int c, bool track) -> C3 {
+    C3 r{0.0, 0.0, 0.0, 0.0, 0.0};
+    const int cls = classify(P, a, b, c);
+    if (cls < 0) return r;
+    const int64_t id = fidx(P, a, b, c);
+    double u, src;
+    if (cls == 6) {
+      u = uin[id];
+      src = alpha_from_u ? u : P.u_prev[id];
+    } else {
+      u = ghost_value(P, uin, cls, a, b, c);
+      src = alpha_from_u ? u : ghost_value(P, P.u_prev, cls, a, b, c);
+    }
+    const double rho = P.rho[id];
+    const double kap = isfinite(src) ? k0c * pow_fast(fabs(src), kmode, km, khalf, kn) : 0.0;
+    const double rc = rho * cp;
+    const double inva = rc * rcp_nr(kap);
+    const double Re = kPi + sqrt(kPi * kPi + LLdt * rho * inva);
+    const double iRe = rcp_nr(Re);
+    double dtau = VpL * inva * iRe;
+    double th = LoVp * iRe;
+    dtau = isfinite(dtau) ? dtau : 0.0;
+    th = isfinite(th) ? th : 0.0;
+    const double idd = rcp_nr(dt + dtau);
+    r.u = u;
+    r.g = dt * idd;
+    r.f = dtau * dt * idd;
+    if (HARM) {
+      r.ia = inva;
+      r.it = VpoL * Re;
+    } else {
+      r.ia = kap * rcp_nr(rc);
+      r.it = th;
+    }
+    // validity of α = κ/(ρcₚ) on owned cells and first-layer ghosts
+    if (track) {
+      if (!(isfinite(kap) && isfinite(rc) && rc != 0.0)) bad |= 1;
+      if (kap != 0.0 && ((kap < 0.0) != (rc < 0.0))) bad |= 2;
+    }
+    return r;
+  };
+  // stage plane c into cell slot s: the own cell (returned) and the ring cell
+  auto stage_plane = [&](int c, int s) -> C3 {
+    const bool inz = c >= k0 && c < k1;
+    const C3 own = stage(oa, ob, c, inz || c == -1 || c == nk);
+    sm.U[s][oy][ox] = own.u;
+    sm.IA[s][oy][ox] = own.ia;
+    sm.IT[s][oy][ox] = own.it;
+    if (rx >= 0) {
+      const C3 rg = stage(ra, rb, c, inz);
+      sm.U[s][ry][rx] = rg.u;
+      sm.IA[s][ry][rx] = rg.ia;
+      sm.IT[s][ry][rx] = rg.it;
+    }
+    return own;
+  };
+  auto flux = [&](double ia0, double ia1, double it0, double it1, double du, double qold, double& qp) -> double {
+    double an, qn;
+    if (HARM) {
+      an = 2.0 * rcp_nr(ia0 + ia1);
+      const double St = it0 + it1;
+      qn = isfinite(St) ? (2.0 * qold - an * du * St) * rcp_nr(St + 2.0) : -an * du;
+    } else {
+      an = 0.5 * (ia0 + ia1);
+      const double tn = 0.5 * (it0 + it1);
+      qn = (qold * tn - an * du) * rcp_nr(1.0 + tn);
+    }
+    qp = -an * du;
+    return qn;
+  };
+  constexpr int NQI = RY * (TX + 1), NQJ = (TY + 1) * RX, NQK = RY * RX;
+  // i- and j-faces of plane c (cells in slot s) into face slot fs; k-faces
+  // between planes ck (slot sl) and ck + 1 (slot sh), stored at index ck, into k-slot kf
+  auto faces = [&](int c, int s, int fs, bool do_ij, int ck, int sl, int sh, int kf, bool do_k) {
+    const bool inz = c >= k0 && c < k1;
+    const bool cin = c >= 0 && c < nk;
+    const bool kown = (ck >= k0 && ck < k1) || ck == -1;
+    const int total = (do_ij ? NQI + NQJ : 0) + (do_k ? NQK : 0);
+    for (int w = tid; w < total; w += NT) {
+      int f = do_ij ? w : w + NQI + NQJ;
+      double qn = 0.0, qp = 0.0;
+      if (f < NQI) {
+        const int y = f / (TX + 1), x = f - y * (TX + 1);
+        const int a = i0 - 1 + x, b = j0 - 1 + y;
+        if (cin && a >= -1 && a <= ni - 1 && b >= 0 && b <= nj - 1) {
+          const int64_t id = fidx(P, a, b, c);
+          qn = flux(sm.IA[s][y][x], sm.IA[s][y][x + 1], sm.IT[s][y][x], sm.IT[s][y][x + 1],
+                    sm.U[s][y][x + 1] - sm.U[s][y][x], qiin[id], qp);
+          if (inz && y >= 1 && y <= TY && (x >= 1 || a == -1)) qiout[id] = qn;
+        }
+        sm.QI[fs][y][x] = qn;
+        if (check) sm.PI[fs][y][x] = qp;
+      } else if (f < NQI + NQJ) {
+        f -= NQI;
+        const int y = f / RX, x = f - y * RX;
+        const int a = i0 - 1 + x, b = j0 - 1 + y;
+        if (cin && a >= 0 && a <= ni - 1 && b >= -1 && b <= nj - 1) {
+          const int64_t id = fidx(P, a, b, c);
+          qn = flux(sm.IA[s][y][x], sm.IA[s][y + 1][x], sm.IT[s][y][x], sm.IT[s][y + 1][x],
+                    sm.U[s][y + 1][x] - sm.U[s][y][x], qjin[id], qp);
+          if (inz && x >= 1 && x <= TX && (y >= 1 || b == -1)) qjout[id] = qn;
+        }
+        sm.QJ[fs][y][x] = qn;
+        if (check) sm.PJ[fs][y][x] = qp;
+      } else {
+        f -= NQI + NQJ;
+        const int y = f / RX, x = f - y * RX;
+        const int a = i0 - 1 + x, b = j0 - 1 + y;
+        if (ck >= -1 && ck <= nk - 1 && a >= 0 && a <= ni - 1 && b >= 0 && b <= nj - 1) {
+          const int64_t id = fidx(P, a, b, ck);
+          qn = flux(sm.IA[sl][y][x], sm.IA[sh][y][x], sm.IT[sl][y][x], sm.IT[sh][y][x],
+                    sm.U[sh][y][x] - sm.U[sl][y][x], qkin[id], qp);
+          if (kown && x >= 1 && x <= TX && y >= 1 && y <= TY) qkout[id] = qn;
+        }
+        sm.QK[kf][y][x] = qn;
+        if (check) sm.PK[kf][y][x] = qp;
+      }
+    }
+  };
+  // flux_divergence.jl:119-239 at the own cell from face slots (zm, z0, zp) and k-slots (km, kp)
+  auto divergence = [&](const double (*QI)[RY][TX + 1], const double (*QJ)[TY + 1][RX],
+                        const double (*QK)[RY][RX], int zm, int z0, int zp, int kmn, int kpl, const double* cf) {
+    const int x = ox, y = oy;
+    const double t_ii = cf[0] * (QI[z0][y][x] - QI[z0][y][x - 1]);
+    const double t_jj = cf[1] * (QJ[z0][y][x] - QJ[z0][y - 1][x]);
+    const double t_kk = cf[2] * (QK[kpl][y][x] - QK[kmn][y][x]);
+    const double qi_eta = cf[3] * (0.5 * (QI[z0][y + 1][x] + QI[z0][y + 1][x - 1]) -
+                                   0.5 * (QI[z0][y - 1][x] + QI[z0][y - 1][x - 1]));
+    const double qj_xi = cf[3] * (0.5 * (QJ[z0][y][x + 1] + QJ[z0][y - 1][x + 1]) -
+                                  0.5 * (QJ[z0][y][x - 1] + QJ[z0][y - 1][x - 1]));
+    const double qj_zeta = cf[4] * (0.5 * (QJ[zp][y][x] + QJ[zp][y - 1][x]) - 0.5 * (QJ[zm][y][x] + QJ[zm][y - 1][x]));
+    const double qk_eta = cf[4] * (0.5 * (QK[kpl][y + 1][x] + QK[kmn][y + 1][x]) -
+                                   0.5 * (QK[kpl][y - 1][x] + QK[kmn][y - 1][x]));
+    const double qi_zeta = cf[5] * (0.5 * (QI[zp][y][x] + QI[zp][y][x - 1]) - 0.5 * (QI[zm][y][x] + QI[zm][y][x - 1]));
+    const double qk_xi = cf[5] * (0.5 * (QK[kpl][y][x + 1] + QK[kmn][y][x + 1]) -
+                                  0.5 * (QK[kpl][y][x - 1] + QK[kmn][y][x - 1]));
+    const double h_a = cf[6] * (0.5 * (QI[z0][y][x] + QI[z0][y][x - 1]));
+    const double h_b = cf[7] * (0.5 * (QJ[z0][y][x] + QJ[z0][y - 1][x]));
+    const double h_c = cf[8] * (0.5 * (QK[kpl][y][x] + QK[kmn][y][x]));
+    return t_ii + t_jj + t_kk + qi_eta + qi_zeta + qj_xi + qj_zeta + qk_eta + qk_xi + h_a + h_b + h_c;
+  };
+
+  // prologue: planes k0-1 and k0, their i/j faces and the k faces between them
+  int s_0 = 1, s_p = 0;  // cell slots of planes z and z+1 (z-1 staged into 0 first)
+  int f_m = 0, f_0 = 1, f_p = 2, k_m = 0, k_p = 1;
+  C3 prv = stage_plane(k0 - 1, 0);
+  C3 cur = stage_plane(k0, 1);
+  __syncthreads();
+  faces(k0 - 1, 0, f_m, true, k0 - 1, 0, 1, k_m, true);
+  faces(k0, 1, f_0, true, 0, 0, 0, 0, false);
+  __syncthreads();
+
+  double local = 0.0;
+  bool local_nan = false;
+  for (int z = k0; z < k1; ++z) {
+    double cf[9], up = 0.0, S = 0.0;
+    const int64_t id = fidx(P, oa, ob, z);
+    if (own_in) {
+#pragma unroll
+      for (int q = 0; q < 9; ++q) cf[q] = P.coef[q][id];
+      up = P.u_prev[id];
+      S = P.S[id];
+    }
+    const C3 nxt = stage_plane(z + 1, s_p);
+    __syncthreads();
+    faces(z + 1, s_p, f_p, true, z, s_0, s_p, k_p, true);
+    // ghost neighbours of plane z, read before the barrier after which the next
+    // plane may overwrite this cell slot
+    const double g_im = sm.U[s_0][oy][ox - 1], g_ip = sm.U[s_0][oy][ox + 1];
+    const double g_jm = sm.U[s_0][oy - 1][ox], g_jp = sm.U[s_0][oy + 1][ox];
+    __syncthreads();
+    if (own_in) {
+      const double dq = divergence(sm.QI, sm.QJ, sm.QK, f_m, f_0, f_p, k_m, k_p, cf);
+      const double un = cur.g * cur.u + cur.f * (up * inv_dt - dq + S);
+      uout[id] = un;
+      // ghosts of u after applybcs! of this iteration (copy!(T, u) returns them)
+      if (oa == 0) uout[fidx(P, -1, ob, z)] = g_im;
+      if (oa == ni - 1) uout[fidx(P, ni, ob, z)] = g_ip;
+      if (ob == 0) uout[fidx(P, oa, -1, z)] = g_jm;
+      if (ob == nj - 1) uout[fidx(P, oa, nj, z)] = g_jp;
+      if (z == 0) uout[fidx(P, oa, ob, -1)] = prv.u;
+      if (z == nk - 1) uout[fidx(P, oa, ob, nk)] = nxt.u;
+      if (check) {
+        const double dqp = divergence(sm.PI, sm.PJ, sm.PK, f_m, f_0, f_p, k_m, k_p, cf);
+        double du = un - up;
+        if (isapprox_eps(un, up)) du = 0.0;
+        const double r = -du * inv_dt - dqp + S;
+        if (rms) local += r * r;
+        else {
+          const double ar = fabs(r);
+          if (ar != ar) local_nan = true;
+          else local = fmax(local, ar);
+        }
+      }
+    }
+    // rotate: planes (z, z+1) become (z-1, z)
+    prv = cur;
+    cur = nxt;
+    const int ts = s_0;
+    s_0 = s_p;
+    s_p = ts;
+    const int tf = f_m;
+    f_m = f_0;
+    f_0 = f_p;
+    f_p = tf;
+    const int tk = k_m;
+    k_m = k_p;
+    k_p = tk;
+  }
+  finish_iteration<NT>(P, C, tile, iter, check, local, local_nan, bad, sm.red, &sm.flag);
+}
+
+template <bool HARM>
+static cudaError_t launch3m(const Problem* probs, const int2* items, int nitems, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(march3d_fast<HARM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(M3Smem));
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  march3d_fast<HARM><<<nitems, NT, sizeof(M3Smem), s>>>(probs, items);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_march3d_fast(int harmonic, const Problem* probs, const int2* items, int nitems, cudaStream_t s) {
+  return harmonic ? launch3m<true>(probs, items, nitems, s) : launch3m<false>(probs, items, nitems, s);
+}
+
+}  // namespace cdm

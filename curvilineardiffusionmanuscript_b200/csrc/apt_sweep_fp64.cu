@@ -29,39 +29,6 @@
 
 namespace cdm {
 
-// ghost value of side `side` (0 ilo, 1 ihi, 2 jlo, 3 jhi, 4 klo, 5 khi) at the
-// ghost cell (a, b, c); `src` is the field the rule reads (u or u_prev)
-__device__ __forceinline__ double ghost_value(const Problem& P, const double* __restrict__ src,
-                                              int side, int a, int b, int c) {
-  const int rule = P.rule[side];
-  if (rule == GR_DIRICHLET) return P.val[side];
-  const int axis = side >> 1;
-  const bool lo = (side & 1) == 0;
-  const int n = axis == 0 ? P.ni : (axis == 1 ? P.nj : P.nk);
-  int p;  // position along the axis of the cell the rule reads
-  if (rule == GR_NONE) p = lo ? -1 : n;
-  else if (rule == GR_PERIODIC) p = lo ? n - 1 : 0;
-  else p = lo ? 0 : n - 1;  // Neumann, negative symmetry
-  int aa = a, bb = b, cc = c;
-  if (axis == 0) aa = p;
-  else if (axis == 1) bb = p;
-  else cc = p;
-  const double v = src[fidx(P, aa, bb, cc)];
-  return rule == GR_NEGSYM ? -v : v;
-}
-
-// classify a ring cell: returns -1 if it is neither a domain cell nor a
-// first-layer (non-corner) ghost, else 6 for a domain cell or the side index
-__device__ __forceinline__ int classify(const Problem& P, int a, int b, int c) {
-  const bool ia = a >= 0 && a < P.ni, ib = b >= 0 && b < P.nj;
-  const bool ic = (P.ndim == 2) || (c >= 0 && c < P.nk);
-  if (ia && ib && ic) return 6;
-  if (ib && ic && (a == -1 || a == P.ni)) return a < 0 ? 0 : 1;
-  if (ia && ic && (b == -1 || b == P.nj)) return b < 0 ? 2 : 3;
-  if (P.ndim == 3 && ia && ib && (c == -1 || c == P.nk)) return c < 0 ? 4 : 5;
-  return -1;
-}
-
 // stage one ring cell: u (with ghost rule), diffusivity and parameters
 __device__ __forceinline__ void stage_cell(const Problem& P, const double* __restrict__ uin, int iter,
                                            int a, int b, int c, double& us, double& as, double& ts,
@@ -417,11 +384,13 @@ __global__ void __launch_bounds__(NT) sweep3d_fp64(const Problem* __restrict__ p
 static const TileShape kShapes2D[] = {
     {128, 0, 0, 128, 1}, {64, 0, 0, 64, 1}, {32, 16, 1, 256, 0}, {32, 8, 1, 256, 0},
 };
+// 3D: variant 0 is the plane-marching kernel (reciprocal form); the tile
+// kernels keep the operation-for-operation form
 static const TileShape kShapes3D[] = {
-    {32, 4, 4, 256, 0}, {16, 8, 4, 256, 0},
+    {32, 8, 1, 256, 2}, {32, 4, 4, 256, 0}, {16, 8, 4, 256, 0},
 };
 
-int num_tile_shapes(int ndim) { return ndim == 2 ? 4 : 2; }
+int num_tile_shapes(int ndim) { return ndim == 2 ? 4 : 3; }
 TileShape tile_shape(int ndim, int v) { return ndim == 2 ? kShapes2D[v] : kShapes3D[v]; }
 
 template <int TX, int TY, int TZ, int NT>
@@ -455,7 +424,8 @@ cudaError_t launch_sweep_fp64(int ndim, int variant, int exact, int harmonic, co
     return cudaGetLastError();
   }
   switch (variant) {
-    case 0: return launch3<32, 4, 4, 256>(probs, items, nitems, s);
+    case 0: return launch_march3d_fast(harmonic, probs, items, nitems, s);
+    case 1: return launch3<32, 4, 4, 256>(probs, items, nitems, s);
     default: return launch3<16, 8, 4, 256>(probs, items, nitems, s);
   }
 }

@@ -151,4 +151,37 @@ __device__ __forceinline__ double ld_cg_double(const double* p) {
   return v;
 }
 
+// ghost value of side `side` (0 ilo, 1 ihi, 2 jlo, 3 jhi, 4 klo, 5 khi) at the
+// ghost cell (a, b, c); `src` is the field the rule reads (u or u_prev)
+__device__ __forceinline__ double ghost_value(const Problem& P, const double* __restrict__ src,
+                                              int side, int a, int b, int c) {
+  const int rule = P.rule[side];
+  if (rule == GR_DIRICHLET) return P.val[side];
+  const int axis = side >> 1;
+  const bool lo = (side & 1) == 0;
+  const int n = axis == 0 ? P.ni : (axis == 1 ? P.nj : P.nk);
+  int p;  // position along the axis of the cell the rule reads
+  if (rule == GR_NONE) p = lo ? -1 : n;
+  else if (rule == GR_PERIODIC) p = lo ? n - 1 : 0;
+  else p = lo ? 0 : n - 1;  // Neumann, negative symmetry
+  int aa = a, bb = b, cc = c;
+  if (axis == 0) aa = p;
+  else if (axis == 1) bb = p;
+  else cc = p;
+  const double v = src[fidx(P, aa, bb, cc)];
+  return rule == GR_NEGSYM ? -v : v;
+}
+
+// classify a ring cell: returns -1 if it is neither a domain cell nor a
+// first-layer (non-corner) ghost, else 6 for a domain cell or the side index
+__device__ __forceinline__ int classify(const Problem& P, int a, int b, int c) {
+  const bool ia = a >= 0 && a < P.ni, ib = b >= 0 && b < P.nj;
+  const bool ic = (P.ndim == 2) || (c >= 0 && c < P.nk);
+  if (ia && ib && ic) return 6;
+  if (ib && ic && (a == -1 || a == P.ni)) return a < 0 ? 0 : 1;
+  if (ia && ic && (b == -1 || b == P.nj)) return b < 0 ? 2 : 3;
+  if (P.ndim == 3 && ia && ib && (c == -1 || c == P.nk)) return c < 0 ? 4 : 5;
+  return -1;
+}
+
 }  // namespace cdm

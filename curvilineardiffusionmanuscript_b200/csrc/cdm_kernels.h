@@ -10,7 +10,8 @@ struct Ctrl;
 
 struct TileShape {
   int tx, ty, tz, threads;
-  int march;  // 1: row-marching kernel, tx = threads per block (tx-2 owned columns)
+  int march;  // 1: 2D row-marching kernel, tx = threads per block (tx-2 owned columns);
+              // 2: 3D plane-marching kernel, tx x ty owned cells per k-plane
 };
 
 int num_tile_shapes(int ndim);
@@ -30,6 +31,8 @@ struct SweepStreams {
 cudaError_t launch_march2d_fast(int variant, int harmonic, const Problem* probs, const int2* items, int n_edge,
                                 int n_int, unsigned int* counters, const SweepStreams& ss);
 bool march_tile_interior(int ni, int nj, int tiles_i, int strip_h, int tx, int tile);
+// 3D plane-marching kernel (reciprocal form); items are (problem, column tile + strip)
+cudaError_t launch_march3d_fast(int harmonic, const Problem* probs, const int2* items, int nitems, cudaStream_t s);
 
 // one fused FP64 pseudo-iteration over all items (problem, tile)
 // exact = 1: operation-for-operation reference arithmetic (bit-identical to the

@@ -185,6 +185,9 @@ int Engine::init(int nprob, const cdm_mesh_desc* meshes, const cdm_bc* bcs, cons
     set_error("ndim must be 2 or 3");
     return CDM_BAD_INPUT;
   }
+  // 3D: the plane-marching kernel computes the reciprocal form; the exact form
+  // runs the operation-for-operation tile kernel
+  variant = (ndim == 3 && precision == CDM_PREC_FP64_EXACT) ? 1 : 0;
   if (mean != CDM_MEAN_HARMONIC && mean != CDM_MEAN_ARITHMETIC) {
     set_error("mean must be CDM_MEAN_HARMONIC or CDM_MEAN_ARITHMETIC");
     return CDM_BAD_INPUT;
@@ -387,7 +390,23 @@ int Engine::build_items() {
   const int nprob = (int)ps.size();
   for (int p = 0; p < nprob; ++p) {
     ProbState& s = ps[p];
-    if (ts.march) {
+    if (ts.march == 2) {
+      // 3D: (i, j) column tiles of tx x ty cells marching strips of k-planes;
+      // a single problem gets about 12 strips per SM, none shorter than 8 planes
+      s.tiles_i = (s.ni + ts.tx - 1) / ts.tx;
+      s.tiles_j = (s.nj + ts.ty - 1) / ts.ty;
+      int h = 32;
+      if (strip_h_override > 0) {
+        h = strip_h_override;
+      } else if (nprob == 1) {
+        const int cols = s.tiles_i * s.tiles_j;
+        int nstrips = (148 * 12 + cols - 1) / cols;
+        nstrips = std::max(1, std::min(nstrips, (s.nk + 7) / 8));
+        h = (s.nk + nstrips - 1) / nstrips;
+      }
+      s.strip_h = std::max(1, std::min(h, s.nk));
+      s.tiles_k = (s.nk + s.strip_h - 1) / s.strip_h;
+    } else if (ts.march) {
       // column blocks of tx-2 owned columns; strips of rows sized so that a
       // single problem fills several waves of 148 SMs
       const int ow = ts.tx - 2;
@@ -434,7 +453,7 @@ int Engine::build_items() {
   }
   // the fast 2D kernel runs boundary strips and interior strips as two launches
   n_edge = (int)items.size();
-  if (ts.march && precision != CDM_PREC_FP64_EXACT) {
+  if (ts.march == 1 && precision != CDM_PREC_FP64_EXACT) {
     std::vector<int2> edge, inner;
     for (const int2& it : items) {
       const ProbState& s = ps[it.x];

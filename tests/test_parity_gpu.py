@@ -354,6 +354,41 @@ def test_caller_stream_other_than_the_default():
     assert rel_l2(T.cpu().numpy(), Tr.cpu().numpy()) == 0.0
 
 
+def test_fast_3d_small():
+    """3D plane-marching kernel (reciprocal form) against the oracle."""
+    _, _, out = run_pair(small_case_3d(), **FAST)
+    assert_parity(out, exact=False)
+
+
+@pytest.mark.parametrize("mean", ["harmonic", "arithmetic"])
+def test_fast_3d_mixed_bcs(mean):
+    pr = small_case_3d(n=(12, 7, 9), bcs=[DirichletBC(1.0), NeumannBC(), PeriodicBC(), PeriodicBC(),
+                                          NeumannBC(), DirichletBC(3.0)])
+    _, _, out = run_pair(pr, mean=mean, **FAST)
+    assert_parity(out, exact=False)
+
+
+def test_fast_3d_no_subcycle_negsym():
+    pr = small_case_3d(n=(10, 9, 11), bcs=[FixedNegSymmetryBC(), NeumannBC(), NeumannBC(), DirichletBC(2.0),
+                                           PeriodicBC(), PeriodicBC()])
+    _, _, out = run_pair(pr, subcycle_conductivity=False, **FAST)
+    assert_parity(out, exact=False)
+
+
+def test_fast_and_exact_agree_on_large_3d_grid():
+    """Several column tiles and k-strips (70 x 45 x 37 cells)."""
+    pr = small_case_3d(n=(70, 45, 37))
+    ge = PseudoTransientSolver(pr.mesh, pr.bcs, precision="fp64_exact")
+    gf = PseudoTransientSolver(pr.mesh, pr.bcs, precision="fp64")
+    Te, Tf = pr.T0.clone().cuda(), pr.T0.clone().cuda()
+    rho = pr.rho.cuda()
+    for _ in range(2):
+        se, _ = step(ge, pr.mesh, Te, rho, pr.cp, pr.kappa, pr.dt, rtol=1e-8, atol=1e-8)
+        sf, _ = step(gf, pr.mesh, Tf, rho, pr.cp, pr.kappa, pr.dt, rtol=1e-8, atol=1e-8)
+        assert se["niter"] == sf["niter"]
+        assert rel_l2(Tf.cpu().numpy(), Te.cpu().numpy()) <= TOL
+
+
 def test_divergent_case_reports_nonfinite_like_the_reference():
     """A 300 x 70 mesh makes the reference iteration diverge; the library reports
     the same NONFINITE error at the same pseudo-iteration (exact form)."""
