@@ -45,7 +45,7 @@ struct C3 {
 }  // namespace
 
 template <bool HARM>
-__global__ void __launch_bounds__(NT, 3) march3d_fast(const Problem* __restrict__ probs,
+__global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict__ probs,
                                                       const int2* __restrict__ items) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   M3Smem& sm = *reinterpret_cast<M3Smem*>(smem_raw);
@@ -173,47 +173,80 @@ __global__ void __launch_bounds__(NT, 3) march3d_fast(const Problem* __restrict_
     return qn;
   };
   constexpr int NQI = RY * (TX + 1), NQJ = (TY + 1) * RX, NQK = RY * RX;
-  // i- and j-faces of plane c (cells in slot s) into face slot fs; k-faces
-  // between planes ck (slot sl) and ck + 1 (slot sh), stored at index ck, into k-slot kf
-  auto faces = [&](int c, int s, int fs, bool do_ij, int ck, int sl, int sh, int kf, bool do_k) {
+  constexpr int NSLOT = (NQI + NQJ + NQK + NT - 1) / NT;
+  // Face w of a plane: i-faces [0, NQI), j-faces [NQI, NQI+NQJ) of plane c,
+  // k-faces after that between planes ck and ck + 1 (stored at index ck).
+  // Returns the global index of its old flux, or -1 outside the domain.
+  auto face_at = [&](int w, int c, int ck, int& kind, int& x, int& y) -> int64_t {
+    if (w < NQI) {
+      kind = 0;
+      y = w / (TX + 1);
+      x = w - y * (TX + 1);
+      const int a = i0 - 1 + x, b = j0 - 1 + y;
+      return (c >= 0 && c < nk && a >= -1 && a <= ni - 1 && b >= 0 && b <= nj - 1) ? fidx(P, a, b, c) : -1;
+    }
+    if (w < NQI + NQJ) {
+      kind = 1;
+      w -= NQI;
+      y = w / RX;
+      x = w - y * RX;
+      const int a = i0 - 1 + x, b = j0 - 1 + y;
+      return (c >= 0 && c < nk && a >= 0 && a <= ni - 1 && b >= -1 && b <= nj - 1) ? fidx(P, a, b, c) : -1;
+    }
+    kind = 2;
+    w -= NQI + NQJ;
+    y = w / RX;
+    x = w - y * RX;
+    const int a = i0 - 1 + x, b = j0 - 1 + y;
+    return (ck >= -1 && ck <= nk - 1 && a >= 0 && a <= ni - 1 && b >= 0 && b <= nj - 1) ? fidx(P, a, b, ck) : -1;
+  };
+  // old fluxes of this thread's face slots (w = tid + r·NT), loaded ahead of use
+  auto load_faces = [&](int c, int ck, bool do_k, double* qv) {
+    const int total = NQI + NQJ + (do_k ? NQK : 0);
+#pragma unroll
+    for (int r = 0; r < NSLOT; ++r) {
+      const int w = tid + r * NT;
+      qv[r] = 0.0;
+      if (w < total) {
+        int kind, x, y;
+        const int64_t id = face_at(w, c, ck, kind, x, y);
+        if (id >= 0) qv[r] = kind == 0 ? qiin[id] : (kind == 1 ? qjin[id] : qkin[id]);
+      }
+    }
+  };
+  // new fluxes: i/j faces of plane c (cells in slot s) into face slot fs; k-faces
+  // between planes ck (slot sl) and ck + 1 (slot sh) into k-slot kf
+  auto faces = [&](int c, int s, int fs, int ck, int sl, int sh, int kf, bool do_k, const double* qv) {
     const bool inz = c >= k0 && c < k1;
-    const bool cin = c >= 0 && c < nk;
     const bool kown = (ck >= k0 && ck < k1) || ck == -1;
-    const int total = (do_ij ? NQI + NQJ : 0) + (do_k ? NQK : 0);
-    for (int w = tid; w < total; w += NT) {
-      int f = do_ij ? w : w + NQI + NQJ;
+    const int total = NQI + NQJ + (do_k ? NQK : 0);
+#pragma unroll
+    for (int r = 0; r < NSLOT; ++r) {
+      const int w = tid + r * NT;
+      if (w >= total) continue;
+      int kind, x, y;
+      const int64_t id = face_at(w, c, ck, kind, x, y);
       double qn = 0.0, qp = 0.0;
-      if (f < NQI) {
-        const int y = f / (TX + 1), x = f - y * (TX + 1);
-        const int a = i0 - 1 + x, b = j0 - 1 + y;
-        if (cin && a >= -1 && a <= ni - 1 && b >= 0 && b <= nj - 1) {
-          const int64_t id = fidx(P, a, b, c);
+      if (kind == 0) {
+        if (id >= 0) {
           qn = flux(sm.IA[s][y][x], sm.IA[s][y][x + 1], sm.IT[s][y][x], sm.IT[s][y][x + 1],
-                    sm.U[s][y][x + 1] - sm.U[s][y][x], qiin[id], qp);
-          if (inz && y >= 1 && y <= TY && (x >= 1 || a == -1)) qiout[id] = qn;
+                    sm.U[s][y][x + 1] - sm.U[s][y][x], qv[r], qp);
+          if (inz && y >= 1 && y <= TY && (x >= 1 || i0 + x == 0)) qiout[id] = qn;
         }
         sm.QI[fs][y][x] = qn;
         if (check) sm.PI[fs][y][x] = qp;
-      } else if (f < NQI + NQJ) {
-        f -= NQI;
-        const int y = f / RX, x = f - y * RX;
-        const int a = i0 - 1 + x, b = j0 - 1 + y;
-        if (cin && a >= 0 && a <= ni - 1 && b >= -1 && b <= nj - 1) {
-          const int64_t id = fidx(P, a, b, c);
+      } else if (kind == 1) {
+        if (id >= 0) {
           qn = flux(sm.IA[s][y][x], sm.IA[s][y + 1][x], sm.IT[s][y][x], sm.IT[s][y + 1][x],
-                    sm.U[s][y + 1][x] - sm.U[s][y][x], qjin[id], qp);
-          if (inz && x >= 1 && x <= TX && (y >= 1 || b == -1)) qjout[id] = qn;
+                    sm.U[s][y + 1][x] - sm.U[s][y][x], qv[r], qp);
+          if (inz && x >= 1 && x <= TX && (y >= 1 || j0 + y == 0)) qjout[id] = qn;
         }
         sm.QJ[fs][y][x] = qn;
         if (check) sm.PJ[fs][y][x] = qp;
       } else {
-        f -= NQI + NQJ;
-        const int y = f / RX, x = f - y * RX;
-        const int a = i0 - 1 + x, b = j0 - 1 + y;
-        if (ck >= -1 && ck <= nk - 1 && a >= 0 && a <= ni - 1 && b >= 0 && b <= nj - 1) {
-          const int64_t id = fidx(P, a, b, ck);
+        if (id >= 0) {
           qn = flux(sm.IA[sl][y][x], sm.IA[sh][y][x], sm.IT[sl][y][x], sm.IT[sh][y][x],
-                    sm.U[sh][y][x] - sm.U[sl][y][x], qkin[id], qp);
+                    sm.U[sh][y][x] - sm.U[sl][y][x], qv[r], qp);
           if (kown && x >= 1 && x <= TX && y >= 1 && y <= TY) qkout[id] = qn;
         }
         sm.QK[kf][y][x] = qn;
@@ -247,16 +280,25 @@ __global__ void __launch_bounds__(NT, 3) march3d_fast(const Problem* __restrict_
   // prologue: planes k0-1 and k0, their i/j faces and the k faces between them
   int s_0 = 1, s_p = 0;  // cell slots of planes z and z+1 (z-1 staged into 0 first)
   int f_m = 0, f_0 = 1, f_p = 2, k_m = 0, k_p = 1;
-  C3 prv = stage_plane(k0 - 1, 0);
+  double qa[NSLOT], qb[NSLOT];
+  load_faces(k0 - 1, k0 - 1, true, qa);
+  load_faces(k0, 0, false, qb);
+  double prv_u = stage_plane(k0 - 1, 0).u;  // own cell of the plane below (ghost write at z = 0)
   C3 cur = stage_plane(k0, 1);
   __syncthreads();
-  faces(k0 - 1, 0, f_m, true, k0 - 1, 0, 1, k_m, true);
-  faces(k0, 1, f_0, true, 0, 0, 0, 0, false);
+  faces(k0 - 1, 0, f_m, k0 - 1, 0, 1, k_m, true, qa);
+  faces(k0, 1, f_0, 0, 0, 0, 0, false, qb);
+  load_faces(k0 + 1, k0, true, qa);  // used by the first plane of the loop
   __syncthreads();
 
   double local = 0.0;
   bool local_nan = false;
   for (int z = k0; z < k1; ++z) {
+    // old fluxes of the next plane's faces, one plane ahead of their use
+    if (z + 1 < k1) load_faces(z + 2, z + 1, true, qb);
+    const C3 nxt = stage_plane(z + 1, s_p);
+    __syncthreads();
+    // own cell's coefficients: their loads overlap the face computations
     double cf[9], up = 0.0, S = 0.0;
     const int64_t id = fidx(P, oa, ob, z);
     if (own_in) {
@@ -265,9 +307,7 @@ __global__ void __launch_bounds__(NT, 3) march3d_fast(const Problem* __restrict_
       up = P.u_prev[id];
       S = P.S[id];
     }
-    const C3 nxt = stage_plane(z + 1, s_p);
-    __syncthreads();
-    faces(z + 1, s_p, f_p, true, z, s_0, s_p, k_p, true);
+    faces(z + 1, s_p, f_p, z, s_0, s_p, k_p, true, qa);
     // ghost neighbours of plane z, read before the barrier after which the next
     // plane may overwrite this cell slot
     const double g_im = sm.U[s_0][oy][ox - 1], g_ip = sm.U[s_0][oy][ox + 1];
@@ -282,7 +322,7 @@ __global__ void __launch_bounds__(NT, 3) march3d_fast(const Problem* __restrict_
       if (oa == ni - 1) uout[fidx(P, ni, ob, z)] = g_ip;
       if (ob == 0) uout[fidx(P, oa, -1, z)] = g_jm;
       if (ob == nj - 1) uout[fidx(P, oa, nj, z)] = g_jp;
-      if (z == 0) uout[fidx(P, oa, ob, -1)] = prv.u;
+      if (z == 0) uout[fidx(P, oa, ob, -1)] = prv_u;
       if (z == nk - 1) uout[fidx(P, oa, ob, nk)] = nxt.u;
       if (check) {
         const double dqp = divergence(sm.PI, sm.PJ, sm.PK, f_m, f_0, f_p, k_m, k_p, cf);
@@ -298,7 +338,7 @@ __global__ void __launch_bounds__(NT, 3) march3d_fast(const Problem* __restrict_
       }
     }
     // rotate: planes (z, z+1) become (z-1, z)
-    prv = cur;
+    prv_u = cur.u;
     cur = nxt;
     const int ts = s_0;
     s_0 = s_p;
@@ -310,6 +350,8 @@ __global__ void __launch_bounds__(NT, 3) march3d_fast(const Problem* __restrict_
     const int tk = k_m;
     k_m = k_p;
     k_p = tk;
+#pragma unroll
+    for (int r = 0; r < NSLOT; ++r) qa[r] = qb[r];
   }
   finish_iteration<NT>(P, C, tile, iter, check, local, local_nan, bad, sm.red, &sm.flag);
 }
