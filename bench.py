@@ -77,23 +77,15 @@ def barrier(ws):
 
 
 def allreduce_max(x, ws, device=None):
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device=device)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    """Maximum over ranks (curvilineardiffusionmanuscript_b200.sharding.reduce_max)."""
+    from curvilineardiffusionmanuscript_b200.sharding import reduce_max
+    return reduce_max(x) if ws > 1 else x
 
 
 def allreduce_sum(x, ws, device=None):
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device=device)
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    """Sum over ranks (curvilineardiffusionmanuscript_b200.sharding.reduce_sum)."""
+    from curvilineardiffusionmanuscript_b200.sharding import reduce_sum
+    return reduce_sum(x) if ws > 1 else x
 
 
 # -------------------------------------------------------------------- clocks

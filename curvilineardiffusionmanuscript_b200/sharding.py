@@ -1,0 +1,117 @@
+"""Multi-GPU sharding of independent APT problems (one process per GPU).
+
+A batch of independent problems (the reference runs one `step!` per problem)
+partitions without any exchange of field data: each rank steps the problems
+assigned to it on its own GPU, and only the per-problem statistics are
+gathered on the host.  Problems are assigned longest-processing-time first by
+their cost (cells, optionally × expected pseudo-iterations), which bounds the
+slowest rank at 4/3 of the optimum.
+
+Collectives here are host-side bookkeeping (statistics, timing maxima) over
+whatever process group is initialised: NCCL on GPUs, gloo on CPU (the tests).
+"""
+from __future__ import annotations
+
+from typing import Callable, List, Optional, Sequence
+
+import torch
+import torch.distributed as dist
+
+
+def world() -> tuple:
+    """(rank, world_size) of the default process group, (0, 1) without one."""
+    if dist.is_available() and dist.is_initialized():
+        return dist.get_rank(), dist.get_world_size()
+    return 0, 1
+
+
+def _device():
+    if dist.is_initialized() and dist.get_backend() == "nccl":
+        return torch.device("cuda", torch.cuda.current_device())
+    return torch.device("cpu")
+
+
+def reduce_max(x: float) -> float:
+    """Maximum of x over ranks (the job's time is the slowest rank's)."""
+    r, ws = world()
+    if ws == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=_device())
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(x: float) -> float:
+    """Sum of x over ranks (whole-job work)."""
+    r, ws = world()
+    if ws == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=_device())
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def lpt_assign(costs: Sequence[float], nranks: int) -> List[List[int]]:
+    """Longest-processing-time-first assignment of problem indices to ranks;
+    ties go to the lowest rank, so every rank computes the same assignment."""
+    order = sorted(range(len(costs)), key=lambda i: (-float(costs[i]), i))
+    load = [0.0] * nranks
+    out: List[List[int]] = [[] for _ in range(nranks)]
+    for i in order:
+        r = min(range(nranks), key=lambda k: (load[k], k))
+        out[r].append(i)
+        load[r] += float(costs[i])
+    for lst in out:
+        lst.sort()
+    return out
+
+
+class ShardedBatch:
+    """A batch of problems split over the ranks of the default process group.
+
+    Every rank is given the full lists (meshes, boundary conditions, and at each
+    step the arrays of all problems); it builds a local batch of its own
+    problems only and updates only their temperature arrays.  `step` returns
+    the statistics of all problems in the global order on every rank.
+    """
+
+    def __init__(self, meshes, bcs, costs: Optional[Sequence[float]] = None,
+                 make_batch: Optional[Callable] = None, **batch_kwargs):
+        self.rank, self.world = world()
+        self.n = len(meshes)
+        if costs is None:
+            costs = [m.ni * m.nj * max(1, getattr(m, "nk", 1) or 1) for m in meshes]
+        self.assignment = lpt_assign(costs, self.world)
+        self.local = self.assignment[self.rank]
+        if make_batch is None:
+            from .solver import PseudoTransientBatch
+            make_batch = PseudoTransientBatch
+        self.batch = (make_batch([meshes[i] for i in self.local], [bcs[i] for i in self.local], **batch_kwargs)
+                      if self.local else None)
+
+    def _pick(self, xs):
+        return [xs[i] for i in self.local]
+
+    def step(self, Ts, rhos, cps, kappas, dts, **kwargs):
+        stats, ndts = [], []
+        if self.batch is not None:
+            stats, ndts = self.batch.step(self._pick(Ts), self._pick(rhos), self._pick(cps), self._pick(kappas),
+                                          self._pick(dts), **kwargs)
+        mine = list(zip(self.local, stats, ndts))
+        if self.world > 1:
+            parts: list = [None] * self.world
+            dist.all_gather_object(parts, mine)
+        else:
+            parts = [mine]
+        all_stats: list = [None] * self.n
+        all_ndt: list = [None] * self.n
+        for part in parts:
+            for i, st, nd in part:
+                all_stats[i] = st
+                all_ndt[i] = nd
+        return all_stats, all_ndt
+
+    def close(self):
+        if self.batch is not None:
+            self.batch.close()
+            self.batch = None

@@ -1,0 +1,98 @@
+"""Multi-rank host logic of the sharded batch, as world-size-2 gloo process
+groups on CPU (no GPU): assignment, statistics gather, timing reductions."""
+import os
+import socket
+
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from curvilineardiffusionmanuscript_b200.sharding import ShardedBatch, lpt_assign, reduce_max, reduce_sum
+
+
+class FakeMesh:
+    def __init__(self, n):
+        self.ni = self.nj = n
+        self.nk = 1
+
+
+class FakeBatch:
+    """Stands in for PseudoTransientBatch: records its problems and returns
+    per-problem statistics derived from them."""
+
+    def __init__(self, meshes, bcs, **kw):
+        self.sizes = [m.ni for m in meshes]
+        self.bcs = bcs
+
+    def step(self, Ts, rhos, cps, kappas, dts, **kw):
+        for T in Ts:
+            T += 1.0
+        return [{"niter": s, "bc": b} for s, b in zip(self.sizes, self.bcs)], [d * 2 for d in dts]
+
+    def close(self):
+        pass
+
+
+def test_lpt_assignment_covers_and_balances():
+    costs = [9, 7, 6, 5, 4, 4, 3, 1]
+    parts = lpt_assign(costs, 3)
+    assert sorted(i for p in parts for i in p) == list(range(len(costs)))
+    loads = [sum(costs[i] for i in p) for p in parts]
+    assert max(loads) <= 4 / 3 * (sum(costs) / 3) + max(costs)
+    assert lpt_assign(costs, 1) == [list(range(len(costs)))]
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _worker(rank, world, port, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        sizes = [64, 512, 128, 96, 300, 200, 80]
+        meshes = [FakeMesh(n) for n in sizes]
+        bcs = [f"bc{i}" for i in range(len(sizes))]
+        sb = ShardedBatch(meshes, bcs, make_batch=FakeBatch)
+        Ts = [torch.zeros(3) for _ in sizes]
+        stats, ndt = sb.step(Ts, [None] * 7, [1.0] * 7, [None] * 7, [0.5 * (i + 1) for i in range(7)])
+        updated = [i for i, T in enumerate(Ts) if float(T[0]) == 1.0]
+        tmax = reduce_max(10.0 + rank)
+        tsum = reduce_sum(rank + 1)
+        q.put((rank, sb.local, updated, [s["niter"] for s in stats], [s["bc"] for s in stats], ndt, tmax, tsum))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_batch_two_ranks_gloo():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    sizes = [64, 512, 128, 96, 300, 200, 80]
+    l0, l1 = res[0][1], res[1][1]
+    assert sorted(l0 + l1) == list(range(7)) and not set(l0) & set(l1)
+    for rank, local, updated, niters, bcs, ndt, tmax, tsum in res:
+        # each rank updates only its own problems' arrays
+        assert updated == local
+        # statistics of every problem, in global order, on every rank
+        assert niters == sizes and bcs == [f"bc{i}" for i in range(7)]
+        assert ndt == [1.0 * (i + 1) for i in range(7)]
+        assert tmax == 11.0 and tsum == 3.0
+    # the heaviest problem (512²) sits alone with lighter ones on its rank
+    cost = [n * n for n in sizes]
+    loads = [sum(cost[i] for i in r[1]) for r in res]
+    assert max(loads) <= 1.34 * max(max(cost), sum(cost) / 2)
