@@ -171,10 +171,10 @@ struct RestartIO {
   float* ub32;
   float* ab32;             // diffusivity of the new base state, rounded
   float* R32;
-  const float* e_in[2];    // flux correction of the last sweep (NULL at the first restart)
-  const double* q_in[2];   // FP64 damped-flux state (first restart)
-  float* e_out[2];
-  double* q_out[2];        // FP64 damped-flux state (written at every restart)
+  const float* e_in[3];    // flux correction of the last sweep (NULL at the first restart)
+  const double* q_in[3];   // FP64 damped-flux state (first restart)
+  float* e_out[3];
+  double* q_out[3];        // FP64 damped-flux state (written at every restart)
 };
 
 __global__ void __launch_bounds__(RNT) mixed_restart2d(const Problem* __restrict__ probs, RestartIO io) {
@@ -739,6 +739,502 @@ static cudaError_t launch_mixed_sweep(bool harmonic, const Problem* probs, const
                   : launch_mixed_pair<128, false>(probs, items, n_edge, n_int, counters, ss);
 }
 
+// ---------------------------------------------------------------------------
+// 3D.  Ghost source (offset) of cell (a, b, c) for the side rules: -1 for a
+// constant (Dirichlet) ghost, -2 for a cell that is neither a domain cell nor
+// a first-layer non-corner ghost.
+__device__ __forceinline__ int64_t ghost_src3(const Problem& P, int a, int b, int c, bool& cst, bool& neg,
+                                              double& val) {
+  cst = false;
+  neg = false;
+  val = 0.0;
+  const int cls = classify(P, a, b, c);
+  if (cls < 0) return -2;
+  if (cls == 6) return fidx(P, a, b, c);
+  const int rule = P.rule[cls];
+  if (rule == GR_DIRICHLET) {
+    cst = true;
+    val = P.val[cls];
+    return -1;
+  }
+  const int axis = cls >> 1;
+  const bool lo = (cls & 1) == 0;
+  const int n = axis == 0 ? P.ni : (axis == 1 ? P.nj : P.nk);
+  const int p = rule == GR_NONE ? (lo ? -1 : n) : (rule == GR_PERIODIC ? (lo ? n - 1 : 0) : (lo ? 0 : n - 1));
+  neg = rule == GR_NEGSYM;
+  int aa = a, bb = b, cc = c;
+  if (axis == 0) aa = p;
+  else if (axis == 1) bb = p;
+  else cc = p;
+  return fidx(P, aa, bb, cc);
+}
+
+// FP64 restart in 3D (the 2D restart above, on 16 x 8 x 4 tiles with a ring):
+// u = u_b + δ, ghosts, the carried damped flux split into q′(u) + e, the FP64
+// residual with the undamped fluxes (residuals.jl:105-160) and its max-norm,
+// and the FP32 copies the sweeps read.
+constexpr int R3X = 16, R3Y = 8, R3Z = 4, R3NT = 256;
+struct R3Tile {
+  static constexpr int RX = R3X + 2, RY = R3Y + 2, RZ = R3Z + 2, NR = RX * RY * RZ;
+  static constexpr int NQI = RZ * RY * (R3X + 1), NQJ = RZ * (R3Y + 1) * RX, NQK = (R3Z + 1) * RY * RX;
+  static constexpr size_t bytes = sizeof(double) * (4 * NR + NQI + NQJ + NQK);
+};
+
+__global__ void __launch_bounds__(R3NT) mixed_restart3d(const Problem* __restrict__ probs, RestartIO io, int rti,
+                                                        int rtj) {
+  constexpr int RX = R3Tile::RX, RY = R3Tile::RY, RZ = R3Tile::RZ, NR = R3Tile::NR;
+  extern __shared__ double sm3[];
+  double* s_u = sm3;
+  double* s_a = s_u + NR;
+  double* s_uo = s_a + NR;
+  double* s_ao = s_uo + NR;
+  double* s_qi = s_ao + NR;
+  double* s_qj = s_qi + R3Tile::NQI;
+  double* s_qk = s_qj + R3Tile::NQJ;
+  __shared__ double s_red[R3NT / 32];
+  __shared__ int s_flag;
+  auto R = [](int x, int y, int z) { return x + RX * (y + RY * z); };
+  auto QI = [](int x, int y, int z) { return x + (R3X + 1) * (y + RY * z); };
+  auto QJ = [](int x, int y, int z) { return x + RX * (y + (R3Y + 1) * z); };
+  auto QK = [](int x, int y, int z) { return x + RX * (y + RY * z); };
+  const Problem& P = probs[0];
+  Ctrl* C = P.ctrl;
+  const int tile = blockIdx.x;
+  const int ti = tile % rti, tj = (tile / rti) % rtj, tk = tile / (rti * rtj);
+  const int i0 = ti * R3X, j0 = tj * R3Y, k0 = tk * R3Z;
+  const int tid = threadIdx.x;
+  const int ni = P.ni, nj = P.nj, nk = P.nk;
+  const double dt = P.dt;
+  for (int r = tid; r < NR; r += R3NT) {
+    const int rz = r / (RX * RY), rem = r - rz * RX * RY, ry = rem / RX, rx = rem - ry * RX;
+    const int a = i0 - 1 + rx, b = j0 - 1 + ry, c = k0 - 1 + rz;
+    bool cst, neg;
+    double val;
+    const int64_t so = ghost_src3(P, a, b, c, cst, neg, val);
+    double u = 0.0, al = 0.0, uo = 0.0, alo = 0.0;
+    if (so != -2) {
+      if (cst) {
+        u = uo = val;
+      } else {
+        uo = io.ub_in[so];
+        u = uo + (io.d_in ? (double)io.d_in[so] : 0.0);
+        if (neg) {
+          u = -u;
+          uo = -uo;
+        }
+      }
+      const int64_t o = fidx(P, a, b, c);
+      const double rh = P.rho[o];
+      const double kap = isfinite(u) ? P.k0 * pow_m64(fabs(u), P.kmode, P.km, P.khalf, P.kn) : 0.0;
+      al = kap / (rh * P.cp);
+      if (io.e_in[0]) {
+        const double ko = isfinite(uo) ? P.k0 * pow_m64(fabs(uo), P.kmode, P.km, P.khalf, P.kn) : 0.0;
+        alo = ko / (rh * P.cp);
+      }
+      const bool inx = rx >= 1 && rx <= R3X, iny = ry >= 1 && ry <= R3Y, inz = rz >= 1 && rz <= R3Z;
+      const bool own = (inx && iny && inz) || ((a == -1 || a == ni) && iny && inz) ||
+                       ((b == -1 || b == nj) && inx && inz) || ((c == -1 || c == nk) && inx && iny);
+      if (own) {
+        io.ub_out[o] = u;
+        io.ub32[o] = (float)u;
+        io.ab32[o] = (float)al;
+      }
+    }
+    s_u[r] = u;
+    s_a[r] = al;
+    s_uo[r] = uo;
+    s_ao[r] = alo;
+  }
+  __syncthreads();
+  // faces: the plain flux of the new base, and the split of the carried damped flux
+  auto face = [&](int comp, int r0, int r1, int64_t o, bool own) -> double {
+    const double q = -face_mean(P.mean, s_a[r0], s_a[r1]) * (s_u[r1] - s_u[r0]);
+    if (own) {
+      double total;
+      if (io.e_in[0]) {
+        const double qo = -face_mean(P.mean, s_ao[r0], s_ao[r1]) * (s_uo[r1] - s_uo[r0]);
+        total = qo + (double)io.e_in[comp][o];
+      } else {
+        total = io.q_in[comp][o];
+      }
+      io.e_out[comp][o] = (float)(total - q);
+      io.q_out[comp][o] = total;
+    }
+    return q;
+  };
+  for (int f = tid; f < R3Tile::NQI; f += R3NT) {
+    const int z = f / ((R3X + 1) * RY), rem = f - z * (R3X + 1) * RY, y = rem / (R3X + 1), x = rem - y * (R3X + 1);
+    const int a = i0 - 1 + x, b = j0 - 1 + y, c = k0 - 1 + z;
+    double q = 0.0;
+    if (a >= -1 && a <= ni - 1 && b >= 0 && b <= nj - 1 && c >= 0 && c <= nk - 1)
+      q = face(0, R(x, y, z), R(x + 1, y, z), fidx(P, a, b, c),
+               y >= 1 && y <= R3Y && z >= 1 && z <= R3Z && (x >= 1 || a == -1));
+    s_qi[f] = q;
+  }
+  for (int f = tid; f < R3Tile::NQJ; f += R3NT) {
+    const int z = f / (RX * (R3Y + 1)), rem = f - z * RX * (R3Y + 1), y = rem / RX, x = rem - y * RX;
+    const int a = i0 - 1 + x, b = j0 - 1 + y, c = k0 - 1 + z;
+    double q = 0.0;
+    if (a >= 0 && a <= ni - 1 && b >= -1 && b <= nj - 1 && c >= 0 && c <= nk - 1)
+      q = face(1, R(x, y, z), R(x, y + 1, z), fidx(P, a, b, c),
+               x >= 1 && x <= R3X && z >= 1 && z <= R3Z && (y >= 1 || b == -1));
+    s_qj[f] = q;
+  }
+  for (int f = tid; f < R3Tile::NQK; f += R3NT) {
+    const int z = f / (RX * RY), rem = f - z * RX * RY, y = rem / RX, x = rem - y * RX;
+    const int a = i0 - 1 + x, b = j0 - 1 + y, c = k0 - 1 + z;
+    double q = 0.0;
+    if (a >= 0 && a <= ni - 1 && b >= 0 && b <= nj - 1 && c >= -1 && c <= nk - 1)
+      q = face(2, R(x, y, z), R(x, y, z + 1), fidx(P, a, b, c),
+               x >= 1 && x <= R3X && y >= 1 && y <= R3Y && (z >= 1 || c == -1));
+    s_qk[f] = q;
+  }
+  __syncthreads();
+  double local = 0.0;
+  bool nan = false;
+  for (int e = tid; e < R3X * R3Y * R3Z; e += R3NT) {
+    const int cz = e / (R3X * R3Y), rem = e - cz * R3X * R3Y, cy = rem / R3X, cx = rem - cy * R3X;
+    const int a = i0 + cx, b = j0 + cy, c = k0 + cz;
+    if (a >= ni || b >= nj || c >= nk) continue;
+    const int64_t o = fidx(P, a, b, c);
+    const int x = cx + 1, y = cy + 1, z = cz + 1;
+    const double* cf[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) cf[k] = P.coef[k];
+    // flux_divergence.jl:119-239
+    const double dq =
+        cf[0][o] * (s_qi[QI(x, y, z)] - s_qi[QI(x - 1, y, z)]) + cf[1][o] * (s_qj[QJ(x, y, z)] - s_qj[QJ(x, y - 1, z)]) +
+        cf[2][o] * (s_qk[QK(x, y, z)] - s_qk[QK(x, y, z - 1)]) +
+        cf[3][o] * (0.5 * (s_qi[QI(x, y + 1, z)] + s_qi[QI(x - 1, y + 1, z)]) -
+                    0.5 * (s_qi[QI(x, y - 1, z)] + s_qi[QI(x - 1, y - 1, z)])) +
+        cf[5][o] * (0.5 * (s_qi[QI(x, y, z + 1)] + s_qi[QI(x - 1, y, z + 1)]) -
+                    0.5 * (s_qi[QI(x, y, z - 1)] + s_qi[QI(x - 1, y, z - 1)])) +
+        cf[3][o] * (0.5 * (s_qj[QJ(x + 1, y, z)] + s_qj[QJ(x + 1, y - 1, z)]) -
+                    0.5 * (s_qj[QJ(x - 1, y, z)] + s_qj[QJ(x - 1, y - 1, z)])) +
+        cf[4][o] * (0.5 * (s_qj[QJ(x, y, z + 1)] + s_qj[QJ(x, y - 1, z + 1)]) -
+                    0.5 * (s_qj[QJ(x, y, z - 1)] + s_qj[QJ(x, y - 1, z - 1)])) +
+        cf[4][o] * (0.5 * (s_qk[QK(x, y + 1, z)] + s_qk[QK(x, y + 1, z - 1)]) -
+                    0.5 * (s_qk[QK(x, y - 1, z)] + s_qk[QK(x, y - 1, z - 1)])) +
+        cf[5][o] * (0.5 * (s_qk[QK(x + 1, y, z)] + s_qk[QK(x + 1, y, z - 1)]) -
+                    0.5 * (s_qk[QK(x - 1, y, z)] + s_qk[QK(x - 1, y, z - 1)])) +
+        cf[6][o] * (0.5 * (s_qi[QI(x, y, z)] + s_qi[QI(x - 1, y, z)])) +
+        cf[7][o] * (0.5 * (s_qj[QJ(x, y, z)] + s_qj[QJ(x, y - 1, z)])) +
+        cf[8][o] * (0.5 * (s_qk[QK(x, y, z)] + s_qk[QK(x, y, z - 1)]));
+    const double u = s_u[R(x, y, z)], up = P.u_prev[o];
+    double du = u - up;
+    if (isapprox_eps(u, up)) du = 0.0;
+    const double r = -du / dt - dq + P.S[o];
+    io.R32[o] = (float)r;
+    const double ar = fabs(r);
+    if (ar != ar) nan = true;
+    else local = fmax(local, ar);
+  }
+  reduce_and_publish<R3NT>(P, C, tile, local, nan, s_red, &s_flag, true);
+}
+
+// FP32 correction sweep in 3D: the plane-marching layout of apt_march3d.cu
+// (32 x 8 column, two staged planes, three i/j face planes, two k face planes)
+// with the cells and faces of the 2D increment form above.
+constexpr int X3 = 32, Y3 = 8, NT3 = X3 * Y3, RX3 = X3 + 2, RY3 = Y3 + 2;
+constexpr int NRING3 = RX3 * RY3 - NT3;
+
+struct MixSmem3 {
+  float D[2][RY3][RX3], UB[2][RY3][RX3], AB[2][RY3][RX3], DA[2][RY3][RX3], IT[2][RY3][RX3];
+  float EI[3][RY3][X3 + 1], EJ[3][Y3 + 1][RX3], EK[2][RY3][RX3];
+  float PI[3][RY3][X3 + 1], PJ[3][Y3 + 1][RX3], PK[2][RY3][RX3];
+  double red[NT3 / 32];
+  int flag;
+};
+
+template <bool HARM>
+__global__ void __launch_bounds__(NT3, 3) mixed_sweep3d(const Problem* __restrict__ probs,
+                                                        const int2* __restrict__ items) {
+  __shared__ MixSmem3 sm;
+  const int2 item = items[blockIdx.x];
+  const Problem& P = probs[item.x];
+  Ctrl* C = P.ctrl;
+  if (ld_cg_int(&C->inner_done) || ld_cg_int(&C->done)) return;
+  const int kk = ld_cg_int(&C->inner_iter) + 1;  // inner iteration of this cycle
+  const bool check = (kk % C->inner_check_every) == 0;
+  const int tid = threadIdx.x;
+  const int tile = item.y;
+  const int ti = tile % P.tiles_i, tj = (tile / P.tiles_i) % P.tiles_j, sk = tile / (P.tiles_i * P.tiles_j);
+  const int ni = P.ni, nj = P.nj, nk = P.nk;
+  const int i0 = ti * X3, j0 = tj * Y3;
+  const int k0 = sk * P.strip_h, k1 = min(k0 + P.strip_h, nk);
+  const float* __restrict__ din = P.d32[(kk - 1) & 1];
+  float* __restrict__ dout = P.d32[kk & 1];
+  const float* __restrict__ ein[3] = {P.e32[(kk - 1) & 1][0], P.e32[(kk - 1) & 1][1], P.e32[(kk - 1) & 1][2]};
+  float* __restrict__ eout[3] = {P.e32[kk & 1][0], P.e32[kk & 1][1], P.e32[kk & 1][2]};
+  const float* __restrict__ ub = P.ub32;
+  const float* __restrict__ abv = P.ab32;
+  const float* __restrict__ Rb = P.R32;
+  const float* __restrict__ rho = P.rho32;
+  const float inv_dt = (float)(1.0 / P.dt), dt = (float)P.dt, cp = (float)P.cp, k0c = (float)P.k0;
+  const float LLdt = (float)(P.LL / P.dt), VpL = (float)P.VpL, VpoL = (float)(P.Vpdtau / P.L);
+  const float LoVp = (float)(P.L / P.Vpdtau), VpLdt = (float)(P.VpL * P.dt);
+  const float kn = (float)P.kn;
+  const int kmode = P.kmode, km = P.km, khalf = P.khalf;
+  constexpr float kPiF = 3.14159265358979f;
+
+  const int ox = tid % X3 + 1, oy = tid / X3 + 1;
+  const int oa = i0 + ox - 1, ob = j0 + oy - 1;
+  const bool own_in = oa < ni && ob < nj;
+  int rx = -1, ry = -1;
+  if (tid < NRING3) {
+    if (tid < RX3) {
+      rx = tid;
+      ry = 0;
+    } else if (tid < 2 * RX3) {
+      rx = tid - RX3;
+      ry = RY3 - 1;
+    } else {
+      const int t = tid - 2 * RX3;
+      rx = (t & 1) ? RX3 - 1 : 0;
+      ry = 1 + (t >> 1);
+    }
+  }
+  const int ra = i0 + rx - 1, rb = j0 + ry - 1;
+
+  // cell (a, b, c): correction with its ghost rule, base state and diffusivity
+  // at the cell itself (the restart writes first-layer ghosts), increments
+  auto stage = [&](int a, int b, int c) -> MCell {
+    MCell r{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    bool cst, neg;
+    double val;
+    const int64_t so = ghost_src3(P, a, b, c, cst, neg, val);
+    if (so == -2) return r;
+    const int64_t o = fidx(P, a, b, c);
+    r.d = cst ? 0.f : (neg ? -din[so] : din[so]);
+    r.ub = ub[o];
+    r.ab = abv[o];
+    const float rh = rho[o];
+    float da = 0.f;
+    if (kmode != 0) {
+      const float x = r.d * rcp_a(r.ub);
+      if (fabsf(r.ub) > 1e-30f && fabsf(x) < 1e30f) da = r.ab * incr_pow32(x, kmode, km, khalf, kn);
+      else da = k0c * pow_m32(fabsf(r.ub + r.d), kmode, km, khalf, kn) * rcp_a(rh * cp) - r.ab;
+    }
+    r.da = da;
+    const float al = r.ab + da;
+    if (al > 0.f) {
+      const float Re = kPiF + sqrt_a(kPiF * kPiF + LLdt * rh * rcp_a(al));
+      r.f = VpLdt * rcp_a(fmaf(al * Re, dt, VpL));
+      r.it = HARM ? VpoL * Re : LoVp * rcp_a(Re);
+    } else {
+      r.f = 0.f;
+      r.it = HARM ? __int_as_float(0x7f800000) : 0.f;
+    }
+    return r;
+  };
+  auto stage_plane = [&](int c, int s) -> MCell {
+    const MCell own = stage(oa, ob, c);
+    sm.D[s][oy][ox] = own.d;
+    sm.UB[s][oy][ox] = own.ub;
+    sm.AB[s][oy][ox] = own.ab;
+    sm.DA[s][oy][ox] = own.da;
+    sm.IT[s][oy][ox] = own.it;
+    if (rx >= 0) {
+      const MCell rg = stage(ra, rb, c);
+      sm.D[s][ry][rx] = rg.d;
+      sm.UB[s][ry][rx] = rg.ub;
+      sm.AB[s][ry][rx] = rg.ab;
+      sm.DA[s][ry][rx] = rg.da;
+      sm.IT[s][ry][rx] = rg.it;
+    }
+    return own;
+  };
+  // new flux correction between cells (s0, y0, x0) and (s1, y1, x1), and its undamped part
+  auto face = [&](int s0, int y0, int x0, int s1, int y1, int x1, float eold, float& dqp) -> float {
+    const float ab0 = sm.AB[s0][y0][x0], ab1 = sm.AB[s1][y1][x1];
+    const float da0 = sm.DA[s0][y0][x0], da1 = sm.DA[s1][y1][x1];
+    const float d0 = sm.D[s0][y0][x0], d1 = sm.D[s1][y1][x1];
+    const float ub0 = sm.UB[s0][y0][x0], ub1 = sm.UB[s1][y1][x1];
+    const float it0 = sm.IT[s0][y0][x0], it1 = sm.IT[s1][y1][x1];
+    float en;
+    if (HARM) {
+      const float s = ab0 + ab1;
+      const float is = rcp_a(s);
+      const float abar = 2.f * ab0 * ab1 * is;
+      const float dabar = 2.f * (ab1 * ab1 * da0 + ab0 * ab0 * da1 + da0 * da1 * s) * is * rcp_a(s + da0 + da1);
+      const float St = it0 + it1;
+      dqp = -((abar + dabar) * (d1 - d0) + dabar * (ub1 - ub0));
+      en = fabsf(St) < __int_as_float(0x7f800000) ? (2.f * eold + dqp * St) * rcp_a(St + 2.f) : dqp;
+    } else {
+      const float abar = 0.5f * (ab0 + ab1);
+      const float dabar = 0.5f * (da0 + da1);
+      const float tn = 0.5f * (it0 + it1);
+      dqp = -((abar + dabar) * (d1 - d0) + dabar * (ub1 - ub0));
+      en = (eold * tn + dqp) * rcp_a(1.f + tn);
+    }
+    return en;
+  };
+  constexpr int NQI = RY3 * (X3 + 1), NQJ = (Y3 + 1) * RX3, NQK = RY3 * RX3;
+  constexpr int NSLOT = (NQI + NQJ + NQK + NT3 - 1) / NT3;
+  auto face_at = [&](int w, int c, int ck, int& kind, int& x, int& y) -> int64_t {
+    if (w < NQI) {
+      kind = 0;
+      y = w / (X3 + 1);
+      x = w - y * (X3 + 1);
+      const int a = i0 - 1 + x, b = j0 - 1 + y;
+      return (c >= 0 && c < nk && a >= -1 && a <= ni - 1 && b >= 0 && b <= nj - 1) ? fidx(P, a, b, c) : -1;
+    }
+    if (w < NQI + NQJ) {
+      kind = 1;
+      w -= NQI;
+      y = w / RX3;
+      x = w - y * RX3;
+      const int a = i0 - 1 + x, b = j0 - 1 + y;
+      return (c >= 0 && c < nk && a >= 0 && a <= ni - 1 && b >= -1 && b <= nj - 1) ? fidx(P, a, b, c) : -1;
+    }
+    kind = 2;
+    w -= NQI + NQJ;
+    y = w / RX3;
+    x = w - y * RX3;
+    const int a = i0 - 1 + x, b = j0 - 1 + y;
+    return (ck >= -1 && ck <= nk - 1 && a >= 0 && a <= ni - 1 && b >= 0 && b <= nj - 1) ? fidx(P, a, b, ck) : -1;
+  };
+  auto load_faces = [&](int c, int ck, bool do_k, float* ev) {
+    const int total = NQI + NQJ + (do_k ? NQK : 0);
+#pragma unroll
+    for (int r = 0; r < NSLOT; ++r) {
+      const int w = tid + r * NT3;
+      ev[r] = 0.f;
+      if (w < total) {
+        int kind, x, y;
+        const int64_t id = face_at(w, c, ck, kind, x, y);
+        if (id >= 0) ev[r] = ein[kind][id];
+      }
+    }
+  };
+  auto faces = [&](int c, int s, int fs, int ck, int sl, int sh, int kf, bool do_k, const float* ev) {
+    const bool inz = c >= k0 && c < k1;
+    const bool kown = (ck >= k0 && ck < k1) || ck == -1;
+    const int total = NQI + NQJ + (do_k ? NQK : 0);
+#pragma unroll
+    for (int r = 0; r < NSLOT; ++r) {
+      const int w = tid + r * NT3;
+      if (w >= total) continue;
+      int kind, x, y;
+      const int64_t id = face_at(w, c, ck, kind, x, y);
+      float en = 0.f, dqp = 0.f;
+      if (kind == 0) {
+        if (id >= 0) {
+          en = face(s, y, x, s, y, x + 1, ev[r], dqp);
+          if (inz && y >= 1 && y <= Y3 && (x >= 1 || i0 + x == 0)) eout[0][id] = en;
+        }
+        sm.EI[fs][y][x] = en;
+        if (check) sm.PI[fs][y][x] = dqp;
+      } else if (kind == 1) {
+        if (id >= 0) {
+          en = face(s, y, x, s, y + 1, x, ev[r], dqp);
+          if (inz && x >= 1 && x <= X3 && (y >= 1 || j0 + y == 0)) eout[1][id] = en;
+        }
+        sm.EJ[fs][y][x] = en;
+        if (check) sm.PJ[fs][y][x] = dqp;
+      } else {
+        if (id >= 0) {
+          en = face(sl, y, x, sh, y, x, ev[r], dqp);
+          if (kown && x >= 1 && x <= X3 && y >= 1 && y <= Y3) eout[2][id] = en;
+        }
+        sm.EK[kf][y][x] = en;
+        if (check) sm.PK[kf][y][x] = dqp;
+      }
+    }
+  };
+  auto divergence = [&](const float (*QI)[RY3][X3 + 1], const float (*QJ)[Y3 + 1][RX3], const float (*QK)[RY3][RX3],
+                        int zm, int z0, int zp, int kmn, int kpl, const float* cf) -> float {
+    const int x = ox, y = oy;
+    return cf[0] * (QI[z0][y][x] - QI[z0][y][x - 1]) + cf[1] * (QJ[z0][y][x] - QJ[z0][y - 1][x]) +
+           cf[2] * (QK[kpl][y][x] - QK[kmn][y][x]) +
+           cf[3] * (0.5f * (QI[z0][y + 1][x] + QI[z0][y + 1][x - 1]) - 0.5f * (QI[z0][y - 1][x] + QI[z0][y - 1][x - 1])) +
+           cf[5] * (0.5f * (QI[zp][y][x] + QI[zp][y][x - 1]) - 0.5f * (QI[zm][y][x] + QI[zm][y][x - 1])) +
+           cf[3] * (0.5f * (QJ[z0][y][x + 1] + QJ[z0][y - 1][x + 1]) - 0.5f * (QJ[z0][y][x - 1] + QJ[z0][y - 1][x - 1])) +
+           cf[4] * (0.5f * (QJ[zp][y][x] + QJ[zp][y - 1][x]) - 0.5f * (QJ[zm][y][x] + QJ[zm][y - 1][x])) +
+           cf[4] * (0.5f * (QK[kpl][y + 1][x] + QK[kmn][y + 1][x]) - 0.5f * (QK[kpl][y - 1][x] + QK[kmn][y - 1][x])) +
+           cf[5] * (0.5f * (QK[kpl][y][x + 1] + QK[kmn][y][x + 1]) - 0.5f * (QK[kpl][y][x - 1] + QK[kmn][y][x - 1])) +
+           cf[6] * (0.5f * (QI[z0][y][x] + QI[z0][y][x - 1])) + cf[7] * (0.5f * (QJ[z0][y][x] + QJ[z0][y - 1][x])) +
+           cf[8] * (0.5f * (QK[kpl][y][x] + QK[kmn][y][x]));
+  };
+
+  int s_0 = 1, s_p = 0;
+  int f_m = 0, f_0 = 1, f_p = 2, k_m = 0, k_p = 1;
+  float ea[NSLOT], eb[NSLOT];
+  load_faces(k0 - 1, k0 - 1, true, ea);
+  load_faces(k0, 0, false, eb);
+  stage_plane(k0 - 1, 0);
+  MCell cur = stage_plane(k0, 1);
+  __syncthreads();
+  faces(k0 - 1, 0, f_m, k0 - 1, 0, 1, k_m, true, ea);
+  faces(k0, 1, f_0, 0, 0, 0, 0, false, eb);
+  load_faces(k0 + 1, k0, true, ea);
+  __syncthreads();
+  float local = 0.f;
+  bool nan = false;
+  for (int z = k0; z < k1; ++z) {
+    if (z + 1 < k1) load_faces(z + 2, z + 1, true, eb);
+    const MCell nxt = stage_plane(z + 1, s_p);
+    __syncthreads();
+    float cf[9], R = 0.f;
+    const int64_t id = fidx(P, oa, ob, z);
+    if (own_in) {
+#pragma unroll
+      for (int q = 0; q < 9; ++q) cf[q] = P.coef32[q][id];
+      R = Rb[id];
+    }
+    faces(z + 1, s_p, f_p, z, s_0, s_p, k_p, true, ea);
+    __syncthreads();
+    if (own_in) {
+      const float dq = divergence(sm.EI, sm.EJ, sm.EK, f_m, f_0, f_p, k_m, k_p, cf);
+      const float dn = cur.d + cur.f * (R - cur.d * inv_dt - dq);
+      dout[id] = dn;
+      if (check) {
+        const float dqp = divergence(sm.PI, sm.PJ, sm.PK, f_m, f_0, f_p, k_m, k_p, cf);
+        const float ar = fabsf(R - dn * inv_dt - dqp);
+        if (ar != ar) nan = true;
+        else local = fmaxf(local, ar);
+      }
+    }
+    cur = nxt;
+    const int ts = s_0;
+    s_0 = s_p;
+    s_p = ts;
+    const int tf = f_m;
+    f_m = f_0;
+    f_0 = f_p;
+    f_p = tf;
+    const int tk = k_m;
+    k_m = k_p;
+    k_p = tk;
+#pragma unroll
+    for (int r = 0; r < NSLOT; ++r) ea[r] = eb[r];
+  }
+  if (check) {
+    reduce_and_publish<NT3>(P, C, tile, (double)local, nan, sm.red, &sm.flag, false);
+    if (threadIdx.x == 0 && sm.flag) {
+      C->inner_iter = kk;
+      C->iter += 1;
+      __threadfence();
+    }
+  } else if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned prev = atomicAdd(&C->arrive, 1u);
+    if (prev == (unsigned)P.ntiles - 1u) {
+      C->arrive = 0u;
+      C->inner_iter = kk;
+      C->iter += 1;
+      __threadfence();
+    }
+  }
+}
+
+static cudaError_t launch_mixed_sweep3d(bool harmonic, const Problem* probs, const int2* items, int nitems,
+                                        cudaStream_t s) {
+  if (harmonic) mixed_sweep3d<true><<<nitems, NT3, 0, s>>>(probs, items);
+  else mixed_sweep3d<false><<<nitems, NT3, 0, s>>>(probs, items);
+  return cudaGetLastError();
+}
+
 // FP32 copies of the metric coefficients and of rho
 __global__ void to_f32(const double* __restrict__ src, float* __restrict__ dst, int64_t n) {
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
@@ -748,8 +1244,8 @@ __global__ void to_f32(const double* __restrict__ src, float* __restrict__ dst, 
 // ---------------------------------------------------------------------------
 // host side
 int Engine::mixed_alloc() {
-  if (ndim != 2 || ps.size() != 1) {
-    set_error("mixed precision is available for single 2D problems");
+  if (ps.size() != 1) {
+    set_error("mixed precision is available for single problems (2D or 3D)");
     return CDM_BAD_INPUT;
   }
   ProbState& s = ps[0];
@@ -761,14 +1257,14 @@ int Engine::mixed_alloc() {
   };
   for (int b = 0; b < 2; ++b) {
     CDM_CK(fa(&s.d32[b]));
-    for (int d = 0; d < 2; ++d) CDM_CK(fa(&s.e32[b][d]));
+    for (int d = 0; d < ndim; ++d) CDM_CK(fa(&s.e32[b][d]));
     CDM_CK(cudaMalloc((void**)&s.ub64[b], N * sizeof(double)));
   }
   CDM_CK(fa(&s.ub32));
   CDM_CK(fa(&s.ab32));
   CDM_CK(fa(&s.R32));
   CDM_CK(fa(&s.rho32));
-  for (int k = 0; k < 5; ++k) {
+  for (int k = 0; k < (ndim == 2 ? 5 : 9); ++k) {
     CDM_CK(fa(&s.coef32[k]));
     to_f32<<<1184, 256, 0, stream>>>(s.coef[k], s.coef32[k], (int64_t)N);
     CDM_CK(cudaGetLastError());
@@ -780,8 +1276,18 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
   ProbState& s = ps[0];
   Problem& P = hp[0];
   const size_t N = (size_t)s.nfull;
-  // restart tiling: tiles_j column tiles x rows of RTY
-  const int rti = (s.ni + RTX - 1) / RTX, rtj = (s.nj + RTY - 1) / RTY;
+  // restart tiling: 2D rti x rtj tiles of RTX x RTY, 3D rti x rtj x rtk tiles of R3X x R3Y x R3Z
+  const int rti = ndim == 2 ? (s.ni + RTX - 1) / RTX : (s.ni + R3X - 1) / R3X;
+  const int rtj = ndim == 2 ? (s.nj + RTY - 1) / RTY : (s.nj + R3Y - 1) / R3Y;
+  const int rtk = ndim == 2 ? 1 : (s.nk + R3Z - 1) / R3Z;
+  if (ndim == 3) {
+    static bool attr = false;
+    if (!attr) {
+      CDM_CK(cudaFuncSetAttribute(mixed_restart3d, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)R3Tile::bytes));
+      attr = true;
+    }
+  }
   // the FP32 sweep uses the strips of the 2D row-marching layout (variant 0)
   to_f32<<<1184, 256, 0, stream>>>(P.rho, s.rho32, (int64_t)N);
   CDM_CK(cudaGetLastError());
@@ -807,8 +1313,9 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
   auto restart = [&](const float* d, int ecur) -> int {
     const double* in = restarts == 0 ? s.u[0] : s.ub64[(restarts - 1) & 1];
     double* out = s.ub64[restarts & 1];
-    P.tiles_j = rti;
-    P.ntiles = rti * rtj;
+    const int saved_tj = P.tiles_j;
+    if (ndim == 2) P.tiles_j = rti;
+    P.ntiles = rti * rtj * rtk;
     int rc = upload();
     if (rc != CDM_OK) return rc;
     // the carried flux correction lands in buffer 0, read by the next cycle's
@@ -820,19 +1327,21 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
     io.ub32 = s.ub32;
     io.ab32 = s.ab32;
     io.R32 = s.R32;
-    for (int c = 0; c < 2; ++c) {
-      io.e_in[c] = ecur >= 0 ? s.e32[ecur][c] : nullptr;
-      io.q_in[c] = s.q[s.qpar][c];
-      io.e_out[c] = s.e32[0][c];
-      io.q_out[c] = s.q[s.qpar][c];
+    for (int c = 0; c < 3; ++c) {
+      const bool has = c < ndim;
+      io.e_in[c] = has && ecur >= 0 ? s.e32[ecur][c] : nullptr;
+      io.q_in[c] = has ? s.q[s.qpar][c] : nullptr;
+      io.e_out[c] = has ? s.e32[0][c] : nullptr;
+      io.q_out[c] = has ? s.q[s.qpar][c] : nullptr;
     }
-    mixed_restart2d<<<rti * rtj, RNT, 0, stream>>>(d_probs, io);
+    if (ndim == 2) mixed_restart2d<<<rti * rtj, RNT, 0, stream>>>(d_probs, io);
+    else mixed_restart3d<<<rti * rtj * rtk, R3NT, R3Tile::bytes, stream>>>(d_probs, io, rti, rtj);
     CDM_CK(cudaGetLastError());
     prof.other_launches += 1;
     prof.fp64_cell_evals += s.ndomain;
     rc = poll();
     if (rc != CDM_OK) return rc;
-    P.tiles_j = s.tiles_j;
+    P.tiles_j = saved_tj;
     P.ntiles = s.ntiles;
     ++restarts;
     // clear the correction for the next cycle (the flux correction carries over)
@@ -862,8 +1371,9 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
       CDM_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
       cudaError_t le = cudaSuccess;
       for (int k = 0; k < K && le == cudaSuccess; ++k)
-        le = launch_mixed_sweep(mean == CDM_MEAN_HARMONIC, d_probs, d_items, n_edge, nitems - n_edge, d_counters,
-                                sweep_streams());
+        le = ndim == 2 ? launch_mixed_sweep(mean == CDM_MEAN_HARMONIC, d_probs, d_items, n_edge, nitems - n_edge,
+                                            d_counters, sweep_streams())
+                       : launch_mixed_sweep3d(mean == CDM_MEAN_HARMONIC, d_probs, d_items, nitems, stream);
       cudaError_t ce = cudaStreamEndCapture(stream, &g);
       CDM_CK(le);
       CDM_CK(ce);
@@ -880,8 +1390,9 @@ int Engine::step_mixed(const cdm_step_opts* o, double t_start, double timeout_s)
         prof.sweep_launches += K;
       } else {
         for (int k = 0; k < n - done; ++k)
-          CDM_CK(launch_mixed_sweep(mean == CDM_MEAN_HARMONIC, d_probs, d_items, n_edge, nitems - n_edge, d_counters,
-                                    sweep_streams()));
+          CDM_CK(ndim == 2 ? launch_mixed_sweep(mean == CDM_MEAN_HARMONIC, d_probs, d_items, n_edge, nitems - n_edge,
+                                                d_counters, sweep_streams())
+                           : launch_mixed_sweep3d(mean == CDM_MEAN_HARMONIC, d_probs, d_items, nitems, stream));
         prof.sweep_launches += n - done;
         done = n;
       }

@@ -85,8 +85,46 @@ def test_mixed_state_carries_into_fp64():
     assert np.isfinite(q).all() and np.abs(q).max() > 0 and last > 0
 
 
-def test_mixed_rejects_batches_and_3d():
-    from curvilineardiffusionmanuscript_b200.mesh import wavy_mesh_3d
-    m = wavy_mesh_3d(8, 8, 8)
+def test_mixed_rejects_batches():
+    """The mixed path runs single problems (2D or 3D); a batch asks for FP64."""
+    from curvilineardiffusionmanuscript_b200.mesh import wavy_mesh_2d
+    from curvilineardiffusionmanuscript_b200.solver import PseudoTransientBatch
+    ms = [wavy_mesh_2d(16, 16), wavy_mesh_2d(24, 24)]
     with pytest.raises(APTError):
-        PseudoTransientSolver(m, [NeumannBC()] * 6, precision="mixed")
+        PseudoTransientBatch(ms, [[NeumannBC()] * 4] * 2, precision="mixed")
+
+
+# ----------------------------------------------------------------------- 3D
+def test_mixed_3d_gaussian_matches_oracle():
+    """3D FP32 plane-marching sweeps with FP64 3D restarts against the oracle."""
+    from helpers import small_case_3d
+    for so, sg, To, Tg in run_mixed_vs_oracle(small_case_3d(n=(20, 18, 16)), 3):
+        assert so["status"] == 0 and sg["status"] == 0
+        assert sg["n_restarts"] >= 2
+        assert rel_l2(Tg, To) <= 1e-6, rel_l2(Tg, To)
+
+
+@pytest.mark.parametrize("mean", ["harmonic", "arithmetic"])
+def test_mixed_3d_boundary_conditions(mean):
+    from helpers import small_case_3d
+    from curvilineardiffusionmanuscript_b200.solver import FixedNegSymmetryBC
+    pr = small_case_3d(n=(14, 11, 13), bcs=[DirichletBC(1.0), NeumannBC(), PeriodicBC(), PeriodicBC(),
+                                             FixedNegSymmetryBC(), DirichletBC(3.0)])
+    for so, sg, To, Tg in run_mixed_vs_oracle(pr, 2, mean=mean):
+        assert so["status"] == 0 and sg["status"] == 0
+        assert rel_l2(Tg, To) <= 1e-6, rel_l2(Tg, To)
+
+
+def test_mixed_and_fp64_agree_on_large_3d_grid():
+    """Several column tiles, k-strips and restart tiles (70 x 45 x 37)."""
+    from helpers import small_case_3d
+    pr = small_case_3d(n=(70, 45, 37))
+    gm = PseudoTransientSolver(pr.mesh, pr.bcs, precision="mixed")
+    gf = PseudoTransientSolver(pr.mesh, pr.bcs, precision="fp64")
+    Tm, Tf = pr.T0.clone().cuda(), pr.T0.clone().cuda()
+    rho = pr.rho.cuda()
+    for _ in range(2):
+        sm, _ = step(gm, pr.mesh, Tm, rho, pr.cp, pr.kappa, pr.dt, **KW)
+        sf, _ = step(gf, pr.mesh, Tf, rho, pr.cp, pr.kappa, pr.dt, **KW)
+        assert sm["status"] == 0 and sm["n_restarts"] >= 2
+        assert rel_l2(Tm.cpu().numpy(), Tf.cpu().numpy()) <= 1e-6
