@@ -280,6 +280,10 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
     const Pre Lc = Ln;
     if (j + 1 < j1) prefetch(j + 2, Ln);
     const int o = col + nx * (j + nh);
+    const Cell cp1 = stage(j + 1, Lc);
+    publish(s_p, cp1);
+    __syncthreads();
+    // the row's coefficients: their loads overlap the face computations
     double g11 = 0, g22 = 0, c12 = 0, ca = 0, cbv = 0, up = 0, S = 0;
     if (owner) {
       g11 = G11[o];
@@ -290,9 +294,6 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
       up = uprev[o];
       S = Sg[o];
     }
-    const Cell cp1 = stage(j + 1, Lc);
-    publish(s_p, cp1);
-    __syncthreads();
     double px_p1, py_0n;
     const double qx_p1 = face_x(j + 1, s_p, cp1, Lc.qx, px_p1);
     const double qy_0n = face_y(j, c0, cp1, Lc.qy, py_0n);
@@ -365,7 +366,7 @@ __global__ void __launch_bounds__(TX, 4) march2d_fast_edge(const Problem* __rest
 // Interior strips: persistent blocks claim strips from counters[0] until
 // `nitems` are taken; the last block to leave resets the counters.
 template <int TX, bool HARM>
-__global__ void __launch_bounds__(TX, 5) march2d_fast_inner(const Problem* __restrict__ probs,
+__global__ void __launch_bounds__(TX, 6) march2d_fast_inner(const Problem* __restrict__ probs,
                                                             const int2* __restrict__ items, int nitems,
                                                             unsigned int* counters) {
   __shared__ FastSmem<TX> sm;
