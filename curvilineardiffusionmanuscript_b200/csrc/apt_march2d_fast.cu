@@ -351,7 +351,7 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
 
 // Boundary strips: one block per strip.
 template <int TX, bool HARM>
-__global__ void __launch_bounds__(TX, 4) march2d_fast_edge(const Problem* __restrict__ probs,
+__global__ void __launch_bounds__(TX, 5) march2d_fast_edge(const Problem* __restrict__ probs,
                                                            const int2* __restrict__ items) {
   __shared__ FastSmem<TX> sm;
   const int2 item = items[blockIdx.x];

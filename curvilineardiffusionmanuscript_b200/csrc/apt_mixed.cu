@@ -576,6 +576,10 @@ __device__ __forceinline__ void mixed_body(const Problem& P, Ctrl* C, int tile, 
     const Pre Lc = Ln;
     if (j + 1 < j1) prefetch(j + 2, Ln);
     const int o = col + nx * (j + nh);
+    const MCell cp1 = stage(Lc);
+    publish(s_p, cp1);
+    __syncthreads();
+    // the row's coefficients: their loads overlap the face computations
     float g11 = 0, g22 = 0, c12 = 0, ca = 0, cbv = 0, R = 0;
     if (owner) {
       g11 = G11[o];
@@ -585,9 +589,6 @@ __device__ __forceinline__ void mixed_body(const Problem& P, Ctrl* C, int tile, 
       cbv = CB[o];
       R = Rb[o];
     }
-    const MCell cp1 = stage(Lc);
-    publish(s_p, cp1);
-    __syncthreads();
     float px_p1, py_0n;
     const float qx_p1 = face_x(j + 1, s_p, cp1, Lc.ex, px_p1);
     const float qy_0n = face_y(j, c0, cp1, Lc.ey, py_0n);
@@ -668,7 +669,7 @@ __global__ void __launch_bounds__(TX, 4) mixed_sweep2d_edge(const Problem* __res
 // Interior strips: persistent blocks claim strips from counters[0] until
 // `nitems` are taken; the last block to leave resets the counters.
 template <int TX, bool HARM>
-__global__ void __launch_bounds__(TX, 6) mixed_sweep2d_inner(const Problem* __restrict__ probs,
+__global__ void __launch_bounds__(TX, 7) mixed_sweep2d_inner(const Problem* __restrict__ probs,
                                                              const int2* __restrict__ items, int nitems,
                                                              unsigned int* counters) {
   __shared__ MixSmem<TX> sm;
