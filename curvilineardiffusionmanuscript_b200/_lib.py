@@ -100,6 +100,8 @@ SIGNATURES = {
     "cdm_apt_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, Kappa, C.c_double,
                                C.POINTER(StepOpts), C.POINTER(Stats), PD]),
     "cdm_apt_set_guess": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "cdm_apt_advance": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, Kappa, PD, C.c_double, C.c_int,
+                                  PD, C.c_double, C.POINTER(StepOpts), C.POINTER(Stats), C.POINTER(C.c_int)]),
     "cdm_apt_get_state": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
     "cdm_apt_set_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "cdm_apt_get_metric_cache": (C.c_int, [C.c_void_p, C.c_void_p]),

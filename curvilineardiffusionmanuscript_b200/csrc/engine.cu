@@ -1010,6 +1010,66 @@ int cdm_apt_step(cdm_apt* h, double* T, const double* rho, double cp, cdm_kappa 
   return h->e.step(Ts, rs, &cp, &kappa, &dt, opts, stats, next_dt);
 }
 
+int cdm_apt_advance(cdm_apt* h, double* T, const double* rho, double cp, cdm_kappa kappa, double* t,
+                    double t_end, int max_cycles, double* dt, double dt_max, const cdm_step_opts* opts,
+                    cdm_stats* last, int* nsteps) {
+  if (!h || !T || !rho || !t || !dt || !last || !nsteps) {
+    cdm::set_error("NULL argument");
+    return CDM_BAD_INPUT;
+  }
+  Engine& e = h->e;
+  cdm_step_opts o;
+  cdm_step_opts_default(&o);
+  if (opts) o = *opts;
+  *nsteps = 0;
+  std::memset(last, 0, sizeof(cdm_stats));
+  CDM_CK(cudaSetDevice(e.device));
+  // host arrays are staged on the device once for the whole loop
+  const cdm::ProbState& s = e.ps[0];
+  const size_t bytes = (size_t)s.nfull * sizeof(double);
+  double* Td = T;
+  double* rd = const_cast<double*>(rho);
+  const bool host = o.mem != CDM_MEM_DEVICE;
+  if (host) {
+    CDM_CK(cudaMalloc((void**)&Td, bytes));
+    if (cudaMalloc((void**)&rd, bytes) != cudaSuccess) {
+      cudaFree(Td);
+      cdm::set_error("cdm_apt_advance: allocation failed");
+      return CDM_CUDA_ERROR;
+    }
+    cudaMemcpyAsync(Td, T, bytes, cudaMemcpyHostToDevice, e.stream);
+    cudaMemcpyAsync(rd, rho, bytes, cudaMemcpyHostToDevice, e.stream);
+    o.mem = CDM_MEM_DEVICE;
+  }
+  int rc = CDM_OK;
+  int iter = 0;
+  double ndt = *dt;
+  // the drivers' time loop (test/integrated/2d/gaussian/run.jl:192-231)
+  while (true) {
+    double* Ts[1] = {Td};
+    const double* rs[1] = {rd};
+    rc = e.step(Ts, rs, &cp, &kappa, dt, &o, last, &ndt);
+    if (rc != CDM_OK) break;
+    ++*nsteps;
+    if (*t >= t_end) break;
+    iter += 1;
+    *t += *dt;
+    if (iter >= max_cycles - 1) break;
+    *dt = ndt < dt_max ? ndt : dt_max;
+  }
+  if (host) {
+    cudaError_t ce = cudaMemcpyAsync(T, Td, bytes, cudaMemcpyDeviceToHost, e.stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e.stream);
+    cudaFree(Td);
+    cudaFree(rd);
+    if (ce != cudaSuccess && rc == CDM_OK) {
+      cdm::set_error(std::string("cdm_apt_advance: ") + cudaGetErrorString(ce));
+      rc = CDM_CUDA_ERROR;
+    }
+  }
+  return rc;
+}
+
 int cdm_apt_set_guess(cdm_apt* h, const double* u0, int mem) {
   if (!h || !u0) return CDM_BAD_INPUT;
   return h->e.set_guess(0, u0, mem);

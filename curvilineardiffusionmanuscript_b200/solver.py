@@ -286,6 +286,26 @@ def nonlinear_thermal_conduction_step(solver, mesh, T, rho, cp, kappa, dt, *, sh
     return stats, next_dt
 
 
+def advance(solver: PseudoTransientSolver, mesh, T, rho, cp: float, kappa: PowerLawConductivity, dt: float,
+            t: float = 0.0, t_end: float = math.inf, max_cycles: int = 2 ** 31 - 1, dt_max: float = math.inf,
+            **kwargs):
+    """The drivers' time loop (test/integrated/2d/gaussian/run.jl:192-231) in one
+    library call: -> (t, next_dt, nsteps, last_stats); T is updated in place."""
+    o = step_opts(**kwargs)
+    o.mem = _mem(T)
+    if _mem(rho) != o.mem:
+        raise ValueError("T and rho must live in the same memory space")
+    st = L.Stats()
+    tc, dtc, ns = C.c_double(float(t)), C.c_double(float(dt)), C.c_int(0)
+    rc = solver._lib.cdm_apt_advance(solver._h, _ptr(T), _ptr(rho), float(cp), kappa.as_c(), C.byref(tc),
+                                     float(t_end), int(max_cycles), C.byref(dtc), float(dt_max), C.byref(o),
+                                     C.byref(st), C.byref(ns))
+    stats = stats_dict(st)
+    if rc != L.CDM_OK:
+        raise APTError(rc, L.last_error(), stats)
+    return tc.value, dtc.value, ns.value, stats
+
+
 # ------------------------------------------------------------------------- batch
 class PseudoTransientBatch:
     """Many independent PseudoTransientSolver problems advanced by one launch per

@@ -216,6 +216,19 @@ int cdm_apt_set_source(cdm_apt* h, const double* S, int mem);
 int cdm_apt_step(cdm_apt* h, double* T, const double* rho, double cp, cdm_kappa kappa, double dt,
                  const cdm_step_opts* opts, cdm_stats* stats, double* next_dt);
 
+/* The drivers' time loop around nonlinear_thermal_conduction_step!
+ * (test/integrated/2d/gaussian/run.jl:192-231), in one call: step with *dt;
+ * stop if *t >= t_end (tested before t advances, as the drivers do); else
+ * *t += *dt, count the cycle, stop at max_cycles - 1 cycles, and continue
+ * with *dt = min(next_dt, dt_max).  T (updated in place) and rho are staged on
+ * the device once when opts->mem is host.  On return *t and *dt are the
+ * loop's time and next time step, *nsteps the steps taken and *last the
+ * statistics of the last step; a failing step ends the loop with its status,
+ * T holding the last successful step. */
+int cdm_apt_advance(cdm_apt* h, double* T, const double* rho, double cp, cdm_kappa kappa, double* t,
+                    double t_end, int max_cycles, double* dt, double dt_max, const cdm_step_opts* opts,
+                    cdm_stats* last, int* nsteps);
+
 /* initial guess for the next step (CDM_GUESS_USER); full-size array */
 int cdm_apt_set_guess(cdm_apt* h, const double* u0, int mem);
 

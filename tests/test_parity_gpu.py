@@ -402,3 +402,62 @@ def test_divergent_case_reports_nonfinite_like_the_reference():
              subcycle_conductivity=False)
     assert so["status"] == 2 and ei.value.status == 2
     assert ei.value.stats["niter"] == so["niter"]
+
+
+def drivers_loop(g, pr, T, rho, dt, t_end, max_cycles, dt_max, **kw):
+    """test/integrated/2d/gaussian/run.jl:192-231 with step() calls."""
+    t, it, n = 0.0, 0, 0
+    while True:
+        st, ndt = step(g, pr.mesh, T, rho, pr.cp, pr.kappa, dt, **kw)
+        n += 1
+        if t >= t_end:
+            break
+        it += 1
+        t += dt
+        if it >= max_cycles - 1:
+            break
+        dt = min(ndt, dt_max)
+    return t, dt, n, st
+
+
+@pytest.mark.parametrize("host", [True, False])
+def test_advance_matches_the_drivers_loop(host):
+    """cdm_apt_advance runs the drivers' loop with adaptive Δt in one call:
+    the same steps, times, next Δt and fields as step() called in that loop."""
+    from curvilineardiffusionmanuscript_b200.solver import advance
+    pr = problems.gaussian_2d(64)
+    kw = dict(rtol=1e-8, atol=1e-8)
+    for t_end, max_cycles in ((4e-5, 100), (1.0, 4)):
+        g1 = PseudoTransientSolver(pr.mesh, pr.bcs, precision="fp64_exact")
+        g2 = PseudoTransientSolver(pr.mesh, pr.bcs, precision="fp64_exact")
+        T1 = pr.T0.numpy().copy() if host else pr.T0.clone().cuda()
+        T2 = pr.T0.numpy().copy() if host else pr.T0.clone().cuda()
+        rho = pr.rho.numpy() if host else pr.rho.cuda()
+        r1 = drivers_loop(g1, pr, T1, rho, 1e-5, t_end, max_cycles, 2e-5, **kw)
+        t, dt, n, st = advance(g2, pr.mesh, T2, rho, pr.cp, pr.kappa, 1e-5, t_end=t_end, max_cycles=max_cycles,
+                               dt_max=2e-5, **kw)
+        assert (t, dt, n) == r1[:3]
+        assert st["niter"] == r1[3]["niter"]
+        a = T1 if host else T1.cpu().numpy()
+        b = T2 if host else T2.cpu().numpy()
+        assert np.array_equal(a, b)
+
+
+def test_save_vtk_from_device_state(tmp_path, monkeypatch):
+    """save_vtk writes the state of a step taken on device arrays, in the background."""
+    from test_vtk_cpu import read_vts
+    from curvilineardiffusionmanuscript_b200.vtk import save_vtk
+    monkeypatch.chdir(tmp_path)
+    pr = problems.gaussian_2d(32)
+    g = PseudoTransientSolver(pr.mesh, pr.bcs)
+    T, rho = pr.T0.clone().cuda(), pr.rho.cuda()
+    step(g, pr.mesh, T, rho, pr.cp, pr.kappa, pr.dt, rtol=1e-8, atol=1e-8)
+    fut = save_vtk(g, T, rho, pr.mesh, iteration=3, t=pr.dt, name="gauss", cp=pr.cp, kappa=pr.kappa, dt=pr.dt,
+                   background=True)
+    tv, ext, arr = read_vts(fut.result(timeout=60))
+    dom = pr.mesh.domain()
+    assert tv == pr.dt and ext == [0, 32, 0, 32, 0, 0]
+    assert np.array_equal(arr["u"], T.cpu().numpy()[dom].astype(np.float32).reshape(-1))
+    q, _ = g.get_state()
+    assert np.array_equal(arr["q1"], q[0][dom].astype(np.float32).reshape(-1))
+    assert {"rho", "diffusivity", "dτ_ρ", "θr_dτ", "q2"} <= set(arr)
