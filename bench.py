@@ -190,7 +190,8 @@ def run_reference(args, ws, rank):
     if rank != 0:
         return
     import torch
-    from oracle.oracle import OracleSolver, num_threads
+    from oracle.oracle import OracleSolver, num_threads, set_threads
+    set_threads(len(os.sched_getaffinity(0)))  # every host core this process may use
     probs, cfg = make_workload(args.workload, args.nprob, 0, "cpu")
     sample = probs[: min(len(probs), 6)] if args.workload == "batch" else probs
     solvers = [OracleSolver(p.mesh, p.bcs) for p in sample]
@@ -224,7 +225,8 @@ def run_reference(args, ws, rank):
 
 def cpu_baseline(probs, budget_s=15.0):
     """Oracle (OpenMP, all host threads) on a bounded sample of the workload."""
-    from oracle.oracle import OracleSolver, num_threads
+    from oracle.oracle import OracleSolver, num_threads, set_threads
+    set_threads(len(os.sched_getaffinity(0)))  # every host core this process may use
     t_start = time.perf_counter()
     ci, tt, used = 0, 0.0, 0
     for p in probs:
