@@ -32,6 +32,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 BYTES_PER_CELL_ITER = {2: 120, 3: 184}  # canonical algorithmic bytes, FP64 sweep
+BYTES_PER_CELL_ITER_FP32 = {2: 60, 3: 92}  # FP32 correction sweep (mixed precision)
 
 
 def parse():
@@ -255,7 +256,9 @@ def run_ours(args, ws, rank, local):
     probs, cfg = make_workload(args.workload, args.nprob, rank, dev)
     nd = probs[0].mesh.ndim
     stream = torch.cuda.current_stream(dev)
-    batch = PseudoTransientBatch([p.mesh for p in probs], [p.bcs for p in probs], stream=stream.cuda_stream)
+    mixed = args.precision == "mixed"
+    batch = PseudoTransientBatch([p.mesh for p in probs], [p.bcs for p in probs], stream=stream.cuda_stream,
+                                 precision=args.precision)
     for i, p in enumerate(probs):
         if p.source is not None:
             batch.set_source(i, p.source)
@@ -298,11 +301,12 @@ def run_ours(args, ws, rank, local):
     ci_tot = allreduce_sum(float(ci), ws, dev)
     value = ci_tot / (ms_max / 1e3) / 1e9
     peak, peak_kind = measured_peak()
-    achieved = ci * BYTES_PER_CELL_ITER[nd] / (sweep_ms / 1e3) / 1e9 if sweep_ms > 0 else 0.0
+    bpc = (BYTES_PER_CELL_ITER_FP32 if mixed else BYTES_PER_CELL_ITER)[nd]
+    achieved = ci * bpc / (sweep_ms / 1e3) / 1e9 if sweep_ms > 0 else 0.0
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None, "kernel": f"sweep{nd}d_fp64", "peak_kind": peak_kind,
-            "bytes_per_cell_iter": BYTES_PER_CELL_ITER[nd]}
-    tb, tsrc = traffic_per_cell_iter(nd, args.workload)
+            "traffic": None, "kernel": f"sweep{nd}d_{'fp32' if mixed else 'fp64'}", "peak_kind": peak_kind,
+            "bytes_per_cell_iter": bpc}
+    tb, tsrc = traffic_per_cell_iter(nd, args.workload) if not mixed else (None, None)
     if tb is not None:
         # DRAM bytes per cell-iteration from one ncu capture, times the cells one sweep updates
         roof["traffic"] = tb * ci / max(1, sweep_launches)
@@ -339,7 +343,8 @@ def run_ours(args, ws, rank, local):
         sum(p.mesh.ncells_full for p in probs) * 8 * 16 / 1e9), "parallelism": f"dp{ws} (independent batches)"})
     line = {"metric": "Gcell-iter/s", "value": value, "unit": "Gcell-iter/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
+            "config": cfg,
             "s_per_timestep": ms_max / args.steps / 1e3, "pseudo_iters_per_step": statistics.mean(iters),
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk.summary()}
