@@ -114,7 +114,8 @@ SIGNATURES = {
                                  C.POINTER(Kappa), PD, C.POINTER(StepOpts), C.POINTER(Stats), PD]),
     "cdm_batch_autotune": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), PD,
                                      C.POINTER(Kappa), PD, C.POINTER(StepOpts), C.c_char_p, C.POINTER(C.c_int)]),
-    "cdm_batch_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "cdm_batch_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "cdm_batch_set_tuning": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
     "cdm_apt_get_profile": (C.c_int, [C.c_void_p, C.POINTER(Profile)]),
     "cdm_batch_get_profile": (C.c_int, [C.c_void_p, C.POINTER(Profile)]),
     "cdm_step_reductions_noalloc": (C.c_int, [C.c_int] * 5 + [C.c_void_p] * 5 + [C.c_double] * 5 + [PD, C.c_void_p]),

@@ -29,7 +29,21 @@ namespace {
 constexpr int kStripH[] = {8, 16, 32, 64};
 constexpr int kBlock[] = {4, 8, 16};
 constexpr int kNumBlock = 3;
-constexpr int kNumCand = 4 * kNumBlock;
+// candidates 0..11: marching kernel, strip height kStripH[c / 3], block kBlock[c % 3];
+// 12..17 (2D FP64): tile kernels (variants 2, 3: 32x16 and 32x8 tiles, every row of a
+// tile at once, for grids too small to hide a strip's serial march), block kBlock[c % 3]
+constexpr int kNumMarch = 4 * kNumBlock;
+constexpr int kNumCand = kNumMarch + 2 * kNumBlock;
+
+struct Cand {
+  int variant, strip_h, block;
+};
+
+Cand candidate(int c) {
+  if (c < kNumMarch) return {0, kStripH[c / kNumBlock], kBlock[c % kNumBlock]};
+  const int t = c - kNumMarch;
+  return {2 + t / kNumBlock, 0, kBlock[t % kNumBlock]};
+}
 
 double seconds() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -94,15 +108,19 @@ int Engine::autotune(double* const* T, const double* const* rho, const double* c
                      const double* dt, const cdm_step_opts* opts, const char* cache_path, int* chosen) {
   *chosen = -1;
   if (!tile_shape(ndim, variant).march) return CDM_OK;  // the 3D tile kernels have no strip height
+  // the tile kernels are candidates for 2D FP64 (the mixed sweeps use the marching layout)
+  const int ncand = (ndim == 2 && precision != CDM_PREC_MIXED) ? kNumCand : kNumMarch;
   const std::string key = fingerprint(*this);
   auto apply = [&](int c) -> int {
-    strip_h_override = kStripH[c / kNumBlock];
-    tuned_iter_block = kBlock[c % kNumBlock];
+    const Cand k = candidate(c);
+    variant = k.variant;
+    strip_h_override = k.strip_h;
+    tuned_iter_block = k.block;
     return build_items();
   };
   if (cache_path) {
     const int c = cache_lookup(cache_path, key);
-    if (c >= 0) {
+    if (c >= 0 && c < ncand) {
       *chosen = c;
       return apply(c);
     }
@@ -177,7 +195,7 @@ int Engine::autotune(double* const* T, const double* const* rho, const double* c
   std::vector<double> ndt(nprob);
   int best = -1;
   double best_t = 1e300;
-  for (int c = 0; c < kNumCand && rc == CDM_OK; ++c) {
+  for (int c = 0; c < ncand && rc == CDM_OK; ++c) {
     rc = apply(c);
     // twice from the same state: the first also captures the graph
     for (int rep = 0; rep < 2 && rc == CDM_OK; ++rep) {
@@ -214,9 +232,29 @@ extern "C" int cdm_batch_autotune(cdm_batch* b, double* const* T, const double* 
   return b->e.autotune(T, rho, cp, kappa, dt, opts, cache_path, chosen);
 }
 
-extern "C" int cdm_batch_tuning(const cdm_batch* b, int* strip_h, int* iter_block) {
-  if (!b || !strip_h || !iter_block) return CDM_BAD_INPUT;
+extern "C" int cdm_batch_tuning(const cdm_batch* b, int* variant, int* strip_h, int* iter_block) {
+  if (!b || !variant || !strip_h || !iter_block) return CDM_BAD_INPUT;
+  *variant = b->e.variant;
   *strip_h = b->e.strip_h_override;
   *iter_block = b->e.tuned_iter_block;
   return CDM_OK;
+}
+
+extern "C" int cdm_batch_set_tuning(cdm_batch* b, int variant, int strip_h, int iter_block) {
+  if (!b) return CDM_BAD_INPUT;
+  cdm::Engine& e = b->e;
+  const int nv = cdm::num_tile_shapes(e.ndim);
+  const bool exact3d = e.ndim == 3 && e.precision == CDM_PREC_FP64_EXACT;
+  bool ok = variant >= 0 && variant < nv && strip_h >= 0 && iter_block >= 1 && iter_block <= 64;
+  if (e.precision == CDM_PREC_MIXED) ok = ok && variant == 0;           // FP32 sweeps march
+  if (e.ndim == 3) ok = ok && (exact3d ? variant != 0 : variant == 0);  // 3D: form fixes the kernel
+  if (!ok) {
+    cdm::set_error("cdm_batch_set_tuning: variant, strip height or block length not valid for this batch");
+    return CDM_BAD_INPUT;
+  }
+  CDM_CK(cudaSetDevice(e.device));
+  e.variant = variant;
+  e.strip_h_override = strip_h;
+  e.tuned_iter_block = iter_block;
+  return e.build_items();
 }

@@ -381,10 +381,15 @@ class PseudoTransientBatch:
             raise APTError(rc, L.last_error())
         return ch.value
 
+    def set_tuning(self, variant: int = 0, strip_h: int = 0, iter_block: int = 8):
+        rc = self._lib.cdm_batch_set_tuning(self._h, int(variant), int(strip_h), int(iter_block))
+        if rc != L.CDM_OK:
+            raise APTError(rc, L.last_error())
+
     def tuning(self) -> dict:
-        h, k = C.c_int(0), C.c_int(0)
-        self._lib.cdm_batch_tuning(self._h, C.byref(h), C.byref(k))
-        return {"strip_h": h.value, "iter_block": k.value}
+        v, h, k = C.c_int(0), C.c_int(0), C.c_int(0)
+        self._lib.cdm_batch_tuning(self._h, C.byref(v), C.byref(h), C.byref(k))
+        return {"variant": v.value, "strip_h": h.value, "iter_block": k.value}
 
     def step(self, Ts, rhos, cps, kappas, dts, raise_on_error=True, **kwargs):
         n = self.n

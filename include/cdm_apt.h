@@ -263,7 +263,8 @@ int cdm_batch_step(cdm_batch* b, double* const* T, const double* const* rho, con
 /* Autotuner (no counterpart in the reference).  Times one complete step of
  * this batch per candidate — row-marching strip height h ∈ {8, 16, 32, 64} x
  * iteration-block length K ∈ {4, 8, 16} (graph-replayed iterations between
- * host polls), candidate index 3·index(h) + index(K) — from the given inputs
+ * host polls), candidate index 3·index(h) + index(K); for 2D FP64 also the
+ * tile kernels (32x16 and 32x8 tiles) x K, indices 12..17 — from the given inputs
  * (arguments as cdm_batch_step; T is not modified and the solver state is
  * restored after every trial) and keeps the fastest for later steps.  With
  * cache_path not NULL the choice is read from / written to that JSON file,
@@ -272,8 +273,14 @@ int cdm_batch_step(cdm_batch* b, double* const* T, const double* const* rho, con
 int cdm_batch_autotune(cdm_batch* b, double* const* T, const double* const* rho, const double* cp,
                        const cdm_kappa* kappa, const double* dt, const cdm_step_opts* opts,
                        const char* cache_path, int* chosen);
-/* strip height (0 = built-in heuristic) and iteration-block length in use */
-int cdm_batch_tuning(const cdm_batch* b, int* strip_h, int* iter_block);
+/* kernel variant (0 marching; 2, 3 tile kernels), strip height (0 = built-in
+ * heuristic) and iteration-block length in use */
+int cdm_batch_tuning(const cdm_batch* b, int* variant, int* strip_h, int* iter_block);
+/* apply a tuning without timing (e.g. one found by cdm_batch_autotune on another
+ * run): 2D variant 0 (marching, strip_h 0 = heuristic), 2 or 3 (tile kernels);
+ * 3D variant 0 (marching; the exact form keeps its tile kernel); the mixed path
+ * takes variant 0 only.  iter_block in [1, 64]. */
+int cdm_batch_set_tuning(cdm_batch* b, int variant, int strip_h, int iter_block);
 int cdm_batch_get_profile(const cdm_batch* b, cdm_profile* out);
 
 /* ---- allocation-free end-of-step reductions ------------------------------

@@ -245,10 +245,13 @@ def test_batch_autotune_changes_speed_not_results(tmp_path):
     kw = dict(rtol=0.0, atol=1e-8, max_iter=50000)
     cache = str(tmp_path / "tune.json")
     c = b.autotune(Ts, *args, cache_path=cache, **kw)
-    assert 0 <= c < 12
+    assert 0 <= c < 18
     assert all(np.array_equal(a, t) for a, t in zip(Ts, T0))
     tun = b.tuning()
-    assert tun["strip_h"] == [8, 16, 32, 64][c // 3] and tun["iter_block"] == [4, 8, 16][c % 3]
+    if c < 12:
+        assert tun == {"variant": 0, "strip_h": [8, 16, 32, 64][c // 3], "iter_block": [4, 8, 16][c % 3]}
+    else:
+        assert tun["variant"] == 2 + (c - 12) // 3 and tun["iter_block"] == [4, 8, 16][c % 3]
     for _ in range(2):
         stats, _ = b.step(Ts, *args, **kw)
     for p, pr in enumerate(probs):
@@ -262,6 +265,48 @@ def test_batch_autotune_changes_speed_not_results(tmp_path):
     b2 = PseudoTransientBatch([p.mesh for p in probs], [p.bcs for p in probs], precision="fp64_exact")
     assert b2.autotune([p.T0.numpy().copy() for p in probs], *args, cache_path=cache, **kw) == c
     assert b2.tuning() == tun
+
+
+@pytest.mark.parametrize("tuning", [(0, 0, 8), (0, 8, 4), (2, 0, 16), (3, 0, 1)])
+def test_every_2d_kernel_variant_matches_the_oracle(tuning):
+    """Marching kernel at two strip heights and both tile kernels, exact form:
+    bit-identical to the oracle whatever the tuning."""
+    probs = problems.batch_2d(nprob=4, nmin=20, nmax=90, seed=11)
+    b = PseudoTransientBatch([p.mesh for p in probs], [p.bcs for p in probs], precision="fp64_exact")
+    b.set_tuning(*tuning)
+    assert b.tuning() == dict(zip(("variant", "strip_h", "iter_block"), tuning))
+    Ts = [p.T0.numpy().copy() for p in probs]
+    stats, _ = b.step(Ts, [p.rho.numpy() for p in probs], [p.cp for p in probs], [p.kappa for p in probs],
+                      [p.dt for p in probs], rtol=0.0, atol=1e-8, max_iter=50000)
+    for p, pr in enumerate(probs):
+        o = OracleSolver(pr.mesh, pr.bcs)
+        T = pr.T0.numpy().copy()
+        so, _ = o.step(T, pr.rho.numpy(), pr.cp, pr.kappa.k0, pr.kappa.n, pr.dt, rtol=0.0, atol=1e-8,
+                       max_iter=50000)
+        assert so["niter"] == stats[p]["niter"] and np.array_equal(T, Ts[p]), p
+
+
+def test_fast_form_tile_variant_matches_the_oracle():
+    probs = problems.batch_2d(nprob=3, nmin=30, nmax=80, seed=12)
+    b = PseudoTransientBatch([p.mesh for p in probs], [p.bcs for p in probs], precision="fp64")
+    b.set_tuning(2, 0, 8)
+    Ts = [p.T0.clone().cuda() for p in probs]
+    stats, _ = b.step(Ts, [p.rho.cuda() for p in probs], [p.cp for p in probs], [p.kappa for p in probs],
+                      [p.dt for p in probs], rtol=1e-8, atol=1e-8, max_iter=50000)
+    for p, pr in enumerate(probs):
+        o = OracleSolver(pr.mesh, pr.bcs)
+        T = pr.T0.numpy().copy()
+        so, _ = o.step(T, pr.rho.numpy(), pr.cp, pr.kappa.k0, pr.kappa.n, pr.dt, rtol=1e-8, atol=1e-8,
+                       max_iter=50000)
+        assert so["niter"] == stats[p]["niter"] and rel_l2(Ts[p].cpu().numpy(), T) <= TOL, p
+
+
+def test_set_tuning_rejects_invalid_choices():
+    probs = problems.batch_2d(nprob=2, nmin=20, nmax=30, seed=1)
+    b = PseudoTransientBatch([p.mesh for p in probs], [p.bcs for p in probs])
+    for bad in ((7, 0, 8), (0, -1, 8), (0, 0, 0), (0, 0, 65)):
+        with pytest.raises(APTError):
+            b.set_tuning(*bad)
 
 
 # --------------------------------------------------------------- fast FP64 form
