@@ -206,7 +206,7 @@ template <int TX, int TY, int TZ, int NT>
 __global__ void __launch_bounds__(NT) sweep3d_fp64(const Problem* __restrict__ probs,
                                                    const int2* __restrict__ items) {
   using SM = Smem3<TX, TY, TZ>;
-  constexpr int RX = SM::RX, RY = SM::RY, RZ = SM::RZ;
+  constexpr int RX = SM::RX, RY = SM::RY;
   extern __shared__ double smem[];
   double* s_u = smem;
   double* s_a = s_u + SM::NR;
