@@ -50,6 +50,10 @@ def parse():
     ap.add_argument("--learned-steps", type=int, default=2000, help="APT steps of guess-network training data")
     ap.add_argument("--train-steps", type=int, default=3000, help="optimisation steps of the guess network")
     ap.add_argument("--smooth", type=int, default=8, help="smoothing passes of the predicted correction")
+    ap.add_argument("--net-timing", type=int, default=0, metavar="N",
+                    help="time the guess network: one training step on 16 x 128^2 crops, one N^2 prediction")
+    ap.add_argument("--tuning", default="", metavar="V,H,K",
+                    help="kernel variant, strip height, iteration block (skips the autotuner)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -269,8 +273,12 @@ def run_ours(args, ws, rank, local):
     dts = [p.dt for p in probs]
     kw = dict(rtol=probs[0].rtol, atol=probs[0].atol, max_iter=100000)
     # strip height and iteration-block length timed on this batch (set-up, outside the timed region)
-    tuned = batch.autotune(Ts, rhos, cps, kaps, dts, **kw)
-    cfg["autotune"] = dict(candidate=tuned, **batch.tuning())
+    if args.tuning:
+        batch.set_tuning(*[int(v) for v in args.tuning.split(",")])
+        cfg["tuning"] = batch.tuning()
+    else:
+        tuned = batch.autotune(Ts, rhos, cps, kaps, dts, **kw)
+        cfg["autotune"] = dict(candidate=tuned, **batch.tuning())
 
     def one_step():
         st, _ = batch.step(Ts, rhos, cps, kaps, dts, **kw)
@@ -463,8 +471,48 @@ def run_compare(args):
     print(json.dumps({"compare": res}), flush=True)
 
 
+def run_net_timing(args):
+    """Milliseconds per guess-network training step (16 crops of 128², Adam
+    included) and per N² prediction, CUDA events on the current stream, after
+    `--warmup` untimed repetitions; trained on 2 seeds × 3 APT steps."""
+    import torch
+    from curvilineardiffusionmanuscript_b200 import learned, problems
+    n = args.net_timing
+    make = lambda seed: problems.multi_gaussian_2d(n, seed=seed, device="cuda")
+    pr = make(1)
+    trajs = learned.generate_trajectories(make, seeds=[1, 2], nsteps=3)
+    net = learned.GuessNet(seed=0)
+    ljm = learned.log_jmean(pr.mesh)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, reps):
+        fn(args.warmup)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn(reps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def train(k):
+        learned.train(net, trajs, pr.mesh, pr.kappa.k0, pr.kappa.n, steps=k, batch=16, crop=128)
+
+    def predict(k):
+        for _ in range(k):
+            net.predict(trajs[0][0], trajs[0][1], pr.mesh, pr.kappa.k0, pr.kappa.n, ljm)
+
+    out = {"net_timing": {"train_step_ms": timed(train, args.steps), "predict_ms": timed(predict, args.steps),
+                          "n": n, "batch": 16, "crop": 128, "params": net.nparams}}
+    net.close()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
+    if args.net_timing:
+        run_net_timing(args)
+        return
     if args.compare:
         run_compare(args)
         return
