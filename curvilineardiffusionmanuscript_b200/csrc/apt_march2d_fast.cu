@@ -46,6 +46,7 @@ struct FastSmem {
   double red[TX / 32];
   int flag;
   int ticket;
+  int wok;
 };
 
 struct Cell {
@@ -54,9 +55,12 @@ struct Cell {
 
 }  // namespace
 
-template <int TX, bool EDGE, bool HARM>
+// WAVE: the wavefront schedule, in which other blocks of the same launch write
+// u and q between this block's iterations; those arrays are then read through
+// L2 only (no read-only-path or L1 copies of another block's writes).
+template <int TX, bool EDGE, bool HARM, bool WAVE = false>
 __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, int iter, bool check,
-                                          FastSmem<TX>& sm) {
+                                          FastSmem<TX>& sm, int* wave_count = nullptr) {
   constexpr int OW = TX - 2;
   const int tid = threadIdx.x;
   const int cb = tile % P.tiles_i, sj = tile / P.tiles_i;
@@ -126,11 +130,11 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
     L.ua = 0.0;
     if (!EDGE) {
       L.off = ro;
-      L.u = uin[ro];
+      L.u = WAVE ? __ldcg(uin + ro) : uin[ro];
       if (!alpha_from_u) L.ua = uprev[ro];
       L.rho = rho[ro];
-      L.qx = qx_col ? qxin[ro] : 0.0;
-      L.qy = qyin[ro - nx];
+      L.qx = qx_col ? (WAVE ? __ldcg(qxin + ro) : qxin[ro]) : 0.0;
+      L.qy = WAVE ? __ldcg(qyin + ro - nx) : qyin[ro - nx];
       return;
     }
     int off = -2;
@@ -164,14 +168,14 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
     L.u = cv;
     L.rho = 1.0;
     if (off >= 0) {
-      L.u = uin[off];
+      L.u = WAVE ? __ldcg(uin + off) : uin[off];
       if (!alpha_from_u) L.ua = uprev[off];
     } else if (off == -1) {
       L.ua = cv;
     }
     if (off != -2) L.rho = rho[ro];
-    L.qx = (qx_col && rIn) ? qxin[ro] : 0.0;
-    L.qy = (colIn && r >= 0 && r <= nj) ? qyin[ro - nx] : 0.0;
+    L.qx = (qx_col && rIn) ? (WAVE ? __ldcg(qxin + ro) : qxin[ro]) : 0.0;
+    L.qy = (colIn && r >= 0 && r <= nj) ? (WAVE ? __ldcg(qyin + ro - nx) : qyin[ro - nx]) : 0.0;
   };
 
   int bad = 0;
@@ -346,7 +350,10 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
     y_m = y_0;
     y_0 = u2;
   }
-  finish_iteration<TX>(P, C, tile, iter, check, local, local_nan, bad, sm.red, &sm.flag);
+  // wavefront: every thread's stores are ordered before the arrival that can
+  // release the problem's next iteration to other blocks
+  if (WAVE) __threadfence();
+  finish_iteration<TX>(P, C, tile, iter, check, local, local_nan, bad, sm.red, &sm.flag, wave_count);
 }
 
 // Boundary strips: one block per strip.
@@ -394,6 +401,118 @@ __global__ void __launch_bounds__(TX, 6) march2d_fast_inner(const Problem* __res
       __threadfence();
     }
   }
+}
+
+// Wavefront schedule: one persistent launch runs K pseudo-iterations of every
+// problem.  Ticket t = k·nitems + i stands for iteration k of the launch on
+// item i (a problem's strips together; bit 30 of the tile index marks a
+// boundary strip).  A block holding ticket t with k > 0 waits until its
+// problem has finished iteration k − 1 of the launch (wave_count[p] >= k);
+// only the blocks holding the problem's tickets of iteration k − 1, all below
+// t, can bring that about.  Tickets are taken in order by running blocks, so
+// the lowest unfinished ticket never waits and the schedule cannot deadlock.
+// A problem starts its next iteration as soon as its own strips are done,
+// instead of when the slowest strip of the whole batch is.  Every wait is
+// bounded (about 2 s); a wait that runs out sets counters[3], after which
+// every block of the launch leaves without work and the host reports the step
+// as failed.
+__device__ __forceinline__ int ld_acquire_int(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// thread 0: true once *count >= target; false when the launch's error flag is
+// set or the wait runs out (then it sets the flag)
+__device__ bool wave_wait(const int* count, int target, unsigned int* err) {
+  const unsigned long long t0 = global_ns();
+  unsigned ns = 32;
+  for (int n = 0; n < (1 << 22); ++n) {
+    if (ld_acquire_int(count) >= target) return true;
+    if (ld_cg_int((const int*)err)) return false;
+    if (global_ns() - t0 > 2000000000ull) break;
+    __nanosleep(ns);
+    if (ns < 1024) ns <<= 1;
+  }
+  atomicExch(err, 1u);
+  return false;
+}
+
+// launch prologue: problems already done pass every wait; the ticket restarts
+__global__ void march2d_wave_init(const Problem* __restrict__ probs, int nprob, int* wave_count,
+                                  unsigned int* counters) {
+  for (int p = threadIdx.x; p < nprob; p += blockDim.x)
+    wave_count[p] = ld_cg_int(&probs[p].ctrl->done) ? kWaveDone : 0;
+  if (threadIdx.x == 0) counters[2] = 0u;
+}
+
+template <int TX, bool HARM>
+__global__ void __launch_bounds__(TX, 5) march2d_fast_wave(const Problem* __restrict__ probs,
+                                                           const int2* __restrict__ items, int nitems, int K,
+                                                           unsigned int* counters, int* wave_count) {
+  __shared__ FastSmem<TX> sm;
+  const int total = K * nitems;
+  while (true) {
+    // thread 0 takes the ticket and waits for the problem's previous iteration
+    if (threadIdx.x == 0) {
+      const int t = ld_cg_int((const int*)&counters[3]) ? total : (int)atomicAdd(&counters[2], 1u);
+      int ok = 1;
+      if (t < total && t >= nitems) {
+        const int k = t / nitems;
+        ok = wave_wait(&wave_count[items[t - k * nitems].x], k, &counters[3]);
+      }
+      sm.ticket = t;
+      sm.wok = ok;
+    }
+    __syncthreads();
+    const int t = sm.ticket, ok = sm.wok;
+    __syncthreads();
+    if (t >= total) break;
+    if (!ok) continue;
+    const int k = t / nitems, i = t - k * nitems;
+    const int2 item = items[i];
+    const Problem& P = probs[item.x];
+    Ctrl* C = P.ctrl;
+    if (ld_cg_int(&C->done)) continue;
+    const int iter = ld_cg_int(&C->iter) + 1;
+    const bool check = is_check_iter(C, iter);
+    const int tile = item.y & ((1 << 30) - 1);
+    if (item.y >> 30) fast_body<TX, true, HARM, true>(P, C, tile, iter, check, sm, &wave_count[item.x]);
+    else fast_body<TX, false, HARM, true>(P, C, tile, iter, check, sm, &wave_count[item.x]);
+    __syncthreads();
+  }
+}
+
+template <int TX, bool HARM>
+static cudaError_t launch_wave(const Problem* probs, int nprob, const int2* items, int nitems, int K,
+                               unsigned int* counters, int* wave_count, cudaStream_t s) {
+  static int per_sm = -1, nsm = 0;
+  if (per_sm < 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, march2d_fast_wave<TX, HARM>, TX, 0);
+    if (per_sm < 1) per_sm = 1;
+  }
+  const long long total = (long long)K * nitems;
+  const int grid = (int)(total < (long long)nsm * per_sm ? total : (long long)nsm * per_sm);
+  march2d_wave_init<<<1, 256, 0, s>>>(probs, nprob, wave_count, counters);
+  march2d_fast_wave<TX, HARM><<<grid, TX, 0, s>>>(probs, items, nitems, K, counters, wave_count);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_march2d_wave(int harmonic, const Problem* probs, int nprob, const int2* items, int nitems,
+                                int K, unsigned int* counters, int* wave_count, cudaStream_t s) {
+  if (nitems <= 0 || K <= 0) return cudaSuccess;
+  if ((long long)K * nitems >= (1ll << 31)) return cudaErrorInvalidValue;
+  return harmonic ? launch_wave<128, true>(probs, nprob, items, nitems, K, counters, wave_count, s)
+                  : launch_wave<128, false>(probs, nprob, items, nitems, K, counters, wave_count, s);
 }
 
 // Is tile `tile` of a problem free of domain-boundary logic (no ghost column,

@@ -29,11 +29,16 @@ namespace {
 constexpr int kStripH[] = {8, 16, 32, 64};
 constexpr int kBlock[] = {4, 8, 16};
 constexpr int kNumBlock = 3;
+constexpr int kWaveH[] = {16, 32, 64};
+constexpr int kWaveBlock[] = {8, 16, 32};
 // candidates 0..11: marching kernel, strip height kStripH[c / 3], block kBlock[c % 3];
 // 12..17 (2D FP64): tile kernels (variants 2, 3: 32x16 and 32x8 tiles, every row of a
-// tile at once, for grids too small to hide a strip's serial march), block kBlock[c % 3]
+// tile at once, for grids too small to hide a strip's serial march), block kBlock[c % 3];
+// 18..26 (2D FP64, reciprocal form): the marching kernel on the wavefront schedule
+// (variant 4), strip height kWaveH[t / 3], iterations per launch kWaveBlock[t % 3]
 constexpr int kNumMarch = 4 * kNumBlock;
-constexpr int kNumCand = kNumMarch + 2 * kNumBlock;
+constexpr int kNumTile = kNumMarch + 2 * kNumBlock;
+constexpr int kNumCand = kNumTile + 9;
 
 struct Cand {
   int variant, strip_h, block;
@@ -41,8 +46,12 @@ struct Cand {
 
 Cand candidate(int c) {
   if (c < kNumMarch) return {0, kStripH[c / kNumBlock], kBlock[c % kNumBlock]};
-  const int t = c - kNumMarch;
-  return {2 + t / kNumBlock, 0, kBlock[t % kNumBlock]};
+  if (c < kNumTile) {
+    const int t = c - kNumMarch;
+    return {2 + t / kNumBlock, 0, kBlock[t % kNumBlock]};
+  }
+  const int t = c - kNumTile;
+  return {4, kWaveH[t / 3], kWaveBlock[t % 3]};
 }
 
 double seconds() {
@@ -108,8 +117,10 @@ int Engine::autotune(double* const* T, const double* const* rho, const double* c
                      const double* dt, const cdm_step_opts* opts, const char* cache_path, int* chosen) {
   *chosen = -1;
   if (!tile_shape(ndim, variant).march) return CDM_OK;  // the 3D tile kernels have no strip height
-  // the tile kernels are candidates for 2D FP64 (the mixed sweeps use the marching layout)
-  const int ncand = (ndim == 2 && precision != CDM_PREC_MIXED) ? kNumCand : kNumMarch;
+  // the tile kernels are candidates for 2D FP64 (the mixed sweeps use the marching layout),
+  // the wavefront schedule for the reciprocal form
+  const int ncand = (ndim != 2 || precision == CDM_PREC_MIXED) ? kNumMarch
+                    : (precision == CDM_PREC_FP64_EXACT ? kNumTile : kNumCand);
   const std::string key = fingerprint(*this);
   auto apply = [&](int c) -> int {
     const Cand k = candidate(c);
@@ -248,6 +259,7 @@ extern "C" int cdm_batch_set_tuning(cdm_batch* b, int variant, int strip_h, int 
   bool ok = variant >= 0 && variant < nv && strip_h >= 0 && iter_block >= 1 && iter_block <= 64;
   if (e.precision == CDM_PREC_MIXED) ok = ok && variant == 0;           // FP32 sweeps march
   if (e.ndim == 3) ok = ok && (exact3d ? variant != 0 : variant == 0);  // 3D: form fixes the kernel
+  if (variant == 4) ok = ok && e.precision == CDM_PREC_FP64;              // wavefront: reciprocal form
   if (!ok) {
     cdm::set_error("cdm_batch_set_tuning: variant, strip height or block length not valid for this batch");
     return CDM_BAD_INPUT;

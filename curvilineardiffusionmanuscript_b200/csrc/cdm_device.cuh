@@ -12,6 +12,8 @@
 namespace cdm {
 
 constexpr double kPi = 3.14159265358979323846;
+// wavefront schedule: added to a problem's launch iteration count once it is done
+constexpr int kWaveDone = 1 << 24;
 
 // Resolved ghost-cell rule of one boundary side (applybcs! order semantics,
 // boundary_operators.jl:26-30, folded into one rule per side on the host).

@@ -6,11 +6,13 @@
 
 namespace cdm {
 
-// block-wide reduction of the residual partial and the last-block finish
+// block-wide reduction of the residual partial and the last-block finish.
+// `wave_count` (wavefront schedule only): the problem's count of iterations
+// finished in the current launch, raised by kWaveDone once it is done.
 template <int NT>
 __device__ __forceinline__ void finish_iteration(const Problem& P, Ctrl* C, int tile, int iter,
                                                  bool check, double local, bool local_nan, int bad,
-                                                 double* s_red, int* s_flag) {
+                                                 double* s_red, int* s_flag, int* wave_count = nullptr) {
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   const bool rms = C->norm_kind == 1;
@@ -90,6 +92,10 @@ __device__ __forceinline__ void finish_iteration(const Problem& P, Ctrl* C, int 
     C->arrive = 0u;
     __threadfence();
     C->iter = iter;
+    if (wave_count) {
+      __threadfence();
+      atomicAdd(wave_count, C->done ? kWaveDone : 1);
+    }
   }
 }
 

@@ -11,7 +11,8 @@ struct Ctrl;
 struct TileShape {
   int tx, ty, tz, threads;
   int march;  // 1: 2D row-marching kernel, tx = threads per block (tx-2 owned columns);
-              // 2: 3D plane-marching kernel, tx x ty owned cells per k-plane
+              // 2: 3D plane-marching kernel, tx x ty owned cells per k-plane;
+              // 3: the 2D row-marching kernel on the wavefront schedule
 };
 
 int num_tile_shapes(int ndim);
@@ -31,6 +32,13 @@ struct SweepStreams {
 cudaError_t launch_march2d_fast(int variant, int harmonic, const Problem* probs, const int2* items, int n_edge,
                                 int n_int, unsigned int* counters, const SweepStreams& ss);
 bool march_tile_interior(int ni, int nj, int tiles_i, int strip_h, int tx, int tile);
+// the same kernel on the wavefront schedule: K pseudo-iterations of every problem in one
+// persistent launch, each problem's next iteration starting when its own strips are done.
+// items: each problem's strips together, boundary strips with bit 30 of the tile set.
+// counters[2] is the launch's ticket, counters[3] a flag set when a bounded dependency
+// wait ran out (left set; clear it before the next step); wave_count holds nprob ints.
+cudaError_t launch_march2d_wave(int harmonic, const Problem* probs, int nprob, const int2* items, int nitems,
+                                int K, unsigned int* counters, int* wave_count, cudaStream_t s);
 // 3D plane-marching kernel (reciprocal form); items are (problem, column tile + strip)
 cudaError_t launch_march3d_fast(int harmonic, const Problem* probs, const int2* items, int nitems, cudaStream_t s);
 

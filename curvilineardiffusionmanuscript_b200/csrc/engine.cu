@@ -114,10 +114,12 @@ Engine::~Engine() {
   dfree(d_items);
   dfree(d_flags);
   dfree(d_counters);
+  dfree(d_wave);
   dfree(d_red);
   dfree(d_redout);
   if (h_ctrl) cudaFreeHost(h_ctrl);
   if (h_redout) cudaFreeHost(h_redout);
+  if (h_wave_err) cudaFreeHost(h_wave_err);
   if (ev) cudaEventDestroy(ev);
   for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
   if (ev_caller) cudaEventDestroy(ev_caller);
@@ -370,7 +372,10 @@ int Engine::init(int nprob, const cdm_mesh_desc* meshes, const cdm_bc* bcs, cons
   CDM_CK(cudaMallocHost((void**)&h_ctrl, sizeof(Ctrl) * nprob));
   std::memset(h_ctrl, 0, sizeof(Ctrl) * nprob);
   CDM_CK(dalloc(&d_flags, (size_t)nprob));
-  CDM_CK(dalloc(&d_counters, (size_t)2));
+  CDM_CK(dalloc(&d_counters, (size_t)4));
+  CDM_CK(dalloc(&d_wave, (size_t)nprob));
+  CDM_CK(cudaMallocHost((void**)&h_wave_err, sizeof(unsigned int)));
+  *h_wave_err = 0u;
   CDM_CK(dalloc(&d_red, (size_t)4 * 1024));
   CDM_CK(dalloc(&d_redout, (size_t)8 * nprob));
   CDM_CK(cudaMallocHost((void**)&h_redout, sizeof(double) * 8 * nprob));
@@ -435,8 +440,17 @@ int Engine::build_items() {
     for (int t = 0; t < s.ntiles; ++t) items.push_back(make_int2((int)p, t));
   }
   // interleave tiles of different problems so that a launch spreads every
-  // problem over the whole GPU (uneven batches)
-  if (ps.size() > 1) {
+  // problem over the whole GPU (uneven batches).  The wavefront schedule keeps
+  // each problem's strips together instead: a problem's strips of the next
+  // iteration then come a whole batch of tickets after its strips of this one,
+  // which have finished by the time they are reached, and boundary strips are
+  // tagged in bit 30 of the tile index.
+  if (ts.march == 3) {
+    for (int2& it : items) {
+      const ProbState& s = ps[it.x];
+      if (!march_tile_interior(s.ni, s.nj, s.tiles_i, s.strip_h, ts.tx, it.y)) it.y |= 1 << 30;
+    }
+  } else if (ps.size() > 1) {
     std::vector<int2> mixed;
     mixed.reserve(items.size());
     std::vector<int> next(ps.size(), 0);
@@ -565,12 +579,25 @@ double Engine::collect_profile_ms() {
   return ms;
 }
 
+// K pseudo-iterations: K sweep launches, or one wavefront launch (and its prologue)
+cudaError_t Engine::launch_iters(int K) {
+  if (tile_shape(ndim, variant).march == 3)
+    return launch_march2d_wave(mean == CDM_MEAN_HARMONIC, d_probs, (int)ps.size(), d_items, nitems, K, d_counters,
+                               d_wave, stream);
+  cudaError_t le = cudaSuccess;
+  for (int k = 0; k < K && le == cudaSuccess; ++k)
+    le = launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT, mean == CDM_MEAN_HARMONIC, d_probs,
+                           d_items, nitems, n_edge, d_counters, sweep_streams());
+  return le;
+}
+
 int Engine::launch_block(int K, bool use_graph) {
   const int pe = record_pair();
   if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe], stream));
-  prof.sweep_launches += K;
+  const bool wave = tile_shape(ndim, variant).march == 3;
+  prof.sweep_launches += wave ? 2 : K;
   if (!use_graph) {
-    for (int k = 0; k < K; ++k) CDM_CK(launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT, mean == CDM_MEAN_HARMONIC, d_probs, d_items, nitems, n_edge, d_counters, sweep_streams()));
+    CDM_CK(launch_iters(K));
     if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe + 1], stream));
     return CDM_OK;
   }
@@ -582,9 +609,7 @@ int Engine::launch_block(int K, bool use_graph) {
   if (it == graphs.end()) {
     cudaGraph_t g;
     CDM_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t le = cudaSuccess;
-    for (int k = 0; k < K && le == cudaSuccess; ++k)
-      le = launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT, mean == CDM_MEAN_HARMONIC, d_probs, d_items, nitems, n_edge, d_counters, sweep_streams());
+    const cudaError_t le = launch_iters(K);
     cudaError_t ce = cudaStreamEndCapture(stream, &g);
     if (le != cudaSuccess) {
       set_error(std::string("sweep launch during capture: ") + cudaGetErrorString(le));
@@ -619,8 +644,13 @@ int Engine::run_iterations(const cdm_step_opts* o, int predicted, double t_start
     if (rc != CDM_OK) return rc;
     launched += K;
     CDM_CK(cudaMemcpyAsync(h_ctrl, d_ctrl, sizeof(Ctrl) * nprob, cudaMemcpyDeviceToHost, stream));
+    CDM_CK(cudaMemcpyAsync(h_wave_err, d_counters + 3, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream));
     rc = wait_stream(timeout_s - (now_seconds() - t_start));
     if (rc != CDM_OK) return rc;
+    if (*h_wave_err) {
+      set_error("wavefront sweep: a dependency wait exceeded its limit");
+      return CDM_TIMEOUT;
+    }
     bool all = true;
     for (int p = 0; p < nprob; ++p) all = all && h_ctrl[p].done;
     if (all) return CDM_OK;
@@ -683,7 +713,7 @@ int Engine::probe_plain_norm(const std::vector<int>& guessed, const std::vector<
       prof.other_launches += 1;
     }
   }
-  CDM_CK(cudaMemsetAsync(d_counters, 0, 2 * sizeof(unsigned int), stream));
+  CDM_CK(cudaMemsetAsync(d_counters, 0, 4 * sizeof(unsigned int), stream));
   CDM_CK(cudaMemcpyAsync(d_ctrl, h_ctrl, sizeof(Ctrl) * nprob, cudaMemcpyHostToDevice, stream));
   return CDM_OK;
 }
@@ -838,7 +868,7 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
     predicted = std::min(predicted, o.check_every > 0 ? 0 : std::max(0, C.min_err_check - 1));
   }
   CDM_CK(cudaMemcpyAsync(d_probs, hp.data(), sizeof(Problem) * nprob, cudaMemcpyHostToDevice, stream));
-  CDM_CK(cudaMemsetAsync(d_counters, 0, 2 * sizeof(unsigned int), stream));
+  CDM_CK(cudaMemsetAsync(d_counters, 0, 4 * sizeof(unsigned int), stream));
   CDM_CK(cudaMemcpyAsync(d_ctrl, h_ctrl, sizeof(Ctrl) * nprob, cudaMemcpyHostToDevice, stream));
   int rc = CDM_OK;
   if (any_guess) rc = probe_plain_norm(guessed, inits, t0, timeout_s);

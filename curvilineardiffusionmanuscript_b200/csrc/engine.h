@@ -84,7 +84,10 @@ struct Engine {
   Ctrl* h_ctrl = nullptr;  // pinned mirror
   int2* d_items = nullptr;
   int nitems = 0;
-  unsigned int* d_counters = nullptr;  // tile tickets of the persistent sweep
+  unsigned int* d_counters = nullptr;  // [0, 1] tile tickets of the persistent sweep; [2] wavefront
+                                       // ticket, [3] wavefront wait-expired flag
+  int* d_wave = nullptr;               // wavefront schedule: per problem, iterations done in the launch
+  unsigned int* h_wave_err = nullptr;  // pinned mirror of d_counters[3]
   int n_edge = 0;                      // items [0, n_edge) touch a domain boundary
   cudaStream_t side_stream = nullptr;  // boundary strips run here, concurrently
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -114,6 +117,7 @@ struct Engine {
            const double* dt, const cdm_step_opts* opts, cdm_stats* stats, double* next_dt);
   int run_iterations(const cdm_step_opts* o, int predicted, double t_start, double timeout_s);
   int launch_block(int K, bool use_graph);
+  cudaError_t launch_iters(int K);
   int wait_stream(double timeout_s);
   // Orders a private stream after the work the caller issued to the legacy
   // default stream before this call, so that the caller's device arrays are

@@ -301,12 +301,91 @@ def test_fast_form_tile_variant_matches_the_oracle():
         assert so["niter"] == stats[p]["niter"] and rel_l2(Ts[p].cpu().numpy(), T) <= TOL, p
 
 
+def _run_tunings(probs, tunings, nsteps=3, **kw):
+    """Each tuning on a fresh batch from the same inputs: per-step iteration counts and final fields."""
+    kw = dict(dict(rtol=1e-8, atol=1e-8, max_iter=50000), **kw)
+    out = []
+    for tun in tunings:
+        b = PseudoTransientBatch([p.mesh for p in probs], [p.bcs for p in probs], precision="fp64")
+        for i, pr in enumerate(probs):
+            if pr.source is not None:
+                b.set_source(i, pr.source.cuda())
+        b.set_tuning(*tun)
+        assert b.tuning() == dict(zip(("variant", "strip_h", "iter_block"), tun))
+        Ts = [p.T0.clone().cuda() for p in probs]
+        args = ([p.rho.cuda() for p in probs], [p.cp for p in probs], [p.kappa for p in probs],
+                [p.dt for p in probs])
+        its = []
+        for _ in range(nsteps):
+            st, _ = b.step(Ts, *args, **kw)
+            its.append([x["niter"] for x in st])
+        b.close()
+        out.append((its, [t.cpu() for t in Ts]))
+    return out
+
+
+@pytest.mark.parametrize("K", [1, 7, 32])
+def test_wavefront_schedule_equals_per_iteration_launches(K):
+    """Variant 4 runs the same strips with the same arithmetic as one launch per
+    pseudo-iteration; only strips of different problems' iterations overlap in
+    time, so fields and iteration counts are identical bit for bit, also for
+    problems that converge in the middle of a launch."""
+    probs = problems.batch_2d(nprob=10, nmin=20, nmax=400, seed=21)
+    (i0, T0), (i1, T1) = _run_tunings(probs, [(0, 32, 8), (4, 32, K)])
+    assert len({n for step in i0 for n in step}) > 3  # problems stop at different iterations
+    assert i0 == i1
+    assert all(torch.equal(a, b) for a, b in zip(T0, T1))
+
+
+def test_wavefront_boundary_conditions_sources_and_one_problem():
+    bcs = [[DirichletBC(1.5), NeumannBC(), PeriodicBC(), PeriodicBC()],
+           [FixedNegSymmetryBC(), NeumannBC(), NeumannBC(), DirichletBC(2.0)],
+           [NeumannBC(), PeriodicBC(), NeumannBC(), NeumannBC()]]
+    probs = [small_case_2d(ni=29 + 97 * k, nj=19 + 61 * k, bcs=b, source=True, seed=k) for k, b in enumerate(bcs)]
+    (i0, T0), (i1, T1) = _run_tunings(probs, [(0, 16, 4), (4, 16, 16)])
+    assert i0 == i1 and all(torch.equal(a, b) for a, b in zip(T0, T1))
+    one = [problems.gaussian_2d(300)]
+    (i0, T0), (i1, T1) = _run_tunings(one, [(0, 8, 8), (4, 8, 8)], nsteps=2)
+    assert i0 == i1 and torch.equal(T0[0], T1[0])
+
+
+def test_wavefront_matches_the_oracle():
+    probs = problems.batch_2d(nprob=3, nmin=30, nmax=140, seed=12)
+    ((its, Ts),) = _run_tunings(probs, [(4, 16, 8)], nsteps=1)
+    for p, pr in enumerate(probs):
+        o = OracleSolver(pr.mesh, pr.bcs)
+        T = pr.T0.numpy().copy()
+        so, _ = o.step(T, pr.rho.numpy(), pr.cp, pr.kappa.k0, pr.kappa.n, pr.dt, rtol=1e-8, atol=1e-8,
+                       max_iter=50000)
+        assert so["niter"] == its[0][p] and rel_l2(Ts[p].numpy(), T) <= TOL, p
+
+
+def test_fast_batch_autotune_includes_the_wavefront():
+    probs = problems.batch_2d(nprob=5, nmin=20, nmax=200, seed=3)
+    b = PseudoTransientBatch([p.mesh for p in probs], [p.bcs for p in probs], precision="fp64")
+    Ts = [p.T0.clone().cuda() for p in probs]
+    T0 = [t.clone() for t in Ts]
+    args = ([p.rho.cuda() for p in probs], [p.cp for p in probs], [p.kappa for p in probs], [p.dt for p in probs])
+    c = b.autotune(Ts, *args, rtol=1e-8, atol=1e-8, max_iter=50000)
+    assert 0 <= c < 27 and all(torch.equal(a, t) for a, t in zip(Ts, T0))
+    if c >= 18:
+        assert b.tuning() == {"variant": 4, "strip_h": [16, 32, 64][(c - 18) // 3],
+                              "iter_block": [8, 16, 32][(c - 18) % 3]}
+    b.close()
+
+
 def test_set_tuning_rejects_invalid_choices():
     probs = problems.batch_2d(nprob=2, nmin=20, nmax=30, seed=1)
     b = PseudoTransientBatch([p.mesh for p in probs], [p.bcs for p in probs])
     for bad in ((7, 0, 8), (0, -1, 8), (0, 0, 0), (0, 0, 65)):
         with pytest.raises(APTError):
             b.set_tuning(*bad)
+    # the wavefront schedule runs the reciprocal-form kernel only
+    for prec in ("fp64_exact", "mixed"):
+        bx = PseudoTransientBatch([probs[0].mesh], [probs[0].bcs], precision=prec)
+        with pytest.raises(APTError):
+            bx.set_tuning(4, 32, 8)
+        bx.close()
 
 
 # --------------------------------------------------------------- fast FP64 form
