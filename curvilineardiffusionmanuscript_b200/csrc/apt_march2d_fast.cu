@@ -2,15 +2,18 @@
 //
 // The same discrete iteration as apt_march2d.cu (and the reference's step!,
 // PseudoTransientSolver.jl:253-319), with the divisions of the reference's
-// expressions rewritten algebraically so that a cell needs three or four
-// reciprocals and a face two, instead of 4 + 3 per face + 3 IEEE divisions:
+// expressions rewritten algebraically so that, with harmonic face means, a cell
+// needs two reciprocals and a face one, instead of 4 + 3 per face + 3 IEEE
+// divisions (arithmetic means: four per cell, one per face):
 //
 //   α⁻¹ = ρcₚ/κ,  Re = π + √(π² + (L²/Δt)·ρ·α⁻¹),  dτ = Vp·L·α⁻¹·Re⁻¹,
 //   θ = (L/Vp)·Re⁻¹,  θ⁻¹ = (Vp/L)·Re,           (iteration_parameters.jl:2-15)
-//   harmonic face means  ᾱ = 2/(α⁻¹ₐ + α⁻¹_b),  θ̄ = 2/S_θ with S_θ = θ⁻¹ₐ + θ⁻¹_b,
-//   q ← (qθ̄ − ᾱΔu)/(1 + θ̄) = (2q − ᾱΔu·S_θ)/(S_θ + 2)          (fluxes.jl:5-16)
+//   harmonic face means  ᾱ = 2/A, A = α⁻¹ₐ + α⁻¹_b,  θ̄ = 2/S_θ, S_θ = θ⁻¹ₐ + θ⁻¹_b,
+//   q ← (qθ̄ − ᾱΔu)/(1 + θ̄) = (2qA − 2Δu·S_θ)/(A(S_θ + 2))        (fluxes.jl:5-16)
 //   u ← (u + dτ(uⁿ/Δt − ∇·q + S))/(1 + dτ/Δt)
 //     = u·Δt/(Δt + dτ) + dτΔt/(Δt + dτ)·(uⁿ·Δt⁻¹ − ∇·q + S)      (update.jl:13-15)
+//   with Δt/(Δt + dτ) = Δt·Re/D, dτΔt/(Δt + dτ) = Vp·L·α⁻¹·Δt/D,
+//   D = Δt·Re + Vp·L·α⁻¹
 //
 // Reciprocals come from the hardware approximation refined by two Newton–
 // Raphson steps (y ← y + y(1 − b·y)), accurate to about one ulp, and
@@ -37,6 +40,7 @@ namespace {
 
 using fastmath::pow_fast;
 using fastmath::rcp_nr;
+using fastmath::rcp_pos;
 
 template <int TX>
 struct FastSmem {
@@ -189,19 +193,29 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
     const double rc = L.rho * cp;
     const double inva = rc * rcp_nr(kap);
     const double Re = kPi + sqrt(kPi * kPi + LLdt * L.rho * inva);
-    const double iRe = rcp_nr(Re);
-    double dtau = VpL * inva * iRe;
-    double th = LoVp * iRe;
-    dtau = isfinite(dtau) ? dtau : 0.0;
-    th = isfinite(th) ? th : 0.0;
-    const double id = rcp_nr(dt + dtau);
     c.u = us;
-    c.g = dt * id;
-    c.f = dtau * dt * id;
     if (HARM) {
+      // g = Δt/(Δt + dτ) = Δt·Re/D and f = dτ·g = Vp·L·α⁻¹·Δt/D with
+      // D = Δt·Re + Vp·L·α⁻¹: one reciprocal.  A cell whose dτ is not finite
+      // (κ = 0) keeps its value: g = 1, f = 0, as dτ = 0 gives.
+      const double VA = VpL * inva;
+      const double dRe = dt * Re;
+      const double D = dRe + VA;
+      const bool fin = isfinite(D);
+      const double iD = rcp_pos(fin ? D : 1.0);
+      c.g = fin ? dRe * iD : 1.0;
+      c.f = fin ? VA * dt * iD : 0.0;
       c.ia = inva;
       c.it = VpoL * Re;
     } else {
+      const double iRe = rcp_nr(Re);
+      double dtau = VpL * inva * iRe;
+      double th = LoVp * iRe;
+      dtau = isfinite(dtau) ? dtau : 0.0;
+      th = isfinite(th) ? th : 0.0;
+      const double id = rcp_nr(dt + dtau);
+      c.g = dt * id;
+      c.f = dtau * dt * id;
       c.ia = kap * rcp_nr(rc);
       c.it = th;
     }
@@ -215,19 +229,22 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
   };
 
   auto flux = [&](double ia0, double ia1, double it0, double it1, double du, double qold, double& qp) -> double {
-    double an, qn;
     if (HARM) {
-      an = 2.0 * rcp_nr(ia0 + ia1);
-      const double St = it0 + it1;
-      // θ̄ = 0 when a cell has θ = 0 (θ⁻¹ infinite): q ← −ᾱΔu
-      qn = isfinite(St) ? (2.0 * qold - an * du * St) * rcp_nr(St + 2.0) : -an * du;
-    } else {
-      an = 0.5 * (ia0 + ia1);
-      const double tn = 0.5 * (it0 + it1);
-      qn = (qold * tn - an * du) * rcp_nr(1.0 + tn);
+      // ᾱ = 2/A with A = α⁻¹ₐ + α⁻¹_b: q ← (2q − ᾱΔu·S_θ)/(S_θ + 2)
+      // = (2qA − 2Δu·S_θ)/(A(S_θ + 2)) and the plain flux −ᾱΔu = −2Δu(S_θ + 2)/(A(S_θ + 2)),
+      // over one reciprocal.  θ̄ = 0 when a cell has θ = 0 (θ⁻¹ infinite): q ← −ᾱΔu.
+      const double A = ia0 + ia1, St = it0 + it1;
+      const bool fin = isfinite(St);
+      const double S2 = fin ? St + 2.0 : 1.0;
+      const double R = rcp_nr(A * S2);
+      const double du2 = 2.0 * du;
+      qp = -du2 * S2 * R;
+      return fin ? (2.0 * qold * A - du2 * St) * R : qp;
     }
+    const double an = 0.5 * (ia0 + ia1);
+    const double tn = 0.5 * (it0 + it1);
     qp = -an * du;
-    return qn;
+    return (qold * tn - an * du) * rcp_nr(1.0 + tn);
   };
   // i+1/2 face of row r between this column and the next (neighbour from shared memory)
   auto face_x = [&](int r, int s, const Cell& c, double qold, double& qp) -> double {
@@ -266,11 +283,13 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
   const double qx_0 = face_x(j0, s_0, c0, L1.qx, px_0);
   const double qy_m = face_y(j0 - 1, cm, c0, L1.qy, py_m);
   sm.QX[s_m][tid] = qx_m;
-  sm.PX[s_m][tid] = px_m;
   sm.QX[s_0][tid] = qx_0;
-  sm.PX[s_0][tid] = px_0;
   sm.QY[y_m][tid] = qy_m;
-  sm.PY[y_m][tid] = py_m;
+  if (check) {  // the plain fluxes feed the residual only
+    sm.PX[s_m][tid] = px_m;
+    sm.PX[s_0][tid] = px_0;
+    sm.PY[y_m][tid] = py_m;
+  }
   if (EDGE && j0 == 0 && owner) {
     qyout[col + nx * (nh - 1)] = qy_m;
     uout[col + nx * (nh - 1)] = cm.u;  // row -1 ghost after applybcs!
@@ -302,9 +321,11 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
     const double qx_p1 = face_x(j + 1, s_p, cp1, Lc.qx, px_p1);
     const double qy_0n = face_y(j, c0, cp1, Lc.qy, py_0n);
     sm.QX[s_p][tid] = qx_p1;
-    sm.PX[s_p][tid] = px_p1;
     sm.QY[y_0][tid] = qy_0n;
-    sm.PY[y_0][tid] = py_0n;
+    if (check) {
+      sm.PX[s_p][tid] = px_p1;
+      sm.PY[y_0][tid] = py_0n;
+    }
     __syncthreads();
     if (owner) {
       const int x = tid;

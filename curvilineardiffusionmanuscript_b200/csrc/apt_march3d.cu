@@ -26,6 +26,7 @@ namespace {
 
 using fastmath::pow_fast;
 using fastmath::rcp_nr;
+using fastmath::rcp_pos;
 
 constexpr int TX = 32, TY = 8, NT = TX * TY, RX = TX + 2, RY = TY + 2;
 constexpr int NRING = RX * RY - TX * TY;  // 84 ring cells per plane
@@ -120,19 +121,28 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
     const double rc = rho * cp;
     const double inva = rc * rcp_nr(kap);
     const double Re = kPi + sqrt(kPi * kPi + LLdt * rho * inva);
-    const double iRe = rcp_nr(Re);
-    double dtau = VpL * inva * iRe;
-    double th = LoVp * iRe;
-    dtau = isfinite(dtau) ? dtau : 0.0;
-    th = isfinite(th) ? th : 0.0;
-    const double idd = rcp_nr(dt + dtau);
     r.u = u;
-    r.g = dt * idd;
-    r.f = dtau * dt * idd;
     if (HARM) {
+      // g = Δt·Re/D, f = Vp·L·α⁻¹·Δt/D with D = Δt·Re + Vp·L·α⁻¹ (one reciprocal);
+      // a cell whose dτ is not finite (κ = 0) keeps its value
+      const double VA = VpL * inva;
+      const double dRe = dt * Re;
+      const double D = dRe + VA;
+      const bool fin = isfinite(D);
+      const double iD = rcp_pos(fin ? D : 1.0);
+      r.g = fin ? dRe * iD : 1.0;
+      r.f = fin ? VA * dt * iD : 0.0;
       r.ia = inva;
       r.it = VpoL * Re;
     } else {
+      const double iRe = rcp_nr(Re);
+      double dtau = VpL * inva * iRe;
+      double th = LoVp * iRe;
+      dtau = isfinite(dtau) ? dtau : 0.0;
+      th = isfinite(th) ? th : 0.0;
+      const double idd = rcp_nr(dt + dtau);
+      r.g = dt * idd;
+      r.f = dtau * dt * idd;
       r.ia = kap * rcp_nr(rc);
       r.it = th;
     }
@@ -159,18 +169,21 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
     return own;
   };
   auto flux = [&](double ia0, double ia1, double it0, double it1, double du, double qold, double& qp) -> double {
-    double an, qn;
     if (HARM) {
-      an = 2.0 * rcp_nr(ia0 + ia1);
-      const double St = it0 + it1;
-      qn = isfinite(St) ? (2.0 * qold - an * du * St) * rcp_nr(St + 2.0) : -an * du;
-    } else {
-      an = 0.5 * (ia0 + ia1);
-      const double tn = 0.5 * (it0 + it1);
-      qn = (qold * tn - an * du) * rcp_nr(1.0 + tn);
+      // (2qA − 2Δu·S_θ)/(A(S_θ + 2)) and −2Δu(S_θ + 2)/(A(S_θ + 2)) over one
+      // reciprocal, A = α⁻¹ₐ + α⁻¹_b; θ̄ = 0 (S_θ infinite): q ← −ᾱΔu
+      const double A = ia0 + ia1, St = it0 + it1;
+      const bool fin = isfinite(St);
+      const double S2 = fin ? St + 2.0 : 1.0;
+      const double R = rcp_nr(A * S2);
+      const double du2 = 2.0 * du;
+      qp = -du2 * S2 * R;
+      return fin ? (2.0 * qold * A - du2 * St) * R : qp;
     }
+    const double an = 0.5 * (ia0 + ia1);
+    const double tn = 0.5 * (it0 + it1);
     qp = -an * du;
-    return qn;
+    return (qold * tn - an * du) * rcp_nr(1.0 + tn);
   };
   constexpr int NQI = RY * (TX + 1), NQJ = (TY + 1) * RX, NQK = RY * RX;
   constexpr int NSLOT = (NQI + NQJ + NQK + NT - 1) / NT;

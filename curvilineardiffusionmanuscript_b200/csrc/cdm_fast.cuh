@@ -19,6 +19,17 @@ __device__ __forceinline__ double rcp_nr(double b) {
   return (y0 == 0.0 || fabs(y0) == __longlong_as_double(0x7ff0000000000000ll)) ? y0 : y;
 }
 
+// the same refinement without the 0 / ±inf fix-ups, for arguments known to be
+// positive, finite and normal
+__device__ __forceinline__ double rcp_pos(double b) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+  double e = fma(-b, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-b, y, 1.0);
+  return fma(y, e, y);
+}
+
 // general exponents go through pow() out of line, keeping its temporaries out
 // of the sweep's register budget
 static __device__ __noinline__ double pow_general(double x, double n) { return pow(x, n); }
@@ -26,11 +37,11 @@ static __device__ __noinline__ double pow_general(double x, double n) { return p
 __device__ __forceinline__ double pow_fast(double x, int mode, int m, int half, double n) {
   if (mode == 0) return 1.0;
   if (mode == 1) {
-    double p = 1.0;
-    if (m >= 1) {
-      p = x;
-      for (int e = 1; e < m; ++e) p *= x;
-    }
+    // x^m by repeated products (predicated for the common m <= 3), times √x for half exponents
+    double p = m >= 1 ? x : 1.0;
+    if (m >= 2) p *= x;
+    if (m >= 3) p *= x;
+    for (int e = 3; e < m; ++e) p *= x;
     if (half) p = (m >= 1) ? p * sqrt(x) : sqrt(x);
     return p;
   }
