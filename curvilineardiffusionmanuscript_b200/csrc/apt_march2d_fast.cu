@@ -511,8 +511,7 @@ __global__ void __launch_bounds__(TX, 5) march2d_fast_wave(const Problem* __rest
 }
 
 template <int TX, bool HARM>
-static cudaError_t launch_wave(const Problem* probs, int nprob, const int2* items, int nitems, int K,
-                               unsigned int* counters, int* wave_count, cudaStream_t s) {
+static int wave_slots() {
   static int per_sm = -1, nsm = 0;
   if (per_sm < 0) {
     int dev = 0;
@@ -521,8 +520,17 @@ static cudaError_t launch_wave(const Problem* probs, int nprob, const int2* item
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, march2d_fast_wave<TX, HARM>, TX, 0);
     if (per_sm < 1) per_sm = 1;
   }
+  return nsm * per_sm;
+}
+
+int march2d_wave_slots(int harmonic) { return harmonic ? wave_slots<128, true>() : wave_slots<128, false>(); }
+
+template <int TX, bool HARM>
+static cudaError_t launch_wave(const Problem* probs, int nprob, const int2* items, int nitems, int K,
+                               unsigned int* counters, int* wave_count, cudaStream_t s) {
+  const long long slots = wave_slots<TX, HARM>();
   const long long total = (long long)K * nitems;
-  const int grid = (int)(total < (long long)nsm * per_sm ? total : (long long)nsm * per_sm);
+  const int grid = (int)(total < slots ? total : slots);
   march2d_wave_init<<<1, 256, 0, s>>>(probs, nprob, wave_count, counters);
   march2d_fast_wave<TX, HARM><<<grid, TX, 0, s>>>(probs, items, nitems, K, counters, wave_count);
   return cudaGetLastError();

@@ -39,6 +39,8 @@ bool march_tile_interior(int ni, int nj, int tiles_i, int strip_h, int tx, int t
 // wait ran out (left set; clear it before the next step); wave_count holds nprob ints.
 cudaError_t launch_march2d_wave(int harmonic, const Problem* probs, int nprob, const int2* items, int nitems,
                                 int K, unsigned int* counters, int* wave_count, cudaStream_t s);
+// blocks one wavefront launch keeps resident on the current device
+int march2d_wave_slots(int harmonic);
 // 3D plane-marching kernel (reciprocal form); items are (problem, column tile + strip)
 cudaError_t launch_march3d_fast(int harmonic, const Problem* probs, const int2* items, int nitems, cudaStream_t s);
 

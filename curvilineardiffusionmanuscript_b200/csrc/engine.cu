@@ -479,6 +479,8 @@ int Engine::build_items() {
   }
   dfree(d_items);
   nitems = (int)items.size();
+  items_cap = nitems;
+  retiled = false;
   CDM_CK(cudaMalloc((void**)&d_items, sizeof(int2) * items.size()));
   CDM_CK(cudaMemcpyAsync(d_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, stream));
   CDM_CK(cudaStreamSynchronize(stream));
@@ -658,7 +660,71 @@ int Engine::run_iterations(const cdm_step_opts* o, int predicted, double t_start
       set_error("step exceeded its wall-clock limit");
       return CDM_TIMEOUT;
     }
+    if (tile_shape(ndim, variant).march == 3 && h_ctrl[0].norm_kind == CDM_NORM_MAX) {
+      rc = retile_tail();
+      if (rc != CDM_OK) return rc;
+    }
   }
+}
+
+// Wavefront schedule, once most problems of a batch have converged: the
+// strips of the problems still iterating no longer fill the GPU, and an
+// iteration of each costs the march of one whole strip.  Halve the strip
+// height of those problems (down to 8 rows) until their strips number at least
+// twice the blocks the launch keeps resident, and drop converged problems from
+// the ticket list.  Tiling changes no result under the max norm (the partials
+// of a problem reduce by max), so this applies between launches only.  The
+// step after restores the tuned tiling.
+int Engine::retile_tail() {
+  const int nprob = (int)ps.size();
+  const TileShape ts = tile_shape(ndim, variant);
+  const long long target = 2ll * march2d_wave_slots(mean == CDM_MEAN_HARMONIC);
+  long long strips = 0;
+  int h = 0;
+  for (int p = 0; p < nprob; ++p)
+    if (!h_ctrl[p].done) {
+      strips += ps[p].ntiles;
+      h = std::max(h, ps[p].strip_h);
+    }
+  if (strips >= target || h <= 8) return CDM_OK;
+  auto count = [&](int hh) {
+    long long n = 0;
+    for (int p = 0; p < nprob; ++p)
+      if (!h_ctrl[p].done) n += (long long)ps[p].tiles_i * ((ps[p].nj + hh - 1) / hh);
+    return n;
+  };
+  int hn = h;
+  while (hn > 8 && count(hn) < target) hn = std::max(8, hn / 2);
+  std::vector<int2> items;
+  for (int p = 0; p < nprob; ++p) {
+    if (h_ctrl[p].done) continue;
+    ProbState& s = ps[p];
+    s.strip_h = std::min(hn, s.nj);
+    s.tiles_j = (s.nj + s.strip_h - 1) / s.strip_h;
+    s.ntiles = s.tiles_i * s.tiles_j;
+    hp[p].strip_h = s.strip_h;
+    hp[p].tiles_j = s.tiles_j;
+    hp[p].ntiles = s.ntiles;
+    for (int t = 0; t < s.ntiles; ++t) {
+      int2 it = make_int2(p, t);
+      if (!march_tile_interior(s.ni, s.nj, s.tiles_i, s.strip_h, ts.tx, t)) it.y |= 1 << 30;
+      items.push_back(it);
+    }
+  }
+  if (items.empty()) return CDM_OK;
+  if ((int)items.size() > items_cap) {
+    dfree(d_items);
+    CDM_CK(cudaMalloc((void**)&d_items, sizeof(int2) * items.size()));
+    items_cap = (int)items.size();
+  }
+  CDM_CK(cudaMemcpyAsync(d_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, stream));
+  CDM_CK(cudaMemcpyAsync(d_probs, hp.data(), sizeof(Problem) * nprob, cudaMemcpyHostToDevice, stream));
+  CDM_CK(cudaStreamSynchronize(stream));
+  nitems = (int)items.size();
+  n_edge = nitems;
+  retiled = true;
+  free_graphs();
+  return CDM_OK;
 }
 
 // Network prediction of this step's solution from (Tⁿ⁻¹, Tⁿ, κ, J): 1 when
@@ -728,6 +794,10 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
   CDM_CK(cudaSetDevice(device));
   std::memset(&prof, 0, sizeof(prof));
   ev_used = 0;
+  if (retiled) {  // the last step's tail shortened strips: back to the tuned tiling
+    const int rb = build_items();
+    if (rb != CDM_OK) return rb;
+  }
   double timeout_s = 3600.0;
   if (const char* e = std::getenv("CDM_STEP_TIMEOUT_S")) timeout_s = std::atof(e);
   for (int p = 0; p < nprob; ++p) {

@@ -117,6 +117,9 @@ struct Engine {
            const double* dt, const cdm_step_opts* opts, cdm_stats* stats, double* next_dt);
   int run_iterations(const cdm_step_opts* o, int predicted, double t_start, double timeout_s);
   int launch_block(int K, bool use_graph);
+  int retile_tail();
+  int items_cap = 0;     // capacity of d_items
+  bool retiled = false;  // the tail of the last step shortened strips (restored at the next step)
   cudaError_t launch_iters(int K);
   int wait_stream(double timeout_s);
   // Orders a private stream after the work the caller issued to the legacy
