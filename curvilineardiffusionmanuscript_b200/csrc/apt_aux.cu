@@ -1,4 +1,6 @@
 // apt_aux.cu — once-per-step and once-per-mesh kernels of the APT path.
+#include <algorithm>
+
 #include "cdm_device.cuh"
 #include "cdm_kernels.h"
 
@@ -134,20 +136,21 @@ __global__ void clamp_kernel(double* u, int64_t n, int positivity, int cutoff) {
 constexpr int kRedBlocks = 592;  // 4 x 148 SMs
 constexpr int kRedThreads = 256;
 
-// pass 1: max(u_prev) with NaN propagation, energy sums and source integral
-__global__ void reduce_pass1(Problem P, const double* __restrict__ u, const double* __restrict__ J,
-                             double* scratch) {
+// pass 1: max(u_prev) with NaN propagation, energy sums and source integral;
+// block `blk` of `nblk` writes its 4 partials to dst
+__device__ __forceinline__ void pass1_body(const Problem& P, const double* __restrict__ u,
+                                           const double* __restrict__ J, int blk, int nblk, double* dst) {
   const int64_t nfull = (int64_t)P.nx * P.ny * P.nz;
   double mx = -INFINITY;
   bool nan = false;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nfull; e += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t e = blk * (int64_t)blockDim.x + threadIdx.x; e < nfull; e += (int64_t)nblk * blockDim.x) {
     const double v = P.u_prev[e];
     if (v != v) nan = true;
     else mx = fmax(mx, v);
   }
   const int64_t n = (int64_t)P.ni * P.nj * (P.ndim == 3 ? P.nk : 1);
   double e0 = 0.0, e1 = 0.0, sj = 0.0;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t e = blk * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)nblk * blockDim.x) {
     int a, b, c;
     domain_coords(P, e, a, b, c);
     const int64_t id = fidx(P, a, b, c);
@@ -175,16 +178,20 @@ __global__ void reduce_pass1(Problem P, const double* __restrict__ u, const doub
     double a0 = sm[1][0], a1 = sm[2][0], a2 = sm[3][0];
     for (int k = 1; k < kRedThreads / 32; ++k) { a0 += sm[1][k]; a1 += sm[2][k]; a2 += sm[3][k]; }
     if (anynan) mx = __longlong_as_double(0x7ff8000000000000ll);
-    scratch[4 * blockIdx.x + 0] = mx;
-    scratch[4 * blockIdx.x + 1] = a0;
-    scratch[4 * blockIdx.x + 2] = a1;
-    scratch[4 * blockIdx.x + 3] = a2;
+    dst[0] = mx;
+    dst[1] = a0;
+    dst[2] = a1;
+    dst[3] = a2;
   }
 }
 
-// finish pass 1 in one block (fixed order), then pass 2 needs umax
-__global__ void reduce_finish1(const double* scratch, int nb, double* out) {
-  if (threadIdx.x != 0) return;
+__global__ void reduce_pass1(Problem P, const double* __restrict__ u, const double* __restrict__ J,
+                             double* scratch) {
+  pass1_body(P, u, J, blockIdx.x, gridDim.x, scratch + 4 * blockIdx.x);
+}
+
+// finish pass 1 in one thread (fixed order), then pass 2 needs umax
+__device__ __forceinline__ void finish1_body(const double* scratch, int nb, double* out) {
   double mx = -INFINITY, a0 = 0, a1 = 0, a2 = 0;
   bool nan = false;
   for (int k = 0; k < nb; ++k) {
@@ -201,14 +208,19 @@ __global__ void reduce_finish1(const double* scratch, int nb, double* out) {
   out[4] = a2;
 }
 
+__global__ void reduce_finish1(const double* scratch, int nb, double* out) {
+  if (threadIdx.x != 0) return;
+  finish1_body(scratch, nb, out);
+}
+
 // pass 2: max over the full arrays of |a-b|/(a+u0) masked by isfinite
 // (timestep_control.jl:67-73)
-__global__ void reduce_pass2(Problem P, const double* __restrict__ u, double tol, const double* out,
-                             double* scratch) {
+__device__ __forceinline__ void pass2_body(const Problem& P, const double* __restrict__ u, double tol,
+                                           const double* out, int blk, int nblk, double* dst) {
   const int64_t nfull = (int64_t)P.nx * P.ny * P.nz;
   const double u0 = out[0] * tol;
   double mx = -INFINITY;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nfull; e += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t e = blk * (int64_t)blockDim.x + threadIdx.x; e < nfull; e += (int64_t)nblk * blockDim.x) {
     const double a = u[e], b = P.u_prev[e];
     double d = fabs(a - b) / (a + u0);
     d = isfinite(d) ? d : 0.0;
@@ -221,8 +233,13 @@ __global__ void reduce_pass2(Problem P, const double* __restrict__ u, double tol
   __syncthreads();
   if (threadIdx.x == 0) {
     for (int k = 1; k < kRedThreads / 32; ++k) mx = fmax(mx, sm[k]);
-    scratch[blockIdx.x] = mx;
+    *dst = mx;
   }
+}
+
+__global__ void reduce_pass2(Problem P, const double* __restrict__ u, double tol, const double* out,
+                             double* scratch) {
+  pass2_body(P, u, tol, out, blockIdx.x, gridDim.x, scratch + blockIdx.x);
 }
 
 __global__ void reduce_finish2(const double* scratch, int nb, double* out) {
@@ -230,6 +247,48 @@ __global__ void reduce_finish2(const double* scratch, int nb, double* out) {
   double mx = -INFINITY;
   for (int k = 0; k < nb; ++k) mx = fmax(mx, scratch[k]);
   out[1] = mx;
+}
+
+// Batched form: one launch per pass for every problem of a batch.  Job j owns
+// blocks [b0, b0 + nb) of the grid (found by binary search over b0) and its
+// partials at scratch[4·b0 ...]; its results go to out[8·p ...].
+__device__ __forceinline__ int job_of_block(const RedJob* jobs, int njobs) {
+  int lo = 0, hi = njobs - 1;
+  const int b = blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].b0 <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void breduce_pass1(const Problem* __restrict__ probs, const RedJob* __restrict__ jobs, int njobs,
+                              double* scratch) {
+  const RedJob jb = jobs[job_of_block(jobs, njobs)];
+  const int blk = blockIdx.x - jb.b0;
+  pass1_body(probs[jb.p], jb.u, jb.J, blk, jb.nb, scratch + 4 * (jb.b0 + blk));
+}
+
+__global__ void breduce_finish1(const RedJob* __restrict__ jobs, const double* scratch, double* out) {
+  if (threadIdx.x != 0) return;
+  const RedJob jb = jobs[blockIdx.x];
+  finish1_body(scratch + 4 * jb.b0, jb.nb, out + 8 * jb.p);
+}
+
+__global__ void breduce_pass2(const Problem* __restrict__ probs, const RedJob* __restrict__ jobs, int njobs,
+                              double tol, const double* out, double* scratch) {
+  const RedJob jb = jobs[job_of_block(jobs, njobs)];
+  const int blk = blockIdx.x - jb.b0;
+  pass2_body(probs[jb.p], jb.u, tol, out + 8 * jb.p, blk, jb.nb, scratch + jb.b0 + blk);
+}
+
+__global__ void breduce_finish2(const RedJob* __restrict__ jobs, const double* scratch, double* out) {
+  if (threadIdx.x != 0) return;
+  const RedJob jb = jobs[blockIdx.x];
+  double mx = -INFINITY;
+  for (int k = 0; k < jb.nb; ++k) mx = fmax(mx, scratch[jb.b0 + k]);
+  out[8 * jb.p + 1] = mx;
 }
 
 int grid_for(int64_t n, int threads) {
@@ -274,12 +333,42 @@ cudaError_t launch_clamp(double* u, int64_t n, int positivity, int cutoff, cudaS
   return cudaGetLastError();
 }
 
+int step_reduction_blocks(int64_t nfull) {
+  int64_t nb = (nfull + kRedThreads - 1) / kRedThreads;
+  if (nb > kRedBlocks) nb = kRedBlocks;
+  if (nb < 1) nb = 1;
+  return (int)nb;
+}
+
+int plan_step_reductions(RedJob* jobs, int njobs, const int64_t* nfull) {
+  int64_t total = 0;
+  for (int j = 0; j < njobs; ++j) total += nfull[j];
+  int b0 = 0;
+  for (int j = 0; j < njobs; ++j) {
+    // a share of kRedBlocks in proportion to the array size (all of it for a lone problem)
+    int64_t nb = total > 0 ? (kRedBlocks * nfull[j] + total - 1) / total : 1;
+    nb = std::min<int64_t>(std::max<int64_t>(nb, 1), step_reduction_blocks(nfull[j]));
+    jobs[j].b0 = b0;
+    jobs[j].nb = (int)nb;
+    b0 += (int)nb;
+  }
+  return b0;
+}
+
+cudaError_t launch_step_reductions_batch(const Problem* probs, const RedJob* jobs, int njobs, int nblocks,
+                                         double tol, double* scratch, double* out, cudaStream_t s) {
+  if (njobs <= 0) return cudaSuccess;
+  breduce_pass1<<<nblocks, kRedThreads, 0, s>>>(probs, jobs, njobs, scratch);
+  breduce_finish1<<<njobs, 32, 0, s>>>(jobs, scratch, out);
+  breduce_pass2<<<nblocks, kRedThreads, 0, s>>>(probs, jobs, njobs, tol, out, scratch);
+  breduce_finish2<<<njobs, 32, 0, s>>>(jobs, scratch, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_step_reductions(const Problem& P, const double* u, const double* cellJ, double tol,
                                    double* scratch, double* out, cudaStream_t s) {
   const int64_t nfull = (int64_t)P.nx * P.ny * P.nz;
-  int nb = (int)((nfull + kRedThreads - 1) / kRedThreads);
-  if (nb > kRedBlocks) nb = kRedBlocks;
-  if (nb < 1) nb = 1;
+  const int nb = step_reduction_blocks(nfull);
   reduce_pass1<<<nb, kRedThreads, 0, s>>>(P, u, cellJ, scratch);
   reduce_finish1<<<1, 32, 0, s>>>(scratch, nb, out);
   reduce_pass2<<<nb, kRedThreads, 0, s>>>(P, u, tol, out, scratch);

@@ -783,7 +783,7 @@ struct R3Tile {
 
 __global__ void __launch_bounds__(R3NT) mixed_restart3d(const Problem* __restrict__ probs, RestartIO io, int rti,
                                                         int rtj) {
-  constexpr int RX = R3Tile::RX, RY = R3Tile::RY, RZ = R3Tile::RZ, NR = R3Tile::NR;
+  constexpr int RX = R3Tile::RX, RY = R3Tile::RY, NR = R3Tile::NR;
   extern __shared__ double sm3[];
   double* s_u = sm3;
   double* s_a = s_u + NR;

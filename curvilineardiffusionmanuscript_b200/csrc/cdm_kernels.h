@@ -78,5 +78,17 @@ cudaError_t launch_clamp(double* u, int64_t n, int positivity, int cutoff, cudaS
 // out[4] = sum S*J over the domain.  `scratch` holds >= 2*1024 doubles.
 cudaError_t launch_step_reductions(const Problem& P, const double* u, const double* cellJ, double tol,
                                    double* scratch, double* out, cudaStream_t s);
+// the same reductions for several problems in four launches: job j reduces problem p over
+// blocks [b0, b0 + nb) of one grid; plan_step_reductions fills b0 and nb (a lone problem
+// gets the single-problem partition, so its results are bit for bit those above) and
+// returns the grid size; `scratch` holds >= 4 * that doubles, out[8p ...] as above
+struct RedJob {
+  int p, b0, nb;
+  const double* u;
+  const double* J;
+};
+int plan_step_reductions(RedJob* jobs, int njobs, const int64_t* nfull);
+cudaError_t launch_step_reductions_batch(const Problem* probs, const RedJob* jobs, int njobs, int nblocks,
+                                         double tol, double* scratch, double* out, cudaStream_t s);
 
 }  // namespace cdm

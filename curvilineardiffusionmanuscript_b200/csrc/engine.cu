@@ -117,8 +117,11 @@ Engine::~Engine() {
   dfree(d_wave);
   dfree(d_red);
   dfree(d_redout);
+  dfree(d_jobs);
+  dfree(d_bred);
   if (h_ctrl) cudaFreeHost(h_ctrl);
   if (h_redout) cudaFreeHost(h_redout);
+  if (h_jobs) cudaFreeHost(h_jobs);
   if (h_wave_err) cudaFreeHost(h_wave_err);
   if (ev) cudaEventDestroy(ev);
   for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
@@ -379,6 +382,9 @@ int Engine::init(int nprob, const cdm_mesh_desc* meshes, const cdm_bc* bcs, cons
   CDM_CK(dalloc(&d_red, (size_t)4 * 1024));
   CDM_CK(dalloc(&d_redout, (size_t)8 * nprob));
   CDM_CK(cudaMallocHost((void**)&h_redout, sizeof(double) * 8 * nprob));
+  CDM_CK(dalloc(&d_jobs, (size_t)nprob));
+  CDM_CK(cudaMallocHost((void**)&h_jobs, sizeof(RedJob) * nprob));
+  CDM_CK(dalloc(&d_bred, (size_t)4 * (1024 + nprob)));
   if (precision == CDM_PREC_MIXED) {
     int rc = mixed_alloc();
     if (rc != CDM_OK) return rc;
@@ -955,6 +961,8 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
   }
   // after the loop (:321-346)
   int worst = CDM_OK;
+  int njobs = 0;
+  std::vector<int64_t> red_n(nprob);
   for (int p = 0; p < nprob; ++p) {
     ProbState& s = ps[p];
     const Ctrl& C = h_ctrl[p];
@@ -985,11 +993,21 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
     // result: the last ping-pong iterate (FP64 path) or the last restart's base (mixed)
     double* res = precision == CDM_PREC_MIXED ? s.ub64[(C.n_restarts - 1) & 1] : s.u[C.iter & 1];
     CDM_CK(launch_clamp(res, s.nfull, o.enforce_positivity, o.apply_cutoff, stream));
-    CDM_CK(launch_step_reductions(hp[p], res, s.cellJ, o.ndt_tol, d_red, d_redout + 8 * p, stream));
-    prof.other_launches += 4 + ((o.enforce_positivity || o.apply_cutoff) ? 1 : 0);
+    h_jobs[njobs].p = p;
+    h_jobs[njobs].u = res;
+    h_jobs[njobs].J = s.cellJ;
+    red_n[njobs++] = s.nfull;
+    prof.other_launches += (o.enforce_positivity || o.apply_cutoff) ? 1 : 0;
     prof.cell_iters += s.ndomain * (int64_t)C.iter;
     CDM_CK(cudaMemcpyAsync(T[p], res, (size_t)s.nfull * sizeof(double),
                            o.mem == CDM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, stream));
+  }
+  if (njobs > 0) {
+    // next_dt and energy reductions of every problem in four launches
+    const int nblocks = plan_step_reductions(h_jobs, njobs, red_n.data());
+    CDM_CK(cudaMemcpyAsync(d_jobs, h_jobs, sizeof(RedJob) * njobs, cudaMemcpyHostToDevice, stream));
+    CDM_CK(launch_step_reductions_batch(d_probs, d_jobs, njobs, nblocks, o.ndt_tol, d_bred, d_redout, stream));
+    prof.other_launches += 4;
   }
   CDM_CK(cudaMemcpyAsync(h_redout, d_redout, sizeof(double) * 8 * nprob, cudaMemcpyDeviceToHost, stream));
   rc = wait_stream(timeout_s);

@@ -96,6 +96,9 @@ struct Engine {
   int* d_flags = nullptr;        // per problem: source validity bits
   double* d_red = nullptr;       // reduction scratch
   double* d_redout = nullptr;    // per problem 8 doubles
+  RedJob* d_jobs = nullptr;      // batched end-of-step reductions: one job per problem
+  RedJob* h_jobs = nullptr;      // pinned
+  double* d_bred = nullptr;      // their partials
   double* h_redout = nullptr;    // pinned
   cudaEvent_t ev = nullptr;
   std::map<int, cudaGraphExec_t> graphs;
