@@ -252,7 +252,8 @@ __global__ void reduce_finish2(const double* scratch, int nb, double* out) {
 // Batched form: one launch per pass for every problem of a batch.  Job j owns
 // blocks [b0, b0 + nb) of the grid (found by binary search over b0) and its
 // partials at scratch[4·b0 ...]; its results go to out[8·p ...].
-__device__ __forceinline__ int job_of_block(const RedJob* jobs, int njobs) {
+template <class Job>
+__device__ __forceinline__ int job_of_block(const Job* jobs, int njobs) {
   int lo = 0, hi = njobs - 1;
   const int b = blockIdx.x;
   while (lo < hi) {
@@ -353,6 +354,39 @@ int plan_step_reductions(RedJob* jobs, int njobs, const int64_t* nfull) {
     b0 += (int)nb;
   }
   return b0;
+}
+
+// one read of each job's source array, written to up to three destinations
+__global__ void batch_copy_kernel(const CopyJob* __restrict__ jobs, int njobs) {
+  const CopyJob jb = jobs[job_of_block(jobs, njobs)];
+  const int blk = blockIdx.x - jb.b0;
+  for (int64_t e = blk * (int64_t)blockDim.x + threadIdx.x; e < jb.n; e += (int64_t)jb.nb * blockDim.x) {
+    const double v = jb.src[e];
+    jb.dst[0][e] = v;
+    if (jb.dst[1]) jb.dst[1][e] = v;
+    if (jb.dst[2]) jb.dst[2][e] = v;
+  }
+}
+
+int plan_batch_copy(CopyJob* jobs, int njobs) {
+  constexpr int kCopyBlocks = 148 * 8, kCopyThreads = 256;
+  int64_t total = 0;
+  for (int j = 0; j < njobs; ++j) total += jobs[j].n;
+  int b0 = 0;
+  for (int j = 0; j < njobs; ++j) {
+    int64_t nb = total > 0 ? (kCopyBlocks * jobs[j].n + total - 1) / total : 1;
+    nb = std::min<int64_t>(std::max<int64_t>(nb, 1), (jobs[j].n + kCopyThreads - 1) / kCopyThreads);
+    jobs[j].b0 = b0;
+    jobs[j].nb = (int)std::max<int64_t>(nb, 1);
+    b0 += jobs[j].nb;
+  }
+  return b0;
+}
+
+cudaError_t launch_batch_copy(const CopyJob* jobs, int njobs, int nblocks, cudaStream_t s) {
+  if (njobs <= 0) return cudaSuccess;
+  batch_copy_kernel<<<nblocks, 256, 0, s>>>(jobs, njobs);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_step_reductions_batch(const Problem* probs, const RedJob* jobs, int njobs, int nblocks,

@@ -88,6 +88,16 @@ struct RedJob {
   const double* J;
 };
 int plan_step_reductions(RedJob* jobs, int njobs, const int64_t* nfull);
+// batched device copies: job j copies src[0, n) to dst[0] and, where not NULL, dst[1]
+// and dst[2]; plan_batch_copy fills b0 and nb and returns the grid size
+struct CopyJob {
+  const double* src;
+  double* dst[3];
+  int64_t n;
+  int b0, nb;
+};
+int plan_batch_copy(CopyJob* jobs, int njobs);
+cudaError_t launch_batch_copy(const CopyJob* jobs, int njobs, int nblocks, cudaStream_t s);
 cudaError_t launch_step_reductions_batch(const Problem* probs, const RedJob* jobs, int njobs, int nblocks,
                                          double tol, double* scratch, double* out, cudaStream_t s);
 

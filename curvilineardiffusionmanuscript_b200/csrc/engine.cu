@@ -119,9 +119,11 @@ Engine::~Engine() {
   dfree(d_redout);
   dfree(d_jobs);
   dfree(d_bred);
+  dfree(d_cjobs);
   if (h_ctrl) cudaFreeHost(h_ctrl);
   if (h_redout) cudaFreeHost(h_redout);
   if (h_jobs) cudaFreeHost(h_jobs);
+  if (h_cjobs) cudaFreeHost(h_cjobs);
   if (h_wave_err) cudaFreeHost(h_wave_err);
   if (ev) cudaEventDestroy(ev);
   for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
@@ -385,6 +387,8 @@ int Engine::init(int nprob, const cdm_mesh_desc* meshes, const cdm_bc* bcs, cons
   CDM_CK(dalloc(&d_jobs, (size_t)nprob));
   CDM_CK(cudaMallocHost((void**)&h_jobs, sizeof(RedJob) * nprob));
   CDM_CK(dalloc(&d_bred, (size_t)4 * (1024 + nprob)));
+  CDM_CK(dalloc(&d_cjobs, (size_t)2 * nprob));
+  CDM_CK(cudaMallocHost((void**)&h_cjobs, sizeof(CopyJob) * 2 * nprob));
   if (precision == CDM_PREC_MIXED) {
     int rc = mixed_alloc();
     if (rc != CDM_OK) return rc;
@@ -838,6 +842,31 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
   }
   // T and rho may still be written by the caller's kernels
   CDM_CK(fence_caller());
+  // copy!(solver.u, T); copy!(solver.u_prev, T)  (:229-230): Tⁿ into u_prev and both
+  // iterates, every problem in one copy launch (host arrays cross into u_prev first)
+  for (int p = 0; p < nprob; ++p) {
+    ProbState& s = ps[p];
+    CopyJob& j = h_cjobs[p];
+    j.n = s.nfull;
+    if (o.mem == CDM_MEM_DEVICE) {
+      j.src = T[p];
+      j.dst[0] = s.u_prev;
+      j.dst[1] = s.u[0];
+      j.dst[2] = s.u[1];
+    } else {
+      CDM_CK(stage_in(s.u_prev, T[p], s.nfull, o.mem, stream));
+      j.src = s.u_prev;
+      j.dst[0] = s.u[0];
+      j.dst[1] = s.u[1];
+      j.dst[2] = nullptr;
+    }
+  }
+  {
+    const int nb = plan_batch_copy(h_cjobs, nprob);
+    CDM_CK(cudaMemcpyAsync(d_cjobs, h_cjobs, sizeof(CopyJob) * nprob, cudaMemcpyHostToDevice, stream));
+    CDM_CK(launch_batch_copy(d_cjobs, nprob, nb, stream));
+    prof.other_launches += 1;
+  }
   std::vector<const double*> inits(nprob, nullptr);
   std::vector<int> guessed(nprob, 0);
   bool any_guess = false;
@@ -846,8 +875,6 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
     Problem& P = hp[p];
     std::memset(&P, 0, sizeof(P));
     const size_t bytes = (size_t)s.nfull * sizeof(double);
-    // copy!(solver.u, T); copy!(solver.u_prev, T)  (:229-230)
-    CDM_CK(stage_in(s.u_prev, T[p], s.nfull, o.mem, stream));
     // the iteration starts from Tⁿ (:229), a user array, or the network's prediction
     const double* init = s.u_prev;
     if (o.guess == CDM_GUESS_USER && s.has_guess) {
@@ -860,9 +887,8 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
     inits[p] = init;
     guessed[p] = init != s.u_prev;
     any_guess = any_guess || guessed[p];
-    // a guessed start first runs the plain start's first iteration (probe below)
-    CDM_CK(cudaMemcpyAsync(s.u[0], s.u_prev, bytes, cudaMemcpyDeviceToDevice, stream));
-    CDM_CK(cudaMemcpyAsync(s.u[1], s.u_prev, bytes, cudaMemcpyDeviceToDevice, stream));
+    // a guessed start first runs the plain start's first iteration (probe below), from
+    // the copies of Tⁿ made above
     const double* rp = rho[p];
     if (o.mem != CDM_MEM_DEVICE) {
       if (!s.rho_buf) CDM_CK(dalloc(&s.rho_buf, (size_t)s.nfull));
@@ -961,7 +987,7 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
   }
   // after the loop (:321-346)
   int worst = CDM_OK;
-  int njobs = 0;
+  int njobs = 0, nout = 0;
   std::vector<int64_t> red_n(nprob);
   for (int p = 0; p < nprob; ++p) {
     ProbState& s = ps[p];
@@ -999,8 +1025,21 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
     red_n[njobs++] = s.nfull;
     prof.other_launches += (o.enforce_positivity || o.apply_cutoff) ? 1 : 0;
     prof.cell_iters += s.ndomain * (int64_t)C.iter;
-    CDM_CK(cudaMemcpyAsync(T[p], res, (size_t)s.nfull * sizeof(double),
-                           o.mem == CDM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, stream));
+    if (o.mem == CDM_MEM_DEVICE) {  // into the caller's array in one copy launch below
+      CopyJob& j = h_cjobs[nprob + nout++];
+      j.src = res;
+      j.dst[0] = T[p];
+      j.dst[1] = j.dst[2] = nullptr;
+      j.n = s.nfull;
+    } else {
+      CDM_CK(cudaMemcpyAsync(T[p], res, (size_t)s.nfull * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    }
+  }
+  if (nout > 0) {
+    const int nb = plan_batch_copy(h_cjobs + nprob, nout);
+    CDM_CK(cudaMemcpyAsync(d_cjobs + nprob, h_cjobs + nprob, sizeof(CopyJob) * nout, cudaMemcpyHostToDevice, stream));
+    CDM_CK(launch_batch_copy(d_cjobs + nprob, nout, nb, stream));
+    prof.other_launches += 1;
   }
   if (njobs > 0) {
     // next_dt and energy reductions of every problem in four launches

@@ -99,6 +99,8 @@ struct Engine {
   RedJob* d_jobs = nullptr;      // batched end-of-step reductions: one job per problem
   RedJob* h_jobs = nullptr;      // pinned
   double* d_bred = nullptr;      // their partials
+  CopyJob* d_cjobs = nullptr;    // batched copies in and out of a step: 2 x nprob jobs
+  CopyJob* h_cjobs = nullptr;    // pinned
   double* h_redout = nullptr;    // pinned
   cudaEvent_t ev = nullptr;
   std::map<int, cudaGraphExec_t> graphs;
