@@ -183,6 +183,9 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
   };
 
   int bad = 0;
+  // the validity bits of α are read for a step's last iteration only, which is a
+  // check iteration or the one past max_iter: other iterations skip the tests
+  const bool track_iter = check || iter > C->max_iter;
   // diffusivity, pseudo-time parameters and update factors of cell (a, r)
   auto stage = [&](int r, const Pre& L) -> Cell {
     Cell c{0.0, 0.0, 0.0, 0.0, 0.0};
@@ -220,7 +223,7 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
       c.it = th;
     }
     // validity of α = κ/(ρcₚ) on owned cells and first-layer ghosts
-    const bool track = (tid >= 1 && tid <= OW) || (EDGE && cside >= 0);
+    const bool track = ((tid >= 1 && tid <= OW) || (EDGE && cside >= 0)) && track_iter;
     if (track && r >= j0 - (EDGE && j0 == 0) && r < j1 + (EDGE && j1 == nj)) {
       if (!(isfinite(kap) && isfinite(rc) && rc != 0.0)) bad |= 1;
       if (kap != 0.0 && ((kap < 0.0) != (rc < 0.0))) bad |= 2;

@@ -101,6 +101,8 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
   const int ra = i0 + rx - 1, rb = j0 + ry - 1;
 
   int bad = 0;
+  // validity bits of α: read for a step's last iteration only (a check iteration or the one past max_iter)
+  const bool track_iter = check || iter > C->max_iter;
   // stage cell (a, b, c): u with its ghost rule, pseudo-time parameters and
   // update factors (iteration_parameters.jl:2-15 in reciprocal form)
   auto stage = [&](int a, int b, int c, bool track) -> C3 {
@@ -147,7 +149,7 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
       r.it = th;
     }
     // validity of α = κ/(ρcₚ) on owned cells and first-layer ghosts
-    if (track) {
+    if (track && track_iter) {
       if (!(isfinite(kap) && isfinite(rc) && rc != 0.0)) bad |= 1;
       if (kap != 0.0 && ((kap < 0.0) != (rc < 0.0))) bad |= 2;
     }

@@ -374,6 +374,32 @@ def test_fast_batch_autotune_includes_the_wavefront():
     b.close()
 
 
+@pytest.mark.parametrize("tuning", [(0, 8, 8), (4, 8, 8)])
+def test_invalid_diffusivity_stops_the_next_step(tuning):
+    """validate_scalar (PseudoTransientSolver.jl:238-250) checks the diffusivity the
+    previous step's last iteration left, on the domain and the first halo layer.  A
+    negative ρ in one ghost cell of a Neumann side gives that ghost a negative α
+    without touching the iteration (its face has Δu = 0), so with enforce_positivity
+    the first step runs as in the oracle and the second reports CDM_BAD_INPUT."""
+    pr = small_case_2d(ni=40, nj=33, seed=5)
+    nh = pr.mesh.nhalo
+    rho = pr.rho.clone()
+    rho[nh + 11, nh - 1] = -2.0 * rho[nh + 11, nh]  # ghost column of the i-low side, row 11
+    b = PseudoTransientBatch([pr.mesh], [pr.bcs], precision="fp64")
+    b.set_tuning(*tuning)
+    T = pr.T0.clone().cuda()
+    o = OracleSolver(pr.mesh, pr.bcs)
+    To = pr.T0.numpy().copy()
+    kw = dict(rtol=1e-8, atol=1e-8, max_iter=50000, enforce_positivity=True)
+    for k in range(2):
+        st, _ = b.step([T], [rho.cuda()], [pr.cp], [pr.kappa], [pr.dt], raise_on_error=False, **kw)
+        so, _ = o.step(To, rho.numpy(), pr.cp, pr.kappa.k0, pr.kappa.n, pr.dt, **kw)
+        assert st[0]["status"] == so["status"] == (0 if k == 0 else 3), k
+        if k == 0:
+            assert st[0]["niter"] == so["niter"] and rel_l2(T.cpu().numpy(), To) <= TOL
+    b.close()
+
+
 def test_set_tuning_rejects_invalid_choices():
     probs = problems.batch_2d(nprob=2, nmin=20, nmax=30, seed=1)
     b = PseudoTransientBatch([p.mesh for p in probs], [p.bcs for p in probs])
