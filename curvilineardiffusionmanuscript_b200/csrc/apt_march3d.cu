@@ -187,46 +187,69 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
     qp = -an * du;
     return (qold * tn - an * du) * rcp_nr(1.0 + tn);
   };
-  constexpr int NQI = RY * (TX + 1), NQJ = (TY + 1) * RX, NQK = RY * RX;
-  constexpr int NSLOT = (NQI + NQJ + NQK + NT - 1) / NT;
-  // Face w of a plane: i-faces [0, NQI), j-faces [NQI, NQI+NQJ) of plane c,
-  // k-faces after that between planes ck and ck + 1 (stored at index ck).
-  // Returns the global index of its old flux, or -1 outside the domain.
-  auto face_at = [&](int w, int c, int ck, int& kind, int& x, int& y) -> int64_t {
-    if (w < NQI) {
-      kind = 0;
-      y = w / (TX + 1);
-      x = w - y * (TX + 1);
-      const int a = i0 - 1 + x, b = j0 - 1 + y;
-      return (c >= 0 && c < nk && a >= -1 && a <= ni - 1 && b >= 0 && b <= nj - 1) ? fidx(P, a, b, c) : -1;
+  // Face assignment, fixed for the whole strip: every thread computes the i-, j-
+  // and k-faces on the high side of its own cell (face slots x = ox, y = oy);
+  // threads below NRF compute one face of the ring each: the i-faces of column
+  // x = 0 and of rows y = 0, RY-1; the j-faces of row y = 0 and of columns
+  // x = 0, RX-1; the k-faces of the ring cells.  Per plane only the plane
+  // offset and the plane's bounds change.
+  constexpr int NRI = RY + 2 * TX, NRJ = RX + 2 * TY, NRK = 2 * RX + 2 * TY, NRF = NRI + NRJ + NRK;
+  static_assert(NRF <= NT, "one ring face per thread");
+  int fk = -1, fx = 0, fy = 0;
+  if (tid < NRI) {
+    fk = 0;
+    if (tid < RY) {
+      fy = tid;
+    } else {
+      const int t = tid - RY;
+      fy = t < TX ? 0 : RY - 1;
+      fx = 1 + (t < TX ? t : t - TX);
     }
-    if (w < NQI + NQJ) {
-      kind = 1;
-      w -= NQI;
-      y = w / RX;
-      x = w - y * RX;
-      const int a = i0 - 1 + x, b = j0 - 1 + y;
-      return (c >= 0 && c < nk && a >= 0 && a <= ni - 1 && b >= -1 && b <= nj - 1) ? fidx(P, a, b, c) : -1;
+  } else if (tid < NRI + NRJ) {
+    fk = 1;
+    const int t = tid - NRI;
+    if (t < RX) {
+      fx = t;
+    } else {
+      const int u = t - RX;
+      fx = (u & 1) ? RX - 1 : 0;
+      fy = 1 + (u >> 1);
     }
-    kind = 2;
-    w -= NQI + NQJ;
-    y = w / RX;
-    x = w - y * RX;
-    const int a = i0 - 1 + x, b = j0 - 1 + y;
-    return (ck >= -1 && ck <= nk - 1 && a >= 0 && a <= ni - 1 && b >= 0 && b <= nj - 1) ? fidx(P, a, b, ck) : -1;
-  };
-  // old fluxes of this thread's face slots (w = tid + r·NT), loaded ahead of use
+  } else if (tid < NRF) {
+    fk = 2;
+    const int t = tid - NRI - NRJ;
+    if (t < 2 * RX) {
+      fy = t < RX ? 0 : RY - 1;
+      fx = t < RX ? t : t - RX;
+    } else {
+      const int u = t - 2 * RX;
+      fx = (u & 1) ? RX - 1 : 0;
+      fy = 1 + (u >> 1);
+    }
+  }
+  const int fa = i0 - 1 + fx, fb = j0 - 1 + fy;
+  // the ring face's (a, b) range test (faces.jl ranges: an i-face joins cells a and a+1, ...)
+  const bool f_ab = fk == 0   ? (fa >= -1 && fa <= ni - 1 && fb >= 0 && fb <= nj - 1)
+                    : fk == 1 ? (fa >= 0 && fa <= ni - 1 && fb >= -1 && fb <= nj - 1)
+                              : (fa >= 0 && fa <= ni - 1 && fb >= 0 && fb <= nj - 1);
+  // ring i-faces of column 0 and j-faces of row 0 are the domain's low boundary faces
+  const bool f_wr = (fk == 0 && fx == 0 && i0 == 0 && fy >= 1 && fy <= TY) ||
+                    (fk == 1 && fy == 0 && j0 == 0 && fx >= 1 && fx <= TX);
+  const int64_t plane = (int64_t)P.nx * P.ny;
+  const int64_t o_col = fidx(P, oa, ob, 0), f_col = fidx(P, fa, fb, 0);
+  // old fluxes at plane c (i, j) and of the k-faces above plane ck, into
+  // qv = {own i, own j, own k, ring face}
   auto load_faces = [&](int c, int ck, bool do_k, double* qv) {
-    const int total = NQI + NQJ + (do_k ? NQK : 0);
-#pragma unroll
-    for (int r = 0; r < NSLOT; ++r) {
-      const int w = tid + r * NT;
-      qv[r] = 0.0;
-      if (w < total) {
-        int kind, x, y;
-        const int64_t id = face_at(w, c, ck, kind, x, y);
-        if (id >= 0) qv[r] = kind == 0 ? qiin[id] : (kind == 1 ? qjin[id] : qkin[id]);
-      }
+    const bool cin = c >= 0 && c < nk, kin = do_k && ck >= -1 && ck <= nk - 1;
+    const int64_t oc = o_col + plane * c;
+    qv[0] = (own_in && cin) ? qiin[oc] : 0.0;
+    qv[1] = (own_in && cin) ? qjin[oc] : 0.0;
+    qv[2] = (own_in && kin) ? qkin[o_col + plane * ck] : 0.0;
+    qv[3] = 0.0;
+    if (f_ab) {
+      if (fk == 0 && cin) qv[3] = qiin[f_col + plane * c];
+      else if (fk == 1 && cin) qv[3] = qjin[f_col + plane * c];
+      else if (fk == 2 && kin) qv[3] = qkin[f_col + plane * ck];
     }
   };
   // new fluxes: i/j faces of plane c (cells in slot s) into face slot fs; k-faces
@@ -234,39 +257,64 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
   auto faces = [&](int c, int s, int fs, int ck, int sl, int sh, int kf, bool do_k, const double* qv) {
     const bool inz = c >= k0 && c < k1;
     const bool kown = (ck >= k0 && ck < k1) || ck == -1;
-    const int total = NQI + NQJ + (do_k ? NQK : 0);
-#pragma unroll
-    for (int r = 0; r < NSLOT; ++r) {
-      const int w = tid + r * NT;
-      if (w >= total) continue;
-      int kind, x, y;
-      const int64_t id = face_at(w, c, ck, kind, x, y);
+    const bool cin = c >= 0 && c < nk, kin = ck >= -1 && ck <= nk - 1;
+    const int x = ox, y = oy;
+    const int64_t oc = o_col + plane * c;
+    {  // own i-face
       double qn = 0.0, qp = 0.0;
-      if (kind == 0) {
-        if (id >= 0) {
-          qn = flux(sm.IA[s][y][x], sm.IA[s][y][x + 1], sm.IT[s][y][x], sm.IT[s][y][x + 1],
-                    sm.U[s][y][x + 1] - sm.U[s][y][x], qv[r], qp);
-          if (inz && y >= 1 && y <= TY && (x >= 1 || i0 + x == 0)) qiout[id] = qn;
-        }
-        sm.QI[fs][y][x] = qn;
-        if (check) sm.PI[fs][y][x] = qp;
-      } else if (kind == 1) {
-        if (id >= 0) {
-          qn = flux(sm.IA[s][y][x], sm.IA[s][y + 1][x], sm.IT[s][y][x], sm.IT[s][y + 1][x],
-                    sm.U[s][y + 1][x] - sm.U[s][y][x], qv[r], qp);
-          if (inz && x >= 1 && x <= TX && (y >= 1 || j0 + y == 0)) qjout[id] = qn;
-        }
-        sm.QJ[fs][y][x] = qn;
-        if (check) sm.PJ[fs][y][x] = qp;
-      } else {
-        if (id >= 0) {
-          qn = flux(sm.IA[sl][y][x], sm.IA[sh][y][x], sm.IT[sl][y][x], sm.IT[sh][y][x],
-                    sm.U[sh][y][x] - sm.U[sl][y][x], qv[r], qp);
-          if (kown && x >= 1 && x <= TX && y >= 1 && y <= TY) qkout[id] = qn;
-        }
-        sm.QK[kf][y][x] = qn;
-        if (check) sm.PK[kf][y][x] = qp;
+      if (own_in && cin) {
+        qn = flux(sm.IA[s][y][x], sm.IA[s][y][x + 1], sm.IT[s][y][x], sm.IT[s][y][x + 1],
+                  sm.U[s][y][x + 1] - sm.U[s][y][x], qv[0], qp);
+        if (inz) qiout[oc] = qn;
       }
+      sm.QI[fs][y][x] = qn;
+      if (check) sm.PI[fs][y][x] = qp;
+    }
+    {  // own j-face
+      double qn = 0.0, qp = 0.0;
+      if (own_in && cin) {
+        qn = flux(sm.IA[s][y][x], sm.IA[s][y + 1][x], sm.IT[s][y][x], sm.IT[s][y + 1][x],
+                  sm.U[s][y + 1][x] - sm.U[s][y][x], qv[1], qp);
+        if (inz) qjout[oc] = qn;
+      }
+      sm.QJ[fs][y][x] = qn;
+      if (check) sm.PJ[fs][y][x] = qp;
+    }
+    if (do_k) {  // own k-face
+      double qn = 0.0, qp = 0.0;
+      if (own_in && kin) {
+        qn = flux(sm.IA[sl][y][x], sm.IA[sh][y][x], sm.IT[sl][y][x], sm.IT[sh][y][x],
+                  sm.U[sh][y][x] - sm.U[sl][y][x], qv[2], qp);
+        if (kown) qkout[o_col + plane * ck] = qn;
+      }
+      sm.QK[kf][y][x] = qn;
+      if (check) sm.PK[kf][y][x] = qp;
+    }
+    if (fk == 0) {
+      double qn = 0.0, qp = 0.0;
+      if (f_ab && cin) {
+        qn = flux(sm.IA[s][fy][fx], sm.IA[s][fy][fx + 1], sm.IT[s][fy][fx], sm.IT[s][fy][fx + 1],
+                  sm.U[s][fy][fx + 1] - sm.U[s][fy][fx], qv[3], qp);
+        if (inz && f_wr) qiout[f_col + plane * c] = qn;
+      }
+      sm.QI[fs][fy][fx] = qn;
+      if (check) sm.PI[fs][fy][fx] = qp;
+    } else if (fk == 1) {
+      double qn = 0.0, qp = 0.0;
+      if (f_ab && cin) {
+        qn = flux(sm.IA[s][fy][fx], sm.IA[s][fy + 1][fx], sm.IT[s][fy][fx], sm.IT[s][fy + 1][fx],
+                  sm.U[s][fy + 1][fx] - sm.U[s][fy][fx], qv[3], qp);
+        if (inz && f_wr) qjout[f_col + plane * c] = qn;
+      }
+      sm.QJ[fs][fy][fx] = qn;
+      if (check) sm.PJ[fs][fy][fx] = qp;
+    } else if (fk == 2 && do_k) {
+      double qn = 0.0, qp = 0.0;
+      if (f_ab && kin)
+        qn = flux(sm.IA[sl][fy][fx], sm.IA[sh][fy][fx], sm.IT[sl][fy][fx], sm.IT[sh][fy][fx],
+                  sm.U[sh][fy][fx] - sm.U[sl][fy][fx], qv[3], qp);
+      sm.QK[kf][fy][fx] = qn;
+      if (check) sm.PK[kf][fy][fx] = qp;
     }
   };
   // flux_divergence.jl:119-239 at the own cell from face slots (zm, z0, zp) and k-slots (km, kp)
@@ -295,7 +343,7 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
   // prologue: planes k0-1 and k0, their i/j faces and the k faces between them
   int s_0 = 1, s_p = 0;  // cell slots of planes z and z+1 (z-1 staged into 0 first)
   int f_m = 0, f_0 = 1, f_p = 2, k_m = 0, k_p = 1;
-  double qa[NSLOT], qb[NSLOT];
+  double qa[4], qb[4];
   load_faces(k0 - 1, k0 - 1, true, qa);
   load_faces(k0, 0, false, qb);
   double prv_u = stage_plane(k0 - 1, 0).u;  // own cell of the plane below (ghost write at z = 0)
@@ -366,7 +414,7 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
     k_m = k_p;
     k_p = tk;
 #pragma unroll
-    for (int r = 0; r < NSLOT; ++r) qa[r] = qb[r];
+    for (int r = 0; r < 4; ++r) qa[r] = qb[r];
   }
   finish_iteration<NT>(P, C, tile, iter, check, local, local_nan, bad, sm.red, &sm.flag);
 }
