@@ -189,12 +189,14 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
   };
   // Face assignment, fixed for the whole strip: every thread computes the i-, j-
   // and k-faces on the high side of its own cell (face slots x = ox, y = oy);
-  // threads below NRF compute one face of the ring each: the i-faces of column
-  // x = 0 and of rows y = 0, RY-1; the j-faces of row y = 0 and of columns
-  // x = 0, RX-1; the k-faces of the ring cells.  Per plane only the plane
-  // offset and the plane's bounds change.
-  constexpr int NRI = RY + 2 * TX, NRJ = RX + 2 * TY, NRK = 2 * RX + 2 * TY, NRF = NRI + NRJ + NRK;
-  static_assert(NRF <= NT, "one ring face per thread");
+  // NRI + NRJ + NRK threads compute one face of the ring each: the i-faces of
+  // column x = 0 and of rows y = 0, RY-1; the j-faces of row y = 0 and of
+  // columns x = 0, RX-1; the k-faces of the ring cells.  Per plane only the
+  // plane offset and the plane's bounds change.
+  constexpr int NRI = RY + 2 * TX, NRJ = RX + 2 * TY, NRK = 2 * RX + 2 * TY;
+  // each kind starts on a warp boundary, so that no warp computes two kinds
+  constexpr int BJ = (NRI + 31) / 32 * 32, BK = BJ + (NRJ + 31) / 32 * 32;
+  static_assert(BK + NRK <= NT, "ring faces fit the block");
   int fk = -1, fx = 0, fy = 0;
   if (tid < NRI) {
     fk = 0;
@@ -205,9 +207,9 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
       fy = t < TX ? 0 : RY - 1;
       fx = 1 + (t < TX ? t : t - TX);
     }
-  } else if (tid < NRI + NRJ) {
+  } else if (tid >= BJ && tid < BJ + NRJ) {
     fk = 1;
-    const int t = tid - NRI;
+    const int t = tid - BJ;
     if (t < RX) {
       fx = t;
     } else {
@@ -215,9 +217,9 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
       fx = (u & 1) ? RX - 1 : 0;
       fy = 1 + (u >> 1);
     }
-  } else if (tid < NRF) {
+  } else if (tid >= BK && tid < BK + NRK) {
     fk = 2;
-    const int t = tid - NRI - NRJ;
+    const int t = tid - BK;
     if (t < 2 * RX) {
       fy = t < RX ? 0 : RY - 1;
       fx = t < RX ? t : t - RX;
