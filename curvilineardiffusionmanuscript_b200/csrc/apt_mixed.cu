@@ -1070,77 +1070,120 @@ __global__ void __launch_bounds__(NT3, 3) mixed_sweep3d(const Problem* __restric
     }
     return en;
   };
-  constexpr int NQI = RY3 * (X3 + 1), NQJ = (Y3 + 1) * RX3, NQK = RY3 * RX3;
-  constexpr int NSLOT = (NQI + NQJ + NQK + NT3 - 1) / NT3;
-  auto face_at = [&](int w, int c, int ck, int& kind, int& x, int& y) -> int64_t {
-    if (w < NQI) {
-      kind = 0;
-      y = w / (X3 + 1);
-      x = w - y * (X3 + 1);
-      const int a = i0 - 1 + x, b = j0 - 1 + y;
-      return (c >= 0 && c < nk && a >= -1 && a <= ni - 1 && b >= 0 && b <= nj - 1) ? fidx(P, a, b, c) : -1;
+  // Face assignment, fixed for the whole strip (as in the FP64 plane march):
+  // every thread computes the three faces on the high side of its own cell;
+  // NRI + NRJ + NRK threads, each kind starting on a warp boundary, compute one
+  // ring face each (i-faces of column 0 and rows 0, RY3-1; j-faces of row 0
+  // and columns 0, RX3-1; k-faces of the ring cells).
+  constexpr int NRI = RY3 + 2 * X3, NRJ = RX3 + 2 * Y3, NRK = 2 * RX3 + 2 * Y3;
+  constexpr int BJ = (NRI + 31) / 32 * 32, BK = BJ + (NRJ + 31) / 32 * 32;
+  static_assert(BK + NRK <= NT3, "ring faces fit the block");
+  int fk = -1, fx = 0, fy = 0;
+  if (tid < NRI) {
+    fk = 0;
+    if (tid < RY3) {
+      fy = tid;
+    } else {
+      const int t = tid - RY3;
+      fy = t < X3 ? 0 : RY3 - 1;
+      fx = 1 + (t < X3 ? t : t - X3);
     }
-    if (w < NQI + NQJ) {
-      kind = 1;
-      w -= NQI;
-      y = w / RX3;
-      x = w - y * RX3;
-      const int a = i0 - 1 + x, b = j0 - 1 + y;
-      return (c >= 0 && c < nk && a >= 0 && a <= ni - 1 && b >= -1 && b <= nj - 1) ? fidx(P, a, b, c) : -1;
+  } else if (tid >= BJ && tid < BJ + NRJ) {
+    fk = 1;
+    const int t = tid - BJ;
+    if (t < RX3) {
+      fx = t;
+    } else {
+      const int u = t - RX3;
+      fx = (u & 1) ? RX3 - 1 : 0;
+      fy = 1 + (u >> 1);
     }
-    kind = 2;
-    w -= NQI + NQJ;
-    y = w / RX3;
-    x = w - y * RX3;
-    const int a = i0 - 1 + x, b = j0 - 1 + y;
-    return (ck >= -1 && ck <= nk - 1 && a >= 0 && a <= ni - 1 && b >= 0 && b <= nj - 1) ? fidx(P, a, b, ck) : -1;
-  };
+  } else if (tid >= BK && tid < BK + NRK) {
+    fk = 2;
+    const int t = tid - BK;
+    if (t < 2 * RX3) {
+      fy = t < RX3 ? 0 : RY3 - 1;
+      fx = t < RX3 ? t : t - RX3;
+    } else {
+      const int u = t - 2 * RX3;
+      fx = (u & 1) ? RX3 - 1 : 0;
+      fy = 1 + (u >> 1);
+    }
+  }
+  const int fa = i0 - 1 + fx, fb = j0 - 1 + fy;
+  const bool f_ab = fk == 0   ? (fa >= -1 && fa <= ni - 1 && fb >= 0 && fb <= nj - 1)
+                    : fk == 1 ? (fa >= 0 && fa <= ni - 1 && fb >= -1 && fb <= nj - 1)
+                              : (fa >= 0 && fa <= ni - 1 && fb >= 0 && fb <= nj - 1);
+  const bool f_wr = (fk == 0 && fx == 0 && i0 == 0 && fy >= 1 && fy <= Y3) ||
+                    (fk == 1 && fy == 0 && j0 == 0 && fx >= 1 && fx <= X3);
+  const float* f_in = fk == 0 ? ein[0] : (fk == 1 ? ein[1] : ein[2]);
+  float* f_out = fk == 0 ? eout[0] : eout[1];
+  const int64_t plane = (int64_t)P.nx * P.ny;
+  const int64_t o_col = fidx(P, oa, ob, 0), f_col = fidx(P, fa, fb, 0);
+  // old flux corrections at plane c (i, j) and above plane ck (k): {own i, own j, own k, ring}
   auto load_faces = [&](int c, int ck, bool do_k, float* ev) {
-    const int total = NQI + NQJ + (do_k ? NQK : 0);
-#pragma unroll
-    for (int r = 0; r < NSLOT; ++r) {
-      const int w = tid + r * NT3;
-      ev[r] = 0.f;
-      if (w < total) {
-        int kind, x, y;
-        const int64_t id = face_at(w, c, ck, kind, x, y);
-        if (id >= 0) ev[r] = ein[kind][id];
-      }
-    }
+    const bool cin = c >= 0 && c < nk, kin = do_k && ck >= -1 && ck <= nk - 1;
+    const int64_t oc = o_col + plane * c;
+    ev[0] = (own_in && cin) ? ein[0][oc] : 0.f;
+    ev[1] = (own_in && cin) ? ein[1][oc] : 0.f;
+    ev[2] = (own_in && kin) ? ein[2][o_col + plane * ck] : 0.f;
+    ev[3] = 0.f;
+    if (f_ab && (fk == 2 ? kin : (fk >= 0 && cin))) ev[3] = f_in[f_col + plane * (fk == 2 ? ck : c)];
   };
   auto faces = [&](int c, int s, int fs, int ck, int sl, int sh, int kf, bool do_k, const float* ev) {
     const bool inz = c >= k0 && c < k1;
     const bool kown = (ck >= k0 && ck < k1) || ck == -1;
-    const int total = NQI + NQJ + (do_k ? NQK : 0);
-#pragma unroll
-    for (int r = 0; r < NSLOT; ++r) {
-      const int w = tid + r * NT3;
-      if (w >= total) continue;
-      int kind, x, y;
-      const int64_t id = face_at(w, c, ck, kind, x, y);
+    const bool cin = c >= 0 && c < nk, kin = ck >= -1 && ck <= nk - 1;
+    const int x = ox, y = oy;
+    const int64_t oc = o_col + plane * c;
+    {  // own i-face
       float en = 0.f, dqp = 0.f;
-      if (kind == 0) {
-        if (id >= 0) {
-          en = face(s, y, x, s, y, x + 1, ev[r], dqp);
-          if (inz && y >= 1 && y <= Y3 && (x >= 1 || i0 + x == 0)) eout[0][id] = en;
-        }
-        sm.EI[fs][y][x] = en;
-        if (check) sm.PI[fs][y][x] = dqp;
-      } else if (kind == 1) {
-        if (id >= 0) {
-          en = face(s, y, x, s, y + 1, x, ev[r], dqp);
-          if (inz && x >= 1 && x <= X3 && (y >= 1 || j0 + y == 0)) eout[1][id] = en;
-        }
-        sm.EJ[fs][y][x] = en;
-        if (check) sm.PJ[fs][y][x] = dqp;
-      } else {
-        if (id >= 0) {
-          en = face(sl, y, x, sh, y, x, ev[r], dqp);
-          if (kown && x >= 1 && x <= X3 && y >= 1 && y <= Y3) eout[2][id] = en;
-        }
-        sm.EK[kf][y][x] = en;
-        if (check) sm.PK[kf][y][x] = dqp;
+      if (own_in && cin) {
+        en = face(s, y, x, s, y, x + 1, ev[0], dqp);
+        if (inz) eout[0][oc] = en;
       }
+      sm.EI[fs][y][x] = en;
+      if (check) sm.PI[fs][y][x] = dqp;
+    }
+    {  // own j-face
+      float en = 0.f, dqp = 0.f;
+      if (own_in && cin) {
+        en = face(s, y, x, s, y + 1, x, ev[1], dqp);
+        if (inz) eout[1][oc] = en;
+      }
+      sm.EJ[fs][y][x] = en;
+      if (check) sm.PJ[fs][y][x] = dqp;
+    }
+    if (do_k) {  // own k-face
+      float en = 0.f, dqp = 0.f;
+      if (own_in && kin) {
+        en = face(sl, y, x, sh, y, x, ev[2], dqp);
+        if (kown) eout[2][o_col + plane * ck] = en;
+      }
+      sm.EK[kf][y][x] = en;
+      if (check) sm.PK[kf][y][x] = dqp;
+    }
+    if (fk == 0) {
+      float en = 0.f, dqp = 0.f;
+      if (f_ab && cin) {
+        en = face(s, fy, fx, s, fy, fx + 1, ev[3], dqp);
+        if (inz && f_wr) f_out[f_col + plane * c] = en;
+      }
+      sm.EI[fs][fy][fx] = en;
+      if (check) sm.PI[fs][fy][fx] = dqp;
+    } else if (fk == 1) {
+      float en = 0.f, dqp = 0.f;
+      if (f_ab && cin) {
+        en = face(s, fy, fx, s, fy + 1, fx, ev[3], dqp);
+        if (inz && f_wr) f_out[f_col + plane * c] = en;
+      }
+      sm.EJ[fs][fy][fx] = en;
+      if (check) sm.PJ[fs][fy][fx] = dqp;
+    } else if (fk == 2 && do_k) {
+      float en = 0.f, dqp = 0.f;
+      if (f_ab && kin) en = face(sl, fy, fx, sh, fy, fx, ev[3], dqp);
+      sm.EK[kf][fy][fx] = en;
+      if (check) sm.PK[kf][fy][fx] = dqp;
     }
   };
   auto divergence = [&](const float (*QI)[RY3][X3 + 1], const float (*QJ)[Y3 + 1][RX3], const float (*QK)[RY3][RX3],
@@ -1160,7 +1203,7 @@ __global__ void __launch_bounds__(NT3, 3) mixed_sweep3d(const Problem* __restric
 
   int s_0 = 1, s_p = 0;
   int f_m = 0, f_0 = 1, f_p = 2, k_m = 0, k_p = 1;
-  float ea[NSLOT], eb[NSLOT];
+  float ea[4], eb[4];
   load_faces(k0 - 1, k0 - 1, true, ea);
   load_faces(k0, 0, false, eb);
   stage_plane(k0 - 1, 0);
@@ -1208,7 +1251,7 @@ __global__ void __launch_bounds__(NT3, 3) mixed_sweep3d(const Problem* __restric
     k_m = k_p;
     k_p = tk;
 #pragma unroll
-    for (int r = 0; r < NSLOT; ++r) ea[r] = eb[r];
+    for (int r = 0; r < 4; ++r) ea[r] = eb[r];
   }
   if (check) {
     reduce_and_publish<NT3>(P, C, tile, (double)local, nan, sm.red, &sm.flag, false);
