@@ -13,7 +13,15 @@ aggregated over all ranks (each rank solves its own seeded batch: weak
 scaling, no collective in the data path).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload batch|gaussian128|mms4096|gauss3d256]
+                  [--workload batch|gaussian128|gaussian2048|mms4096|mms1024|multigauss1024|
+                              gauss3d256|gauss3d128]
+                  [--precision fp64|fp64_exact|mixed] [--tuning V,H,K]
+  python bench.py --compare [--workload W]     seconds per time step, FP64 vs mixed (vs learned)
+  python bench.py --net-timing N               guess network: training step and N^2 prediction
+
+Without --tuning the kernel variant, strip height and iteration block are
+chosen by the library's autotuner before the warm-up (outside the timed
+region); the choice is reported in `config`.
 """
 from __future__ import annotations
 
