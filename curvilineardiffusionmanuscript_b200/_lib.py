@@ -91,6 +91,7 @@ PF = C.POINTER(C.c_float)
 # every symbol declared in include/cdm_apt.h and include/cdm_net.h: name -> (restype, argtypes)
 SIGNATURES = {
     "cdm_apt_version": (C.c_int, []),
+    "cdm_selftest_bounded_wait": (C.c_int, [C.c_int, C.c_double, C.POINTER(C.c_int)]),
     "cdm_apt_last_error": (C.c_char_p, []),
     "cdm_step_opts_default": (None, [C.POINTER(StepOpts)]),
     "cdm_apt_config_default": (None, [C.POINTER(Config)]),

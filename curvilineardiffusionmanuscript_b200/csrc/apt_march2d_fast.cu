@@ -453,19 +453,31 @@ __device__ __forceinline__ unsigned long long global_ns() {
 }
 
 // thread 0: true once *count >= target; false when the launch's error flag is
-// set or the wait runs out (then it sets the flag)
-__device__ bool wave_wait(const int* count, int target, unsigned int* err) {
+// set or the wait runs out after limit_ns (then it sets the flag)
+__device__ bool wave_wait(const int* count, int target, unsigned int* err,
+                          unsigned long long limit_ns = 2000000000ull) {
   const unsigned long long t0 = global_ns();
   unsigned ns = 32;
   for (int n = 0; n < (1 << 22); ++n) {
     if (ld_acquire_int(count) >= target) return true;
     if (ld_cg_int((const int*)err)) return false;
-    if (global_ns() - t0 > 2000000000ull) break;
+    if (global_ns() - t0 > limit_ns) break;
     __nanosleep(ns);
     if (ns < 1024) ns <<= 1;
   }
   atomicExch(err, 1u);
   return false;
+}
+
+// self-test of the bounded wait: thread 0 of one block waits for a count that
+// nothing raises, gives up after limit_ns and sets *err
+__global__ void wave_wait_probe(const int* count, unsigned int* err, unsigned long long limit_ns) {
+  if (threadIdx.x == 0) wave_wait(count, 1, err, limit_ns);
+}
+
+cudaError_t launch_wave_wait_probe(const int* count, unsigned int* err, double limit_s, cudaStream_t s) {
+  wave_wait_probe<<<1, 32, 0, s>>>(count, err, (unsigned long long)(limit_s * 1e9));
+  return cudaGetLastError();
 }
 
 // launch prologue: problems already done pass every wait; the ticket restarts

@@ -41,6 +41,9 @@ cudaError_t launch_march2d_wave(int harmonic, const Problem* probs, int nprob, c
                                 int K, unsigned int* counters, int* wave_count, cudaStream_t s);
 // blocks one wavefront launch keeps resident on the current device
 int march2d_wave_slots(int harmonic);
+// one block whose thread 0 runs the wavefront's dependency wait on *count (which
+// must stay 0) with a limit of limit_s seconds; sets *err when the wait runs out
+cudaError_t launch_wave_wait_probe(const int* count, unsigned int* err, double limit_s, cudaStream_t s);
 // 3D plane-marching kernel (reciprocal form); items are (problem, column tile + strip)
 cudaError_t launch_march3d_fast(int harmonic, const Problem* probs, const int2* items, int nitems, cudaStream_t s);
 

@@ -1091,6 +1091,29 @@ extern "C" {
 
 int cdm_apt_version(void) { return CDM_APT_ABI_VERSION; }
 
+int cdm_selftest_bounded_wait(int device, double limit_s, int* expired) {
+  if (!expired || !(limit_s > 0.0) || limit_s > 10.0) {
+    cdm::set_error("cdm_selftest_bounded_wait: expired must not be NULL and 0 < limit_s <= 10");
+    return CDM_BAD_INPUT;
+  }
+  *expired = 0;
+  CDM_CK(cudaSetDevice(device));
+  int* buf = nullptr;  // [0] the count nothing raises, [1] the error flag
+  CDM_CK(cudaMalloc((void**)&buf, 2 * sizeof(int)));
+  cudaError_t e = cudaMemset(buf, 0, 2 * sizeof(int));
+  if (e == cudaSuccess) e = cdm::launch_wave_wait_probe(buf, (unsigned int*)(buf + 1), limit_s, nullptr);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  int flag = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&flag, buf + 1, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(buf);
+  if (e != cudaSuccess) {
+    cdm::set_error(std::string("cdm_selftest_bounded_wait: ") + cudaGetErrorString(e));
+    return CDM_CUDA_ERROR;
+  }
+  *expired = flag != 0;
+  return CDM_OK;
+}
+
 const char* cdm_apt_last_error(void) { return cdm::g_error.c_str(); }
 
 void cdm_step_opts_default(cdm_step_opts* o) {

@@ -192,6 +192,13 @@ typedef struct cdm_profile {
 /* ---- library ---------------------------------------------------------------- */
 int cdm_apt_version(void);
 const char* cdm_apt_last_error(void);
+/* Diagnostic, no counterpart in the reference: runs the wavefront schedule's
+ * bounded dependency wait (the spin of a block waiting for its problem's
+ * previous iteration) on device `device` against a counter that nothing
+ * raises, with a limit of limit_s seconds (0 < limit_s <= 10).  *expired = 1
+ * when the wait gave up and raised the error flag, as the sweep does before
+ * the host reports CDM_TIMEOUT; the context stays usable. */
+int cdm_selftest_bounded_wait(int device, double limit_s, int* expired);
 void cdm_step_opts_default(cdm_step_opts* opts);
 void cdm_apt_config_default(cdm_apt_config* cfg);
 

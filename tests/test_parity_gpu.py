@@ -400,6 +400,26 @@ def test_invalid_diffusivity_stops_the_next_step(tuning):
     b.close()
 
 
+def test_bounded_wait_runs_out_and_reports():
+    """The wavefront kernel's dependency wait is bounded: waiting on a count that
+    nothing raises gives up after the limit, raises the error flag the host turns
+    into CDM_TIMEOUT, and leaves the context usable (a step runs afterwards)."""
+    import ctypes as C
+    import time
+    from curvilineardiffusionmanuscript_b200 import _lib as L
+    lib = L.load()
+    expired = C.c_int(0)
+    t0 = time.perf_counter()
+    rc = lib.cdm_selftest_bounded_wait(0, 0.05, C.byref(expired))
+    dt = time.perf_counter() - t0
+    assert rc == L.CDM_OK, L.last_error()
+    assert expired.value == 1 and 0.05 <= dt < 5.0
+    assert lib.cdm_selftest_bounded_wait(0, 0.0, C.byref(expired)) == L.CDM_BAD_INPUT
+    probs = problems.batch_2d(nprob=2, nmin=20, nmax=40, seed=4)
+    (its, _), = _run_tunings(probs, [(4, 8, 8)], nsteps=1)
+    assert all(n > 0 for n in its[0])
+
+
 def test_set_tuning_rejects_invalid_choices():
     probs = problems.batch_2d(nprob=2, nmin=20, nmax=30, seed=1)
     b = PseudoTransientBatch([p.mesh for p in probs], [p.bcs for p in probs])
