@@ -66,6 +66,10 @@ def lpt_assign(costs: Sequence[float], nranks: int) -> List[List[int]]:
     return out
 
 
+class ShardError(RuntimeError):
+    """A rank's step failed; raised on every rank with the failed ranks' errors."""
+
+
 class ShardedBatch:
     """A batch of problems split over the ranks of the default process group.
 
@@ -93,19 +97,30 @@ class ShardedBatch:
         return [xs[i] for i in self.local]
 
     def step(self, Ts, rhos, cps, kappas, dts, **kwargs):
-        stats, ndts = [], []
+        """Steps this rank's problems, then gathers every problem's statistics.
+        A rank whose own step fails still takes part in the gather, with its
+        error in place of statistics, so that every rank takes the same
+        collective steps and raises the same ShardError instead of waiting for
+        the failed rank until the process group's timeout."""
+        stats, ndts, err = [], [], None
         if self.batch is not None:
-            stats, ndts = self.batch.step(self._pick(Ts), self._pick(rhos), self._pick(cps), self._pick(kappas),
-                                          self._pick(dts), **kwargs)
-        mine = list(zip(self.local, stats, ndts))
+            try:
+                stats, ndts = self.batch.step(self._pick(Ts), self._pick(rhos), self._pick(cps),
+                                              self._pick(kappas), self._pick(dts), **kwargs)
+            except Exception as e:  # reported on every rank after the gather
+                err = f"rank {self.rank}: {type(e).__name__}: {e}"
+        mine = (err, list(zip(self.local, stats, ndts)))
         if self.world > 1:
             parts: list = [None] * self.world
             dist.all_gather_object(parts, mine)
         else:
             parts = [mine]
+        errors = [e for e, _ in parts if e]
+        if errors:
+            raise ShardError("; ".join(errors))
         all_stats: list = [None] * self.n
         all_ndt: list = [None] * self.n
-        for part in parts:
+        for _, part in parts:
             for i, st, nd in part:
                 all_stats[i] = st
                 all_ndt[i] = nd

@@ -1,5 +1,6 @@
 """Multi-rank host logic of the sharded batch, as world-size-2 gloo process
-groups on CPU (no GPU): assignment, statistics gather, timing reductions."""
+groups on CPU (no GPU): assignment, statistics gather, timing reductions, and
+failures made on the host (a rank whose step raises, a rank that leaves)."""
 import os
 import socket
 
@@ -8,7 +9,7 @@ import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from curvilineardiffusionmanuscript_b200.sharding import ShardedBatch, lpt_assign, reduce_max, reduce_sum
+from curvilineardiffusionmanuscript_b200.sharding import ShardError, ShardedBatch, lpt_assign, reduce_max, reduce_sum
 
 
 class FakeMesh:
@@ -96,3 +97,77 @@ def test_sharded_batch_two_ranks_gloo():
     cost = [n * n for n in sizes]
     loads = [sum(cost[i] for i in r[1]) for r in res]
     assert max(loads) <= 1.34 * max(max(cost), sum(cost) / 2)
+
+
+class FailingBatch(FakeBatch):
+    """A FakeBatch whose step raises on the rank that holds the 512² problem."""
+
+    def step(self, Ts, rhos, cps, kappas, dts, **kw):
+        if 512 in self.sizes:
+            raise RuntimeError("injected failure")
+        return super().step(Ts, rhos, cps, kappas, dts, **kw)
+
+
+def _put_and_exit(q, item):
+    # flush the queue's feeder thread before leaving without interpreter teardown
+    q.put(item)
+    q.close()
+    q.join_thread()
+    os._exit(0)
+
+
+def _failure_worker(rank, world, port, q, mode):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    import time
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=20))
+    sizes = [64, 512, 128, 96, 300, 200, 80]
+    meshes = [FakeMesh(n) for n in sizes]
+    sb = ShardedBatch(meshes, [None] * 7, make_batch=FailingBatch if mode == "raise" else FakeBatch)
+    args = ([torch.zeros(3) for _ in sizes], [None] * 7, [1.0] * 7, [None] * 7, [1.0] * 7)
+    if mode == "leave" and rank == 1:
+        _put_and_exit(q, (rank, "left", 0.0))  # leaves between steps, with no collective in flight
+    t0 = time.time()
+    try:
+        sb.step(*args)
+        out = (rank, "ok", time.time() - t0)
+    except ShardError as e:
+        out = (rank, "ShardError: " + str(e), time.time() - t0)
+    except Exception as e:  # the process group reports the missing peer
+        out = (rank, type(e).__name__, time.time() - t0)
+    _put_and_exit(q, out)
+
+
+def _run_failure(mode):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_failure_worker, args=(r, 2, port, q, mode)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    return res
+
+
+def test_a_failing_rank_is_reported_on_every_rank():
+    """The rank holding the 512² problem raises in its step; both ranks finish
+    the gather and raise the same ShardError naming it."""
+    res = _run_failure("raise")
+    failed = 0 if 1 in lpt_assign([n * n for n in [64, 512, 128, 96, 300, 200, 80]], 2)[0] else 1
+    for rank, what, dt in res:
+        assert what.startswith("ShardError") and f"rank {failed}" in what and "injected failure" in what, what
+        assert dt < 15.0
+
+
+def test_a_rank_that_leaves_ends_the_others_step_with_an_error():
+    """Rank 1 exits between steps; rank 0's statistics gather ends with an error
+    (the closed connection, at the latest the process group's 20 s timeout)
+    instead of waiting for good."""
+    res = _run_failure("leave")
+    assert res[1][1] == "left"
+    rank, what, dt = res[0]
+    assert what != "ok" and dt < 60.0, (what, dt)
