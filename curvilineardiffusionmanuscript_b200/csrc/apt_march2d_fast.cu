@@ -299,6 +299,7 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
   }
   // own-column fluxes in registers: x faces of rows j-1 and j, y face of row j-1
   double rqx_m = qx_m, rqx_0 = qx_0, rpx_m = px_m, rpx_0 = px_0, rqy_m = qy_m, rpy_m = py_m;
+  double g0 = c0.g, f0 = c0.f;  // update factors of row j; its u, α⁻¹, θ⁻¹ are read from shared memory
 
   double local = 0.0;
   bool local_nan = false;
@@ -322,7 +323,8 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
     }
     double px_p1, py_0n;
     const double qx_p1 = face_x(j + 1, s_p, cp1, Lc.qx, px_p1);
-    const double qy_0n = face_y(j, c0, cp1, Lc.qy, py_0n);
+    const Cell lo{sm.U[s_0][tid], sm.IA[s_0][tid], sm.IT[s_0][tid], 0.0, 0.0};
+    const double qy_0n = face_y(j, lo, cp1, Lc.qy, py_0n);
     sm.QX[s_p][tid] = qx_p1;
     sm.QY[y_0][tid] = qy_0n;
     if (check) {
@@ -336,7 +338,7 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
                         c12 * ((qx_p1 + sm.QX[s_p][x - 1]) - (rqx_m + sm.QX[s_m][x - 1])) +
                         c12 * ((sm.QY[y_0][x + 1] + sm.QY[y_m][x + 1]) - (sm.QY[y_0][x - 1] + sm.QY[y_m][x - 1])) +
                         ca * (0.5 * (rqx_0 + sm.QX[s_0][x - 1])) + cbv * (0.5 * (qy_0n + rqy_m));
-      const double un = c0.g * c0.u + c0.f * (up * inv_dt - dq + S);
+      const double un = g0 * sm.U[s_0][tid] + f0 * (up * inv_dt - dq + S);
       uout[o] = un;
       qyout[o] = qy_0n;
       if (check) {
@@ -357,9 +359,10 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
       if (EDGE && j == nj - 1) uout[o + nx] = cp1.u;
     }
     if (qx_own) qxout[o] = rqx_0;
-    if (EDGE && cside >= 0) uout[o] = c0.u;
+    if (EDGE && cside >= 0) uout[o] = sm.U[s_0][tid];
     // rotate: rows (j, j+1) become (j-1, j)
-    c0 = cp1;
+    g0 = cp1.g;
+    f0 = cp1.f;
     rqx_m = rqx_0;
     rqx_0 = qx_p1;
     rpx_m = rpx_0;
