@@ -570,6 +570,7 @@ __device__ __forceinline__ void mixed_body(const Problem& P, Ctrl* C, int tile, 
   sm.PY[y_m][tid] = py_m;
   if (EDGE && j0 == 0 && owner) eyout[col + nx * (nh - 1)] = rqy_m;
   float rpx_m = px_m, rpx_0 = px_0, rpy_m = py_m;
+  float f0 = c0.f;  // update factor of row j; its other values are read from the staged window
   float local = 0.f;
   bool nan = false;
   for (int j = j0; j < j1; ++j) {
@@ -591,11 +592,14 @@ __device__ __forceinline__ void mixed_body(const Problem& P, Ctrl* C, int tile, 
     }
     float px_p1, py_0n;
     const float qx_p1 = face_x(j + 1, s_p, cp1, Lc.ex, px_p1);
-    const float qy_0n = face_y(j, c0, cp1, Lc.ey, py_0n);
+    const MCell lo{sm.D[s_0][tid], sm.UB[s_0][tid], sm.AB[s_0][tid], sm.DA[s_0][tid], sm.IT[s_0][tid], 0.f};
+    const float qy_0n = face_y(j, lo, cp1, Lc.ey, py_0n);
     sm.EX[s_p][tid] = qx_p1;
-    sm.PX[s_p][tid] = px_p1;
     sm.EY[y_0][tid] = qy_0n;
-    sm.PY[y_0][tid] = py_0n;
+    if (check) {  // the plain fluxes feed the residual only
+      sm.PX[s_p][tid] = px_p1;
+      sm.PY[y_0][tid] = py_0n;
+    }
     __syncthreads();
     if (owner) {
       const int x = tid;
@@ -603,7 +607,8 @@ __device__ __forceinline__ void mixed_body(const Problem& P, Ctrl* C, int tile, 
                        c12 * ((qx_p1 + sm.EX[s_p][x - 1]) - (rqx_m + sm.EX[s_m][x - 1])) +
                        c12 * ((sm.EY[y_0][x + 1] + sm.EY[y_m][x + 1]) - (sm.EY[y_0][x - 1] + sm.EY[y_m][x - 1])) +
                        ca * (0.5f * (rqx_0 + sm.EX[s_0][x - 1])) + cbv * (0.5f * (qy_0n + rqy_m));
-      const float dn = c0.d + c0.f * (R - c0.d * inv_dt - dq);
+      const float d0 = sm.D[s_0][x];
+      const float dn = d0 + f0 * (R - d0 * inv_dt - dq);
       dout[o] = dn;
       eyout[o] = qy_0n;
       if (check) {
@@ -617,7 +622,7 @@ __device__ __forceinline__ void mixed_body(const Problem& P, Ctrl* C, int tile, 
       }
     }
     if (qx_own) exout[o] = rqx_0;
-    c0 = cp1;
+    f0 = cp1.f;
     rqx_m = rqx_0;
     rqx_0 = qx_p1;
     rpx_m = rpx_0;
