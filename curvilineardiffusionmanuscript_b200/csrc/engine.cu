@@ -606,8 +606,18 @@ cudaError_t Engine::launch_iters(int K) {
 int Engine::launch_block(int K, bool use_graph) {
   const int pe = record_pair();
   if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe], stream));
-  const bool wave = tile_shape(ndim, variant).march == 3;
-  prof.sweep_launches += wave ? 2 : K;
+  // kernels launched: the wavefront kernel (its prologue counts as another
+  // kernel), or per iteration the fast 2D pair (boundary and interior strips) or
+  // one sweep kernel
+  const TileShape ts = tile_shape(ndim, variant);
+  if (ts.march == 3) {
+    prof.sweep_launches += 1;
+    prof.other_launches += 1;
+  } else if (ts.march == 1 && precision != CDM_PREC_FP64_EXACT) {
+    prof.sweep_launches += (int64_t)K * ((n_edge > 0 ? 1 : 0) + (nitems - n_edge > 0 ? 1 : 0));
+  } else {
+    prof.sweep_launches += K;
+  }
   if (!use_graph) {
     CDM_CK(launch_iters(K));
     if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe + 1], stream));

@@ -182,7 +182,9 @@ typedef struct cdm_apt cdm_apt; /* opaque solver handle */
  * reference times stages with TimerOutputs, PseudoTransientSolver.jl:232-339) */
 typedef struct cdm_profile {
   double sweep_ms;          /* CUDA-event time of the pseudo-iteration launches     */
-  int64_t sweep_launches;   /* fused-sweep launches (including early-exit tails)    */
+  int64_t sweep_launches;   /* fused-sweep kernel launches (including early-exit
+                               tails; the 2D boundary and interior kernels of an
+                               iteration count separately)                         */
   int64_t other_launches;   /* every other kernel launched by the step              */
   int64_t cell_iters;       /* sum over problems of domain cells x pseudo-iterations */
   int64_t fp32_cell_iters;  /* mixed precision: cells x FP32 correction sweeps      */
