@@ -18,7 +18,7 @@ import numpy as np
 import pytest
 import torch
 
-from helpers import small_case_2d, small_case_3d
+from helpers import decaying_mode_error, small_case_2d, small_case_3d
 from oracle.oracle import OracleSolver, applybcs
 from curvilineardiffusionmanuscript_b200.mesh import uniform_mesh_2d, wavy_mesh_2d
 from curvilineardiffusionmanuscript_b200.solver import (DirichletBC, FixedNegSymmetryBC, NeumannBC, PeriodicBC,
@@ -219,6 +219,26 @@ def test_mms_second_order_on_wavy_mesh():
     e1, e2 = _mms_periodic_error(16), _mms_periodic_error(32)
     order = math.log2(e1 / e2)
     assert 1.7 < order < 2.4, (e1, e2, order)
+
+
+def _oracle_steps(m, bcs, T0, rho, dt, nsteps):
+    o = OracleSolver(m, bcs)
+    T = T0.numpy().copy()
+    for _ in range(nsteps):
+        # relative stop: the residual's rounding floor (u − uⁿ)/Δt is ~1e-11 at this Δt
+        st, _ = o.step(T, rho.numpy(), 1.0, 1.0, 0.0, dt, rtol=1e-10, atol=0.0, max_iter=200000)
+        assert st["status"] == 0
+    return T[m.domain()]
+
+
+def test_decaying_mode_second_order():
+    """The reference's analytic case (test/integrated/2d/analytic/run.jl: sin(3πx)e^{−9π²t}
+    with negative-symmetry and periodic sides): error against the exact mode falls
+    by about 4 per halving of h."""
+    e1 = decaying_mode_error(16, _oracle_steps)
+    e2 = decaying_mode_error(32, _oracle_steps)
+    order = math.log2(e1 / e2)
+    assert 1.8 < order < 2.2, (e1, e2, order)
 
 
 # ------------------------------------------------------------------ golden

@@ -8,16 +8,18 @@ counts on the same seeded inputs.
 * precision "fp64" (the default, reciprocal form) differs in the last bits:
   the 1e-10 bar and equal iteration counts are asserted.
 """
+import math
+
 import numpy as np
 import pytest
 import torch
 
-from helpers import rel_l2, small_case_2d, small_case_3d
+from helpers import decaying_mode_error, rel_l2, small_case_2d, small_case_3d
 from oracle.oracle import OracleSolver
 from curvilineardiffusionmanuscript_b200 import problems
 from curvilineardiffusionmanuscript_b200.solver import (APTError, DirichletBC, FixedNegSymmetryBC, NeumannBC,
-                                                        PeriodicBC, PseudoTransientBatch, PseudoTransientSolver,
-                                                        step)
+                                                        PeriodicBC, PowerLawConductivity, PseudoTransientBatch,
+                                                        PseudoTransientSolver, step)
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-10
@@ -418,6 +420,34 @@ def test_bounded_wait_runs_out_and_reports():
     probs = problems.batch_2d(nprob=2, nmin=20, nmax=40, seed=4)
     (its, _), = _run_tunings(probs, [(4, 8, 8)], nsteps=1)
     assert all(n > 0 for n in its[0])
+
+
+def _gpu_steps(m, bcs, T0, rho, dt, nsteps):
+    g = PseudoTransientSolver(m, bcs, precision="fp64")
+    T, r = T0.clone().cuda(), rho.cuda()
+    for _ in range(nsteps):
+        step(g, m, T, r, 1.0, PowerLawConductivity(1.0, 0.0), dt, rtol=1e-10, atol=0.0, max_iter=200000)
+    g.close()
+    return T.cpu().numpy()[m.domain()]
+
+
+def _oracle_steps(m, bcs, T0, rho, dt, nsteps):
+    o = OracleSolver(m, bcs)
+    T = T0.numpy().copy()
+    for _ in range(nsteps):
+        o.step(T, rho.numpy(), 1.0, 1.0, 0.0, dt, rtol=1e-10, atol=0.0, max_iter=200000)
+    return T[m.domain()]
+
+
+def test_decaying_mode_second_order_on_the_gpu():
+    """The reference's analytic case (sin(3πx)e^{−9π²t}, negative-symmetry and
+    periodic sides) through the fast FP64 path: second order in h, and the same
+    errors as the oracle's."""
+    e = [decaying_mode_error(n, _gpu_steps) for n in (16, 32)]
+    order = math.log2(e[0] / e[1])
+    assert 1.8 < order < 2.2, (e, order)
+    eo = decaying_mode_error(16, _oracle_steps)
+    assert abs(e[0] - eo) <= 1e-6 * eo, (e[0], eo)
 
 
 def test_set_tuning_rejects_invalid_choices():
