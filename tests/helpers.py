@@ -58,3 +58,19 @@ def decaying_mode_error(n, run_steps, nsteps=10, dt=2e-6):
     exact = (torch.sin(3 * math.pi * x) * math.exp(-9 * math.pi ** 2 * dt * nsteps))[m.domain()]
     d = np.asarray(T, dtype=np.float64) - exact.numpy()
     return float(np.sqrt((d * d).mean()))
+
+
+def richardson_order(run_steps, sizes=(9, 27, 81), dt=1e-3, nsteps=5):
+    """The reference's Richardson study (test/integrated/2d/richardson_wavy_2D/run.jl:
+    κ = 2.5, Neumann sides, wavy mesh, grids refined by 3 so that coarse cell centres
+    are fine cell centres): log₃ of ‖u_h − u_{h/3}‖∞ / ‖u_{h/3} − u_{h/9}‖∞ on the
+    coarse points, for a pulse 1 + exp(−|x − (½, ½)|²/0.05) that stays off the walls.
+    `run_steps(mesh, bcs, T0, rho, dt, nsteps)` returns the domain field."""
+    u = []
+    for n in sizes:
+        m = wavy_mesh_2d(n, n, 0.05)
+        x, y = m.centroids
+        T0 = (1.0 + torch.exp(-((x - 0.5) ** 2 + (y - 0.5) ** 2) / 0.05)).contiguous()
+        u.append(np.asarray(run_steps(m, [NeumannBC()] * 4, T0, torch.ones_like(T0), dt, nsteps)))
+    c0, c1, c2 = u[0], u[1][1::3, 1::3], u[2][4::9, 4::9]
+    return math.log(np.abs(c0 - c1).max() / np.abs(c1 - c2).max(), 3)

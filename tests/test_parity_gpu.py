@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 import torch
 
-from helpers import decaying_mode_error, rel_l2, small_case_2d, small_case_3d
+from helpers import decaying_mode_error, rel_l2, richardson_order, small_case_2d, small_case_3d
 from oracle.oracle import OracleSolver
 from curvilineardiffusionmanuscript_b200 import problems
 from curvilineardiffusionmanuscript_b200.solver import (APTError, DirichletBC, FixedNegSymmetryBC, NeumannBC,
@@ -448,6 +448,21 @@ def test_decaying_mode_second_order_on_the_gpu():
     assert 1.8 < order < 2.2, (e, order)
     eo = decaying_mode_error(16, _oracle_steps)
     assert abs(e[0] - eo) <= 1e-6 * eo, (e[0], eo)
+
+
+def _gpu_k25_steps(m, bcs, T0, rho, dt, nsteps):
+    g = PseudoTransientSolver(m, bcs, precision="fp64")
+    T, r = T0.clone().cuda(), rho.cuda()
+    for _ in range(nsteps):
+        step(g, m, T, r, 1.0, PowerLawConductivity(2.5, 0.0), dt, rtol=1e-10, atol=0.0, max_iter=500000)
+    g.close()
+    return T.cpu().numpy()[m.domain()]
+
+
+def test_richardson_order_on_the_gpu():
+    """The reference's Richardson study through the fast FP64 path (9², 27², 81²)."""
+    order = richardson_order(_gpu_k25_steps)
+    assert 1.8 < order < 2.4, order
 
 
 def test_set_tuning_rejects_invalid_choices():
