@@ -43,17 +43,18 @@ def small_case_3d(n=(10, 9, 8), amp=0.04, kn=2.5, bcs=None):
     return problems.Problem("small3d", m, bcs, T0, rho, 1.0, PowerLawConductivity(1.0, kn), 1e-5, 3)
 
 
-def decaying_mode_error(n, run_steps, nsteps=10, dt=2e-6):
+def decaying_mode_error(n, run_steps, nsteps=10, dt=2e-6, ndim=2):
     """Known answer of the reference's analytic case: u = sin(3πx)·exp(−9π²t)
     with κ = 1, ρ = cₚ = 1, negative-symmetry ghosts on the x sides (u = 0 at
-    the walls) and periodic y sides, on a rectilinear n × n mesh of [0,1]².
+    the walls) and periodic other sides, on a rectilinear mesh of n cells per
+    side of [0,1]^ndim.
     `run_steps(mesh, bcs, T0, rho, dt, nsteps)` advances T0 and returns the
     domain field; the result is the RMS error against the exact solution."""
-    m = wavy_mesh_2d(n, n, 0.0)
-    x, _ = m.centroids
+    m = wavy_mesh_2d(n, n, 0.0) if ndim == 2 else wavy_mesh_3d(n, n, n, amp=0.0)
+    x = m.centroids[0]
     T0 = torch.sin(3 * math.pi * x).contiguous()
     rho = torch.ones_like(T0)
-    bcs = [FixedNegSymmetryBC(), FixedNegSymmetryBC(), PeriodicBC(), PeriodicBC()]
+    bcs = [FixedNegSymmetryBC(), FixedNegSymmetryBC()] + [PeriodicBC()] * (2 * ndim - 2)
     T = run_steps(m, bcs, T0, rho, dt, nsteps)
     exact = (torch.sin(3 * math.pi * x) * math.exp(-9 * math.pi ** 2 * dt * nsteps))[m.domain()]
     d = np.asarray(T, dtype=np.float64) - exact.numpy()

@@ -239,6 +239,11 @@ def test_decaying_mode_second_order():
     e2 = decaying_mode_error(32, _oracle_steps)
     order = math.log2(e1 / e2)
     assert 1.8 < order < 2.2, (e1, e2, order)
+    # the same mode in 3D (negative-symmetry x sides, periodic y and z sides)
+    e1 = decaying_mode_error(12, _oracle_steps, ndim=3)
+    e2 = decaying_mode_error(24, _oracle_steps, ndim=3)
+    order = math.log2(e1 / e2)
+    assert 1.8 < order < 2.2, (e1, e2, order)
 
 
 def _oracle_k25_steps(m, bcs, T0, rho, dt, nsteps):

@@ -448,6 +448,12 @@ def test_decaying_mode_second_order_on_the_gpu():
     assert 1.8 < order < 2.2, (e, order)
     eo = decaying_mode_error(16, _oracle_steps)
     assert abs(e[0] - eo) <= 1e-6 * eo, (e[0], eo)
+    # 3D, through the plane-marching kernel
+    e = [decaying_mode_error(n, _gpu_steps, ndim=3) for n in (12, 24)]
+    order = math.log2(e[0] / e[1])
+    assert 1.8 < order < 2.2, (e, order)
+    eo = decaying_mode_error(12, _oracle_steps, ndim=3)
+    assert abs(e[0] - eo) <= 1e-6 * eo, (e[0], eo)
 
 
 def _gpu_k25_steps(m, bcs, T0, rho, dt, nsteps):
