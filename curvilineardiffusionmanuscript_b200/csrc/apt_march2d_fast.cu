@@ -304,10 +304,10 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
   double local = 0.0;
   bool local_nan = false;
   for (int j = j0; j < j1; ++j) {
-    const Pre Lc = Ln;
-    if (j + 1 < j1) prefetch(j + 2, Ln);
     const int o = col + nx * (j + nh);
-    const Cell cp1 = stage(j + 1, Lc);
+    const Cell cp1 = stage(j + 1, Ln);
+    const double lqx = Ln.qx, lqy = Ln.qy;  // old fluxes of row j + 1, used below
+    if (j + 1 < j1) prefetch(j + 2, Ln);
     publish(s_p, cp1);
     __syncthreads();
     // the row's coefficients: their loads overlap the face computations
@@ -322,9 +322,9 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
       S = Sg[o];
     }
     double px_p1, py_0n;
-    const double qx_p1 = face_x(j + 1, s_p, cp1, Lc.qx, px_p1);
+    const double qx_p1 = face_x(j + 1, s_p, cp1, lqx, px_p1);
     const Cell lo{sm.U[s_0][tid], sm.IA[s_0][tid], sm.IT[s_0][tid], 0.0, 0.0};
-    const double qy_0n = face_y(j, lo, cp1, Lc.qy, py_0n);
+    const double qy_0n = face_y(j, lo, cp1, lqy, py_0n);
     sm.QX[s_p][tid] = qx_p1;
     sm.QY[y_0][tid] = qy_0n;
     if (check) {
