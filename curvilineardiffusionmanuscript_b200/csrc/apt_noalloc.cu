@@ -20,12 +20,27 @@
 // once) race on the scratch and must not be issued.
 //
 // Set-up: the first call on a device looks up the device address of the
-// scratch with cudaGetSymbolAddress while that device is current; make that
-// first call before any stream capture begins.
+// scratch with cudaGetSymbolAddress while that device is current.
+//
+// The call is synchronous: it copies the results into host memory and returns
+// once they are there, so it cannot be issued inside a stream capture at any
+// time.  Its wait for the device is bounded (CDM_STEP_TIMEOUT_S seconds,
+// default 3600) and ends with CDM_TIMEOUT, like every other entry point.
+//
+// Arguments are checked before anything is launched: every array must be
+// device (or managed) memory of the current device, reaching at least the full
+// array's size within its allocation, and the stream must belong to the
+// current device.  A host pointer or a short array is CDM_BAD_INPUT, not a
+// fault on the GPU.
+#include <cuda.h>
+
+#include <chrono>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <mutex>
 #include <string>
+#include <thread>
 
 #include "cdm_apt.h"
 #include "engine.h"
@@ -187,6 +202,87 @@ int scratch_on_current_device(double** out) {
   return CDM_OK;
 }
 
+// cuMemGetAddressRange through the runtime's driver entry point (no link
+// against the driver library); NULL when the driver does not provide it
+using AddressRangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+AddressRangeFn address_range_fn() {
+  static AddressRangeFn fn = nullptr;
+  static bool looked = false;
+  std::lock_guard<std::mutex> lock(g_setup_mutex);
+  if (!looked) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuMemGetAddressRange", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<AddressRangeFn>(p);
+    looked = true;
+  }
+  return fn;
+}
+
+// `name` must be device or managed memory that the current device `dev` can
+// read for `bytes` bytes from `ptr` within one allocation
+int check_device_array(const char* name, const void* ptr, int64_t bytes, int dev) {
+  cudaPointerAttributes at;
+  cudaError_t e = cudaPointerGetAttributes(&at, ptr);
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // the query's error is not sticky; clear it
+    set_error(std::string("cdm_step_reductions_noalloc: ") + name + " is not a CUDA pointer (" +
+              cudaGetErrorString(e) + ")");
+    return CDM_BAD_INPUT;
+  }
+  if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) {
+    set_error(std::string("cdm_step_reductions_noalloc: ") + name + " must be device memory (got " +
+              (at.type == cudaMemoryTypeHost ? "page-locked host memory" : "host memory") + ")");
+    return CDM_BAD_INPUT;
+  }
+  if (at.type == cudaMemoryTypeDevice && at.device != dev) {
+    set_error(std::string("cdm_step_reductions_noalloc: ") + name + " lives on device " +
+              std::to_string(at.device) + ", the current device is " + std::to_string(dev));
+    return CDM_BAD_INPUT;
+  }
+  // the extent check is what keeps a short array from being read past its end
+  const AddressRangeFn fn = address_range_fn();
+  if (!fn) {
+    set_error("cdm_step_reductions_noalloc: the driver does not provide cuMemGetAddressRange");
+    return CDM_CUDA_ERROR;
+  }
+  CUdeviceptr base = 0;
+  size_t size = 0;
+  if (fn(&base, &size, (CUdeviceptr)ptr) != CUDA_SUCCESS) {
+    set_error(std::string("cdm_step_reductions_noalloc: ") + name + " is not inside a device allocation");
+    return CDM_BAD_INPUT;
+  }
+  const uint64_t left = (uint64_t)base + size - (uint64_t)(uintptr_t)ptr;
+  if ((uint64_t)bytes > left) {
+    set_error(std::string("cdm_step_reductions_noalloc: ") + name + " holds " + std::to_string(left / 8) +
+              " doubles within its allocation; the full array needs " + std::to_string(bytes / 8));
+    return CDM_BAD_INPUT;
+  }
+  return CDM_OK;
+}
+
+// wait for `s` with a bound, polling (no event: nothing is created here)
+int wait_bounded(cudaStream_t s) {
+  double limit = 3600.0;
+  if (const char* v = std::getenv("CDM_STEP_TIMEOUT_S")) limit = std::atof(v);
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int spins = 0;; ++spins) {
+    const cudaError_t e = cudaStreamQuery(s);
+    if (e == cudaSuccess) return CDM_OK;
+    if (e != cudaErrorNotReady) {
+      set_error(std::string("cdm_step_reductions_noalloc: device error: ") + cudaGetErrorString(e));
+      return CDM_CUDA_ERROR;
+    }
+    if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > limit) {
+      set_error("cdm_step_reductions_noalloc: timed out waiting for the device");
+      return CDM_TIMEOUT;
+    }
+    if (spins > 64) std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
+}
+
 }  // namespace
 
 }  // namespace cdm
@@ -217,10 +313,29 @@ extern "C" int cdm_step_reductions_noalloc(int ndim, int ni, int nj, int nk, int
               " cells; the allocation-free scratch holds at most " + std::to_string(kMaxCells));
     return CDM_BAD_INPUT;
   }
-  double* scratch = nullptr;
-  int rc = scratch_on_current_device(&scratch);
-  if (rc != CDM_OK) return rc;
+  int dev = 0;
+  CDM_CK(cudaGetDevice(&dev));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (s) {
+    int sdev = -1;
+    CDM_CK(cudaStreamGetDevice(s, &sdev));
+    if (sdev != dev) {
+      set_error("cdm_step_reductions_noalloc: the stream belongs to device " + std::to_string(sdev) +
+                ", the current device is " + std::to_string(dev));
+      return CDM_BAD_INPUT;
+    }
+  }
+  const int64_t bytes = g.nfull * (int64_t)sizeof(double);
+  int rc = CDM_OK;
+  const struct {
+    const char* name;
+    const double* p;
+  } arrays[] = {{"u_new", u_new}, {"u_prev", u_prev}, {"rho", rho}, {"S", S}, {"cell_J", cell_J}};
+  for (const auto& a : arrays)
+    if (a.p && (rc = check_device_array(a.name, a.p, bytes, dev)) != CDM_OK) return rc;
+  double* scratch = nullptr;
+  rc = scratch_on_current_device(&scratch);
+  if (rc != CDM_OK) return rc;
   const int nb = (int)((g.nfull + kChunk - 1) / kChunk);
   noalloc_pass1<<<nb, kThreads, 0, s>>>(g, u_new, u_prev, rho, S, cell_J, cp, scratch);
   noalloc_finish1<<<1, 32, 0, s>>>(nb, scratch);
@@ -228,8 +343,13 @@ extern "C" int cdm_step_reductions_noalloc(int ndim, int ni, int nj, int nk, int
   noalloc_finish2<<<1, 32, 0, s>>>(nb, scratch);
   double r[5];
   CDM_CK(cudaGetLastError());
+  // a bounded wait for the reductions; the copy into pageable host memory that
+  // follows then completes at once
+  rc = wait_bounded(s);
+  if (rc != CDM_OK) return rc;
   CDM_CK(cudaMemcpyAsync(r, scratch + kResults, sizeof(r), cudaMemcpyDeviceToHost, s));
-  CDM_CK(cudaStreamSynchronize(s));
+  rc = wait_bounded(s);
+  if (rc != CDM_OK) return rc;
   // next_dt (timestep_control.jl:49-51), the same formula cdm_apt_step applies
   const double cand = dt * std::sqrt(std::fabs(maximum_u_change / r[1]));
   const double cap = timestep_growth_factor * dt;

@@ -307,9 +307,14 @@ int cdm_batch_get_profile(const cdm_batch* b, cdm_profile* out);
  * (may be NULL) and cell_J are full-size device arrays; out (host) receives
  * {next_dt, energy_before, energy_after, source_work} as in cdm_stats.
  * Limit: at most 134,217,728 cells in the full array (CDM_BAD_INPUT beyond).
- * The first call on a device sets the scratch up and must come before any
- * stream capture; calls that overlap on the GPU race on the shared scratch.
- * stream: cudaStream_t or NULL. */
+ * Every array must be device (or managed) memory of the current device that
+ * holds the full array within its allocation, and `stream` (cudaStream_t or
+ * NULL) must belong to the current device: anything else is CDM_BAD_INPUT,
+ * returned before any launch.  The call is synchronous (it returns the results
+ * in host memory), so it cannot be made inside a stream capture at any time;
+ * its wait is bounded by CDM_STEP_TIMEOUT_S (CDM_TIMEOUT).  The first call on a
+ * device looks up the scratch's device address.  Calls that overlap on the
+ * GPU race on the shared scratch. */
 int cdm_step_reductions_noalloc(int ndim, int ni, int nj, int nk, int nhalo, const double* u_new,
                                 const double* u_prev, const double* rho, const double* S,
                                 const double* cell_J, double cp, double dt, double ndt_tol,

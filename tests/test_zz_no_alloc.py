@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 import torch
 
-from helpers import small_case_2d
+from helpers import small_case_2d, small_case_3d
 from curvilineardiffusionmanuscript_b200 import _lib as L
 from curvilineardiffusionmanuscript_b200.solver import PseudoTransientSolver, step
 
@@ -33,9 +33,10 @@ def noalloc(mesh, u_new, u_prev, rho, S, J, cp, dt, tol=1e-3, max_change=0.05, g
     return list(out)
 
 
-@pytest.mark.parametrize("source", [False, True])
-def test_noalloc_matches_step(source):
-    pr = small_case_2d(ni=150, nj=97, source=source)
+@pytest.mark.parametrize("case", ["2d", "2d_source", "3d"])
+def test_noalloc_matches_step(case):
+    source = case == "2d_source"
+    pr = small_case_3d(n=(41, 30, 23)) if case == "3d" else small_case_2d(ni=150, nj=97, source=source)
     g = PseudoTransientSolver(pr.mesh, pr.bcs)
     S = pr.source.cuda() if source else None
     if source:
@@ -61,3 +62,26 @@ def test_noalloc_rejects_oversized_mesh():
                                               None, z.data_ptr(), 1.0, 1e-5, 1e-3, 0.05, 1.1, out, None)
     assert rc == L.CDM_BAD_INPUT
     assert "at most" in L.last_error()
+
+
+def test_noalloc_rejects_host_and_short_arrays():
+    """Arrays the device cannot read over the full mesh are refused before
+    anything is launched: a host array, and a device array shorter than the
+    full array (larger than the allocation it sits in)."""
+    pr = small_case_2d(ni=40, nj=30)
+    J = pr.mesh.cell_J.cuda()
+    u = pr.T0.clone().cuda()
+    rho = pr.rho.cuda()
+    lib = L.load()
+    out = (C.c_double * 4)()
+    host = pr.T0.clone()
+    rc = lib.cdm_step_reductions_noalloc(2, 40, 30, 1, 1, u.data_ptr(), host.data_ptr(), rho.data_ptr(), None,
+                                         J.data_ptr(), 1.0, 1e-5, 1e-3, 0.05, 1.1, out, None)
+    assert rc == L.CDM_BAD_INPUT and "u_prev" in L.last_error()
+    short = torch.zeros(1000, dtype=torch.float64, device="cuda")
+    rc = lib.cdm_step_reductions_noalloc(2, 2000, 2000, 1, 1, short.data_ptr(), short.data_ptr(), short.data_ptr(),
+                                         None, short.data_ptr(), 1.0, 1e-5, 1e-3, 0.05, 1.1, out, None)
+    assert rc == L.CDM_BAD_INPUT and "holds" in L.last_error()
+    # the entry point still works afterwards
+    nd, *_ = noalloc(pr.mesh, u, u.clone(), rho, None, J, 1.0, 1e-5)
+    assert nd == pytest.approx(1.1e-5, rel=1e-15)
