@@ -47,6 +47,12 @@ class MeshDesc(C.Structure):
     ]
 
 
+class TzDesc(C.Structure):
+    """cdm_tz_desc (include/cdm_apt.h)."""
+    _fields_ = [("mem", C.c_int), ("nnodes", C.c_int * 2), ("x", C.c_void_p), ("y", C.c_void_p),
+                ("x_xi", C.c_void_p), ("x_eta", C.c_void_p), ("y_xi", C.c_void_p), ("y_eta", C.c_void_p)]
+
+
 class Config(C.Structure):
     _fields_ = [("mean", C.c_int), ("precision", C.c_int), ("device", C.c_int), ("stream", C.c_void_p)]
 
@@ -101,6 +107,8 @@ SIGNATURES = {
     "cdm_apt_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, Kappa, C.c_double,
                                C.POINTER(StepOpts), C.POINTER(Stats), PD]),
     "cdm_apt_set_guess": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "cdm_apt_set_twilight_zone": (C.c_int, [C.c_void_p, C.POINTER(TzDesc)]),
+    "cdm_batch_set_twilight_zone": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(TzDesc)]),
     "cdm_apt_advance": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, Kappa, PD, C.c_double, C.c_int,
                                   PD, C.c_double, C.POINTER(StepOpts), C.POINTER(Stats), C.POINTER(C.c_int)]),
     "cdm_apt_get_state": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),

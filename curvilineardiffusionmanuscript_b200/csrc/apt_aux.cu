@@ -3,6 +3,7 @@
 
 #include "cdm_device.cuh"
 #include "cdm_kernels.h"
+#include "cdm_tz.cuh"
 
 namespace cdm {
 
@@ -80,6 +81,30 @@ __global__ void coefficient_kernel(Problem P, MeshPtrs m, double* ca0, double* c
       k7[id] = ca1[id];
       k8[id] = ca2[id];
     }
+  }
+}
+
+// twilight_zone.jl:69-183: the α-independent forcing terms of every domain
+// cell for this step (tz::terms), written as kNumTerms full-size arrays
+__global__ void tz_terms_kernel(Problem P, TzMesh m, const double* __restrict__ rho, double cp, double t, int no_t,
+                                double* __restrict__ out) {
+  const int64_t n = (int64_t)P.ni * P.nj;
+  const int64_t st = (int64_t)P.nx * P.ny;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t I = e % P.ni + P.nh, J = e / P.ni + P.nh;
+    const int64_t id = I + (int64_t)P.nx * J;
+    const tz::Terms T = tz::terms(m.x[id], m.y[id], m.xxi[id], m.xeta[id], m.yxi[id], m.yeta[id], rho[id], cp, t,
+                                  no_t, I, J, m.nnx, m.nny);
+    out[id] = T.ut;
+    out[id + st] = T.p1;
+    out[id + 2 * st] = T.uxx;
+    out[id + 3 * st] = T.p2;
+    out[id + 4 * st] = T.uee;
+    out[id + 5 * st] = T.uxe;
+    out[id + 6 * st] = T.p3;
+    out[id + 7 * st] = T.p4;
+    out[id + 8 * st] = T.ux;
+    out[id + 9 * st] = T.ue;
   }
 }
 
@@ -313,6 +338,14 @@ cudaError_t launch_coefficients(const Problem& P, const MeshPtrs& m, double* con
   coefficient_kernel<<<grid_for(n, 256), 256, 0, s>>>(P, m, cache[0], cache[1], cache[2], coef[0], coef[1],
                                                        coef[2], coef[3], coef[4], coef[5], coef[6], coef[7],
                                                        coef[8]);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tz_terms(const Problem& P, const TzMesh& m, const double* rho, double cp, double t, int no_t,
+                            double* out, cudaStream_t s) {
+  if (P.ndim != 2) return cudaErrorInvalidValue;
+  const int64_t n = (int64_t)P.ni * P.nj;
+  tz_terms_kernel<<<grid_for(n, 256), 256, 0, s>>>(P, m, rho, cp, t, no_t, out);
   return cudaGetLastError();
 }
 

@@ -16,10 +16,14 @@
 //    divergence of row j reads, so each face is computed once per strip;
 //  * the global loads of the next row are issued one row ahead into
 //    registers, so memory latency overlaps the FP64 work of the current row;
-//  * all offsets are 32-bit (the engine rejects 2D meshes with nx*ny >= 2^31).
+//  * all offsets are 32-bit (the engine rejects 2D meshes with nx*ny >= 2^31);
+//  * TZ: the twilight-zone forcing (update.jl:23-71, residuals.jl:49-99) is
+//    added to the update and the residual, from the step's precomputed terms
+//    and the row's diffusivity (cdm_tz.cuh).
 #include "cdm_device.cuh"
 #include "cdm_kernels.h"
 #include "cdm_finish.cuh"
+#include "cdm_tz.cuh"
 
 namespace cdm {
 
@@ -61,6 +65,7 @@ struct RowLoads {
   double u, up_bc, rho;   // stage of cell (a, r): u_in (rule applied later), u_prev (rule), rho
   double qx, qy;          // old fluxes at faces (a, r) i+1/2 and (a, r-1) j+1/2
   double g11, g22, c12, ca, cb, up, S;  // update of cell (a, r-1)
+  tz::Terms tzt;          // its twilight-zone terms (TZ only)
   int usrc;               // -1 const, -2 inactive, else offset
   bool neg;
   double cval;
@@ -68,7 +73,7 @@ struct RowLoads {
 
 }  // namespace
 
-template <int TX>
+template <int TX, bool TZ>
 __global__ void __launch_bounds__(TX) march2d_fp64(const Problem* __restrict__ probs, const int2* __restrict__ items) {
   constexpr int OW = TX - 2;
   __shared__ double sU[3][TX], sA[3][TX], sT[3][TX], sD[3][TX];
@@ -139,6 +144,20 @@ __global__ void __launch_bounds__(TX) march2d_fp64(const Problem* __restrict__ p
       L.cb = CB[o];
       L.up = uprev[o];
       L.S = Sg[o];
+      if (TZ) {
+        const double* tzp = P.tz + o;
+        const int64_t st = (int64_t)P.nx * P.ny;
+        L.tzt.ut = tzp[0];
+        L.tzt.p1 = tzp[st];
+        L.tzt.uxx = tzp[2 * st];
+        L.tzt.p2 = tzp[3 * st];
+        L.tzt.uee = tzp[4 * st];
+        L.tzt.uxe = tzp[5 * st];
+        L.tzt.p3 = tzp[6 * st];
+        L.tzt.p4 = tzp[7 * st];
+        L.tzt.ux = tzp[8 * st];
+        L.tzt.ue = tzp[9 * st];
+      }
     }
   };
 
@@ -237,7 +256,10 @@ __global__ void __launch_bounds__(TX) march2d_fp64(const Problem* __restrict__ p
                         Lc.c12 * ((sQY[y0][x + 1] + sQY[ym][x + 1]) - (sQY[y0][x - 1] + sQY[ym][x - 1])) +
                         Lc.ca * (0.5 * (sQX[s0][x] + sQX[s0][x - 1])) + Lc.cb * (0.5 * (sQY[y0][x] + sQY[ym][x]));
       const double dtau = sD[s0][x];
-      const double un = (sU[s0][x] + dtau * (Lc.up / dt - dq + Lc.S)) / (1.0 + dtau / dt);
+      // forcing of this cell with the iteration's diffusivity; g12 = 4·c12 exactly
+      const double f = TZ ? tz::combine(Lc.tzt, sA[s0][x], Lc.g11, Lc.g22, 4.0 * Lc.c12, Lc.ca, Lc.cb, Lc.S) : 0.0;
+      const double un = TZ ? (sU[s0][x] + dtau * (Lc.up / dt - dq + Lc.S + f)) / (1.0 + dtau / dt)
+                           : (sU[s0][x] + dtau * (Lc.up / dt - dq + Lc.S)) / (1.0 + dtau / dt);
       uout[o] = un;
       qyout[o] = qyn;
       if (check) {
@@ -248,7 +270,7 @@ __global__ void __launch_bounds__(TX) march2d_fp64(const Problem* __restrict__ p
                            Lc.cb * (0.5 * (sPY[y0][x] + sPY[ym][x]));
         double du = un - Lc.up;
         if (isapprox_eps(un, Lc.up)) du = 0.0;
-        const double r = -du / dt - dqp + Lc.S;
+        const double r = TZ ? -du / dt - dqp + Lc.S + f : -du / dt - dqp + Lc.S;
         if (rms) local += r * r;
         else {
           const double ar = fabs(r);
@@ -266,10 +288,16 @@ __global__ void __launch_bounds__(TX) march2d_fp64(const Problem* __restrict__ p
   finish_iteration<TX>(P, C, tile, iter, check, local, local_nan, bad, s_red, &s_flag);
 }
 
-cudaError_t launch_march2d_fp64(int variant, const Problem* probs, const int2* items, int nitems, cudaStream_t s) {
+cudaError_t launch_march2d_fp64(int variant, int tz, const Problem* probs, const int2* items, int nitems,
+                                cudaStream_t s) {
   if (nitems <= 0) return cudaSuccess;
-  if (variant == 0) march2d_fp64<128><<<nitems, 128, 0, s>>>(probs, items);
-  else march2d_fp64<64><<<nitems, 64, 0, s>>>(probs, items);
+  if (tz) {
+    if (variant == 0) march2d_fp64<128, true><<<nitems, 128, 0, s>>>(probs, items);
+    else march2d_fp64<64, true><<<nitems, 64, 0, s>>>(probs, items);
+  } else {
+    if (variant == 0) march2d_fp64<128, false><<<nitems, 128, 0, s>>>(probs, items);
+    else march2d_fp64<64, false><<<nitems, 64, 0, s>>>(probs, items);
+  }
   return cudaGetLastError();
 }
 

@@ -409,14 +409,14 @@ static cudaError_t launch3(const Problem* probs, const int2* items, int nitems, 
 
 cudaError_t launch_sweep_fp64(int ndim, int variant, int exact, int harmonic, const Problem* probs,
                               const int2* items, int nitems, int n_edge, unsigned int* counters,
-                              const SweepStreams& ss) {
+                              const SweepStreams& ss, int tz) {
   if (nitems <= 0) return cudaSuccess;
   cudaStream_t s = ss.main;
   if (ndim == 2) {
     switch (variant) {
       case 0:
       case 1:
-        if (exact) return launch_march2d_fp64(variant, probs, items, nitems, s);
+        if (exact || tz) return launch_march2d_fp64(variant, tz, probs, items, nitems, s);
         return launch_march2d_fast(variant, harmonic, probs, items, n_edge, nitems - n_edge, counters, ss);
       case 4:  // the wavefront variant launches through launch_march2d_wave (tagged items)
         return cudaErrorInvalidValue;

@@ -84,6 +84,9 @@ struct Problem {
   const float* rho32;
   const float* coef32[9];
   double* ub64[2];                  // base temperature, FP64 ping-pong
+  // twilight zone: the α-independent forcing terms of the step (tz::kNumTerms
+  // full-size arrays back to back, nx*ny apart), NULL when the forcing is off
+  const double* tz;
 };
 
 __host__ __device__ inline int64_t fidx(const Problem& P, int a, int b, int c = 0) {

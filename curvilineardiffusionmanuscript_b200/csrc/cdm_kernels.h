@@ -18,7 +18,9 @@ struct TileShape {
 int num_tile_shapes(int ndim);
 TileShape tile_shape(int ndim, int variant);
 
-cudaError_t launch_march2d_fp64(int variant, const Problem* probs, const int2* items, int nitems, cudaStream_t s);
+// tz: the problems carry twilight-zone forcing terms (Problem::tz)
+cudaError_t launch_march2d_fp64(int variant, int tz, const Problem* probs, const int2* items, int nitems,
+                                cudaStream_t s);
 // streams of a sweep launch: boundary strips may run on `side`, concurrently
 // with the interior strips on `main` (fork/join through the two events)
 struct SweepStreams {
@@ -50,9 +52,10 @@ cudaError_t launch_march3d_fast(int harmonic, const Problem* probs, const int2* 
 // one fused FP64 pseudo-iteration over all items (problem, tile)
 // exact = 1: operation-for-operation reference arithmetic (bit-identical to the
 // CPU restatement); exact = 0: reciprocal form (last-bit differences)
+// tz = 1 (2D row-marching exact form only): add the twilight-zone forcing
 cudaError_t launch_sweep_fp64(int ndim, int variant, int exact, int harmonic, const Problem* probs,
                               const int2* items, int nitems, int n_edge, unsigned int* counters,
-                              const SweepStreams& ss);
+                              const SweepStreams& ss, int tz = 0);
 
 // metric cache (mesh_metric_cache.jl:39-250) and the packed divergence
 // coefficients derived from the cell-centre metrics and the cache
@@ -64,6 +67,21 @@ struct MeshPtrs {
 cudaError_t launch_metric_cache(const Problem& P, const MeshPtrs& m, double* cache[3], cudaStream_t s);
 cudaError_t launch_coefficients(const Problem& P, const MeshPtrs& m, double* const cache[3], double* coef[9],
                                 cudaStream_t s);
+
+// twilight-zone forcing terms of every domain cell for time t (cdm_tz.cuh):
+// centroids and forward metrics of the mesh, the step's density and cₚ;
+// writes tz::kNumTerms full-size arrays to out (nx*ny apart)
+struct TzMesh {
+  const double* x;
+  const double* y;
+  const double* xxi;
+  const double* xeta;
+  const double* yxi;
+  const double* yeta;
+  int nnx, nny;
+};
+cudaError_t launch_tz_terms(const Problem& P, const TzMesh& m, const double* rho, double cp, double t, int no_t,
+                            double* out, cudaStream_t s);
 
 // finite-value check of a field on the domain and the first halo layer
 // (validity_checks.jl:1-43); writes bit 0 (non-finite) / bit 1 (negative) to *flag

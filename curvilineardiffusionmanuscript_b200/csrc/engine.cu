@@ -15,6 +15,7 @@
 #include <thread>
 
 #include "engine.h"
+#include "cdm_tz.cuh"
 
 namespace cdm {
 
@@ -104,6 +105,8 @@ Engine::~Engine() {
     dfree(s.partial);
     dfree(s.guess);
     dfree(s.t_hist);
+    dfree(s.tz_mesh);
+    dfree(s.tz_terms);
     dfree(s.ub32);
     dfree(s.ab32);
     dfree(s.R32);
@@ -533,6 +536,58 @@ int Engine::set_guess(int p, const double* u0, int mem) {
   return CDM_OK;
 }
 
+// define_forcing_wavy's mesh inputs beyond the mesh description: centroids,
+// forward metrics and mesh.nnodes (twilight_zone.jl:72-75, :115-118)
+int Engine::set_twilight_zone(int p, const cdm_tz_desc* d) {
+  ProbState& s = ps[p];
+  if (ndim != 2) {
+    set_error("the twilight-zone forcing is two-dimensional (twilight_zone.jl:70)");
+    return CDM_BAD_INPUT;
+  }
+  const double* src[6] = {d->x, d->y, d->x_xi, d->x_eta, d->y_xi, d->y_eta};
+  for (const double* a : src)
+    if (!a) {
+      set_error("cdm_tz_desc: every array must be given");
+      return CDM_BAD_INPUT;
+    }
+  if (d->nnodes[0] < 2 || d->nnodes[1] < 2 || (d->mem != CDM_MEM_HOST && d->mem != CDM_MEM_DEVICE)) {
+    set_error("cdm_tz_desc: nnodes must be >= 2 and mem a cdm_mem value");
+    return CDM_BAD_INPUT;
+  }
+  CDM_CK(cudaSetDevice(device));
+  if (!s.tz_mesh) CDM_CK(dalloc(&s.tz_mesh, (size_t)6 * s.nfull));
+  if (!s.tz_terms) CDM_CK(dalloc(&s.tz_terms, (size_t)tz::kNumTerms * s.nfull));
+  CDM_CK(fence_caller());
+  for (int k = 0; k < 6; ++k) CDM_CK(stage_in(s.tz_mesh + k * s.nfull, src[k], s.nfull, d->mem, stream));
+  CDM_CK(cudaStreamSynchronize(stream));
+  s.tz_nn[0] = d->nnodes[0];
+  s.tz_nn[1] = d->nnodes[1];
+  return CDM_OK;
+}
+
+// A twilight-zone step runs the operation-for-operation row-marching kernel
+// (the only one that adds the forcing): other tuned variants are set aside
+// for the step and restored after it.
+int Engine::begin_tz_step() {
+  tz_active = true;
+  if (variant != 0 && variant != 1) {
+    tz_saved_variant = variant;
+    variant = 0;
+    return build_items();
+  }
+  return CDM_OK;
+}
+
+int Engine::end_tz_step() {
+  tz_active = false;
+  if (tz_saved_variant >= 0) {
+    variant = tz_saved_variant;
+    tz_saved_variant = -1;
+    return build_items();
+  }
+  return CDM_OK;
+}
+
 cudaError_t Engine::fence_caller() {
   if (!own_stream) return cudaSuccess;
   cudaError_t e = cudaEventRecord(ev_caller, cudaStreamLegacy);
@@ -598,8 +653,8 @@ cudaError_t Engine::launch_iters(int K) {
                                d_wave, stream);
   cudaError_t le = cudaSuccess;
   for (int k = 0; k < K && le == cudaSuccess; ++k)
-    le = launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT, mean == CDM_MEAN_HARMONIC, d_probs,
-                           d_items, nitems, n_edge, d_counters, sweep_streams());
+    le = launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT || tz_active, mean == CDM_MEAN_HARMONIC,
+                           d_probs, d_items, nitems, n_edge, d_counters, sweep_streams(), tz_active ? 1 : 0);
   return le;
 }
 
@@ -613,7 +668,7 @@ int Engine::launch_block(int K, bool use_graph) {
   if (ts.march == 3) {
     prof.sweep_launches += 1;
     prof.other_launches += 1;
-  } else if (ts.march == 1 && precision != CDM_PREC_FP64_EXACT) {
+  } else if (ts.march == 1 && precision != CDM_PREC_FP64_EXACT && !tz_active) {
     prof.sweep_launches += (int64_t)K * ((n_edge > 0 ? 1 : 0) + (nitems - n_edge > 0 ? 1 : 0));
   } else {
     prof.sweep_launches += K;
@@ -623,9 +678,10 @@ int Engine::launch_block(int K, bool use_graph) {
     if (pe >= 0) CDM_CK(cudaEventRecord(ev_pool[pe + 1], stream));
     return CDM_OK;
   }
-  if (graph_variant != variant) {
+  if (graph_variant != variant || graph_tz != tz_active) {
     free_graphs();
     graph_variant = variant;
+    graph_tz = tz_active;
   }
   auto it = graphs.find(K);
   if (it == graphs.end()) {
@@ -846,9 +902,34 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
       bad = CDM_BAD_INPUT;
     }
   }
+  if (o.tz && bad == CDM_OK) {
+    // twilight_zone.jl:54-195 (update.jl:23-71, residuals.jl:49-99)
+    std::string why;
+    if (ndim != 2) why = "tz = true: the twilight-zone forcing is two-dimensional (twilight_zone.jl:70)";
+    else if (precision == CDM_PREC_MIXED) why = "tz = true needs an FP64 precision (CDM_PREC_FP64 or _EXACT)";
+    for (int p = 0; p < nprob && why.empty(); ++p)
+      if (!ps[p].tz_mesh) why = "tz = true needs the mesh inputs of cdm_apt_set_twilight_zone first";
+    if (!why.empty()) {
+      for (int p = 0; p < nprob; ++p) stats[p].status = CDM_BAD_INPUT;
+      set_error(why);
+      bad = CDM_BAD_INPUT;
+    }
+  }
   if (bad != CDM_OK) {
     for (int p = 0; p < nprob; ++p) stats[p].time = now_seconds() - t0;
     return bad;
+  }
+  // a twilight-zone step restores the tuned kernel variant however it ends
+  struct TzGuard {
+    Engine* e;
+    bool on;
+    ~TzGuard() {
+      if (on) e->end_tz_step();
+    }
+  } tz_guard{this, o.tz != 0};
+  if (o.tz) {
+    const int rb = begin_tz_step();
+    if (rb != CDM_OK) return rb;
   }
   // T and rho may still be written by the caller's kernels
   CDM_CK(fence_caller());
@@ -956,6 +1037,22 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
     P.ab32 = s.ab32;
     P.R32 = s.R32;
     P.rho32 = s.rho32;
+    P.tz = nullptr;
+    if (o.tz) {
+      // the forcing's α-independent terms at this step's t (twilight_zone.jl:69-183)
+      TzMesh tm;
+      tm.x = s.tz_mesh;
+      tm.y = s.tz_mesh + s.nfull;
+      tm.xxi = s.tz_mesh + 2 * s.nfull;
+      tm.xeta = s.tz_mesh + 3 * s.nfull;
+      tm.yxi = s.tz_mesh + 4 * s.nfull;
+      tm.yeta = s.tz_mesh + 5 * s.nfull;
+      tm.nnx = s.tz_nn[0];
+      tm.nny = s.tz_nn[1];
+      CDM_CK(launch_tz_terms(P, tm, rp, cp[p], o.t, o.no_t, s.tz_terms, stream));
+      prof.other_launches += 1;
+      P.tz = s.tz_terms;
+    }
     if (ndim == 2 && s.nh > 1) {
       CDM_CK(launch_dirichlet_fill(P, s.u[0], stream));
       CDM_CK(launch_dirichlet_fill(P, s.u[1], stream));
@@ -1258,6 +1355,22 @@ int cdm_apt_advance(cdm_apt* h, double* T, const double* rho, double cp, cdm_kap
     }
   }
   return rc;
+}
+
+int cdm_apt_set_twilight_zone(cdm_apt* h, const cdm_tz_desc* d) {
+  if (!h || !d) {
+    cdm::set_error("NULL argument");
+    return CDM_BAD_INPUT;
+  }
+  return h->e.set_twilight_zone(0, d);
+}
+
+int cdm_batch_set_twilight_zone(cdm_batch* b, int p, const cdm_tz_desc* d) {
+  if (!b || !d || p < 0 || p >= (int)b->e.ps.size()) {
+    cdm::set_error("bad arguments to cdm_batch_set_twilight_zone");
+    return CDM_BAD_INPUT;
+  }
+  return b->e.set_twilight_zone(p, d);
 }
 
 int cdm_apt_set_guess(cdm_apt* h, const double* u0, int mem) {

@@ -63,6 +63,11 @@ struct ProbState {
   float* rho32 = nullptr;
   float* coef32[9] = {nullptr};
   double* ub64[2] = {nullptr, nullptr};
+  // twilight zone (cdm_apt_set_twilight_zone): centroids and forward metrics
+  // (6 full-size arrays back to back), the step's forcing terms, mesh.nnodes
+  double* tz_mesh = nullptr;
+  double* tz_terms = nullptr;
+  int tz_nn[2] = {0, 0};
 };
 
 struct Engine {
@@ -133,6 +138,13 @@ struct Engine {
   cudaError_t fence_caller();
   cudaEvent_t ev_caller = nullptr;
   int free_graphs();
+  // twilight zone: the step in progress adds the forcing (2D, exact row-marching kernel)
+  bool tz_active = false;
+  bool graph_tz = false;
+  int tz_saved_variant = -1;  // tuned variant to restore after a twilight-zone step
+  int set_twilight_zone(int p, const cdm_tz_desc* d);
+  int begin_tz_step();
+  int end_tz_step();
   // mixed precision (apt_mixed.cu)
   int mixed_alloc();
   int step_mixed(const cdm_step_opts* o, double t_start, double timeout_s);

@@ -48,6 +48,14 @@ class CurvilinearMesh:
     nodes: List[torch.Tensor]                        # domain node coordinates
     L: float = 0.0
     spacing: Sequence[float] = field(default_factory=lambda: (0.0, 0.0, 0.0))
+    # cell_center_metrics.{x₁,x₂}.{ξ,η} (forward metrics x_ξ, x_η, y_ξ, y_η), read by
+    # the twilight-zone forcing only (twilight_zone.jl:115-118); 2D analytic meshes
+    cell_fwd: Optional[List[torch.Tensor]] = None
+
+    @property
+    def nnodes(self):
+        """mesh.nnodes: domain nodes per axis."""
+        return (self.ni + 1, self.nj + 1) if self.ndim == 2 else (self.ni + 1, self.nj + 1, self.nk + 1)
 
     @property
     def full_shape(self):
@@ -77,7 +85,8 @@ class CurvilinearMesh:
             self.ndim, self.ni, self.nj, self.nk, self.nhalo,
             [mv(t) for t in self.cell_inv], mv(self.cell_J),
             [mv(t) for t in self.edge_J], [[mv(t) for t in row] for row in self.edge_hat],
-            [mv(t) for t in self.centroids], [t for t in self.nodes], self.L, tuple(self.spacing))
+            [mv(t) for t in self.centroids], [t for t in self.nodes], self.L, tuple(self.spacing),
+            None if self.cell_fwd is None else [mv(t) for t in self.cell_fwd])
 
 
 def _phys_dims(ndim, nodes, cell_J_domain):
@@ -135,6 +144,54 @@ def wavy_mesh_2d(ni: int, nj: int, amp: float = 0.05, nhalo: int = 1,
     Tn, Sn = torch.meshgrid(t_n, s_n, indexing="ij")
     xn, yn, *_ = mapping(Sn, Tn)
     m = CurvilinearMesh(2, ni, nj, 1, nhalo, cell_inv, J, edge_J, edge_hat, [x, y], [xn, yn])
+    m.cell_fwd = [xi, xj, yi, yj]
+    h = nhalo
+    m.L, m.spacing = _phys_dims(2, m.nodes, J[h:h + nj, h:h + ni])
+    return m
+
+
+def tz_wavy_mesh_2d(ni: int, nj: Optional[int] = None, nhalo: int = 5, device="cpu") -> CurvilinearMesh:
+    """The wavy grid of the reference's twilight-zone study
+    (test/integrated/2d/wavy_manufactured_solution/run.jl:71-96) on [-6, 6]²:
+    node (i, j) at x = xmin + Δx0((i−1) + Ax sinpi(n_xy (j−1) Δy0/Ly)),
+    y = ymin + Δy0((j−1) + Ay sinpi(n_yx (i−1) Δx0/Lx)), Lx = Ly = 12,
+    n_xy = n_yx = 6, Ax = 0.2/Δx0, Ay = 0.4/Δy0, with the metrics evaluated
+    exactly from the mapping (the reference builds them with CurvilinearGrids'
+    :meg6 scheme).  The forcing of that study (twilight_zone.jl:100-101, :123-124)
+    places cell (i, j) at node coordinate i − 4.5, i.e. it assumes 5 halo
+    layers, hence the default nhalo."""
+    nj = ni if nj is None else nj
+    Lx = Ly = 12.0
+    dx0, dy0 = Lx / ni, Ly / nj
+    kx, ky = math.pi * 6.0 * dy0 / Ly, math.pi * 6.0 * dx0 / Lx
+
+    def mapping(S, T):  # S, T: 0-based node index coordinates along i and j
+        x = -Lx / 2 + dx0 * S + 0.2 * torch.sin(kx * T)
+        y = -Ly / 2 + dy0 * T + 0.4 * torch.sin(ky * S)
+        xi, xj = torch.full_like(S, dx0), 0.2 * kx * torch.cos(kx * T)
+        yi, yj = 0.4 * ky * torch.cos(ky * S), torch.full_like(T, dy0)
+        return x, y, xi, xj, yi, yj
+
+    def at(off_i, off_j):
+        s = torch.arange(ni + 2 * nhalo, dtype=torch.float64, device=device) - nhalo + off_i
+        t = torch.arange(nj + 2 * nhalo, dtype=torch.float64, device=device) - nhalo + off_j
+        T, S = torch.meshgrid(t, s, indexing="ij")
+        return mapping(S, T)
+
+    x, y, xi, xj, yi, yj = at(0.5, 0.5)
+    J = xi * yj - xj * yi
+    cell_inv = [yj / J, -xj / J, None, -yi / J, xi / J, None, None, None, None]
+    edge_J, edge_hat = [None] * 3, [[None] * 9 for _ in range(3)]
+    for f, (oi, oj) in enumerate(((1.0, 0.5), (0.5, 1.0))):
+        _, _, fxi, fxj, fyi, fyj = at(oi, oj)
+        edge_J[f] = fxi * fyj - fxj * fyi
+        edge_hat[f][0], edge_hat[f][1] = fyj, -fxj
+        edge_hat[f][3], edge_hat[f][4] = -fyi, fxi
+    Tn, Sn = torch.meshgrid(torch.arange(nj + 1, dtype=torch.float64, device=device),
+                            torch.arange(ni + 1, dtype=torch.float64, device=device), indexing="ij")
+    xn, yn, *_ = mapping(Sn, Tn)
+    m = CurvilinearMesh(2, ni, nj, 1, nhalo, cell_inv, J, edge_J, edge_hat, [x, y], [xn, yn])
+    m.cell_fwd = [xi, xj, yi, yj]
     h = nhalo
     m.L, m.spacing = _phys_dims(2, m.nodes, J[h:h + nj, h:h + ni])
     return m

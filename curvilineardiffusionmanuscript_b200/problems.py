@@ -14,6 +14,10 @@ initial temperature and a conductivity law, generated here from a seed.
                        adds its forcing to the source, update.jl:181-184).
 * ``gaussian_3d``   — 3D pulse (width 0.1) on the perturbed unit cube, κ = T^2.5.
 * ``multi_gaussian_2d`` — 1..8 seeded Gaussians, κ = T³ (learned-guess data).
+* ``tz_wavy_2d``    — the reference's twilight-zone study on its [-6, 6]² wavy
+                       grid (test/integrated/2d/wavy_manufactured_solution/run.jl):
+                       exact solution exp(−(x² + y²))·e^{−4t}, κ = T^{5/2},
+                       Neumann sides, forcing added by the solver (tz = true).
 """
 from __future__ import annotations
 
@@ -24,7 +28,7 @@ from typing import List, Optional
 import numpy as np
 import torch
 
-from .mesh import CurvilinearMesh, wavy_mesh_2d, wavy_mesh_3d
+from .mesh import CurvilinearMesh, tz_wavy_mesh_2d, wavy_mesh_2d, wavy_mesh_3d
 from .solver import DirichletBC, NeumannBC, PowerLawConductivity
 
 BATCH_SEED = 20261203
@@ -156,3 +160,23 @@ def multi_gaussian_2d(n: int = 1024, seed: int = 0, amp: float = 0.05, dt: float
     bcs = [NeumannBC() for _ in range(4)]
     return Problem("multi_gaussian_2d", m, bcs, T0.contiguous(), rho, 1.0, PowerLawConductivity(1.0, 3.0), dt,
                    nsteps, meta={"n": n, "seed": seed, "M": M})
+
+
+# --------------------------------------------------------- twilight zone (a13)
+def tz_exact(x, y, t: float = 0.0, no_t: bool = False):
+    """u_analytic of the reference's study (wavy_manufactured_solution/run.jl:40-53)."""
+    u = torch.exp(-(x * x + y * y))
+    return u if no_t else u * math.exp(-4.0 * t)
+
+
+def tz_wavy_2d(n: int = 64, nhalo: int = 5, dt: float = 1e-7, nsteps: int = 10, device="cpu") -> Problem:
+    """The twilight-zone problem of wavy_manufactured_solution/run.jl:122-179: T0 =
+    exp(−(x² + y²)) at the centroids, ρ = cₚ = 1, κ = T^{5/2}, Neumann sides and the
+    source q = 1e4·exp(−((x − 1)² + (y − 1)²)) (which the forcing cancels, :191)."""
+    m = tz_wavy_mesh_2d(n, n, nhalo=nhalo, device=device)
+    x, y = m.centroids
+    T0 = tz_exact(x, y, 0.0, no_t=True).contiguous()
+    S = (1e4 * torch.exp(-((x - 1.0) ** 2 + (y - 1.0) ** 2))).contiguous()
+    bcs = [NeumannBC() for _ in range(4)]
+    return Problem("tz_wavy_2d", m, bcs, T0, torch.ones_like(T0), 1.0, PowerLawConductivity(1.0, 2.5), dt, nsteps,
+                   source=S, meta={"n": n, "nhalo": nhalo})

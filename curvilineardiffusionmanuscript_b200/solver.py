@@ -143,6 +143,19 @@ def mesh_desc(mesh: CurvilinearMesh):
     return d, keep
 
 
+def tz_desc(mesh: CurvilinearMesh, nnodes=None):
+    """cdm_tz_desc of a 2D mesh with forward metrics; returns (desc, keepalive)."""
+    if mesh.ndim != 2 or mesh.cell_fwd is None:
+        raise ValueError("the twilight-zone forcing needs a 2D mesh with forward metrics (mesh.cell_fwd)")
+    d = L.TzDesc()
+    keep = [t.contiguous() for t in (*mesh.centroids[:2], *mesh.cell_fwd)]
+    d.mem = _mem(keep[0])
+    nn = nnodes or mesh.nnodes
+    d.nnodes[0], d.nnodes[1] = int(nn[0]), int(nn[1])
+    d.x, d.y, d.x_xi, d.x_eta, d.y_xi, d.y_eta = [_ptr(t) for t in keep]
+    return d, keep
+
+
 def _bcs_c(bcs, ndim) -> "C.Array":
     lst = bc_list(bcs)
     if len(lst) != 2 * ndim:
@@ -224,6 +237,15 @@ class PseudoTransientSolver:
     def set_source(self, S):
         S = S.contiguous() if isinstance(S, torch.Tensor) else np.ascontiguousarray(S, dtype=np.float64)
         rc = self._lib.cdm_apt_set_source(self._h, _ptr(S), _mem(S))
+        if rc != L.CDM_OK:
+            raise APTError(rc, L.last_error())
+
+    def set_twilight_zone(self, mesh: Optional[CurvilinearMesh] = None, nnodes=None):
+        """Mesh inputs of the tz=True path (define_forcing_wavy, twilight_zone.jl:54-195):
+        centroids and forward metrics of `mesh` (default: the solver's), mesh.nnodes."""
+        d, keep = tz_desc(mesh or self.mesh, nnodes)
+        rc = self._lib.cdm_apt_set_twilight_zone(self._h, C.byref(d))
+        del keep
         if rc != L.CDM_OK:
             raise APTError(rc, L.last_error())
 
@@ -360,6 +382,14 @@ class PseudoTransientBatch:
 
     def set_source(self, p: int, S):
         rc = self._lib.cdm_batch_set_source(self._h, p, _ptr(S), _mem(S))
+        if rc != L.CDM_OK:
+            raise APTError(rc, L.last_error())
+
+    def set_twilight_zone(self, p: int, mesh: Optional[CurvilinearMesh] = None, nnodes=None):
+        """PseudoTransientSolver.set_twilight_zone for problem p."""
+        d, keep = tz_desc(mesh or self.meshes[p], nnodes)
+        rc = self._lib.cdm_batch_set_twilight_zone(self._h, int(p), C.byref(d))
+        del keep
         if rc != L.CDM_OK:
             raise APTError(rc, L.last_error())
 

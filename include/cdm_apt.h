@@ -140,7 +140,11 @@ typedef struct cdm_apt_config {
  * (timestep_control.jl:33-42), same names and defaults, plus extensions. */
 typedef struct cdm_step_opts {
   double t;
-  int tz, tz_dim, no_t;          /* accepted; manufactured forcing is passed as the source */
+  int tz, tz_dim, no_t;          /* tz = 1: add the twilight-zone forcing of
+                                    define_forcing_wavy (twilight_zone.jl:54-195) at time t,
+                                    time-independent when no_t (tz_dim is unused there, as in
+                                    the reference); needs cdm_apt_set_twilight_zone, 2D and an
+                                    FP64 precision (CDM_BAD_INPUT otherwise) */
   int max_iter;                  /* 1500 */
   double rtol;                   /* 1e-5 */
   double atol;                   /* sqrt(eps(Float64)) */
@@ -238,6 +242,28 @@ int cdm_apt_advance(cdm_apt* h, double* T, const double* rho, double cp, cdm_kap
                     double t_end, int max_cycles, double* dt, double dt_max, const cdm_step_opts* opts,
                     cdm_stats* last, int* nsteps);
 
+/* ---- twilight zone: the mesh fields define_forcing_wavy reads beyond
+ * cdm_mesh_desc (twilight_zone.jl:72-75, :115-118).  Full-size arrays in `mem`
+ * space, copied by the call. */
+typedef struct cdm_tz_desc {
+  int mem;                   /* enum cdm_mem                                      */
+  int nnodes[2];             /* mesh.nnodes: domain nodes per axis (ni+1, nj+1)   */
+  const double* x;           /* centroid_coordinates.x                            */
+  const double* y;           /* centroid_coordinates.y                            */
+  const double* x_xi;        /* cell_center_metrics.x₁.ξ  (∂x/∂ξ)                 */
+  const double* x_eta;       /* cell_center_metrics.x₁.η                          */
+  const double* y_xi;        /* cell_center_metrics.x₂.ξ                          */
+  const double* y_eta;       /* cell_center_metrics.x₂.η                          */
+} cdm_tz_desc;
+
+/* Inputs of the tz = true path of step! (compute_update!, update.jl:73-119, and
+ * update_residual!, residuals.jl:105-160, which call _update_kernel_tz! and
+ * _update_resid_kernel_tz!).  Each tz step evaluates the forcing with the
+ * iteration's diffusivity, in the reference's operation order; it runs the
+ * operation-for-operation FP64 kernel whatever the precision (the reciprocal
+ * form has no forcing term), 2D only. */
+int cdm_apt_set_twilight_zone(cdm_apt* h, const cdm_tz_desc* tz);
+
 /* initial guess for the next step (CDM_GUESS_USER); full-size array */
 int cdm_apt_set_guess(cdm_apt* h, const double* u0, int mem);
 
@@ -266,6 +292,8 @@ int cdm_batch_create(int nprob, const cdm_mesh_desc* meshes, const cdm_bc* bcs /
                      const cdm_apt_config* cfg, cdm_batch** out);
 int cdm_batch_destroy(cdm_batch* b);
 int cdm_batch_set_source(cdm_batch* b, int p, const double* S, int mem);
+/* cdm_apt_set_twilight_zone for problem p of a batch */
+int cdm_batch_set_twilight_zone(cdm_batch* b, int p, const cdm_tz_desc* tz);
 int cdm_batch_step(cdm_batch* b, double* const* T, const double* const* rho, const double* cp,
                    const cdm_kappa* kappa, const double* dt, const cdm_step_opts* opts,
                    cdm_stats* stats /* nprob */, double* next_dt /* nprob */);

@@ -21,6 +21,17 @@
 //
 // Threads: loops over the slowest axis are OpenMP-parallel; results do not
 // depend on the thread count except the optional RMS norm's summation order.
+//
+// Twilight zone: define_forcing_wavy (twilight_zone.jl:54-195) is restated
+// literally and evaluated per cell inside the update and the residual with the
+// iteration's diffusivity, as _update_kernel_tz! / _update_resid_kernel_tz!
+// do.  Its exp and sinpi are evaluated by a Cody–Waite/Taylor exp and an
+// exactly reduced Taylor sinpi (below) rather than libm, the same published
+// methods the CUDA library evaluates, so that the twilight-zone path can be
+// compared bit for bit; both stay within 2 ulp of the correctly rounded
+// values (checked against high-precision values by the test-suite).  Julia's
+// own exp/sinpi may differ from them in the last bit, and exy^(3/2) is taken
+// as exy*sqrt(exy).
 
 #include <algorithm>
 #include <cmath>
@@ -62,6 +73,11 @@ struct Solver {
   double bc_val[6];
   int mean;  // 0 harmonic, 1 arithmetic
   int last_err_check;
+  // twilight zone: mesh.centroid_coordinates.{x,y} and the forward metrics
+  // cell_center_metrics.{x₁,x₂}.{ξ,η} (twilight_zone.jl:74-75, :115-118), mesh.nnodes
+  std::vector<double> tz_x, tz_y, tz_xxi, tz_xeta, tz_yxi, tz_yeta;
+  int tz_nn[2] = {0, 0};
+  bool tz_set = false;
 };
 
 struct StepOpts {
@@ -73,6 +89,7 @@ struct StepOpts {
   double ndt_tol, maximum_u_change, timestep_growth_factor;
   int norm;         // 0 max (GPU reference), 1 rms (CPU reference)
   int check_every;  // 0 = reference schedule
+  int tz, no_t;     // twilight-zone forcing (step! keywords tz, no_t)
 };
 
 struct StepStats {
@@ -333,8 +350,122 @@ inline double divergence(const Solver& s, const std::vector<double>* q, int64_t 
   return flux_divergence_3d(s, q[0].data(), q[1].data(), q[2].data(), i, j, k);
 }
 
-// update.jl:2-21 over the domain (in place: each cell reads only its own u)
-void compute_update(Solver& s, double dt) {
+// ----------------------------------------------------------------------------
+// Elementary functions of the twilight-zone forcing (see the header note).
+// exp: Cody–Waite reduction x = k·ln2 + r with ln2 = LN2_HI + LN2_LO (nearest
+// double and remainder), Taylor polynomial of e^r to degree 13, Horner with
+// fused multiply-adds, times 2^k.
+double exp_cw(double x) {
+  if (x != x) return x;
+  if (x > 709.782712893384) return std::numeric_limits<double>::infinity();
+  if (x < -745.1332191019412) return 0.0;
+  const double k = std::nearbyint(x * 0x1.71547652b82fep+0);
+  const double r = std::fma(-k, 0x1.abc9e3b39803fp-56, std::fma(-k, 0x1.62e42fefa39efp-1, x));
+  static const double inv_fact[14] = {
+      0x1.0000000000000p+0,  0x1.0000000000000p+0,  0x1.0000000000000p-1,  0x1.5555555555555p-3,
+      0x1.5555555555555p-5,  0x1.1111111111111p-7,  0x1.6c16c16c16c17p-10, 0x1.a01a01a01a01ap-13,
+      0x1.a01a01a01a01ap-16, 0x1.71de3a556c734p-19, 0x1.27e4fb7789f5cp-22, 0x1.ae64567f544e4p-26,
+      0x1.1eed8eff8d898p-29, 0x1.6124613a86d09p-33};
+  double p = inv_fact[13];
+  for (int n = 12; n >= 0; --n) p = std::fma(p, r, inv_fact[n]);
+  return std::ldexp(p, (int)k);
+}
+
+// sinpi: x reduced exactly modulo 2 and folded to a in [0, 1/2]; sin(πa) for
+// a <= 1/4, else cos(π(1/2 - a)), each a Taylor polynomial in the square of the
+// argument with coefficients (−1)^k π^(2k+1)/(2k+1)! and (−1)^k π^(2k)/(2k)!.
+double sinpi(double x) {
+  if (!std::isfinite(x)) return x - x;
+  const double y = x - 2.0 * std::nearbyint(0.5 * x);
+  const double sg = y < 0.0 ? -1.0 : 1.0;
+  double a = std::fabs(y);
+  if (a > 0.5) a = 1.0 - a;
+  double v;
+  if (a <= 0.25) {
+    static const double c[9] = {0x1.921fb54442d18p+1,  -0x1.4abbce625be53p+2, 0x1.466bc6775aae2p+1,
+                                -0x1.32d2cce62bd86p-1, 0x1.50783487ee782p-4,  -0x1.e3074fde8871fp-8,
+                                0x1.e8f434d018d63p-12, -0x1.6fadb9f155744p-16, 0x1.aaec32af93359p-21};
+    const double z = a * a;
+    double p = c[8];
+    for (int k = 7; k >= 0; --k) p = std::fma(p, z, c[k]);
+    v = a * p;
+  } else {
+    static const double d[9] = {0x1.0000000000000p+0,  -0x1.3bd3cc9be45dep+2, 0x1.03c1f081b5ac4p+2,
+                                -0x1.55d3c7e3cbffap+0, 0x1.e1f506891babbp-3,  -0x1.a6d1f2a204a8cp-6,
+                                0x1.f9d38a3763cc3p-10, -0x1.b6e24f44b128fp-14, 0x1.20c62c2f2d7f5p-18};
+    const double b = 0.5 - a;
+    const double z = b * b;
+    double p = d[8];
+    for (int k = 7; k >= 0; --k) p = std::fma(p, z, d[k]);
+    v = p;
+  }
+  return sg * v;
+}
+
+// twilight_zone.jl:54-195, the wavy-mesh manufactured solution with the
+// nonlinear diffusivity branch (non_lin_α = true, :86).  (i, j) is the 0-based
+// full-array index of a domain cell; the reference's 1-based index is i + 1.
+double define_forcing_wavy(const Solver& s, const double* rho, double cp, double t, int no_t, int64_t i,
+                           int64_t j) {
+  const Mesh& m = s.m;
+  const int64_t c = m.id(i, j);
+  const int nx = s.tz_nn[0], ny = s.tz_nn[1];  // :72
+  const double x = s.tz_x[c], y = s.tz_y[c];  // :74-75
+  const double sv = s.S[c];                    // :77
+  const double xi_x = m.inv[0][c], xi_y = m.inv[1][c], eta_x = m.inv[3][c], eta_y = m.inv[4][c];  // :80-83
+  const double Lx = 12, Ly = 12;  // :89-98
+  const double n_xy = 6, n_yx = 6;
+  const double dx0 = Lx / (double)(nx - 1);
+  const double dy0 = Ly / (double)(ny - 1);
+  const double Ax = 0.2 / dx0;
+  const double Ay = 0.4 / dy0;
+  const double indi = (double)((i + 1) - 5) + 0.5;  // :100-101
+  const double indj = (double)((j + 1) - 5) + 0.5;
+  const double fwhm = 1.0, x0 = 0, y0 = 0;  // :103-105
+  const double damp = 4;                    // :107
+  const double pi = 3.141592653589793;
+  const double xxi = s.tz_xxi[c], xeta = s.tz_xeta[c], yxi = s.tz_yxi[c], yeta = s.tz_yeta[c];  // :115-118
+  const double xxixi = 0, xxieta = 0;  // :121-122
+  const double K1 = pi * n_xy * dy0 / Ly;
+  const double xetaeta = -dx0 * Ax * (K1 * K1) * sinpi(n_xy * (indj - 1) * dy0 / Ly);  // :123
+  const double K2 = pi * n_yx * dx0 / Lx;
+  const double yxixi = -dy0 * Ay * (K2 * K2) * sinpi(n_yx * (indi - 1) * dx0 / Lx);  // :124
+  const double yxieta = 0, yetaeta = 0;  // :125-126
+  double exy, ut;
+  if (no_t) {  // :128-131
+    exy = exp_cw(-(((x - x0) * (x - x0)) / fwhm + ((y - y0) * (y - y0)) / fwhm));
+    ut = 0;
+  } else {  // :150-153
+    exy = exp_cw(-(((x - x0) * (x - x0)) / fwhm + ((y - y0) * (y - y0)) / fwhm)) * exp_cw(-damp * t);
+    ut = -damp * exy;
+  }
+  // :132-149 (the same expressions in both branches)
+  const double uxi = (-2 / fwhm) * ((x - x0) * xxi + (y - y0) * yxi) * exy;
+  const double sxi = 2 * (x - x0) / fwhm * xxi + 2 * (y - y0) / fwhm * yxi;
+  const double uxixi =
+      (sxi * sxi - (2 / fwhm) * (xxi * xxi + yxi * yxi + (x - x0) * xxixi + (y - y0) * yxixi)) * exy;
+  const double ueta = (-2 / fwhm) * ((x - x0) * xeta + (y - y0) * yeta) * exy;
+  const double seta = 2 * (x - x0) / fwhm * xeta + 2 * (y - y0) / fwhm * yeta;
+  const double uetaeta =
+      (seta * seta - (2 / fwhm) * (xeta * xeta + yeta * yeta + (x - x0) * xetaeta + (y - y0) * yetaeta)) * exy;
+  const double uxieta =
+      (sxi * seta - (2 / fwhm) * (xxi * xeta + yxi * yeta + (x - x0) * xxieta + (y - y0) * yxieta)) * exy;
+  // :181-189, non_lin_α = true
+  const double a = s.alpha[c];
+  const double e15 = exy * std::sqrt(exy);  // exy^(3/2)
+  const double axi = ((5.0 / 2) * e15 * uxi) / (rho[c] * cp);
+  const double aeta = ((5.0 / 2) * e15 * ueta) / (rho[c] * cp);
+  const double orth_xi = (xi_x * xi_x + xi_y * xi_y) * (axi * uxi + a * uxixi);
+  const double orth_eta = (eta_x * eta_x + eta_y * eta_y) * (aeta * ueta + a * uetaeta);
+  const double cross = (xi_x * eta_x + xi_y * eta_y) * (2 * a * uxieta + aeta * uxi + axi * ueta);
+  const double non_orth_xi = a * s.cache[0][c] * uxi;
+  const double non_orth_eta = a * s.cache[1][c] * ueta;
+  return ut - orth_xi - orth_eta - cross - non_orth_xi - non_orth_eta - sv;  // :191
+}
+
+// update.jl:2-21 over the domain (in place: each cell reads only its own u);
+// with the twilight zone, update.jl:23-71
+void compute_update(Solver& s, double dt, const double* rho, double cp, const StepOpts& o) {
   const Mesh& m = s.m;
   const int64_t nh = m.nh;
   const int64_t k0 = (m.ndim == 3) ? nh : 0, k1 = (m.ndim == 3) ? nh + m.nk : 1;
@@ -344,8 +475,14 @@ void compute_update(Solver& s, double dt) {
       for (int64_t i = nh; i < nh + m.ni; ++i) {
         const int64_t c = m.id(i, j, k);
         const double dq = divergence(s, s.q, i, j, k);
-        s.u[c] = ((s.u[c] + s.dtau_rho[c] * (s.u_prev[c] / dt - dq + s.S[c])) /
-                  (1.0 + s.dtau_rho[c] / dt));
+        if (o.tz) {
+          const double f = define_forcing_wavy(s, rho, cp, o.t, o.no_t, i, j);
+          s.u[c] = ((s.u[c] + s.dtau_rho[c] * (s.u_prev[c] / dt - dq + s.S[c] + f)) /
+                    (1.0 + s.dtau_rho[c] / dt));
+        } else {
+          s.u[c] = ((s.u[c] + s.dtau_rho[c] * (s.u_prev[c] / dt - dq + s.S[c])) /
+                    (1.0 + s.dtau_rho[c] / dt));
+        }
       }
 }
 
@@ -356,8 +493,9 @@ inline bool isapprox(double x, double y, double rtol) {
   return std::fabs(x - y) <= rtol * std::max(std::fabs(x), std::fabs(y));
 }
 
-// residuals.jl:24-47 over the domain (res halo stays 0)
-void update_residual(Solver& s, double dt) {
+// residuals.jl:24-47 over the domain (res halo stays 0); with the twilight
+// zone, residuals.jl:49-99
+void update_residual(Solver& s, double dt, const double* rho, double cp, const StepOpts& o) {
   const Mesh& m = s.m;
   const int64_t nh = m.nh;
   const double eps = std::numeric_limits<double>::epsilon();
@@ -371,7 +509,8 @@ void update_residual(Solver& s, double dt) {
         const double un = s.u[c], unm1 = s.u_prev[c];
         double du = un - unm1;
         if (isapprox(un, unm1, eps)) du = 0.0;  // du * !isapprox (strong zero)
-        s.res[c] = -du / dt - dq + s.S[c];
+        if (o.tz) s.res[c] = -du / dt - dq + s.S[c] + define_forcing_wavy(s, rho, cp, o.t, o.no_t, i, j);
+        else s.res[c] = -du / dt - dq + s.S[c];
       }
 }
 
@@ -486,6 +625,10 @@ int step(Solver& s, double* T, const double* rho, double cp, double k0, double n
     st->status = ST_BAD_INPUT;
     return ST_BAD_INPUT;
   }
+  if (o.tz && (m.ndim != 2 || !s.tz_set)) {  // the forcing is 2D (twilight_zone.jl:70)
+    st->status = ST_BAD_INPUT;
+    return ST_BAD_INPUT;
+  }
   std::memcpy(s.u.data(), T, sizeof(double) * N);  // :229-230
   std::memcpy(s.u_prev.data(), T, sizeof(double) * N);
   update_metric_cache(s);  // :232
@@ -506,12 +649,12 @@ int step(Solver& s, double* T, const double* rho, double cp, double k0, double n
     }
     iter += 1;
     compute_flux(s);
-    compute_update(s, dt);
+    compute_update(s, dt, rho, cp, o);
     bool check;
     if (o.check_every > 0) check = (iter % o.check_every == 0) || iter == 1;
     else check = (iter >= min_err_check && iter % err_interval == 0) || iter == 1;
     if (check) {
-      update_residual(s, dt);
+      update_residual(s, dt, rho, cp, o);
       st->n_checks++;
       const double L2 = residual_norm(s, o.norm);
       if (iter == 1) init_L2 = L2;
@@ -634,7 +777,7 @@ void oracle_get_cache(void* h, double* out) {
 
 // opts: doubles {t, rtol, atol, CFL, ndt_tol, maximum_u_change, timestep_growth_factor}
 //       ints    {max_iter, apply_cutoff, calculate_next_dt, subcycle_conductivity,
-//                enforce_positivity, norm, check_every}
+//                enforce_positivity, norm, check_every, tz, no_t}
 // out:  doubles {rel_err, abs_err, next_dt, energy_before, energy_after, source_work}
 //       ints    {niter, status, n_checks}
 int oracle_step(void* h, double* T, const double* rho, double cp, double k0, double n, double dt,
@@ -655,6 +798,8 @@ int oracle_step(void* h, double* T, const double* rho, double cp, double k0, dou
   o.enforce_positivity = oi[4];
   o.norm = oi[5];
   o.check_every = oi[6];
+  o.tz = oi[7];
+  o.no_t = oi[8];
   StepStats st{};
   st.next_dt = dt;
   int rc = step(*s, T, rho, cp, k0, n, dt, o, &st);
@@ -669,6 +814,26 @@ int oracle_step(void* h, double* T, const double* rho, double cp, double k0, dou
   outi[2] = st.n_checks;
   return rc;
 }
+
+// twilight-zone inputs: centroids, forward metrics (full-size arrays) and mesh.nnodes
+void oracle_set_tz(void* h, const double* x, const double* y, const double* xxi, const double* xeta,
+                   const double* yxi, const double* yeta, int nnx, int nny) {
+  Solver* s = static_cast<Solver*>(h);
+  const int64_t n = s->m.n;
+  s->tz_x.assign(x, x + n);
+  s->tz_y.assign(y, y + n);
+  s->tz_xxi.assign(xxi, xxi + n);
+  s->tz_xeta.assign(xeta, xeta + n);
+  s->tz_yxi.assign(yxi, yxi + n);
+  s->tz_yeta.assign(yeta, yeta + n);
+  s->tz_nn[0] = nnx;
+  s->tz_nn[1] = nny;
+  s->tz_set = true;
+}
+
+// the elementary functions of the forcing, for the test-suite's accuracy checks
+double oracle_exp_cw(double x) { return exp_cw(x); }
+double oracle_sinpi(double x) { return sinpi(x); }
 
 // standalone applybcs! on a full-size array (BC known-answer tests)
 void oracle_applybcs(int ndim, int ni, int nj, int nk, int nhalo, const int* bc_kind,

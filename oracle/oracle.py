@@ -39,6 +39,11 @@ def load():
         lib.oracle_step.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.oracle_applybcs.argtypes = [C.c_int] * 5 + [C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.oracle_set_tz.argtypes = [C.c_void_p] + [C.c_void_p] * 6 + [C.c_int, C.c_int]
+        lib.oracle_exp_cw.restype = C.c_double
+        lib.oracle_exp_cw.argtypes = [C.c_double]
+        lib.oracle_sinpi.restype = C.c_double
+        lib.oracle_sinpi.argtypes = [C.c_double]
         lib.oracle_num_threads.restype = C.c_int
         lib.oracle_set_num_threads.argtypes = [C.c_int]
         _lib = lib
@@ -92,6 +97,11 @@ class OracleSolver:
         S = _np(S)
         self._lib.oracle_set_source(self._h, S.ctypes.data)
 
+    def set_twilight_zone(self, x, y, x_xi, x_eta, y_xi, y_eta, nnodes):
+        """Inputs of define_forcing_wavy: centroids, forward metrics, mesh.nnodes."""
+        arrs = [_np(a) for a in (x, y, x_xi, x_eta, y_xi, y_eta)]
+        self._lib.oracle_set_tz(self._h, *[a.ctypes.data for a in arrs], int(nnodes[0]), int(nnodes[1]))
+
     def get_state(self):
         q = np.zeros((self.mesh.ndim,) + tuple(self.mesh.full_shape))
         last = C.c_int(0)
@@ -111,13 +121,14 @@ class OracleSolver:
              rtol=1e-5, atol=np.sqrt(np.finfo(np.float64).eps), CFL=1 / np.sqrt(3.0), tol=1e-3,
              maximum_u_change=0.05, timestep_growth_factor=1.1, max_iter=1500, apply_cutoff=False,
              calculate_next_dt=True, subcycle_conductivity=True, enforce_positivity=False, norm="max",
-             check_every=0, **_):
+             check_every=0, tz=False, no_t=True, **_):
         """In-place step on T (float64 numpy array); returns (stats, next_dt)."""
         assert T.dtype == np.float64 and T.flags["C_CONTIGUOUS"]
         rho = np.ascontiguousarray(rho, dtype=np.float64)
         od = np.array([t, rtol, atol, CFL, tol, maximum_u_change, timestep_growth_factor], dtype=np.float64)
         oi = np.array([max_iter, int(apply_cutoff), int(calculate_next_dt), int(subcycle_conductivity),
-                       int(enforce_positivity), 0 if norm == "max" else 1, check_every], dtype=np.int32)
+                       int(enforce_positivity), 0 if norm == "max" else 1, check_every, int(tz), int(no_t)],
+                      dtype=np.int32)
         outd = np.zeros(6)
         outi = np.zeros(3, dtype=np.int32)
         rc = self._lib.oracle_step(self._h, T.ctypes.data, rho.ctypes.data, float(cp), float(k0), float(n),
@@ -135,6 +146,16 @@ def applybcs(ndim, ni, nj, nk, nhalo, bcs, u: np.ndarray):
     kinds = np.array([b.kind for b in bl], dtype=np.int32)
     vals = np.array([float(getattr(b, "value", 0.0)) for b in bl], dtype=np.float64)
     lib.oracle_applybcs(ndim, ni, nj, nk, nhalo, kinds.ctypes.data, vals.ctypes.data, u.ctypes.data)
+
+
+def exp_cw(x: float) -> float:
+    """The oracle's exp of the twilight-zone forcing (Cody–Waite + Taylor)."""
+    return load().oracle_exp_cw(float(x))
+
+
+def sinpi(x: float) -> float:
+    """The oracle's sinpi of the twilight-zone forcing."""
+    return load().oracle_sinpi(float(x))
 
 
 def set_threads(n: int):

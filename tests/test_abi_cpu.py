@@ -50,8 +50,9 @@ def test_struct_layout_matches_header():
 #include <stdio.h>
 #include "cdm_apt.h"
 #include "cdm_net.h"
-int main(void){printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(cdm_mesh_desc), sizeof(cdm_step_opts),
- sizeof(cdm_stats), sizeof(cdm_apt_config), sizeof(cdm_bc), sizeof(cdm_kappa), sizeof(cdm_net_batch));return 0;}
+int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(cdm_mesh_desc), sizeof(cdm_step_opts),
+ sizeof(cdm_stats), sizeof(cdm_apt_config), sizeof(cdm_bc), sizeof(cdm_kappa), sizeof(cdm_net_batch),
+ sizeof(cdm_tz_desc));return 0;}
 '''
     with tempfile.TemporaryDirectory() as d:
         p = os.path.join(d, "s.c")
@@ -61,7 +62,8 @@ int main(void){printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(cdm_mesh_desc), si
         sizes = [int(x) for x in subprocess.run([exe], capture_output=True, text=True).stdout.split()]
     from curvilineardiffusionmanuscript_b200 import _lib
     assert sizes == [C.sizeof(_lib.MeshDesc), C.sizeof(_lib.StepOpts), C.sizeof(_lib.Stats),
-                     C.sizeof(_lib.Config), C.sizeof(_lib.BC), C.sizeof(_lib.Kappa), C.sizeof(_lib.NetBatch)]
+                     C.sizeof(_lib.Config), C.sizeof(_lib.BC), C.sizeof(_lib.Kappa), C.sizeof(_lib.NetBatch),
+                     C.sizeof(_lib.TzDesc)]
 
 
 def test_create_without_device_reports_error():
