@@ -9,8 +9,16 @@ step (dt = 1e-5) of the whole batch.  Inputs are synthetic (seeded), there is
 no dataset.
 
 Metric: Gcell-iter/s = Σ_p (domain cells_p × pseudo-iterations_p) / time,
-aggregated over all ranks (each rank solves its own seeded batch: weak
-scaling, no collective in the data path).
+aggregated over all ranks.  With N GPUs the job is N seeded batches of 256
+problems (seeds 20261203 .. +N-1, weak scaling) split over the ranks by the
+library's sharded batch (longest-processing-time-first assignment by cells);
+no field data crosses ranks, only each step's per-problem statistics.
+
+CPU arms: `--impl reference` times the reference's CPU algorithm (the oracle
+restatement, OpenMP on every host core) on a size-stratified quarter of the
+256-problem batch (every 4th problem in order of size, 64 problems), each bench
+step one time step of every sampled problem after the warm-up steps; the
+`cpu_baseline` of our line is one post-warm-up time step of the same sample.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload batch|gaussian128|gaussian2048|mms4096|mms1024|multigauss1024|
@@ -166,148 +174,192 @@ def measured_peak():
 
 
 # ------------------------------------------------------------------- workloads
-def make_workload(name, nprob, rank, device):
-    from curvilineardiffusionmanuscript_b200 import problems
+SINGLE = {
+    "gaussian128": (lambda P, d: P.gaussian_2d(128, device=d), 130 * 130,
+                    {"workload": "gaussian2d_128_fp64", "kappa": "T^3"}),
+    "gaussian2048": (lambda P, d: P.gaussian_2d(2048, device=d), 2050 * 2050,
+                     {"workload": "gaussian2d_2048_fp64", "kappa": "T^3"}),
+    "gauss3d128": (lambda P, d: P.gaussian_3d(128, device=d), 130 ** 3,
+                   {"workload": "gaussian3d_128_fp64", "kappa": "T^2.5"}),
+    "gauss3d256": (lambda P, d: P.gaussian_3d(256, device=d), 258 ** 3,
+                   {"workload": "gaussian3d_256_fp64", "kappa": "T^2.5"}),
+    "mms4096": (lambda P, d: P.mms_2d(4096, device=d), 4098 * 4098, {"workload": "mms2d_4096", "kappa": "T^2.5"}),
+    "mms1024": (lambda P, d: P.mms_2d(1024, device=d), 1026 * 1026, {"workload": "mms2d_1024", "kappa": "T^2.5"}),
+    "multigauss1024": (lambda P, d: P.multi_gaussian_2d(1024, seed=12345, device=d), 1026 * 1026,
+                       {"workload": "multigauss2d_1024", "kappa": "T^3"}),
+}
+
+
+def workload(name, nprob, ws):
+    """(costs, build, cfg) of the whole job on ws ranks: one cost per problem
+    (cells), build(indices, device) -> those problems, and the config record,
+    which is the same for every arm of the benchmark."""
+    from curvilineardiffusionmanuscript_b200 import problems as P
     if name == "batch":
-        probs = problems.batch_2d(nprob=nprob, seed=problems.BATCH_SEED + rank, device=device)
-        cfg = {"workload": "batch2d_256_fp64", "nprob": nprob, "sides": "U{64..512}", "seed": problems.BATCH_SEED,
-               "dt": 1e-5, "tol": "rel <= 1e-8 or max|r|/sqrt(N) <= 1e-8", "bcs": "Neumann x4", "mean": "harmonic"}
-    elif name == "gaussian128":
-        probs = [problems.gaussian_2d(128, device=device)]
-        cfg = {"workload": "gaussian2d_128_fp64", "kappa": "T^3", "dt": 1e-5, "tol": 1e-8}
-    elif name == "gaussian2048":
-        probs = [problems.gaussian_2d(2048, device=device)]
-        cfg = {"workload": "gaussian2d_2048_fp64", "kappa": "T^3", "dt": 1e-5, "tol": 1e-8}
-    elif name == "gauss3d128":
-        probs = [problems.gaussian_3d(128, device=device)]
-        cfg = {"workload": "gaussian3d_128_fp64", "kappa": "T^2.5", "dt": 1e-5, "tol": 1e-8}
-    elif name == "mms4096":
-        probs = [problems.mms_2d(4096, device=device)]
-        cfg = {"workload": "mms2d_4096", "kappa": "T^2.5", "dt": 1e-5, "tol": 1e-8}
-    elif name == "mms1024":
-        probs = [problems.mms_2d(1024, device=device)]
-        cfg = {"workload": "mms2d_1024", "kappa": "T^2.5", "dt": 1e-5, "tol": 1e-8}
-    elif name == "multigauss1024":
-        probs = [problems.multi_gaussian_2d(1024, seed=12345, device=device)]
-        cfg = {"workload": "multigauss2d_1024", "kappa": "T^3", "dt": 1e-5, "tol": 1e-8}
+        params = [q for r in range(ws) for q in P.batch_2d_params(nprob, seed=P.BATCH_SEED + r)]
+        costs = [float(q["n"] ** 2) for q in params]
+        build = lambda idx, device: [P.batch_problem(params[i], device=device) for i in idx]
+        full = sum((q["n"] + 2) ** 2 for q in params)
+        cfg = {"workload": "batch2d_256_fp64", "nprob": len(params), "sides": "U{64..512}",
+               "seed": P.BATCH_SEED if ws == 1 else f"{P.BATCH_SEED}..{P.BATCH_SEED + ws - 1}", "dt": 1e-5,
+               "tol": "rel <= 1e-8 or max|r|/sqrt(N) <= 1e-8", "bcs": "Neumann x4", "mean": "harmonic",
+               "parallelism": f"dp{ws} (sharded batch, LPT by cells)"}
     else:
-        probs = [problems.gaussian_3d(256, device=device)]
-        cfg = {"workload": "gaussian3d_256_fp64", "kappa": "T^2.5", "dt": 1e-5, "tol": 1e-8}
-    return probs, cfg
+        make, full1, cfg = SINGLE[name]
+        cfg = dict(cfg, dt=1e-5, tol="rel <= 1e-8 or max|r|/sqrt(N) <= 1e-8",
+                   parallelism=f"dp{ws} (one replica per rank)")
+        costs = [1.0] * ws
+        build = lambda idx, device: [make(P, device) for _ in idx]
+        full = full1 * ws
+    cfg["l2"] = "inputs larger than L2 (working set %.1f GB per job)" % (full * 8 * 16 / 1e9)
+    return costs, build, cfg
 
 
 # ---------------------------------------------------------------- reference arm
-def run_reference(args, ws, rank):
-    """The reference's CPU algorithm (the oracle restatement: the Julia reference
-    cannot run here) on the host cores, each step a bounded sample."""
-    if rank != 0:
-        return
-    import torch
-    from oracle.oracle import OracleSolver, num_threads, set_threads
-    set_threads(len(os.sched_getaffinity(0)))  # every host core this process may use
-    probs, cfg = make_workload(args.workload, args.nprob, 0, "cpu")
-    sample = probs[: min(len(probs), 6)] if args.workload == "batch" else probs
-    solvers = [OracleSolver(p.mesh, p.bcs) for p in sample]
-    Ts = [p.T0.numpy().copy() for p in sample]
-    for p, o in zip(sample, solvers):
-        if p.source is not None:
-            o.set_source(p.source.numpy())
-    tot_ci, tot_t = 0, 0.0
-    for s in range(args.warmup + args.steps):
+def oracle_steps(probs, nsteps, states=None):
+    """One time step of every problem per round with the oracle (the reference's
+    CPU algorithm, OpenMP over every host core); returns per-round seconds and
+    cell-iterations, and the solver states to continue from."""
+    from oracle.oracle import OracleSolver
+    if states is None:
+        states = []
+        for p in probs:
+            o = OracleSolver(p.mesh.to("cpu"), p.bcs)
+            if p.source is not None:
+                o.set_source(p.source.cpu().numpy())
+            states.append((o, p.T0.cpu().numpy().copy()))
+    rounds = []
+    for _ in range(nsteps):
         t0 = time.perf_counter()
         ci = 0
-        for p, o, T in zip(sample, solvers, Ts):
-            st, _ = o.step(T, p.rho.numpy(), p.cp, p.kappa.k0, p.kappa.n, p.dt, rtol=p.rtol, atol=p.atol,
+        for p, (o, T) in zip(probs, states):
+            st, _ = o.step(T, p.rho.cpu().numpy(), p.cp, p.kappa.k0, p.kappa.n, p.dt, rtol=p.rtol, atol=p.atol,
                            max_iter=100000)
             ci += p.mesh.ncells * st["niter"]
-        dt = time.perf_counter() - t0
-        if s >= args.warmup:
-            tot_ci += ci
-            tot_t += dt
-    v = tot_ci / tot_t / 1e9
-    cores = num_threads()
+        rounds.append((time.perf_counter() - t0, ci))
+    return rounds, states
+
+
+def cpu_sample(costs, ws):
+    """Problems the CPU arms time: a size-stratified quarter of the first
+    256-problem batch (every 4th problem in order of cells, from the second), or
+    the single problem of a one-problem workload."""
+    n_one = len(costs) // ws
+    if n_one == 1:
+        return [0], "the workload's problem"
+    order = sorted(range(n_one), key=lambda i: (costs[i], i))
+    idx = sorted(order[1::4])
+    return idx, (f"{len(idx)} of the batch's {n_one} problems, every 4th in order of size "
+                 f"(cells {sum(costs[i] for i in idx) / sum(costs[:n_one]):.3f} of the batch)")
+
+
+def run_reference(args, ws, rank):
+    """The reference's CPU algorithm (the oracle restatement: the Julia reference
+    cannot run here) on the host cores: every bench step is one time step of
+    every problem of the stratified sample (rank 0 alone)."""
+    if rank != 0:
+        return
+    from oracle.oracle import num_threads, set_threads
+    set_threads(len(os.sched_getaffinity(0)))  # every host core this process may use
+    costs, build, cfg = workload(args.workload, args.nprob, ws)
+    idx, what = cpu_sample(costs, ws)
+    probs = build(idx, "cpu")
+    _, states = oracle_steps(probs, args.warmup)
+    rounds, _ = oracle_steps(probs, args.steps, states)
+    tot_t = sum(t for t, _ in rounds)
+    v = sum(c for _, c in rounds) / tot_t / 1e9
     line = {"metric": "Gcell-iter/s", "value": v, "unit": "Gcell-iter/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": cfg, "impl": "reference",
-            "cpu_baseline": {"value": v, "unit": "Gcell-iter/s", "cores": cores, "kind": "port",
-                             "sample": f"first {len(sample)} problems of the workload, one time step each per bench step"},
+            "cpu_baseline": {"value": v, "unit": "Gcell-iter/s", "cores": num_threads(), "kind": "port",
+                             "sample": f"{what}, one time step each per bench step, after {args.warmup} "
+                                       f"warm-up steps"},
             "e2e": {"value": v, "unit": "Gcell-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline(probs, budget_s=15.0):
-    """Oracle (OpenMP, all host threads) on a bounded sample of the workload."""
-    from oracle.oracle import OracleSolver, num_threads, set_threads
+def cpu_baseline(probs, what):
+    """The oracle (OpenMP, all host threads) on a bounded sample of the workload:
+    one untimed time step of every sampled problem (the first step checks the
+    residual at every iteration), then one timed step."""
+    from oracle.oracle import num_threads, set_threads
     set_threads(len(os.sched_getaffinity(0)))  # every host core this process may use
-    t_start = time.perf_counter()
-    ci, tt, used = 0, 0.0, 0
-    for p in probs:
-        o = OracleSolver(p.mesh.to("cpu"), p.bcs)
-        T = p.T0.cpu().numpy().copy()
-        if p.source is not None:
-            o.set_source(p.source.cpu().numpy())
-        t0 = time.perf_counter()
-        st, _ = o.step(T, p.rho.cpu().numpy(), p.cp, p.kappa.k0, p.kappa.n, p.dt, rtol=p.rtol, atol=p.atol,
-                       max_iter=100000)
-        tt += time.perf_counter() - t0
-        ci += p.mesh.ncells * st["niter"]
-        used += 1
-        if time.perf_counter() - t_start > budget_s:
-            break
+    _, states = oracle_steps(probs, 1)
+    ((tt, ci),), _ = oracle_steps(probs, 1, states)
     return {"value": ci / tt / 1e9, "unit": "Gcell-iter/s", "cores": num_threads(), "kind": "port",
-            "sample": f"first time step of {used} problem(s) of the workload"}
+            "sample": f"{what}, the second time step of each"}
 
 
 # ---------------------------------------------------------------------- ours
 def run_ours(args, ws, rank, local):
     import torch
-    from curvilineardiffusionmanuscript_b200.solver import PseudoTransientBatch, PseudoTransientSolver, step
+    from curvilineardiffusionmanuscript_b200.sharding import ShardedBatch
+    from curvilineardiffusionmanuscript_b200.solver import PseudoTransientBatch
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    probs, cfg = make_workload(args.workload, args.nprob, rank, dev)
-    nd = probs[0].mesh.ndim
+    costs, build, cfg = workload(args.workload, args.nprob, ws)
     stream = torch.cuda.current_stream(dev)
     mixed = args.precision == "mixed"
-    batch = PseudoTransientBatch([p.mesh for p in probs], [p.bcs for p in probs], stream=stream.cuda_stream,
-                                 precision=args.precision)
-    for i, p in enumerate(probs):
-        if p.source is not None:
-            batch.set_source(i, p.source)
-    Ts = [p.T0.clone() for p in probs]
-    rhos = [p.rho for p in probs]
-    cps = [p.cp for p in probs]
-    kaps = [p.kappa for p in probs]
-    dts = [p.dt for p in probs]
-    kw = dict(rtol=probs[0].rtol, atol=probs[0].atol, max_iter=100000)
-    # strip height and iteration-block length timed on this batch (set-up, outside the timed region)
-    if args.tuning:
-        batch.set_tuning(*[int(v) for v in args.tuning.split(",")])
-        cfg["tuning"] = batch.tuning()
-    else:
-        tuned = batch.autotune(Ts, rhos, cps, kaps, dts, **kw)
-        cfg["autotune"] = dict(candidate=tuned, **batch.tuning())
+    local_probs = {}
 
-    def one_step():
-        st, _ = batch.step(Ts, rhos, cps, kaps, dts, **kw)
-        return st, batch.profile()
+    def build_local(idx):
+        for i, pr in zip(idx, build(idx, dev)):
+            local_probs[i] = pr
+        return [local_probs[i].mesh for i in idx], [local_probs[i].bcs for i in idx]
+
+    # the library's multi-GPU path: every rank builds and steps its LPT share
+    sb = ShardedBatch.from_factory(costs, build_local, make_batch=PseudoTransientBatch, stream=stream.cuda_stream,
+                                   precision=args.precision)
+    mine = sb.local
+    probs = [local_probs[i] for i in mine]
+    nd = probs[0].mesh.ndim
+    for k, pr in enumerate(probs):
+        if pr.source is not None:
+            sb.batch.set_source(k, pr.source)
+    n = sb.n
+
+    def full(local_list):  # global-order list with this rank's entries
+        out = [None] * n
+        for i, x in zip(mine, local_list):
+            out[i] = x
+        return out
+
+    Ts = [pr.T0.clone() for pr in probs]
+    rhos = [pr.rho for pr in probs]
+    cps, kaps, dts = full([pr.cp for pr in probs]), full([pr.kappa for pr in probs]), full([pr.dt for pr in probs])
+    kw = dict(rtol=probs[0].rtol, atol=probs[0].atol, max_iter=100000)
+    # kernel variant, strip height and iteration block timed on this rank's batch
+    # (set-up, outside the timed region)
+    if args.tuning:
+        sb.batch.set_tuning(*[int(v) for v in args.tuning.split(",")])
+        tuning = sb.batch.tuning()
+    else:
+        cand = sb.batch.autotune(Ts, rhos, [pr.cp for pr in probs], [pr.kappa for pr in probs],
+                                 [pr.dt for pr in probs], **kw)
+        tuning = dict(candidate=cand, **sb.batch.tuning())
+
+    def one_step(T_list, R_list):
+        st, _ = sb.step(full(T_list), full(R_list), cps, kaps, dts, **kw)
+        return st, sb.batch.profile()
 
     for _ in range(args.warmup):
-        one_step()
+        one_step(Ts, rhos)
     barrier(ws)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ci, sweep_ms, launches, sweep_launches, iters = 0, 0.0, 0, 0, []
+    ci, sweep_ms, launches, sweep_launches, iters, last = 0, 0.0, 0, 0, [], None
     with ClockSampler(local) as clk:
         torch.cuda.nvtx.range_push("bench_timed")
         e0.record(stream)
         for _ in range(args.steps):
-            st, pf = one_step()
+            st, pf = one_step(Ts, rhos)
             ci += pf["cell_iters"]
             sweep_ms += pf["sweep_ms"]
             launches += pf["sweep_launches"] + pf["other_launches"]
             sweep_launches += pf["sweep_launches"]
-            iters.append(sum(s["niter"] for s in st))
+            iters.append(sum(x["niter"] for x in st))
+            last = st
         e1.record(stream)
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_pop()
@@ -322,17 +374,21 @@ def run_ours(args, ws, rank, local):
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": None, "kernel": f"sweep{nd}d_{'fp32' if mixed else 'fp64'}", "peak_kind": peak_kind,
             "bytes_per_cell_iter": bpc}
-    tb, tsrc = traffic_per_cell_iter(nd, args.workload) if not mixed else (None, None)
+    tb = traffic_per_cell_iter(nd, args.workload, mixed)
     if tb is not None:
-        # DRAM bytes per cell-iteration from one ncu capture, times the cells one sweep updates
-        roof["traffic"] = tb * ci / max(1, sweep_launches)
-        roof["traffic_source"] = tsrc
+        # DRAM bytes per cell-iteration of one ncu capture, times the cells one sweep launch updates
+        roof["traffic"] = tb[0] * ci / max(1, sweep_launches)
+        roof["traffic_source"] = tb[1]
+    # the residual each problem stopped at in the last timed step (rule: rel <= 1e-8 or abs <= 1e-8)
+    absr = sorted(x["abs_err"] for x in last)
+    final = {"abs_err_max": absr[-1], "abs_err_median": absr[len(absr) // 2],
+             "stopped_by_rel": sum(1 for x in last if x["abs_err"] > kw["atol"]), "problems": len(last)}
     e2e = None
     if not args.no_e2e:
         # end to end through the public API with host (pinned) buffers
         Th = [t.cpu().pin_memory() for t in Ts]
         Rh = [r.cpu().pin_memory() for r in rhos]
-        st, _ = batch.step(Th, Rh, cps, kaps, dts, **kw)  # warm the host path
+        one_step(Th, Rh)  # warm the host path
         barrier(ws)
         torch.cuda.synchronize()
         ci2 = 0
@@ -340,52 +396,46 @@ def run_ours(args, ws, rank, local):
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         f0.record(stream)
         for _ in range(args.steps):
-            st, _ = batch.step(Th, Rh, cps, kaps, dts, **kw)
-            ci2 += batch.profile()["cell_iters"]
+            _, pf = one_step(Th, Rh)
+            ci2 += pf["cell_iters"]
         f1.record(stream)
         torch.cuda.synchronize()
         ms2 = max(f0.elapsed_time(f1), 1e3 * (time.perf_counter() - t0))
         ms2 = allreduce_max(ms2, ws, dev)
         ci2 = allreduce_sum(float(ci2), ws, dev)
-        nbytes = sum(t.numel() for t in Ts) * 8
-        e2e = {"value": ci2 / (ms2 / 1e3) / 1e9, "unit": "Gcell-iter/s", "h2d_bytes_per_step": 2 * nbytes,
-               "d2h_bytes_per_step": nbytes}
-    if rank != 0:
-        return
+        nbytes = allreduce_sum(float(sum(t.numel() for t in Ts) * 8), ws, dev)
+        e2e = {"value": ci2 / (ms2 / 1e3) / 1e9, "unit": "Gcell-iter/s", "h2d_bytes_per_step": int(2 * nbytes),
+               "d2h_bytes_per_step": int(nbytes)}
     cpu = None
     if ws == 1 and not args.no_cpu:
-        cpu = cpu_baseline(probs[:64])
-    cfg.update({"l2": "inputs larger than L2 (working set %.1f GB)" % (
-        sum(p.mesh.ncells_full for p in probs) * 8 * 16 / 1e9), "parallelism": f"dp{ws} (independent batches)"})
+        idx, what = cpu_sample(costs, ws)
+        cpu = cpu_baseline([local_probs[i] for i in idx], what)
+    sb.close()
+    if rank != 0:
+        return
     line = {"metric": "Gcell-iter/s", "value": value, "unit": "Gcell-iter/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
-            "config": cfg,
+            "config": cfg, "tuning": tuning,
             "s_per_timestep": ms_max / args.steps / 1e3, "pseudo_iters_per_step": statistics.mean(iters),
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "final_residual": final, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
-    batch.close()
 
 
-TRAFFIC_SUMMARY = {2: {"batch": "sweep2d_fp64_batch.md"}, 3: {}}
-TRAFFIC_DEFAULT = {2: "sweep2d_fp64_gaussian2048.md", 3: "sweep3d_fp64_gauss3d.md"}
-
-
-def traffic_per_cell_iter(nd, workload):
-    """DRAM bytes per cell-iteration of the sweep, read from the committed ncu summary
-    (line `dram_bytes_per_cell_iter: X`): the capture of this workload where one
-    exists, else the 2048^2 (2D) / 3D capture, scaled by the cells a sweep updates."""
-    import re
-    for name in (TRAFFIC_SUMMARY[nd].get(workload), TRAFFIC_DEFAULT[nd]):
-        if not name:
-            continue
-        f = ROOT / "profiles" / name
-        if f.exists():
-            m = re.search(r"^dram_bytes_per_cell_iter:\s*([0-9.]+)", f.read_text(), re.M)
-            if m:
-                return float(m.group(1)), "profiles/" + name
-    return None, None
+def traffic_per_cell_iter(nd, workload, mixed):
+    """DRAM bytes per cell-iteration of the sweep kernel from profiles/traffic.json
+    (one ncu capture per entry, its command recorded beside it): the entry of this
+    workload where one exists, else the kernel's default entry."""
+    f = ROOT / "profiles" / "traffic.json"
+    if not f.exists():
+        return None
+    data = json.loads(f.read_text())
+    kern = f"sweep{nd}d_{'fp32' if mixed else 'fp64'}"
+    for key in (f"{kern}/{workload}", kern):
+        if key in data:
+            return float(data[key]["dram_bytes_per_cell_iter"]), f"profiles/traffic.json:{key}"
+    return None
 
 
 def time_single(pr, precision, steps, warmup, stream, net=None):
@@ -452,6 +502,11 @@ def train_guess(n, nseeds, nsteps, train_steps):
     return net, info
 
 
+def build_single(name, device):
+    from curvilineardiffusionmanuscript_b200 import problems as P
+    return [SINGLE[name][0](P, device)]
+
+
 def run_compare(args):
     import torch
     dev = torch.device("cuda", 0)
@@ -460,7 +515,7 @@ def run_compare(args):
     for wl in (["mms4096", "multigauss1024"] if args.workload == "batch" else [args.workload]):
         r = {}
         for prec in ("fp64", "mixed"):
-            probs, cfg = make_workload(wl, 1, 0, dev)
+            probs = build_single(wl, dev)
             r[prec] = time_single(probs[0], prec, args.steps, args.warmup, stream)
         r["speedup_mixed_vs_fp64"] = r["fp64"]["s_per_step"] / r["mixed"]["s_per_step"]
         if wl.startswith("multigauss") and args.learned_steps > 0:
@@ -470,7 +525,7 @@ def run_compare(args):
             info["smoothing_passes"] = args.smooth
             r["training"] = info
             for prec in ("fp64", "mixed"):
-                probs, cfg = make_workload(wl, 1, 0, dev)
+                probs = build_single(wl, dev)
                 r["learned_" + prec] = time_single(probs[0], prec, args.steps, args.warmup, stream, net=net)
             r["speedup_learned_fp64_vs_fp64"] = r["fp64"]["s_per_step"] / r["learned_fp64"]["s_per_step"]
             r["speedup_learned_mixed_vs_fp64"] = r["fp64"]["s_per_step"] / r["learned_mixed"]["s_per_step"]

@@ -67,8 +67,8 @@ def gaussian_2d(n: int = 128, amp: float = 0.05, center=(0.5, 0.5), width2: floa
                    meta={"n": n, "amp": amp, "kn": kn, "center": center, "width2": width2})
 
 
-def batch_2d(nprob: int = 256, seed: int = BATCH_SEED, nmin: int = 64, nmax: int = 512, dt: float = 1e-5,
-             device="cpu") -> List[Problem]:
+def batch_2d_params(nprob: int = 256, seed: int = BATCH_SEED, nmin: int = 64, nmax: int = 512) -> List[dict]:
+    """The seeded draws of the batched configuration, without building meshes."""
     rng = np.random.default_rng(seed)
     out = []
     for p in range(nprob):
@@ -77,11 +77,22 @@ def batch_2d(nprob: int = 256, seed: int = BATCH_SEED, nmin: int = 64, nmax: int
         kn = float(rng.choice([0.0, 1.0, 2.5, 3.0]))
         c = (float(rng.uniform(0.3, 0.7)), float(rng.uniform(0.3, 0.7)))
         w = float(rng.uniform(0.05, 0.2))
-        pr = gaussian_2d(n, amp, c, w * w, 10.0, kn, dt, 1, device)
-        pr.name = f"batch_{p}"
-        pr.meta.update({"width": w})
-        out.append(pr)
+        out.append({"index": p, "seed": seed, "n": n, "amp": amp, "kn": kn, "center": c, "width": w})
     return out
+
+
+def batch_problem(params: dict, dt: float = 1e-5, device="cpu") -> Problem:
+    """One problem of the batched configuration from its draws."""
+    w = params["width"]
+    pr = gaussian_2d(params["n"], params["amp"], params["center"], w * w, 10.0, params["kn"], dt, 1, device)
+    pr.name = f"batch_{params['index']}"
+    pr.meta.update({"width": w, "seed": params["seed"]})
+    return pr
+
+
+def batch_2d(nprob: int = 256, seed: int = BATCH_SEED, nmin: int = 64, nmax: int = 512, dt: float = 1e-5,
+             device="cpu") -> List[Problem]:
+    return [batch_problem(p, dt, device) for p in batch_2d_params(nprob, seed, nmin, nmax)]
 
 
 # --------------------------------------------------------------------- MMS (C3)

@@ -81,17 +81,32 @@ class ShardedBatch:
 
     def __init__(self, meshes, bcs, costs: Optional[Sequence[float]] = None,
                  make_batch: Optional[Callable] = None, **batch_kwargs):
-        self.rank, self.world = world()
-        self.n = len(meshes)
         if costs is None:
             costs = [m.ni * m.nj * max(1, getattr(m, "nk", 1) or 1) for m in meshes]
+        self._setup(costs, lambda idx: ([meshes[i] for i in idx], [bcs[i] for i in idx]), make_batch,
+                    batch_kwargs)
+
+    @classmethod
+    def from_factory(cls, costs: Sequence[float], build: Callable, make_batch: Optional[Callable] = None,
+                     **batch_kwargs) -> "ShardedBatch":
+        """A sharded batch whose ranks build only their own problems:
+        build(indices) -> (meshes, bcs) of those global problem indices."""
+        self = cls.__new__(cls)
+        self._setup(costs, build, make_batch, batch_kwargs)
+        return self
+
+    def _setup(self, costs, build, make_batch, batch_kwargs):
+        self.rank, self.world = world()
+        self.n = len(costs)
         self.assignment = lpt_assign(costs, self.world)
         self.local = self.assignment[self.rank]
         if make_batch is None:
             from .solver import PseudoTransientBatch
             make_batch = PseudoTransientBatch
-        self.batch = (make_batch([meshes[i] for i in self.local], [bcs[i] for i in self.local], **batch_kwargs)
-                      if self.local else None)
+        self.batch = None
+        if self.local:
+            meshes, bcs = build(self.local)
+            self.batch = make_batch(meshes, bcs, **batch_kwargs)
 
     def _pick(self, xs):
         return [xs[i] for i in self.local]

@@ -682,3 +682,48 @@ def test_save_vtk_from_device_state(tmp_path, monkeypatch):
     q, _ = g.get_state()
     assert np.array_equal(arr["q1"], q[0][dom].astype(np.float32).reshape(-1))
     assert {"rho", "diffusivity", "dτ_ρ", "θr_dτ", "q2"} <= set(arr)
+
+
+# ------------------------------------------------------ energy balance (n1)
+@pytest.mark.parametrize("case", ["2d", "3d"])
+@pytest.mark.parametrize("precision", ["fp64_exact", "fp64", "mixed"])
+def test_energy_balance_matches_the_oracle(case, precision):
+    """Σρcₚ T J before and after the step and Δt·ΣS J (the energy balance the
+    mixed path keeps in FP64) against the oracle's StepStats: relative 1e-12 for
+    the FP64 forms (summation order differs), and for mixed precision the same
+    bound before the step and the stated 1e-6 solution bound after it."""
+    if case == "2d":
+        pr = small_case_2d(ni=60, nj=47, source=True)
+    else:
+        pr = small_case_3d(n=(20, 18, 16))
+        x, y, z = pr.mesh.centroids
+        pr.source = (3.0 * torch.exp(-((x - 0.4) ** 2 + (y - 0.5) ** 2 + (z - 0.6) ** 2) / 0.05)).contiguous()
+    kw = dict(rtol=1e-8, atol=1e-8, max_iter=50000)
+    _, _, out = run_pair(pr, nsteps=2, precision=precision, device_arrays=True, **kw)
+    for so, sg, *_ in out:
+        assert so["status"] == 0 and sg["status"] == 0
+        for key in ("energy_before", "source_work"):
+            assert abs(sg[key] - so[key]) <= 1e-12 * abs(so[key]), (key, sg[key], so[key])
+        bound = 1e-6 if precision == "mixed" else 1e-12
+        assert abs(sg["energy_after"] - so["energy_after"]) <= bound * abs(so["energy_after"])
+        assert so["source_work"] > 0
+
+
+def test_nonlinear_thermal_conduction_step_wrapper(capsys):
+    """nonlinear_thermal_conduction_step! (nonlinear_thermal_conduction.jl:51-72):
+    forwards to step! with its keywords, prints the convergence line with
+    show_convergence, returns step!'s (stats, next_Δt)."""
+    from curvilineardiffusionmanuscript_b200.solver import nonlinear_thermal_conduction_step
+    pr = small_case_2d()
+    g1 = PseudoTransientSolver(pr.mesh, pr.bcs, precision="fp64_exact")
+    g2 = PseudoTransientSolver(pr.mesh, pr.bcs, precision="fp64_exact")
+    T1, T2 = pr.T0.numpy().copy(), pr.T0.numpy().copy()
+    kw = dict(rtol=0.0, atol=1e-8, t=0.0, tz=False, tz_dim=1, no_t=True)
+    s1, n1 = nonlinear_thermal_conduction_step(g1, pr.mesh, T1, pr.rho.numpy(), pr.cp, pr.kappa, pr.dt, **kw)
+    out = capsys.readouterr().out
+    s2, n2 = step(g2, pr.mesh, T2, pr.rho.numpy(), pr.cp, pr.kappa, pr.dt, **kw)
+    assert np.array_equal(T1, T2) and n1 == n2 and s1["niter"] == s2["niter"]
+    assert out == "\trel error: %.3e, abs err: %.3e, %i\n" % (s1["rel_err"], s1["abs_err"], s1["niter"])
+    nonlinear_thermal_conduction_step(g1, pr.mesh, T1, pr.rho.numpy(), pr.cp, pr.kappa, pr.dt,
+                                      show_convergence=False, **kw)
+    assert capsys.readouterr().out == ""

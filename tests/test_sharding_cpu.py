@@ -171,3 +171,44 @@ def test_a_rank_that_leaves_ends_the_others_step_with_an_error():
     assert res[1][1] == "left"
     rank, what, dt = res[0]
     assert what != "ok" and dt < 60.0, (what, dt)
+
+
+def _factory_worker(rank, world, port, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        sizes = [64, 512, 128, 96, 300, 200, 80]
+        built = []
+
+        def build(idx):
+            built.extend(idx)
+            return [FakeMesh(sizes[i]) for i in idx], [f"bc{i}" for i in idx]
+
+        sb = ShardedBatch.from_factory([n * n for n in sizes], build, make_batch=FakeBatch)
+        # the bench's calling convention: global-order lists holding this rank's entries only
+        Ts = [torch.zeros(3) if i in sb.local else None for i in range(7)]
+        stats, _ = sb.step(Ts, [None] * 7, [1.0] * 7, [None] * 7, [1.0] * 7)
+        q.put((rank, sb.local, sorted(built), [s["niter"] for s in stats]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_batch_from_factory_builds_only_local_problems():
+    """ShardedBatch.from_factory: every rank builds only the problems LPT gives
+    it, and still receives every problem's statistics."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_factory_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    sizes = [64, 512, 128, 96, 300, 200, 80]
+    assert sorted(res[0][1] + res[1][1]) == list(range(7))
+    for rank, local, built, niters in res:
+        assert built == local and niters == sizes
