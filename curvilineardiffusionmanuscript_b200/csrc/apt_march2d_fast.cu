@@ -491,8 +491,9 @@ __global__ void march2d_wave_init(const Problem* __restrict__ probs, int nprob, 
   if (threadIdx.x == 0) counters[2] = 0u;
 }
 
+// 640 threads per SM at the register budget of 5 blocks of 128 (96 registers)
 template <int TX, bool HARM>
-__global__ void __launch_bounds__(TX, 5) march2d_fast_wave(const Problem* __restrict__ probs,
+__global__ void __launch_bounds__(TX, 640 / TX) march2d_fast_wave(const Problem* __restrict__ probs,
                                                            const int2* __restrict__ items, int nitems, int K,
                                                            unsigned int* counters, int* wave_count) {
   __shared__ FastSmem<TX> sm;
@@ -541,7 +542,10 @@ static int wave_slots() {
   return nsm * per_sm;
 }
 
-int march2d_wave_slots(int harmonic) { return harmonic ? wave_slots<128, true>() : wave_slots<128, false>(); }
+int march2d_wave_slots(int tx, int harmonic) {
+  if (tx == 64) return harmonic ? wave_slots<64, true>() : wave_slots<64, false>();
+  return harmonic ? wave_slots<128, true>() : wave_slots<128, false>();
+}
 
 template <int TX, bool HARM>
 static cudaError_t launch_wave(const Problem* probs, int nprob, const int2* items, int nitems, int K,
@@ -554,10 +558,13 @@ static cudaError_t launch_wave(const Problem* probs, int nprob, const int2* item
   return cudaGetLastError();
 }
 
-cudaError_t launch_march2d_wave(int harmonic, const Problem* probs, int nprob, const int2* items, int nitems,
-                                int K, unsigned int* counters, int* wave_count, cudaStream_t s) {
+cudaError_t launch_march2d_wave(int tx, int harmonic, const Problem* probs, int nprob, const int2* items,
+                                int nitems, int K, unsigned int* counters, int* wave_count, cudaStream_t s) {
   if (nitems <= 0 || K <= 0) return cudaSuccess;
   if ((long long)K * nitems >= (1ll << 31)) return cudaErrorInvalidValue;
+  if (tx == 64)
+    return harmonic ? launch_wave<64, true>(probs, nprob, items, nitems, K, counters, wave_count, s)
+                    : launch_wave<64, false>(probs, nprob, items, nitems, K, counters, wave_count, s);
   return harmonic ? launch_wave<128, true>(probs, nprob, items, nitems, K, counters, wave_count, s)
                   : launch_wave<128, false>(probs, nprob, items, nitems, K, counters, wave_count, s);
 }

@@ -15,6 +15,13 @@
 // and above it.  Every face is computed once per strip; the ring costs 1.33x
 // the owned cells per plane and nothing along k.  Ghost cells come from the
 // boundary rules of every side applied on the fly (boundary_operators.jl).
+//
+// Two instantiations: EDGE for tiles whose (i, j) ring touches the domain
+// boundary (general ghost logic per cell), and the interior one, whose cells
+// and ring are all domain cells in (i, j): no per-cell classification, the
+// k-ghost planes handled per plane (block-uniform), and the loads that stage
+// plane z + 2 (u, ρ, uⁿ) issued while plane z is updated, so that their latency
+// overlaps a whole plane of work.  The two run as concurrent launches.
 #include "cdm_device.cuh"
 #include "cdm_fast.cuh"
 #include "cdm_finish.cuh"
@@ -45,7 +52,7 @@ struct C3 {
 
 }  // namespace
 
-template <bool HARM>
+template <bool HARM, bool EDGE>
 __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict__ probs,
                                                       const int2* __restrict__ items) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -83,7 +90,7 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
   // own (i, j) position in ring coordinates, and this thread's ring cell
   const int ox = tid % TX + 1, oy = tid / TX + 1;
   const int oa = i0 + ox - 1, ob = j0 + oy - 1;
-  const bool own_in = oa < ni && ob < nj;
+  const bool own_in = EDGE ? (oa < ni && ob < nj) : true;
   int rx = -1, ry = -1;
   if (tid < NRING) {
     if (tid < RX) {
@@ -155,8 +162,112 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
     }
     return r;
   };
+  // interior tiles: raw loads of the cells of plane c (u from the cell the
+  // k-ghost rule reads, ρ of the cell itself), issued a plane ahead of stage_pre
+  struct Pre3 {
+    double u, rho, up;
+  };
+  const int64_t plane_sz = (int64_t)P.nx * P.ny;
+  const int64_t own_col = fidx(P, oa, ob, 0);
+  const int64_t ring_col = rx >= 0 ? fidx(P, ra, rb, 0) : own_col;
+  // k-ghost rule of plane c (block-uniform): source plane, 1 negate, 2 constant
+  auto kplane = [&](int c, int& cs, int& mode, double& cv) {
+    cs = c;
+    mode = 0;
+    cv = 0.0;
+    if (c >= 0 && c < nk) return;
+    const int side = c < 0 ? 4 : 5;
+    const int rule = P.rule[side];
+    const bool lo = side == 4;
+    if (rule == GR_DIRICHLET) {
+      mode = 2;
+      cv = P.val[side];
+    } else if (rule == GR_PERIODIC) {
+      cs = lo ? nk - 1 : 0;
+    } else if (rule != GR_NONE) {
+      cs = lo ? 0 : nk - 1;
+      mode = rule == GR_NEGSYM ? 1 : 0;
+    }
+  };
+  auto prefetch = [&](int c, Pre3& own, Pre3& rg, int& mode, double& cv) {
+    int cs;
+    kplane(c, cs, mode, cv);
+    const int64_t po = plane_sz * c, ps = plane_sz * cs;
+    own.rho = P.rho[own_col + po];
+    own.u = mode == 2 ? cv : uin[own_col + ps];
+    own.up = (!alpha_from_u && mode != 2) ? P.u_prev[own_col + ps] : cv;
+    if (rx >= 0) {
+      rg.rho = P.rho[ring_col + po];
+      rg.u = mode == 2 ? cv : uin[ring_col + ps];
+      rg.up = (!alpha_from_u && mode != 2) ? P.u_prev[ring_col + ps] : cv;
+    }
+  };
+  // the diffusivity, pseudo-time parameters and update factors from raw loads
+  auto stage_pre = [&](const Pre3& L, int mode, bool track) -> C3 {
+    C3 r{0.0, 0.0, 0.0, 0.0, 0.0};
+    const double u = mode == 1 ? -L.u : L.u;
+    const double src = alpha_from_u ? u : (mode == 1 ? -L.up : L.up);
+    const double rho = L.rho;
+    const double kap = isfinite(src) ? k0c * pow_fast(fabs(src), kmode, km, khalf, kn) : 0.0;
+    const double rc = rho * cp;
+    const double inva = rc * rcp_nr(kap);
+    const double Re = kPi + sqrt(kPi * kPi + LLdt * rho * inva);
+    r.u = u;
+    if (HARM) {
+      const double VA = VpL * inva;
+      const double dRe = dt * Re;
+      const double D = dRe + VA;
+      const bool fin = isfinite(D);
+      const double iD = rcp_pos(fin ? D : 1.0);
+      r.g = fin ? dRe * iD : 1.0;
+      r.f = fin ? VA * dt * iD : 0.0;
+      r.ia = inva;
+      r.it = VpoL * Re;
+    } else {
+      const double iRe = rcp_nr(Re);
+      double dtau = VpL * inva * iRe;
+      double th = LoVp * iRe;
+      dtau = isfinite(dtau) ? dtau : 0.0;
+      th = isfinite(th) ? th : 0.0;
+      const double idd = rcp_nr(dt + dtau);
+      r.g = dt * idd;
+      r.f = dtau * dt * idd;
+      r.ia = kap * rcp_nr(rc);
+      r.it = th;
+    }
+    if (track && track_iter) {
+      if (!(isfinite(kap) && isfinite(rc) && rc != 0.0)) bad |= 1;
+      if (kap != 0.0 && ((kap < 0.0) != (rc < 0.0))) bad |= 2;
+    }
+    return r;
+  };
+  auto publish = [&](int s, const C3& own, const C3& rg) {
+    sm.U[s][oy][ox] = own.u;
+    sm.IA[s][oy][ox] = own.ia;
+    sm.IT[s][oy][ox] = own.it;
+    if (rx >= 0) {
+      sm.U[s][ry][rx] = rg.u;
+      sm.IA[s][ry][rx] = rg.ia;
+      sm.IT[s][ry][rx] = rg.it;
+    }
+  };
+  // stage plane c into cell slot s from loads prefetched earlier (interior tiles)
+  auto stage_plane_pre = [&](int c, int s, const Pre3& own_l, const Pre3& rg_l, int mode) -> C3 {
+    const bool inz = c >= k0 && c < k1;
+    const C3 own = stage_pre(own_l, mode, inz || c == -1 || c == nk);
+    const C3 rg = rx >= 0 ? stage_pre(rg_l, mode, inz) : C3{0.0, 0.0, 0.0, 0.0, 0.0};
+    publish(s, own, rg);
+    return own;
+  };
   // stage plane c into cell slot s: the own cell (returned) and the ring cell
   auto stage_plane = [&](int c, int s) -> C3 {
+    if (!EDGE) {
+      Pre3 lo, lr;
+      int mode;
+      double cv;
+      prefetch(c, lo, lr, mode, cv);
+      return stage_plane_pre(c, s, lo, lr, mode);
+    }
     const bool inz = c >= k0 && c < k1;
     const C3 own = stage(oa, ob, c, inz || c == -1 || c == nk);
     sm.U[s][oy][ox] = own.u;
@@ -231,12 +342,13 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
   }
   const int fa = i0 - 1 + fx, fb = j0 - 1 + fy;
   // the ring face's (a, b) range test (faces.jl ranges: an i-face joins cells a and a+1, ...)
-  const bool f_ab = fk == 0   ? (fa >= -1 && fa <= ni - 1 && fb >= 0 && fb <= nj - 1)
+  const bool f_ab = !EDGE ? fk >= 0
+                    : fk == 0 ? (fa >= -1 && fa <= ni - 1 && fb >= 0 && fb <= nj - 1)
                     : fk == 1 ? (fa >= 0 && fa <= ni - 1 && fb >= -1 && fb <= nj - 1)
                               : (fa >= 0 && fa <= ni - 1 && fb >= 0 && fb <= nj - 1);
   // ring i-faces of column 0 and j-faces of row 0 are the domain's low boundary faces
-  const bool f_wr = (fk == 0 && fx == 0 && i0 == 0 && fy >= 1 && fy <= TY) ||
-                    (fk == 1 && fy == 0 && j0 == 0 && fx >= 1 && fx <= TX);
+  const bool f_wr = EDGE && ((fk == 0 && fx == 0 && i0 == 0 && fy >= 1 && fy <= TY) ||
+                             (fk == 1 && fy == 0 && j0 == 0 && fx >= 1 && fx <= TX));
   const int64_t plane = (int64_t)P.nx * P.ny;
   const int64_t o_col = fidx(P, oa, ob, 0), f_col = fidx(P, fa, fb, 0);
   // old fluxes at plane c (i, j) and of the k-faces above plane ck, into
@@ -356,12 +468,24 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
   load_faces(k0 + 1, k0, true, qa);  // used by the first plane of the loop
   __syncthreads();
 
+  // interior tiles: the stage loads of plane k0 + 1, for the first loop iteration
+  Pre3 p_own{0.0, 0.0, 0.0}, p_rg{0.0, 0.0, 0.0};
+  int p_mode = 0;
+  double p_cv = 0.0;
+  if (!EDGE) prefetch(k0 + 1, p_own, p_rg, p_mode, p_cv);
+
   double local = 0.0;
   bool local_nan = false;
   for (int z = k0; z < k1; ++z) {
     // old fluxes of the next plane's faces, one plane ahead of their use
     if (z + 1 < k1) load_faces(z + 2, z + 1, true, qb);
-    const C3 nxt = stage_plane(z + 1, s_p);
+    C3 nxt;
+    if (EDGE) {
+      nxt = stage_plane(z + 1, s_p);
+    } else {
+      nxt = stage_plane_pre(z + 1, s_p, p_own, p_rg, p_mode);
+      if (z + 1 < k1) prefetch(z + 2, p_own, p_rg, p_mode, p_cv);
+    }
     __syncthreads();
     // own cell's coefficients: their loads overlap the face computations
     double cf[9], up = 0.0, S = 0.0;
@@ -383,10 +507,12 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
       const double un = cur.g * cur.u + cur.f * (up * inv_dt - dq + S);
       uout[id] = un;
       // ghosts of u after applybcs! of this iteration (copy!(T, u) returns them)
-      if (oa == 0) uout[fidx(P, -1, ob, z)] = g_im;
-      if (oa == ni - 1) uout[fidx(P, ni, ob, z)] = g_ip;
-      if (ob == 0) uout[fidx(P, oa, -1, z)] = g_jm;
-      if (ob == nj - 1) uout[fidx(P, oa, nj, z)] = g_jp;
+      if (EDGE) {
+        if (oa == 0) uout[fidx(P, -1, ob, z)] = g_im;
+        if (oa == ni - 1) uout[fidx(P, ni, ob, z)] = g_ip;
+        if (ob == 0) uout[fidx(P, oa, -1, z)] = g_jm;
+        if (ob == nj - 1) uout[fidx(P, oa, nj, z)] = g_jp;
+      }
       if (z == 0) uout[fidx(P, oa, ob, -1)] = prv_u;
       if (z == nk - 1) uout[fidx(P, oa, ob, nk)] = nxt.u;
       if (check) {
@@ -422,20 +548,44 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
 }
 
 template <bool HARM>
-static cudaError_t launch3m(const Problem* probs, const int2* items, int nitems, cudaStream_t s) {
+static cudaError_t launch3m(const Problem* probs, const int2* items, int n_edge, int n_int, const SweepStreams& ss) {
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(march3d_fast<HARM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(march3d_fast<HARM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)sizeof(M3Smem));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(march3d_fast<HARM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(M3Smem));
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  march3d_fast<HARM><<<nitems, NT, sizeof(M3Smem), s>>>(probs, items);
+  // boundary tiles on the side stream, concurrently with the interior tiles
+  const bool fork = n_edge > 0 && n_int > 0 && ss.side != nullptr;
+  cudaError_t e = cudaSuccess;
+  if (fork) {
+    if ((e = cudaEventRecord(ss.ev_fork, ss.main)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(ss.side, ss.ev_fork, 0)) != cudaSuccess) return e;
+  }
+  if (n_edge > 0) march3d_fast<HARM, true><<<n_edge, NT, sizeof(M3Smem), fork ? ss.side : ss.main>>>(probs, items);
+  if (n_int > 0) march3d_fast<HARM, false><<<n_int, NT, sizeof(M3Smem), ss.main>>>(probs, items + n_edge);
+  if (fork) {
+    if ((e = cudaEventRecord(ss.ev_join, ss.side)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(ss.main, ss.ev_join, 0)) != cudaSuccess) return e;
+  }
   return cudaGetLastError();
 }
 
-cudaError_t launch_march3d_fast(int harmonic, const Problem* probs, const int2* items, int nitems, cudaStream_t s) {
-  return harmonic ? launch3m<true>(probs, items, nitems, s) : launch3m<false>(probs, items, nitems, s);
+cudaError_t launch_march3d_fast(int harmonic, const Problem* probs, const int2* items, int n_edge, int n_int,
+                                const SweepStreams& ss) {
+  return harmonic ? launch3m<true>(probs, items, n_edge, n_int, ss) : launch3m<false>(probs, items, n_edge, n_int, ss);
+}
+
+// Is column tile `tile` (any strip) of a 3D problem free of (i, j) ghost logic:
+// its cells and their one-cell ring all domain cells?
+bool march3d_tile_interior(int ni, int nj, int tiles_i, int tiles_j, int tile) {
+  const int ti = tile % tiles_i, tj = (tile / tiles_i) % tiles_j;
+  const int i0 = ti * TX, j0 = tj * TY;
+  return i0 >= 1 && i0 + TX + 1 <= ni && j0 >= 1 && j0 + TY + 1 <= nj;
 }
 
 }  // namespace cdm

@@ -383,6 +383,7 @@ __global__ void __launch_bounds__(NT) sweep3d_fp64(const Problem* __restrict__ p
 // tile shape table (the autotuner picks among these)
 static const TileShape kShapes2D[] = {
     {128, 0, 0, 128, 1}, {64, 0, 0, 64, 1}, {32, 16, 1, 256, 0}, {32, 8, 1, 256, 0}, {128, 0, 0, 128, 3},
+    {64, 0, 0, 64, 3},
 };
 // 3D: variant 0 is the plane-marching kernel (reciprocal form); the tile
 // kernels keep the operation-for-operation form
@@ -390,7 +391,7 @@ static const TileShape kShapes3D[] = {
     {32, 8, 1, 256, 2}, {32, 4, 4, 256, 0}, {16, 8, 4, 256, 0},
 };
 
-int num_tile_shapes(int ndim) { return ndim == 2 ? 5 : 3; }
+int num_tile_shapes(int ndim) { return ndim == 2 ? 6 : 3; }
 TileShape tile_shape(int ndim, int v) { return ndim == 2 ? kShapes2D[v] : kShapes3D[v]; }
 
 template <int TX, int TY, int TZ, int NT>
@@ -418,7 +419,8 @@ cudaError_t launch_sweep_fp64(int ndim, int variant, int exact, int harmonic, co
       case 1:
         if (exact || tz) return launch_march2d_fp64(variant, tz, probs, items, nitems, s);
         return launch_march2d_fast(variant, harmonic, probs, items, n_edge, nitems - n_edge, counters, ss);
-      case 4:  // the wavefront variant launches through launch_march2d_wave (tagged items)
+      case 4:  // the wavefront variants launch through launch_march2d_wave (tagged items)
+      case 5:
         return cudaErrorInvalidValue;
       case 2: sweep2d_fp64<32, 16, 256><<<nitems, 256, 0, s>>>(probs, items); break;
       default: sweep2d_fp64<32, 8, 256><<<nitems, 256, 0, s>>>(probs, items); break;
@@ -426,7 +428,7 @@ cudaError_t launch_sweep_fp64(int ndim, int variant, int exact, int harmonic, co
     return cudaGetLastError();
   }
   switch (variant) {
-    case 0: return launch_march3d_fast(harmonic, probs, items, nitems, s);
+    case 0: return launch_march3d_fast(harmonic, probs, items, n_edge, nitems - n_edge, ss);
     case 1: return launch3<32, 4, 4, 256>(probs, items, nitems, s);
     default: return launch3<16, 8, 4, 256>(probs, items, nitems, s);
   }

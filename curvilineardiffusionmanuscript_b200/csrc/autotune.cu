@@ -35,10 +35,12 @@ constexpr int kWaveBlock[] = {8, 16, 32};
 // 12..17 (2D FP64): tile kernels (variants 2, 3: 32x16 and 32x8 tiles, every row of a
 // tile at once, for grids too small to hide a strip's serial march), block kBlock[c % 3];
 // 18..26 (2D FP64, reciprocal form): the marching kernel on the wavefront schedule
-// (variant 4), strip height kWaveH[t / 3], iterations per launch kWaveBlock[t % 3]
+// (variant 4), strip height kWaveH[t / 3], iterations per launch kWaveBlock[t % 3];
+// 27..35: the same with 64-thread blocks (variant 5), which leave fewer columns of
+// a narrow problem's last block idle
 constexpr int kNumMarch = 4 * kNumBlock;
 constexpr int kNumTile = kNumMarch + 2 * kNumBlock;
-constexpr int kNumCand = kNumTile + 9;
+constexpr int kNumCand = kNumTile + 18;
 
 struct Cand {
   int variant, strip_h, block;
@@ -51,7 +53,7 @@ Cand candidate(int c) {
     return {2 + t / kNumBlock, 0, kBlock[t % kNumBlock]};
   }
   const int t = c - kNumTile;
-  return {4, kWaveH[t / 3], kWaveBlock[t % 3]};
+  return {4 + t / 9, kWaveH[(t % 9) / 3], kWaveBlock[t % 3]};
 }
 
 double seconds() {
@@ -259,7 +261,7 @@ extern "C" int cdm_batch_set_tuning(cdm_batch* b, int variant, int strip_h, int 
   bool ok = variant >= 0 && variant < nv && strip_h >= 0 && iter_block >= 1 && iter_block <= 64;
   if (e.precision == CDM_PREC_MIXED) ok = ok && variant == 0;           // FP32 sweeps march
   if (e.ndim == 3) ok = ok && (exact3d ? variant != 0 : variant == 0);  // 3D: form fixes the kernel
-  if (variant == 4) ok = ok && e.precision == CDM_PREC_FP64;              // wavefront: reciprocal form
+  if (variant >= 4) ok = ok && e.precision == CDM_PREC_FP64;              // wavefront: reciprocal form
   if (!ok) {
     cdm::set_error("cdm_batch_set_tuning: variant, strip height or block length not valid for this batch");
     return CDM_BAD_INPUT;

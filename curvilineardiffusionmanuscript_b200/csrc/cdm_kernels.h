@@ -39,15 +39,19 @@ bool march_tile_interior(int ni, int nj, int tiles_i, int strip_h, int tx, int t
 // items: each problem's strips together, boundary strips with bit 30 of the tile set.
 // counters[2] is the launch's ticket, counters[3] a flag set when a bounded dependency
 // wait ran out (left set; clear it before the next step); wave_count holds nprob ints.
-cudaError_t launch_march2d_wave(int harmonic, const Problem* probs, int nprob, const int2* items, int nitems,
-                                int K, unsigned int* counters, int* wave_count, cudaStream_t s);
-// blocks one wavefront launch keeps resident on the current device
-int march2d_wave_slots(int harmonic);
+// tx: threads per block (128 or 64; tx - 2 owned columns)
+cudaError_t launch_march2d_wave(int tx, int harmonic, const Problem* probs, int nprob, const int2* items,
+                                int nitems, int K, unsigned int* counters, int* wave_count, cudaStream_t s);
+// blocks one wavefront launch of tx-thread blocks keeps resident on the current device
+int march2d_wave_slots(int tx, int harmonic);
 // one block whose thread 0 runs the wavefront's dependency wait on *count (which
 // must stay 0) with a limit of limit_s seconds; sets *err when the wait runs out
 cudaError_t launch_wave_wait_probe(const int* count, unsigned int* err, double limit_s, cudaStream_t s);
-// 3D plane-marching kernel (reciprocal form); items are (problem, column tile + strip)
-cudaError_t launch_march3d_fast(int harmonic, const Problem* probs, const int2* items, int nitems, cudaStream_t s);
+// 3D plane-marching kernel (reciprocal form); items are (problem, column tile + strip),
+// items[0, n_edge) tiles touching the (i, j) boundary, then n_int interior tiles
+cudaError_t launch_march3d_fast(int harmonic, const Problem* probs, const int2* items, int n_edge, int n_int,
+                                const SweepStreams& ss);
+bool march3d_tile_interior(int ni, int nj, int tiles_i, int tiles_j, int tile);
 
 // one fused FP64 pseudo-iteration over all items (problem, tile)
 // exact = 1: operation-for-operation reference arithmetic (bit-identical to the

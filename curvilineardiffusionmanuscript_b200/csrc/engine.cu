@@ -478,9 +478,18 @@ int Engine::build_items() {
     }
     items.swap(mixed);
   }
-  // the fast 2D kernel runs boundary strips and interior strips as two launches
+  // the fast 2D and 3D kernels run boundary strips and interior strips as two launches
   n_edge = (int)items.size();
-  if (ts.march == 1 && precision != CDM_PREC_FP64_EXACT) {
+  if (ts.march == 2) {
+    std::vector<int2> edge, inner;
+    for (const int2& it : items) {
+      const ProbState& s = ps[it.x];
+      (march3d_tile_interior(s.ni, s.nj, s.tiles_i, s.tiles_j, it.y) ? inner : edge).push_back(it);
+    }
+    n_edge = (int)edge.size();
+    items.assign(edge.begin(), edge.end());
+    items.insert(items.end(), inner.begin(), inner.end());
+  } else if (ts.march == 1 && precision != CDM_PREC_FP64_EXACT) {
     std::vector<int2> edge, inner;
     for (const int2& it : items) {
       const ProbState& s = ps[it.x];
@@ -649,8 +658,8 @@ double Engine::collect_profile_ms() {
 // K pseudo-iterations: K sweep launches, or one wavefront launch (and its prologue)
 cudaError_t Engine::launch_iters(int K) {
   if (tile_shape(ndim, variant).march == 3)
-    return launch_march2d_wave(mean == CDM_MEAN_HARMONIC, d_probs, (int)ps.size(), d_items, nitems, K, d_counters,
-                               d_wave, stream);
+    return launch_march2d_wave(tile_shape(ndim, variant).tx, mean == CDM_MEAN_HARMONIC, d_probs, (int)ps.size(),
+                               d_items, nitems, K, d_counters, d_wave, stream);
   cudaError_t le = cudaSuccess;
   for (int k = 0; k < K && le == cudaSuccess; ++k)
     le = launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT || tz_active, mean == CDM_MEAN_HARMONIC,
@@ -668,7 +677,7 @@ int Engine::launch_block(int K, bool use_graph) {
   if (ts.march == 3) {
     prof.sweep_launches += 1;
     prof.other_launches += 1;
-  } else if (ts.march == 1 && precision != CDM_PREC_FP64_EXACT && !tz_active) {
+  } else if ((ts.march == 1 && precision != CDM_PREC_FP64_EXACT && !tz_active) || ts.march == 2) {
     prof.sweep_launches += (int64_t)K * ((n_edge > 0 ? 1 : 0) + (nitems - n_edge > 0 ? 1 : 0));
   } else {
     prof.sweep_launches += K;
@@ -754,7 +763,7 @@ int Engine::run_iterations(const cdm_step_opts* o, int predicted, double t_start
 int Engine::retile_tail() {
   const int nprob = (int)ps.size();
   const TileShape ts = tile_shape(ndim, variant);
-  const long long target = 2ll * march2d_wave_slots(mean == CDM_MEAN_HARMONIC);
+  const long long target = 2ll * march2d_wave_slots(ts.tx, mean == CDM_MEAN_HARMONIC);
   long long strips = 0;
   int h = 0;
   for (int p = 0; p < nprob; ++p)
