@@ -35,6 +35,7 @@ UNITS = {
     "apt_noalloc.cu": ["-fmad=false"],
     "autotune.cu": [],
     "net_kernels.cu": [],
+    "net_conv_tc.cu": [],
     "net.cu": [],
 }
 

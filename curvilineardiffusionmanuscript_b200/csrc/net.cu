@@ -321,6 +321,17 @@ class Net {
     return CDM_OK;
   }
 
+  // CDM_TIMEOUT when a bounded wait of the tensor-core convolution ran out
+  int conv_status() {
+    int flag = 0;
+    CDM_CK(conv3x3_tc_error(&flag));
+    if (flag) {
+      set_error("guess network: a tensor-core convolution's wait ran out");
+      return CDM_TIMEOUT;
+    }
+    return CDM_OK;
+  }
+
   float read_loss() {
     float l = 0.f;
     if (cudaMemcpyAsync(&l, d_loss, sizeof(float), cudaMemcpyDeviceToHost, stream) != cudaSuccess) return NAN;
@@ -412,7 +423,7 @@ int cdm_net_forward(cdm_net* net, const uint16_t* x, int B, int H, int W, float*
   if (rc != CDM_OK) return rc;
   CDM_CK(cudaMemcpyAsync(y, n.Y, np * 16 * sizeof(float), cudaMemcpyDeviceToDevice, n.stream));
   CDM_CK(cudaStreamSynchronize(n.stream));
-  return CDM_OK;
+  return n.conv_status();
 }
 
 int cdm_net_backward(cdm_net* net, const float* target, float* loss) {
@@ -429,7 +440,7 @@ int cdm_net_backward(cdm_net* net, const float* target, float* loss) {
   int rc = n.backward();
   if (rc != CDM_OK) return rc;
   *loss = n.read_loss();
-  return CDM_OK;
+  return n.conv_status();
 }
 
 int cdm_net_train_step(cdm_net* net, const cdm_net_batch* bt, float lr, float* loss) {
@@ -500,7 +511,7 @@ int cdm_net_train_step(cdm_net* net, const cdm_net_batch* bt, float lr, float* l
   rc = n.adam_step(lr);
   if (rc != CDM_OK) return rc;
   *loss = n.read_loss();
-  return CDM_OK;
+  return n.conv_status();
 }
 
 int cdm_net_predict(cdm_net* net, const double* tprev, const double* tcur, const double* J, int ni, int nj,
@@ -554,7 +565,7 @@ int cdm_net_predict(cdm_net* net, const double* tprev, const double* tcur, const
   CDM_CK(cudaMemcpyAsync(u0, tcur, (size_t)nx * ny * sizeof(double), cudaMemcpyDeviceToDevice, n.stream));
   CDM_CK(cdm::net::apply_guess(tprev, tcur, y, ystride, n.d_scale, u0, ni, nj, nx, nhalo, n.stream));
   CDM_CK(cudaStreamSynchronize(n.stream));
-  return CDM_OK;
+  return n.conv_status();
 }
 
 }  // extern "C"

@@ -13,6 +13,8 @@
 #include "net_kernels.cuh"
 
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 
 namespace cdm {
 namespace net {
@@ -529,6 +531,9 @@ cudaError_t launch_wgrad(const WgradArgs& a, cudaStream_t s) {
 }  // namespace
 
 cudaError_t conv3x3(int cin, int cout, const ConvArgs& a, cudaStream_t s) {
+  const char* path = std::getenv("CDM_NET_CONV");
+  const bool mma_only = path && std::strcmp(path, "mma") == 0;
+  if (!mma_only && conv3x3_tc_supported(cin, cout, a.W)) return conv3x3_tc(cin, cout, a, s);
   if (cin == 16 && cout == 32) return launch_conv<16, 32>(a, s);
   if (cin == 32 && cout == 32) return launch_conv<32, 32>(a, s);
   if (cin == 32 && cout == 16) return launch_conv<32, 16>(a, s);

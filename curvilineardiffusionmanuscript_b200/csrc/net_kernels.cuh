@@ -2,7 +2,8 @@
 //
 // Tensors are NHWC bf16 (channels innermost), one image per batch entry.  The
 // 3x3 convolutions ("same" size, zero padding) are implicit GEMMs on the tensor
-// cores (mma.sync m16n8k16, bf16 inputs, FP32 accumulation):
+// cores (tcgen05.mma for widths that are multiples of 128, mma.sync m16n8k16
+// otherwise and for the weight gradients; bf16 inputs, FP32 accumulation):
 //   forward        out[p][co] = Σ_tap Σ_ci x[p + tap][ci] · Wf[tap][co][ci]
 //   backward data  the same kernel with Wb[tap][ci][co] = W[8 - tap][ci][co]
 //   weight grads   dW[tap][ci][co] = Σ_p x[p + tap][ci] · g[p][co]
@@ -39,7 +40,16 @@ struct WgradArgs {
   int B, H, W;
 };
 
+// Dispatch: the tcgen05 kernel (net_conv_tc.cu) for images whose width is a
+// multiple of 128, the mma.sync kernel otherwise or when the environment
+// variable CDM_NET_CONV is "mma" (kept for comparisons).
 cudaError_t conv3x3(int cin, int cout, const ConvArgs& a, cudaStream_t s);
+// tcgen05 / TMA convolution (forward and backward-data), M = 128 pixels per tile
+bool conv3x3_tc_supported(int cin, int cout, int W);
+cudaError_t conv3x3_tc(int cin, int cout, const ConvArgs& a, cudaStream_t s);
+// *flag = 1 when a bounded wait of the tcgen05 convolution ran out since the last
+// call (the flag is cleared); call after the stream has been synchronised
+cudaError_t conv3x3_tc_error(int* flag);
 cudaError_t conv3x3_wgrad(int cin, int cout, const WgradArgs& a, cudaStream_t s);
 
 // elementwise helpers (C = 32 channels)
