@@ -72,6 +72,9 @@ def parse():
                     help="kernel variant, strip height, iteration block (skips the autotuner)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip the per-time-step FP64 / mixed / learned comparison of the default line")
+    ap.add_argument("--compare-steps", type=int, default=3)
     return ap.parse_args()
 
 
@@ -411,6 +414,11 @@ def run_ours(args, ws, rank, local):
         idx, what = cpu_sample(costs, ws)
         cpu = cpu_baseline([local_probs[i] for i in idx], what)
     sb.close()
+    compare = None
+    if ws == 1 and not args.no_compare and args.workload == "batch" and args.precision == "fp64":
+        del Ts, rhos, local_probs, probs
+        torch.cuda.empty_cache()
+        compare = compare_block(args, stream)
     if rank != 0:
         return
     line = {"metric": "Gcell-iter/s", "value": value, "unit": "Gcell-iter/s", "n_gpus": ws, "steps": args.steps,
@@ -419,7 +427,7 @@ def run_ours(args, ws, rank, local):
             "config": cfg, "tuning": tuning,
             "s_per_timestep": ms_max / args.steps / 1e3, "pseudo_iters_per_step": statistics.mean(iters),
             "final_residual": final, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk.summary()}
+            "clocks": clk.summary(), "compare_s_per_timestep": compare}
     print(json.dumps(line), flush=True)
 
 
@@ -480,31 +488,45 @@ def time_single(pr, precision, steps, warmup, stream, net=None):
 def train_guess(n, nseeds, nsteps, train_steps):
     """Guess network trained on APT trajectories of the multi-Gaussian problem
     (seeds disjoint from the timed problem's)."""
-    import time as _t
+    from curvilineardiffusionmanuscript_b200.train_guess import train_multigauss
+    return train_multigauss(n, nseeds, nsteps, train_steps)
+
+
+def compare_block(args, stream):
+    """Seconds per time step to the workloads' stopping rule (rel <= 1e-8 or
+    abs <= 1e-8), one GPU, CUDA events around each step's library call:
+    the 4096^2 manufactured solution in FP64 and in mixed precision (with each
+    one's error against the exact solution), and the 1024^2 multi-Gaussian in
+    FP64, mixed precision and learned guess + mixed precision, the network
+    loaded from the checkpoint the project's trainer wrote
+    (python -m curvilineardiffusionmanuscript_b200.train_guess)."""
     import torch
-    from curvilineardiffusionmanuscript_b200 import learned, problems
-    make = lambda seed: problems.multi_gaussian_2d(n, seed=seed, device="cuda")
-    t0 = _t.time()
-    skipped = []
-    trajs = learned.generate_trajectories(make, seeds=list(range(1000, 1000 + nseeds)), nsteps=nsteps,
-                                          skipped=skipped)
-    t1 = _t.time()
-    net = learned.GuessNet(seed=1)
-    pr0 = make(1000)
-    losses = learned.train(net, trajs, pr0.mesh, pr0.kappa.k0, pr0.kappa.n, steps=train_steps, batch=16, crop=128,
-                           lr=2e-3)
-    torch.cuda.synchronize()
-    info = {"apt_steps": len(trajs) * nsteps, "seeds_diverged": len(skipped), "data_s": round(t1 - t0, 1), "train_s": round(_t.time() - t1, 1),
-            "train_steps": train_steps, "loss_first": float(sum(losses[:10]) / 10),
-            "loss_last": float(sum(losses[-50:]) / 50)}
-    del trajs
-    torch.cuda.empty_cache()
-    return net, info
-
-
-def build_single(name, device):
-    from curvilineardiffusionmanuscript_b200 import problems as P
-    return [SINGLE[name][0](P, device)]
+    from curvilineardiffusionmanuscript_b200 import learned
+    from curvilineardiffusionmanuscript_b200.train_guess import DEFAULT_CHECKPOINT
+    dev = torch.device("cuda", torch.cuda.current_device())
+    out = {"steps": args.compare_steps, "warmup": 2, "timing": "median of the timed steps"}
+    w = {}
+    for prec in ("fp64", "mixed"):
+        w[prec] = time_single(build_single("mms4096", dev)[0], prec, args.compare_steps, 2, stream)
+    w["speedup_mixed_vs_fp64"] = w["fp64"]["s_per_step"] / w["mixed"]["s_per_step"]
+    out["mms2d_4096"] = w
+    w = {}
+    for prec in ("fp64", "mixed"):
+        w[prec] = time_single(build_single("multigauss1024", dev)[0], prec, args.compare_steps, 2, stream)
+    w["speedup_mixed_vs_fp64"] = w["fp64"]["s_per_step"] / w["mixed"]["s_per_step"]
+    if DEFAULT_CHECKPOINT.exists():
+        net = learned.GuessNet(seed=0)
+        net.load(DEFAULT_CHECKPOINT)
+        for prec in ("fp64", "mixed"):
+            w["learned_" + prec] = time_single(build_single("multigauss1024", dev)[0], prec, args.compare_steps, 2,
+                                               stream, net=net)
+        w["speedup_learned_mixed_vs_fp64"] = w["fp64"]["s_per_step"] / w["learned_mixed"]["s_per_step"]
+        w["checkpoint"] = str(DEFAULT_CHECKPOINT.relative_to(ROOT))
+        net.close()
+    else:
+        w["learned_mixed"] = {"unavailable": "no checkpoint at " + str(DEFAULT_CHECKPOINT.relative_to(ROOT))}
+    out["multigauss2d_1024"] = w
+    return out
 
 
 def run_compare(args):
