@@ -225,19 +225,19 @@ def oracle_steps(probs, nsteps, states=None):
     cell-iterations, and the solver states to continue from."""
     from oracle.oracle import OracleSolver
     if states is None:
+        # host copies of every input are made here, outside the timed rounds
         states = []
         for p in probs:
             o = OracleSolver(p.mesh.to("cpu"), p.bcs)
             if p.source is not None:
                 o.set_source(p.source.cpu().numpy())
-            states.append((o, p.T0.cpu().numpy().copy()))
+            states.append((o, p.T0.cpu().numpy().copy(), p.rho.cpu().numpy().copy()))
     rounds = []
     for _ in range(nsteps):
         t0 = time.perf_counter()
         ci = 0
-        for p, (o, T) in zip(probs, states):
-            st, _ = o.step(T, p.rho.cpu().numpy(), p.cp, p.kappa.k0, p.kappa.n, p.dt, rtol=p.rtol, atol=p.atol,
-                           max_iter=100000)
+        for p, (o, T, rho) in zip(probs, states):
+            st, _ = o.step(T, rho, p.cp, p.kappa.k0, p.kappa.n, p.dt, rtol=p.rtol, atol=p.atol, max_iter=100000)
             ci += p.mesh.ncells * st["niter"]
         rounds.append((time.perf_counter() - t0, ci))
     return rounds, states

@@ -701,8 +701,9 @@ def test_save_vtk_from_device_state(tmp_path, monkeypatch):
 def test_energy_balance_matches_the_oracle(case, precision):
     """Σρcₚ T J before and after the step and Δt·ΣS J (the energy balance the
     mixed path keeps in FP64) against the oracle's StepStats: relative 1e-12 for
-    the FP64 forms (summation order differs), and for mixed precision the same
-    bound before the step and the stated 1e-6 solution bound after it."""
+    the FP64 forms (summation order differs).  Mixed precision: the same bound for
+    the first step's Tⁿ and for the source term, and the stated 1e-6 solution
+    bound for every Tⁿ⁺¹ (and for the Tⁿ of later steps, the previous result)."""
     if case == "2d":
         pr = small_case_2d(ni=60, nj=47, source=True)
     else:
@@ -711,12 +712,13 @@ def test_energy_balance_matches_the_oracle(case, precision):
         pr.source = (3.0 * torch.exp(-((x - 0.4) ** 2 + (y - 0.5) ** 2 + (z - 0.6) ** 2) / 0.05)).contiguous()
     kw = dict(rtol=1e-8, atol=1e-8, max_iter=50000)
     _, _, out = run_pair(pr, nsteps=2, precision=precision, device_arrays=True, **kw)
-    for so, sg, *_ in out:
+    bound = 1e-6 if precision == "mixed" else 1e-12
+    for k, (so, sg, *_) in enumerate(out):
         assert so["status"] == 0 and sg["status"] == 0
-        for key in ("energy_before", "source_work"):
-            assert abs(sg[key] - so[key]) <= 1e-12 * abs(so[key]), (key, sg[key], so[key])
-        bound = 1e-6 if precision == "mixed" else 1e-12
-        assert abs(sg["energy_after"] - so["energy_after"]) <= bound * abs(so["energy_after"])
+        assert abs(sg["source_work"] - so["source_work"]) <= 1e-12 * abs(so["source_work"])
+        b0 = 1e-12 if k == 0 else bound
+        assert abs(sg["energy_before"] - so["energy_before"]) <= b0 * abs(so["energy_before"]), k
+        assert abs(sg["energy_after"] - so["energy_after"]) <= bound * abs(so["energy_after"]), k
         assert so["source_work"] > 0
 
 
