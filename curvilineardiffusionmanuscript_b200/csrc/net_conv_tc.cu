@@ -333,6 +333,11 @@ cudaError_t launch_tc(const ConvArgs& a, cudaStream_t s) {
   if (!grid_max) {
     cudaError_t e = cudaFuncSetAttribute(conv3x3_tc_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          smem);
+    // all of the unified L1 / shared storage as shared memory: several CTAs per SM
+    // overlap one CTA's TMA and MMAs with another's epilogue
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(conv3x3_tc_kernel<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     int dev = 0, nsm = 148, per_sm = 1;
     cudaGetDevice(&dev);
