@@ -28,7 +28,11 @@
 // domain boundary run a branch-free instantiation without ghost logic, in a
 // persistent launch whose blocks claim strips from a ticket counter (the last
 // wave is one strip long); boundary strips run the general instantiation in a
-// concurrent launch on a side stream.
+// concurrent launch on a side stream.  Strips whose ring rows are domain rows
+// run the branch-free body even when they hold a ghost column: that column's
+// rule (source column, negation or constant) is resolved per thread once per
+// strip, so only the first and last strip of each column of strips take the
+// general body.
 #include "cdm_device.cuh"
 #include "cdm_finish.cuh"
 #include "cdm_fast.cuh"
@@ -95,17 +99,22 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
   const double LLdt = P.LL / dt, VpL = P.VpL, LoVp = P.L / P.Vpdtau, VpoL = P.Vpdtau / P.L;
   const int kmode = P.kmode, km = P.km, khalf = P.khalf;
   const double kn = P.kn;
-  const bool colIn = EDGE ? (a >= 0 && a < ni) : true;
+  // EDGE = false: the strip's rows and its two ring rows are domain rows, but its
+  // columns may include a ghost column (a = -1 or ni), whose rule is resolved
+  // below once per strip, and inactive threads past it (a < -1 or a > ni)
+  const bool colIn = a >= 0 && a < ni;
+  const bool active = a >= -1 && a <= ni;
   const bool owner = tid >= 1 && tid <= OW && colIn;
-  const bool qx_col = EDGE ? (a >= -1 && a <= ni - 1 && tid < TX - 1) : (tid < TX - 1);
-  const bool qx_own = qx_col && (owner || (EDGE && a == -1));
-  const int col = a + nh;
+  const bool qx_col = a >= -1 && a <= ni - 1 && tid < TX - 1;
+  const bool qx_own = qx_col && (owner || a == -1);
+  // inactive threads read a domain column (their values are never used)
+  const int col = active ? a + nh : nh;
 
   // ghost rule of this thread's column (i sides), resolved once
   int cside = -1, csrc_col = col;
   bool cneg = false, cconst = false;
   double cval = 0.0;
-  if (EDGE) {
+  {
     if (a == -1) cside = 0;
     else if (a == ni) cside = 1;
     if (cside >= 0) {
@@ -133,12 +142,15 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
     L.neg = false;
     L.ua = 0.0;
     if (!EDGE) {
+      // u of the cell the column rule reads (the cell itself off the ghost column)
+      const int so = csrc_col + nx * (r + nh);
       L.off = ro;
-      L.u = WAVE ? __ldcg(uin + ro) : uin[ro];
-      if (!alpha_from_u) L.ua = uprev[ro];
+      L.neg = cneg;
+      L.u = cconst ? cval : (WAVE ? __ldcg(uin + so) : uin[so]);
+      if (!alpha_from_u) L.ua = cconst ? cval : uprev[so];
       L.rho = rho[ro];
       L.qx = qx_col ? (WAVE ? __ldcg(qxin + ro) : qxin[ro]) : 0.0;
-      L.qy = WAVE ? __ldcg(qyin + ro - nx) : qyin[ro - nx];
+      L.qy = colIn ? (WAVE ? __ldcg(qyin + ro - nx) : qyin[ro - nx]) : 0.0;
       return;
     }
     int off = -2;
@@ -189,7 +201,7 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
   // diffusivity, pseudo-time parameters and update factors of cell (a, r)
   auto stage = [&](int r, const Pre& L) -> Cell {
     Cell c{0.0, 0.0, 0.0, 0.0, 0.0};
-    if (EDGE && L.off == -2) return c;
+    if (EDGE ? L.off == -2 : !active) return c;
     const double us = L.neg ? -L.u : L.u;
     const double src = alpha_from_u ? us : (L.neg ? -L.ua : L.ua);
     const double kap = isfinite(src) ? k0 * pow_fast(fabs(src), kmode, km, khalf, kn) : 0.0;
@@ -223,7 +235,7 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
       c.it = th;
     }
     // validity of α = κ/(ρcₚ) on owned cells and first-layer ghosts
-    const bool track = ((tid >= 1 && tid <= OW) || (EDGE && cside >= 0)) && track_iter;
+    const bool track = ((tid >= 1 && tid <= OW) || cside >= 0) && track_iter;
     if (track && r >= j0 - (EDGE && j0 == 0) && r < j1 + (EDGE && j1 == nj)) {
       if (!(isfinite(kap) && isfinite(rc) && rc != 0.0)) bad |= 1;
       if (kap != 0.0 && ((kap < 0.0) != (rc < 0.0))) bad |= 2;
@@ -359,7 +371,7 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
       if (EDGE && j == nj - 1) uout[o + nx] = cp1.u;
     }
     if (qx_own) qxout[o] = rqx_0;
-    if (EDGE && cside >= 0) uout[o] = sm.U[s_0][tid];
+    if (cside >= 0) uout[o] = sm.U[s_0][tid];
     // rotate: rows (j, j+1) become (j-1, j)
     g0 = cp1.g;
     f0 = cp1.f;
@@ -570,12 +582,20 @@ cudaError_t launch_march2d_wave(int tx, int harmonic, const Problem* probs, int 
 }
 
 // Is tile `tile` of a problem free of domain-boundary logic (no ghost column,
-// no ghost row in its staged rows)?  Used by the host item builder.
+// no ghost row in its staged rows)?  The FP32 correction sweep's split.
 bool march_tile_interior(int ni, int nj, int tiles_i, int strip_h, int tx, int tile) {
   const int ow = tx - 2;
   const int cb = tile % tiles_i, sj = tile / tiles_i;
   const int i0 = cb * ow, j0 = sj * strip_h, j1 = (j0 + strip_h < nj) ? j0 + strip_h : nj;
   return cb > 0 && i0 + tx - 2 < ni && j0 > 0 && j1 < nj;
+}
+
+// Does tile `tile` run the FP64 kernels' branch-free body: no ghost row among its
+// staged rows (its columns may include a ghost column, resolved per thread)?
+bool march_tile_no_ghost_rows(int nj, int tiles_i, int strip_h, int tile) {
+  const int sj = tile / tiles_i;
+  const int j0 = sj * strip_h, j1 = (j0 + strip_h < nj) ? j0 + strip_h : nj;
+  return j0 > 0 && j1 < nj;
 }
 
 template <int TX, bool HARM>

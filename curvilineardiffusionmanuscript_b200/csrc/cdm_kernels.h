@@ -33,7 +33,10 @@ struct SweepStreams {
 // interior strips claimed by persistent blocks through counters[0..1] (zero between launches)
 cudaError_t launch_march2d_fast(int variant, int harmonic, const Problem* probs, const int2* items, int n_edge,
                                 int n_int, unsigned int* counters, const SweepStreams& ss);
+// strip classification: no ghost column and no ghost row (the FP32 sweep's interior
+// kernel), and no ghost row only (the FP64 row-marching kernels' branch-free body)
 bool march_tile_interior(int ni, int nj, int tiles_i, int strip_h, int tx, int tile);
+bool march_tile_no_ghost_rows(int nj, int tiles_i, int strip_h, int tile);
 // the same kernel on the wavefront schedule: K pseudo-iterations of every problem in one
 // persistent launch, each problem's next iteration starting when its own strips are done.
 // items: each problem's strips together, boundary strips with bit 30 of the tile set.

@@ -461,7 +461,7 @@ int Engine::build_items() {
   if (ts.march == 3) {
     for (int2& it : items) {
       const ProbState& s = ps[it.x];
-      if (!march_tile_interior(s.ni, s.nj, s.tiles_i, s.strip_h, ts.tx, it.y)) it.y |= 1 << 30;
+      if (!march_tile_no_ghost_rows(s.nj, s.tiles_i, s.strip_h, it.y)) it.y |= 1 << 30;
     }
   } else if (ps.size() > 1) {
     std::vector<int2> mixed;
@@ -493,7 +493,9 @@ int Engine::build_items() {
     std::vector<int2> edge, inner;
     for (const int2& it : items) {
       const ProbState& s = ps[it.x];
-      (march_tile_interior(s.ni, s.nj, s.tiles_i, s.strip_h, ts.tx, it.y) ? inner : edge).push_back(it);
+      const bool in = precision == CDM_PREC_MIXED ? march_tile_interior(s.ni, s.nj, s.tiles_i, s.strip_h, ts.tx, it.y)
+                                                  : march_tile_no_ghost_rows(s.nj, s.tiles_i, s.strip_h, it.y);
+      (in ? inner : edge).push_back(it);
     }
     n_edge = (int)edge.size();
     items.assign(edge.begin(), edge.end());
@@ -792,7 +794,7 @@ int Engine::retile_tail() {
     hp[p].ntiles = s.ntiles;
     for (int t = 0; t < s.ntiles; ++t) {
       int2 it = make_int2(p, t);
-      if (!march_tile_interior(s.ni, s.nj, s.tiles_i, s.strip_h, ts.tx, t)) it.y |= 1 << 30;
+      if (!march_tile_no_ghost_rows(s.nj, s.tiles_i, s.strip_h, t)) it.y |= 1 << 30;
       items.push_back(it);
     }
   }
