@@ -193,6 +193,12 @@ SINGLE = {
 }
 
 
+def build_single(name, device):
+    """The one problem of a single-problem workload, built on `device`."""
+    from curvilineardiffusionmanuscript_b200 import problems as P
+    return [SINGLE[name][0](P, device)]
+
+
 def workload(name, nprob, ws):
     """(costs, build, cfg) of the whole job on ws ranks: one cost per problem
     (cells), build(indices, device) -> those problems, and the config record,

@@ -339,11 +339,22 @@ cudaError_t launch_tc(const ConvArgs& a, cudaStream_t s) {
       e = cudaFuncSetAttribute(conv3x3_tc_kernel<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
-    int dev = 0, nsm = 148, per_sm = 1;
+    // resident CTAs per SM from the SM's shared memory and registers (each CTA
+    // holds 32 of the 512 tensor-memory columns, so those never limit it)
+    int dev = 0, nsm = 148, smem_sm = 0, reserved = 0, regs_sm = 65536;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv3x3_tc_kernel<CIN, COUT>, 128, smem);
-    grid_max = nsm * (per_sm > 0 ? per_sm : 1);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    cudaFuncAttributes fa{};
+    e = cudaFuncGetAttributes(&fa, conv3x3_tc_kernel<CIN, COUT>);
+    if (e != cudaSuccess) return e;
+    const int by_smem = smem_sm / (smem + (int)fa.sharedSizeBytes + reserved);
+    const int by_regs = regs_sm / ((fa.numRegs > 0 ? fa.numRegs : 1) * 128);
+    int per_sm = by_smem < by_regs ? by_smem : by_regs;
+    per_sm = per_sm < 1 ? 1 : per_sm > 16 ? 16 : per_sm;
+    grid_max = nsm * per_sm;
   }
   const int ntiles = a.B * a.H * (a.W / TP);
   const int grid = ntiles < grid_max ? ntiles : grid_max;
