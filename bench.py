@@ -391,7 +391,8 @@ def run_ours(args, ws, rank, local):
     # the residual each problem stopped at in the last timed step (rule: rel <= 1e-8 or abs <= 1e-8)
     absr = sorted(x["abs_err"] for x in last)
     final = {"abs_err_max": absr[-1], "abs_err_median": absr[len(absr) // 2],
-             "stopped_by_rel": sum(1 for x in last if x["abs_err"] > kw["atol"]), "problems": len(last)}
+             "stopped_by_rel": sum(1 for x in last if x["abs_err"] > kw["atol"]), "problems": len(last),
+             "niter_min": min(x["niter"] for x in last), "niter_max": max(x["niter"] for x in last)}
     e2e = None
     if not args.no_e2e:
         # end to end through the public API with host (pinned) buffers
@@ -467,7 +468,7 @@ def time_single(pr, precision, steps, warmup, stream, net=None):
     T = pr.T0.clone()
     t = 0.0
     mms = pr.name == "mms_2d"
-    times, iters, restarts = [], [], []
+    times, iters, restarts, absr, initr = [], [], [], [], []
     for k in range(warmup + steps):
         if mms:
             g.set_source(problems.mms_source(pr, t + pr.dt))
@@ -483,8 +484,13 @@ def time_single(pr, precision, steps, warmup, stream, net=None):
             times.append(e0.elapsed_time(e1) / 1e3)
             iters.append(st["niter"])
             restarts.append(st["n_restarts"])
+            absr.append(st["abs_err"])
+            # the residual the relative test divides by: that of the first iteration
+            if st["rel_err"] > 0:
+                initr.append(st["abs_err"] / st["rel_err"])
     out = {"s_per_step": statistics.median(times), "iters": statistics.mean(iters),
-           "restarts": statistics.mean(restarts)}
+           "restarts": statistics.mean(restarts), "final_abs_err": statistics.mean(absr),
+           "first_residual": statistics.mean(initr) if initr else None}
     if mms:
         out["err_vs_exact"] = problems.mms_error(pr, T, t)
     g.close()

@@ -58,7 +58,9 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
   extern __shared__ __align__(16) unsigned char smem_raw[];
   M3Smem& sm = *reinterpret_cast<M3Smem*>(smem_raw);
   const int2 item = items[blockIdx.x];
-  const Problem& P = probs[item.x];
+  __shared__ __align__(16) Problem sP;
+  stage_problem<NT>(sP, probs + item.x);
+  const Problem& P = sP;
   Ctrl* C = P.ctrl;
   if (ld_cg_int(&C->done)) return;
   const int iter = ld_cg_int(&C->iter) + 1;

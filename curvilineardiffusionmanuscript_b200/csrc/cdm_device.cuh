@@ -89,6 +89,23 @@ struct Problem {
   const double* tz;
 };
 
+// Copy of a problem descriptor into shared memory by the whole block, ending
+// with a barrier.  The 3D plane march reads the descriptor's sizes, scalars
+// and array pointers throughout its loop; from shared memory those reads are
+// short-latency loads instead of L1 round trips (its register budget does not
+// hold all of them), and one copy serves a whole strip.  The 2D wavefront
+// kernel changes problem at every ticket and keeps reading the descriptor
+// from global memory: there the copy's latency, exposed once per ticket, cost
+// more than it saved.  The descriptor is constant during a launch.
+template <int NT>
+__device__ __forceinline__ void stage_problem(Problem& dst, const Problem* __restrict__ src) {
+  static_assert(sizeof(Problem) % 8 == 0, "descriptor copied in 8-byte words");
+  const long long* s = reinterpret_cast<const long long*>(src);
+  long long* d = reinterpret_cast<long long*>(&dst);
+  for (int w = threadIdx.x; w < (int)(sizeof(Problem) / 8); w += NT) d[w] = s[w];
+  __syncthreads();
+}
+
 __host__ __device__ inline int64_t fidx(const Problem& P, int a, int b, int c = 0) {
   // domain coordinates (a, b, c) -> full-array offset
   return (int64_t)(a + P.nh) + (int64_t)P.nx * ((int64_t)(b + P.nh) + (int64_t)P.ny * (int64_t)(c + (P.ndim == 3 ? P.nh : 0)));
