@@ -35,10 +35,10 @@ using fastmath::pow_fast;
 using fastmath::rcp_nr;
 using fastmath::rcp_pos;
 
-constexpr int TX = 32, TY = 8, NT = TX * TY, RX = TX + 2, RY = TY + 2;
-constexpr int NRING = RX * RY - TX * TY;  // 84 ring cells per plane
-
+// column tile of TX x TY cells, one thread per column; RX x RY with the ring
+template <int TX, int TY>
 struct M3Smem {
+  static constexpr int RX = TX + 2, RY = TY + 2, NT = TX * TY;
   double U[2][RY][RX], IA[2][RY][RX], IT[2][RY][RX];  // staged cells of planes z, z+1
   double QI[3][RY][TX + 1], QJ[3][TY + 1][RX], QK[2][RY][RX];  // new damped fluxes
   double PI[3][RY][TX + 1], PJ[3][TY + 1][RX], PK[2][RY][RX];  // undamped (check iterations)
@@ -52,11 +52,15 @@ struct C3 {
 
 }  // namespace
 
-template <bool HARM, bool EDGE>
-__global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict__ probs,
-                                                      const int2* __restrict__ items) {
+template <bool HARM, bool EDGE, int TX, int TY>
+__global__ void __launch_bounds__(TX * TY, 2) march3d_fast(const Problem* __restrict__ probs,
+                                                           const int2* __restrict__ items) {
+  constexpr int NT = TX * TY, RX = TX + 2, RY = TY + 2;
+  constexpr int NRING = RX * RY - NT;  // ring cells per plane (84 for 32 x 8, 68 for 16 x 16)
+  static_assert(NRING <= NT, "one ring cell per thread at most");
+  using Smem = M3Smem<TX, TY>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  M3Smem& sm = *reinterpret_cast<M3Smem*>(smem_raw);
+  Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
   const int2 item = items[blockIdx.x];
   __shared__ __align__(16) Problem sP;
   stage_problem<NT>(sP, probs + item.x);
@@ -549,15 +553,16 @@ __global__ void __launch_bounds__(NT, 2) march3d_fast(const Problem* __restrict_
   finish_iteration<NT>(P, C, tile, iter, check, local, local_nan, bad, sm.red, &sm.flag);
 }
 
-template <bool HARM>
+template <bool HARM, int TX, int TY>
 static cudaError_t launch3m(const Problem* probs, const int2* items, int n_edge, int n_int, const SweepStreams& ss) {
+  constexpr int NT = TX * TY, bytes = (int)sizeof(M3Smem<TX, TY>);
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(march3d_fast<HARM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sizeof(M3Smem));
+    cudaError_t e = cudaFuncSetAttribute(march3d_fast<HARM, true, TX, TY>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(march3d_fast<HARM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)sizeof(M3Smem));
+      e = cudaFuncSetAttribute(march3d_fast<HARM, false, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               bytes);
     if (e != cudaSuccess) return e;
     attr = true;
   }
@@ -568,8 +573,9 @@ static cudaError_t launch3m(const Problem* probs, const int2* items, int n_edge,
     if ((e = cudaEventRecord(ss.ev_fork, ss.main)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(ss.side, ss.ev_fork, 0)) != cudaSuccess) return e;
   }
-  if (n_edge > 0) march3d_fast<HARM, true><<<n_edge, NT, sizeof(M3Smem), fork ? ss.side : ss.main>>>(probs, items);
-  if (n_int > 0) march3d_fast<HARM, false><<<n_int, NT, sizeof(M3Smem), ss.main>>>(probs, items + n_edge);
+  if (n_edge > 0)
+    march3d_fast<HARM, true, TX, TY><<<n_edge, NT, bytes, fork ? ss.side : ss.main>>>(probs, items);
+  if (n_int > 0) march3d_fast<HARM, false, TX, TY><<<n_int, NT, bytes, ss.main>>>(probs, items + n_edge);
   if (fork) {
     if ((e = cudaEventRecord(ss.ev_join, ss.side)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(ss.main, ss.ev_join, 0)) != cudaSuccess) return e;
@@ -577,17 +583,25 @@ static cudaError_t launch3m(const Problem* probs, const int2* items, int n_edge,
   return cudaGetLastError();
 }
 
-cudaError_t launch_march3d_fast(int harmonic, const Problem* probs, const int2* items, int n_edge, int n_int,
-                                const SweepStreams& ss) {
-  return harmonic ? launch3m<true>(probs, items, n_edge, n_int, ss) : launch3m<false>(probs, items, n_edge, n_int, ss);
+// column tiles of tx x ty cells: 32 x 8 or 16 x 16 (a shorter ring: 68 ring cells
+// and 164 ring faces per 256 cells instead of 84 and 208)
+cudaError_t launch_march3d_fast(int harmonic, int tx, int ty, const Problem* probs, const int2* items, int n_edge,
+                                int n_int, const SweepStreams& ss) {
+  if (tx == 32 && ty == 8)
+    return harmonic ? launch3m<true, 32, 8>(probs, items, n_edge, n_int, ss)
+                    : launch3m<false, 32, 8>(probs, items, n_edge, n_int, ss);
+  if (tx == 16 && ty == 16)
+    return harmonic ? launch3m<true, 16, 16>(probs, items, n_edge, n_int, ss)
+                    : launch3m<false, 16, 16>(probs, items, n_edge, n_int, ss);
+  return cudaErrorInvalidValue;
 }
 
 // Is column tile `tile` (any strip) of a 3D problem free of (i, j) ghost logic:
 // its cells and their one-cell ring all domain cells?
-bool march3d_tile_interior(int ni, int nj, int tiles_i, int tiles_j, int tile) {
+bool march3d_tile_interior(int ni, int nj, int tiles_i, int tiles_j, int tx, int ty, int tile) {
   const int ti = tile % tiles_i, tj = (tile / tiles_i) % tiles_j;
-  const int i0 = ti * TX, j0 = tj * TY;
-  return i0 >= 1 && i0 + TX + 1 <= ni && j0 >= 1 && j0 + TY + 1 <= nj;
+  const int i0 = ti * tx, j0 = tj * ty;
+  return i0 >= 1 && i0 + tx + 1 <= ni && j0 >= 1 && j0 + ty + 1 <= nj;
 }
 
 }  // namespace cdm

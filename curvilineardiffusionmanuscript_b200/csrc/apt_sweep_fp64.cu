@@ -385,13 +385,14 @@ static const TileShape kShapes2D[] = {
     {128, 0, 0, 128, 1}, {64, 0, 0, 64, 1}, {32, 16, 1, 256, 0}, {32, 8, 1, 256, 0}, {128, 0, 0, 128, 3},
     {64, 0, 0, 64, 3},
 };
-// 3D: variant 0 is the plane-marching kernel (reciprocal form); the tile
-// kernels keep the operation-for-operation form
+// 3D: variants 0 and 3 are the plane-marching kernel (reciprocal form) on
+// 32 x 8 and 16 x 16 column tiles; the tile kernels (1, 2) keep the
+// operation-for-operation form
 static const TileShape kShapes3D[] = {
-    {32, 8, 1, 256, 2}, {32, 4, 4, 256, 0}, {16, 8, 4, 256, 0},
+    {32, 8, 1, 256, 2}, {32, 4, 4, 256, 0}, {16, 8, 4, 256, 0}, {16, 16, 1, 256, 2},
 };
 
-int num_tile_shapes(int ndim) { return ndim == 2 ? 6 : 3; }
+int num_tile_shapes(int ndim) { return ndim == 2 ? 6 : 4; }
 TileShape tile_shape(int ndim, int v) { return ndim == 2 ? kShapes2D[v] : kShapes3D[v]; }
 
 template <int TX, int TY, int TZ, int NT>
@@ -428,7 +429,11 @@ cudaError_t launch_sweep_fp64(int ndim, int variant, int exact, int harmonic, co
     return cudaGetLastError();
   }
   switch (variant) {
-    case 0: return launch_march3d_fast(harmonic, probs, items, n_edge, nitems - n_edge, ss);
+    case 0:
+    case 3: {
+      const TileShape ts = kShapes3D[variant];
+      return launch_march3d_fast(harmonic, ts.tx, ts.ty, probs, items, n_edge, nitems - n_edge, ss);
+    }
     case 1: return launch3<32, 4, 4, 256>(probs, items, nitems, s);
     default: return launch3<16, 8, 4, 256>(probs, items, nitems, s);
   }

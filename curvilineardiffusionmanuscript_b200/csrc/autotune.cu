@@ -37,7 +37,9 @@ constexpr int kWaveBlock[] = {8, 16, 32};
 // 18..26 (2D FP64, reciprocal form): the marching kernel on the wavefront schedule
 // (variant 4), strip height kWaveH[t / 3], iterations per launch kWaveBlock[t % 3];
 // 27..35: the same with 64-thread blocks (variant 5), which leave fewer columns of
-// a narrow problem's last block idle
+// a narrow problem's last block idle.  3D FP64 (reciprocal form): 0..11 the plane
+// march on 32 x 8 column tiles, 12..23 on 16 x 16 tiles (variant 3), strip height
+// kStripH[c / 3] and block kBlock[c % 3] in both
 constexpr int kNumMarch = 4 * kNumBlock;
 constexpr int kNumTile = kNumMarch + 2 * kNumBlock;
 constexpr int kNumCand = kNumTile + 18;
@@ -46,8 +48,12 @@ struct Cand {
   int variant, strip_h, block;
 };
 
-Cand candidate(int c) {
+Cand candidate(int c, int ndim) {
   if (c < kNumMarch) return {0, kStripH[c / kNumBlock], kBlock[c % kNumBlock]};
+  if (ndim == 3) {
+    const int t = c - kNumMarch;
+    return {3, kStripH[t / kNumBlock], kBlock[t % kNumBlock]};
+  }
   if (c < kNumTile) {
     const int t = c - kNumMarch;
     return {2 + t / kNumBlock, 0, kBlock[t % kNumBlock]};
@@ -121,11 +127,12 @@ int Engine::autotune(double* const* T, const double* const* rho, const double* c
   if (!tile_shape(ndim, variant).march) return CDM_OK;  // the 3D tile kernels have no strip height
   // the tile kernels are candidates for 2D FP64 (the mixed sweeps use the marching layout),
   // the wavefront schedule for the reciprocal form
-  const int ncand = (ndim != 2 || precision == CDM_PREC_MIXED) ? kNumMarch
+  const int ncand = ndim == 3 ? (precision == CDM_PREC_FP64 ? 2 * kNumMarch : kNumMarch)
+                    : precision == CDM_PREC_MIXED ? kNumMarch
                     : (precision == CDM_PREC_FP64_EXACT ? kNumTile : kNumCand);
   const std::string key = fingerprint(*this);
   auto apply = [&](int c) -> int {
-    const Cand k = candidate(c);
+    const Cand k = candidate(c, ndim);
     variant = k.variant;
     strip_h_override = k.strip_h;
     tuned_iter_block = k.block;
@@ -260,7 +267,8 @@ extern "C" int cdm_batch_set_tuning(cdm_batch* b, int variant, int strip_h, int 
   const bool exact3d = e.ndim == 3 && e.precision == CDM_PREC_FP64_EXACT;
   bool ok = variant >= 0 && variant < nv && strip_h >= 0 && iter_block >= 1 && iter_block <= 64;
   if (e.precision == CDM_PREC_MIXED) ok = ok && variant == 0;           // FP32 sweeps march
-  if (e.ndim == 3) ok = ok && (exact3d ? variant != 0 : variant == 0);  // 3D: form fixes the kernel
+  // 3D: the form fixes the kernel (tile kernels for the exact form, the plane march otherwise)
+  if (e.ndim == 3) ok = ok && (exact3d ? (variant == 1 || variant == 2) : (variant == 0 || variant == 3));
   if (variant >= 4) ok = ok && e.precision == CDM_PREC_FP64;              // wavefront: reciprocal form
   if (!ok) {
     cdm::set_error("cdm_batch_set_tuning: variant, strip height or block length not valid for this batch");

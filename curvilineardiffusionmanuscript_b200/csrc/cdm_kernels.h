@@ -52,9 +52,9 @@ int march2d_wave_slots(int tx, int harmonic);
 cudaError_t launch_wave_wait_probe(const int* count, unsigned int* err, double limit_s, cudaStream_t s);
 // 3D plane-marching kernel (reciprocal form); items are (problem, column tile + strip),
 // items[0, n_edge) tiles touching the (i, j) boundary, then n_int interior tiles
-cudaError_t launch_march3d_fast(int harmonic, const Problem* probs, const int2* items, int n_edge, int n_int,
-                                const SweepStreams& ss);
-bool march3d_tile_interior(int ni, int nj, int tiles_i, int tiles_j, int tile);
+cudaError_t launch_march3d_fast(int harmonic, int tx, int ty, const Problem* probs, const int2* items, int n_edge,
+                                int n_int, const SweepStreams& ss);
+bool march3d_tile_interior(int ni, int nj, int tiles_i, int tiles_j, int tx, int ty, int tile);
 
 // one fused FP64 pseudo-iteration over all items (problem, tile)
 // exact = 1: operation-for-operation reference arithmetic (bit-identical to the

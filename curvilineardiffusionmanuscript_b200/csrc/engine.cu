@@ -484,7 +484,7 @@ int Engine::build_items() {
     std::vector<int2> edge, inner;
     for (const int2& it : items) {
       const ProbState& s = ps[it.x];
-      (march3d_tile_interior(s.ni, s.nj, s.tiles_i, s.tiles_j, it.y) ? inner : edge).push_back(it);
+      (march3d_tile_interior(s.ni, s.nj, s.tiles_i, s.tiles_j, ts.tx, ts.ty, it.y) ? inner : edge).push_back(it);
     }
     n_edge = (int)edge.size();
     items.assign(edge.begin(), edge.end());

@@ -13,12 +13,15 @@
 // bytes further on, so the nine taps need no copies.  Weights [tap][co][ci] sit
 // in shared memory as [tap][channel group][co][8 channels] for the whole launch.
 //
-// A CTA of 128 threads is persistent over tiles.  Thread 0 issues the TMA of
-// the next tile into the other halo buffer, then the 9·CIN/16 MMAs of this tile
-// (one instruction each, M = 128, N = COUT, K = 16) and commits them to an
-// mbarrier; the four warps then read the accumulator (warp w: TMEM lanes
-// 32w..32w+31, one pixel per thread, COUT fp32 columns), apply bias and ReLU or
-// the ReLU mask, and store bf16 (or fp32) NHWC rows.  Every wait on an mbarrier
+// A CTA of 128 threads is persistent over tiles, with two halo buffers and two
+// accumulators (64 tensor-memory columns).  Thread 0 issues the 9·CIN/16 MMAs
+// of a tile (one instruction each, M = 128, N = COUT, K = 16) and commits them
+// to that accumulator's mbarrier; the MMAs of tile j + 1 are issued before the
+// block's epilogue of tile j, so the tensor core works while the four warps
+// read accumulator j & 1 (warp w: TMEM lanes 32w..32w+31, one pixel per
+// thread, COUT fp32 columns), apply bias and ReLU or the ReLU mask and store
+// bf16 (or fp32) NHWC rows; the TMA of tile j + 2 goes out as soon as tile j's
+// MMAs have released its halo buffer.  Every wait on an mbarrier
 // is bounded; a wait that runs out sets the error word the host checks, and the
 // CTA waits (bounded) for its own copies and MMAs before it frees its tensor
 // memory.
@@ -147,7 +150,7 @@ struct TcSmem {
   alignas(128) unsigned char w[9 * CG * COUT * 16];
   float bias[COUT];
   unsigned long long bar_tma[2];
-  unsigned long long bar_mma;
+  unsigned long long bar_mma[2];
   uint32_t tmem_base;
   int err;
 };
@@ -175,12 +178,13 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__
   if (tid == 0) {
     mbar_init(smem_addr(&sm.bar_tma[0]), 1);
     mbar_init(smem_addr(&sm.bar_tma[1]), 1);
-    mbar_init(smem_addr(&sm.bar_mma), 1);
+    mbar_init(smem_addr(&sm.bar_mma[0]), 1);
+    mbar_init(smem_addr(&sm.bar_mma[1]), 1);
     sm.err = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) {  // 32 columns of tensor memory: the fp32 accumulator (N <= 32)
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(smem_addr(&sm.tmem_base)));
+  if (warp == 0) {  // 64 columns of tensor memory: two fp32 accumulators (N <= 32 each)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(smem_addr(&sm.tmem_base)));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   // the generic-proxy weight stores become visible to the tensor cores' reads
@@ -201,99 +205,138 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__
       tma_load_4d(smem_addr(sm.halo[buf] + g * PLANE), &xmap, bar, 8 * g, x0 - 1, y - 1, b);
   };
 
-  if (tid == 0 && (int)blockIdx.x < ntiles) issue_tma(blockIdx.x, 0);
-  int it = 0;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
-    const int buf = it & 1;
-    if (tid == 0) {
-      const int nxt = t + gridDim.x;
-      if (nxt < ntiles) issue_tma(nxt, buf ^ 1);  // that buffer's MMAs completed last iteration
-      if (!mbar_wait(smem_addr(&sm.bar_tma[buf]), (it >> 1) & 1)) {
-        sm.err = 1;
-      } else {
-        tc_fence_after();
-        const uint32_t hb = smem_addr(sm.halo[buf]), wb = smem_addr(sm.w);
-        int k = 0;
+  // this CTA's tiles: blockIdx.x + j·gridDim.x, j < nt
+  const int nt = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  auto tile_of = [&](int j) { return (int)blockIdx.x + j * (int)gridDim.x; };
+  // the nine taps' MMAs of halo buffer hb into accumulator ab, committed to bar_mma[ab]
+  auto issue_mmas = [&](int hb, int ab) {
+    tc_fence_after();
+    const uint32_t hs = smem_addr(sm.halo[hb]), wb = smem_addr(sm.w);
+    int k = 0;
 #pragma unroll
-        for (int tap = 0; tap < 9; ++tap) {
-          const int dy = tap / 3, dx = tap - 3 * (tap / 3);
+    for (int tap = 0; tap < 9; ++tap) {
+      const int dy = tap / 3, dx = tap - 3 * (tap / 3);
 #pragma unroll
-          for (int ks = 0; ks < KSTEPS; ++ks, ++k) {
-            const uint64_t ad = smem_desc(hb + 2 * ks * PLANE + (dy * HP + dx) * 16, PLANE, 128);
-            const uint64_t bd = smem_desc(wb + ((tap * CG + 2 * ks) * COUT) * 16, COUT * 16, 128);
-            mma_bf16_tc(tmem, ad, bd, idesc, k > 0 ? 1u : 0u);
-          }
-        }
-        mma_commit(smem_addr(&sm.bar_mma));
+      for (int ks = 0; ks < KSTEPS; ++ks, ++k) {
+        const uint64_t ad = smem_desc(hs + 2 * ks * PLANE + (dy * HP + dx) * 16, PLANE, 128);
+        const uint64_t bd = smem_desc(wb + ((tap * CG + 2 * ks) * COUT) * 16, COUT * 16, 128);
+        mma_bf16_tc(tmem + 32u * (uint32_t)ab, ad, bd, idesc, k > 0 ? 1u : 0u);
       }
     }
-    __syncthreads();
-    if (sm.err) break;
-    // every thread waits for the MMAs; the block agrees on the outcome
-    const bool ok = mbar_wait(smem_addr(&sm.bar_mma), it & 1);
-    if (__syncthreads_or(ok ? 0 : 1)) {
-      if (tid == 0) sm.err = 2;
-      break;
+    mma_commit(smem_addr(&sm.bar_mma[ab]));
+  };
+  // Pipeline (tile j uses halo buffer and accumulator j & 1): thread 0 issues the
+  // MMAs of tile j + 1 before the block's epilogue of tile j, and the TMA of tile
+  // j + 2 once tile j's MMAs have released its halo buffer.  Thread 0 counts what
+  // it issued and what it saw complete on each barrier, for the drain after a
+  // failed wait.
+  // (kept in scalars: counts indexed by buffer would live in local memory)
+  int tma_n0 = 0, tma_n1 = 0, tma_w0 = 0, tma_w1 = 0, mma_n0 = 0, mma_n1 = 0, mma_w0 = 0, mma_w1 = 0;
+  auto bump = [](int& c0, int& c1, int b) {
+    if (b) ++c1;
+    else ++c0;
+  };
+  bool fail = false;
+  if (tid == 0) {
+    for (int j = 0; j < 2 && j < nt; ++j) {
+      issue_tma(tile_of(j), j);
+      bump(tma_n0, tma_n1, j);
+    }
+    if (nt > 0) {
+      if (mbar_wait(smem_addr(&sm.bar_tma[0]), 0)) {
+        ++tma_w0;
+        issue_mmas(0, 0);
+        ++mma_n0;
+      } else {
+        fail = true;
+      }
+    }
+  }
+  bool failed = __syncthreads_or(fail ? 1 : 0) != 0;
+  for (int j = 0; j < nt && !failed; ++j) {
+    const int b = j & 1;
+    if (tid == 0 && j + 1 < nt) {
+      if (mbar_wait(smem_addr(&sm.bar_tma[b ^ 1]), ((j + 1) >> 1) & 1)) {
+        bump(tma_w0, tma_w1, b ^ 1);
+        issue_mmas(b ^ 1, b ^ 1);
+        bump(mma_n0, mma_n1, b ^ 1);
+      } else {
+        fail = true;
+      }
+    }
+    // this tile's MMAs (which also frees its halo buffer for tile j + 2)
+    const bool ok = mbar_wait(smem_addr(&sm.bar_mma[b]), (j >> 1) & 1);
+    if (tid == 0 && ok) {
+      bump(mma_w0, mma_w1, b);
+      if (!fail && j + 2 < nt) {
+        issue_tma(tile_of(j + 2), b);
+        bump(tma_n0, tma_n1, b);
+      }
     }
     tc_fence_after();
-    // epilogue: thread = pixel (lane 32·warp + lane of the accumulator)
-    float v[COUT];
-    tmem_load<COUT>(tmem + ((uint32_t)(32 * warp) << 16), v);
-    const int b = t / (a.H * tiles_x), r = t - b * a.H * tiles_x;
-    const int y = r / tiles_x, x = (r - y * tiles_x) * TP + 32 * warp + lane;
-    const size_t pix = ((size_t)b * a.H + y) * a.W + x;
+    if (ok) {
+      // epilogue: thread = pixel (lane 32·warp + lane of the accumulator)
+      const int t = tile_of(j);
+      float v[COUT];
+      tmem_load<COUT>(tmem + ((uint32_t)(32 * warp) << 16) + 32u * (uint32_t)b, v);
+      const int bi = t / (a.H * tiles_x), r = t - bi * a.H * tiles_x;
+      const int y = r / tiles_x, x = (r - y * tiles_x) * TP + 32 * warp + lane;
+      const size_t pix = ((size_t)bi * a.H + y) * a.W + x;
 #pragma unroll
-    for (int co = 0; co < COUT; ++co) v[co] += sm.bias[co];
-    if (a.epi == EPI_RELU) {
+      for (int co = 0; co < COUT; ++co) v[co] += sm.bias[co];
+      if (a.epi == EPI_RELU) {
 #pragma unroll
-      for (int co = 0; co < COUT; ++co) v[co] = fmaxf(v[co], 0.f);
-    } else if (a.epi == EPI_MASK) {
+        for (int co = 0; co < COUT; ++co) v[co] = fmaxf(v[co], 0.f);
+      } else if (a.epi == EPI_MASK) {
 #pragma unroll
-      for (int c8 = 0; c8 < COUT / 8; ++c8) {
-        const uint4 mk = *reinterpret_cast<const uint4*>(a.mask + pix * COUT + 8 * c8);
-        const __nv_bfloat162* m2 = reinterpret_cast<const __nv_bfloat162*>(&mk);
+        for (int c8 = 0; c8 < COUT / 8; ++c8) {
+          const uint4 mk = *reinterpret_cast<const uint4*>(a.mask + pix * COUT + 8 * c8);
+          const __nv_bfloat162* m2 = reinterpret_cast<const __nv_bfloat162*>(&mk);
 #pragma unroll
-        for (int h = 0; h < 4; ++h) {
-          if (!(__bfloat162float(m2[h].x) > 0.f)) v[8 * c8 + 2 * h] = 0.f;
-          if (!(__bfloat162float(m2[h].y) > 0.f)) v[8 * c8 + 2 * h + 1] = 0.f;
+          for (int h = 0; h < 4; ++h) {
+            if (!(__bfloat162float(m2[h].x) > 0.f)) v[8 * c8 + 2 * h] = 0.f;
+            if (!(__bfloat162float(m2[h].y) > 0.f)) v[8 * c8 + 2 * h + 1] = 0.f;
+          }
         }
       }
-    }
-    if (a.out) {
+      if (a.out) {
 #pragma unroll
-      for (int c8 = 0; c8 < COUT / 8; ++c8) {
-        uint4 o;
-        __nv_bfloat162* o2 = reinterpret_cast<__nv_bfloat162*>(&o);
+        for (int c8 = 0; c8 < COUT / 8; ++c8) {
+          uint4 o;
+          __nv_bfloat162* o2 = reinterpret_cast<__nv_bfloat162*>(&o);
 #pragma unroll
-        for (int h = 0; h < 4; ++h) o2[h] = __floats2bfloat162_rn(v[8 * c8 + 2 * h], v[8 * c8 + 2 * h + 1]);
-        *reinterpret_cast<uint4*>(a.out + pix * COUT + 8 * c8) = o;
+          for (int h = 0; h < 4; ++h) o2[h] = __floats2bfloat162_rn(v[8 * c8 + 2 * h], v[8 * c8 + 2 * h + 1]);
+          *reinterpret_cast<uint4*>(a.out + pix * COUT + 8 * c8) = o;
+        }
+      }
+      if (a.out_f32) {
+#pragma unroll
+        for (int c4 = 0; c4 < COUT / 4; ++c4)
+          *reinterpret_cast<float4*>(a.out_f32 + pix * COUT + 4 * c4) =
+              make_float4(v[4 * c4], v[4 * c4 + 1], v[4 * c4 + 2], v[4 * c4 + 3]);
       }
     }
-    if (a.out_f32) {
-#pragma unroll
-      for (int c4 = 0; c4 < COUT / 4; ++c4)
-        *reinterpret_cast<float4*>(a.out_f32 + pix * COUT + 4 * c4) =
-            make_float4(v[4 * c4], v[4 * c4 + 1], v[4 * c4 + 2], v[4 * c4 + 3]);
-    }
-    // every lane's accumulator reads are done before the next tile's MMAs write it
+    // every lane's reads of accumulator b are done before tile j + 2's MMAs write it
     tc_fence_before();
-    __syncthreads();
+    failed = __syncthreads_or((!ok || fail) ? 1 : 0) != 0;
   }
-  __syncthreads();
-  if (sm.err && tid == 0) {
+  if (failed && tid == 0) {
     atomicExch(&g_tc_error, 1);
     // copies and MMAs issued before the failure complete (bounded waits) before
-    // the CTA leaves and frees its tensor memory: the next tile's TMA, this
-    // tile's TMA (when its wait ran out) or this tile's MMAs (when theirs did)
-    const int t = blockIdx.x + it * gridDim.x, buf = it & 1;
-    if (t + (int)gridDim.x < ntiles) mbar_wait(smem_addr(&sm.bar_tma[buf ^ 1]), ((it + 1) >> 1) & 1);
-    if (sm.err == 1) mbar_wait(smem_addr(&sm.bar_tma[buf]), (it >> 1) & 1);
-    else mbar_wait(smem_addr(&sm.bar_mma), it & 1);
+    // the CTA frees its tensor memory
+    auto drain = [&](unsigned long long* bar, int waited, int issued) {
+      while (waited < issued && mbar_wait(smem_addr(bar), waited & 1)) ++waited;
+    };
+    drain(&sm.bar_tma[0], tma_w0, tma_n0);
+    drain(&sm.bar_tma[1], tma_w1, tma_n1);
+    drain(&sm.bar_mma[0], mma_w0, mma_n0);
+    drain(&sm.bar_mma[1], mma_w1, mma_n1);
   }
   __syncthreads();
   tc_fence_after();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem));
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(tmem));
 }
+
 
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -339,8 +382,8 @@ cudaError_t launch_tc(const ConvArgs& a, cudaStream_t s) {
       e = cudaFuncSetAttribute(conv3x3_tc_kernel<CIN, COUT>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
-    // resident CTAs per SM from the SM's shared memory and registers (each CTA
-    // holds 32 of the 512 tensor-memory columns, so those never limit it)
+    // resident CTAs per SM from the SM's shared memory and registers, at most
+    // 8 (each CTA holds 64 of the SM's 512 tensor-memory columns)
     int dev = 0, nsm = 148, smem_sm = 0, reserved = 0, regs_sm = 65536;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -353,7 +396,7 @@ cudaError_t launch_tc(const ConvArgs& a, cudaStream_t s) {
     const int by_smem = smem_sm / (smem + (int)fa.sharedSizeBytes + reserved);
     const int by_regs = regs_sm / ((fa.numRegs > 0 ? fa.numRegs : 1) * 128);
     int per_sm = by_smem < by_regs ? by_smem : by_regs;
-    per_sm = per_sm < 1 ? 1 : per_sm > 16 ? 16 : per_sm;
+    per_sm = per_sm < 1 ? 1 : per_sm > 8 ? 8 : per_sm;
     grid_max = nsm * per_sm;
   }
   const int ntiles = a.B * a.H * (a.W / TP);

@@ -304,7 +304,9 @@ int cdm_batch_step(cdm_batch* b, double* const* T, const double* const* rho, con
  * tile kernels (32x16 and 32x8 tiles) x K, indices 12..17, and for the
  * reciprocal form the wavefront schedule with 128-thread blocks (variant 4) and
  * with 64-thread blocks (variant 5), each with h ∈ {16, 32, 64} x K ∈ {8, 16, 32},
- * indices 18 + 9·(variant − 4) + 3·index(h) + index(K) — from the given inputs
+ * indices 18 + 9·(variant − 4) + 3·index(h) + index(K); for 3D FP64 (reciprocal
+ * form) the plane march on 32x8 column tiles (indices 0..11) and on 16x16 column
+ * tiles (variant 3, indices 12 + 3·index(h) + index(K)) — from the given inputs
  * (arguments as cdm_batch_step; T is not modified and the solver state is
  * restored after every trial) and keeps the fastest for later steps.  With
  * cache_path not NULL the choice is read from / written to that JSON file,
@@ -313,8 +315,9 @@ int cdm_batch_step(cdm_batch* b, double* const* T, const double* const* rho, con
 int cdm_batch_autotune(cdm_batch* b, double* const* T, const double* const* rho, const double* cp,
                        const cdm_kappa* kappa, const double* dt, const cdm_step_opts* opts,
                        const char* cache_path, int* chosen);
-/* kernel variant (0 marching; 1 marching with 64-thread blocks; 2, 3 tile kernels;
- * 4, 5 marching on the wavefront schedule with 128- / 64-thread blocks), strip height
+/* kernel variant (2D: 0 marching; 1 marching with 64-thread blocks; 2, 3 tile kernels;
+ * 4, 5 marching on the wavefront schedule with 128- / 64-thread blocks; 3D: 0, 3 plane
+ * march on 32x8 / 16x16 column tiles, 1, 2 tile kernels of the exact form), strip height
  * (0 = built-in heuristic) and iteration-block length in use */
 int cdm_batch_tuning(const cdm_batch* b, int* variant, int* strip_h, int* iter_block);
 /* apply a tuning without timing (e.g. one found by cdm_batch_autotune on another
@@ -322,8 +325,9 @@ int cdm_batch_tuning(const cdm_batch* b, int* variant, int* strip_h, int* iter_b
  * blocks), 2 or 3 (tile kernels), 4 and 5 (marching on the wavefront schedule with
  * 128- / 64-thread blocks: iter_block pseudo-iterations of every problem in one
  * persistent launch, a problem's next iteration starting as soon as its own strips
- * are done; CDM_PREC_FP64 only); 3D variant 0 (marching; the
- * exact form keeps its tile kernel); the mixed path takes variant 0 only.
+ * are done; CDM_PREC_FP64 only); 3D variant 0 (plane march on 32x8 column tiles)
+ * or 3 (on 16x16 column tiles, CDM_PREC_FP64 only); the 3D exact form keeps its tile
+ * kernels (1, 2); the mixed path takes variant 0 only.
  * iter_block in [1, 64]. */
 int cdm_batch_set_tuning(cdm_batch* b, int variant, int strip_h, int iter_block);
 int cdm_batch_get_profile(const cdm_batch* b, cdm_profile* out);
