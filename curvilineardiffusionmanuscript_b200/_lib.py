@@ -98,6 +98,7 @@ PF = C.POINTER(C.c_float)
 SIGNATURES = {
     "cdm_apt_version": (C.c_int, []),
     "cdm_selftest_bounded_wait": (C.c_int, [C.c_int, C.c_double, C.POINTER(C.c_int)]),
+    "cdm_selftest_fastmath": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double)]),
     "cdm_apt_last_error": (C.c_char_p, []),
     "cdm_step_opts_default": (None, [C.POINTER(StepOpts)]),
     "cdm_apt_config_default": (None, [C.POINTER(Config)]),

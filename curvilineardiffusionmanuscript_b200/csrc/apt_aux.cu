@@ -2,6 +2,7 @@
 #include <algorithm>
 
 #include "cdm_device.cuh"
+#include "cdm_fast.cuh"
 #include "cdm_kernels.h"
 #include "cdm_tz.cuh"
 
@@ -440,6 +441,24 @@ cudaError_t launch_step_reductions(const Problem& P, const double* u, const doub
   reduce_finish1<<<1, 32, 0, s>>>(scratch, nb, out);
   reduce_pass2<<<nb, kRedThreads, 0, s>>>(P, u, tol, out, scratch);
   reduce_finish2<<<1, 32, 0, s>>>(scratch, nb, out);
+  return cudaGetLastError();
+}
+
+// the reciprocal-form arithmetic next to CUDA's correctly rounded operations:
+// out[4i .. 4i+3] = sqrt_nr(x), sqrt(x), rcp_nr(x), 1/x
+__global__ void fastmath_probe(const double* __restrict__ x, int n, double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double v = x[i];
+  out[4 * i] = fastmath::sqrt_nr(v);
+  out[4 * i + 1] = sqrt(v);
+  out[4 * i + 2] = fastmath::rcp_nr(v);
+  out[4 * i + 3] = 1.0 / v;
+}
+
+cudaError_t launch_fastmath_probe(const double* x, int n, double* out, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  fastmath_probe<<<(n + 255) / 256, 256, 0, s>>>(x, n, out);
   return cudaGetLastError();
 }
 

@@ -1232,6 +1232,25 @@ int cdm_selftest_bounded_wait(int device, double limit_s, int* expired) {
   return CDM_OK;
 }
 
+int cdm_selftest_fastmath(int device, const double* x, int n, double* out) {
+  if (!x || !out || n <= 0 || n > (1 << 22)) {
+    cdm::set_error("cdm_selftest_fastmath: x and out must not be NULL and 0 < n <= 2^22");
+    return CDM_BAD_INPUT;
+  }
+  CDM_CK(cudaSetDevice(device));
+  double* buf = nullptr;  // n inputs, then 4n results
+  CDM_CK(cudaMalloc((void**)&buf, 5 * (size_t)n * sizeof(double)));
+  cudaError_t e = cudaMemcpy(buf, x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cdm::launch_fastmath_probe(buf, n, buf + n, nullptr);
+  if (e == cudaSuccess) e = cudaMemcpy(out, buf + n, 4 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(buf);
+  if (e != cudaSuccess) {
+    cdm::set_error(std::string("cdm_selftest_fastmath: ") + cudaGetErrorString(e));
+    return CDM_CUDA_ERROR;
+  }
+  return CDM_OK;
+}
+
 const char* cdm_apt_last_error(void) { return cdm::g_error.c_str(); }
 
 void cdm_step_opts_default(cdm_step_opts* o) {

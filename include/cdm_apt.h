@@ -205,6 +205,12 @@ const char* cdm_apt_last_error(void);
  * when the wait gave up and raised the error flag, as the sweep does before
  * the host reports CDM_TIMEOUT; the context stays usable. */
 int cdm_selftest_bounded_wait(int device, double limit_s, int* expired);
+/* Diagnostic, no counterpart in the reference: the reciprocal ("fast") form's
+ * arithmetic beside CUDA's correctly rounded operations on device `device`.
+ * For the n host values x (0 < n <= 2^22), out (4n host doubles) receives per
+ * value: the Newton-refined square root, sqrt(x), the Newton-refined
+ * reciprocal, 1/x. */
+int cdm_selftest_fastmath(int device, const double* x, int n, double* out);
 void cdm_step_opts_default(cdm_step_opts* opts);
 void cdm_apt_config_default(cdm_apt_config* cfg);
 
