@@ -444,16 +444,15 @@ cudaError_t launch_step_reductions(const Problem& P, const double* u, const doub
   return cudaGetLastError();
 }
 
-// the reciprocal-form arithmetic next to CUDA's correctly rounded operations:
-// out[4i .. 4i+3] = sqrt_nr(x), sqrt(x), rcp_nr(x), 1/x
+// the reciprocal form's Newton-refined reciprocals next to CUDA's correctly
+// rounded division: out[3i .. 3i+2] = rcp_nr(x), rcp_pos(x), 1/x
 __global__ void fastmath_probe(const double* __restrict__ x, int n, double* __restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double v = x[i];
-  out[4 * i] = fastmath::sqrt_nr(v);
-  out[4 * i + 1] = sqrt(v);
-  out[4 * i + 2] = fastmath::rcp_nr(v);
-  out[4 * i + 3] = 1.0 / v;
+  out[3 * i] = fastmath::rcp_nr(v);
+  out[3 * i + 1] = fastmath::rcp_pos(v);
+  out[3 * i + 2] = 1.0 / v;
 }
 
 cudaError_t launch_fastmath_probe(const double* x, int n, double* out, cudaStream_t s) {

@@ -45,7 +45,6 @@ namespace {
 using fastmath::pow_fast;
 using fastmath::rcp_nr;
 using fastmath::rcp_pos;
-using fastmath::sqrt_nr;
 
 template <int TX>
 struct FastSmem {
@@ -208,7 +207,7 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
     const double kap = isfinite(src) ? k0 * pow_fast(fabs(src), kmode, km, khalf, kn) : 0.0;
     const double rc = L.rho * cp;
     const double inva = rc * rcp_nr(kap);
-    const double Re = kPi + sqrt_nr(kPi * kPi + LLdt * L.rho * inva);
+    const double Re = kPi + sqrt(kPi * kPi + LLdt * L.rho * inva);
     c.u = us;
     if (HARM) {
       // g = Δt/(Δt + dτ) = Δt·Re/D and f = dτ·g = Vp·L·α⁻¹·Δt/D with

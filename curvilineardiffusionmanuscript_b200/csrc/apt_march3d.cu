@@ -34,7 +34,6 @@ namespace {
 using fastmath::pow_fast;
 using fastmath::rcp_nr;
 using fastmath::rcp_pos;
-using fastmath::sqrt_nr;
 
 // column tile of TX x TY cells, one thread per column; RX x RY with the ring
 template <int TX, int TY>
@@ -136,7 +135,7 @@ __global__ void __launch_bounds__(TX * TY, 2) march3d_fast(const Problem* __rest
     const double kap = isfinite(src) ? k0c * pow_fast(fabs(src), kmode, km, khalf, kn) : 0.0;
     const double rc = rho * cp;
     const double inva = rc * rcp_nr(kap);
-    const double Re = kPi + sqrt_nr(kPi * kPi + LLdt * rho * inva);
+    const double Re = kPi + sqrt(kPi * kPi + LLdt * rho * inva);
     r.u = u;
     if (HARM) {
       // g = Δt·Re/D, f = Vp·L·α⁻¹·Δt/D with D = Δt·Re + Vp·L·α⁻¹ (one reciprocal);
@@ -218,7 +217,7 @@ __global__ void __launch_bounds__(TX * TY, 2) march3d_fast(const Problem* __rest
     const double kap = isfinite(src) ? k0c * pow_fast(fabs(src), kmode, km, khalf, kn) : 0.0;
     const double rc = rho * cp;
     const double inva = rc * rcp_nr(kap);
-    const double Re = kPi + sqrt_nr(kPi * kPi + LLdt * rho * inva);
+    const double Re = kPi + sqrt(kPi * kPi + LLdt * rho * inva);
     r.u = u;
     if (HARM) {
       const double VA = VpL * inva;

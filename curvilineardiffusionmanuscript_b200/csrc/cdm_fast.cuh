@@ -30,25 +30,6 @@ __device__ __forceinline__ double rcp_pos(double b) {
   return fma(y, e, y);
 }
 
-// √x from the hardware approximation of 1/√x: two Newton–Raphson steps on
-// y ≈ 1/√x (y ← y + y·(½ − ½x·y²)), then Markstein's correction of s = x·y
-// (s ← s + ½y·(x − s²)), which leaves s within one ulp of √x.  Arguments
-// outside [DBL_MIN, DBL_MAX] — 0, subnormals, ±inf, NaN, negatives — take the
-// IEEE square root.
-__device__ __forceinline__ double sqrt_nr(double x) {
-  if (!(x >= 2.2250738585072014e-308 && x <= 1.7976931348623157e308)) return sqrt(x);
-  double y;
-  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-  const double h = 0.5 * x;
-  double e = fma(-(h * y), y, 0.5);
-  y = fma(y, e, y);
-  e = fma(-(h * y), y, 0.5);
-  y = fma(y, e, y);
-  const double s = x * y;
-  const double r = fma(-s, s, x);
-  return fma(0.5 * y, r, s);
-}
-
 // general exponents go through pow() out of line, keeping its temporaries out
 // of the sweep's register budget
 static __device__ __noinline__ double pow_general(double x, double n) { return pow(x, n); }
@@ -61,7 +42,7 @@ __device__ __forceinline__ double pow_fast(double x, int mode, int m, int half, 
     if (m >= 2) p *= x;
     if (m >= 3) p *= x;
     for (int e = 3; e < m; ++e) p *= x;
-    if (half) p = (m >= 1) ? p * sqrt_nr(x) : sqrt_nr(x);
+    if (half) p = (m >= 1) ? p * sqrt(x) : sqrt(x);
     return p;
   }
   return pow_general(x, n);

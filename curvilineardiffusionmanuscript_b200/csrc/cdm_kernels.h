@@ -50,7 +50,7 @@ int march2d_wave_slots(int tx, int harmonic);
 // one block whose thread 0 runs the wavefront's dependency wait on *count (which
 // must stay 0) with a limit of limit_s seconds; sets *err when the wait runs out
 cudaError_t launch_wave_wait_probe(const int* count, unsigned int* err, double limit_s, cudaStream_t s);
-// sqrt_nr, sqrt, rcp_nr and 1/x of every x (4 results per x)
+// rcp_nr, rcp_pos and 1/x of every x (3 results per x)
 cudaError_t launch_fastmath_probe(const double* x, int n, double* out, cudaStream_t s);
 // 3D plane-marching kernel (reciprocal form); items are (problem, column tile + strip),
 // items[0, n_edge) tiles touching the (i, j) boundary, then n_int interior tiles

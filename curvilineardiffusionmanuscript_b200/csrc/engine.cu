@@ -1238,11 +1238,11 @@ int cdm_selftest_fastmath(int device, const double* x, int n, double* out) {
     return CDM_BAD_INPUT;
   }
   CDM_CK(cudaSetDevice(device));
-  double* buf = nullptr;  // n inputs, then 4n results
-  CDM_CK(cudaMalloc((void**)&buf, 5 * (size_t)n * sizeof(double)));
+  double* buf = nullptr;  // n inputs, then 3n results
+  CDM_CK(cudaMalloc((void**)&buf, 4 * (size_t)n * sizeof(double)));
   cudaError_t e = cudaMemcpy(buf, x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cdm::launch_fastmath_probe(buf, n, buf + n, nullptr);
-  if (e == cudaSuccess) e = cudaMemcpy(out, buf + n, 4 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(out, buf + n, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
   cudaFree(buf);
   if (e != cudaSuccess) {
     cdm::set_error(std::string("cdm_selftest_fastmath: ") + cudaGetErrorString(e));

@@ -206,10 +206,10 @@ const char* cdm_apt_last_error(void);
  * the host reports CDM_TIMEOUT; the context stays usable. */
 int cdm_selftest_bounded_wait(int device, double limit_s, int* expired);
 /* Diagnostic, no counterpart in the reference: the reciprocal ("fast") form's
- * arithmetic beside CUDA's correctly rounded operations on device `device`.
- * For the n host values x (0 < n <= 2^22), out (4n host doubles) receives per
- * value: the Newton-refined square root, sqrt(x), the Newton-refined
- * reciprocal, 1/x. */
+ * Newton-refined reciprocals beside CUDA's correctly rounded division on device
+ * `device`.  For the n host values x (0 < n <= 2^22), out (3n host doubles)
+ * receives per value: the general refined reciprocal (0 and inf kept), the
+ * refined reciprocal for positive normal arguments, 1/x. */
 int cdm_selftest_fastmath(int device, const double* x, int n, double* out);
 void cdm_step_opts_default(cdm_step_opts* opts);
 void cdm_apt_config_default(cdm_apt_config* cfg);
