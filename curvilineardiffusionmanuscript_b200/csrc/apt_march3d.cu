@@ -16,12 +16,16 @@
 // the owned cells per plane and nothing along k.  Ghost cells come from the
 // boundary rules of every side applied on the fly (boundary_operators.jl).
 //
-// Two instantiations: EDGE for tiles whose (i, j) ring touches the domain
-// boundary (general ghost logic per cell), and the interior one, whose cells
-// and ring are all domain cells in (i, j): no per-cell classification, the
-// k-ghost planes handled per plane (block-uniform), and the loads that stage
-// plane z + 2 (u, ρ, uⁿ) issued while plane z is updated, so that their latency
-// overlaps a whole plane of work.  The two run as concurrent launches.
+// Both kinds of tile issue the loads that stage plane z + 2 (u, ρ, uⁿ) while
+// plane z is updated, so that their latency overlaps a whole plane of work,
+// and resolve the k-ghost planes once per plane (block-uniform).  Two
+// instantiations: the interior one, for tiles whose cells and ring are all
+// domain cells in (i, j), and EDGE, for tiles whose ring touches the (i, j)
+// boundary, where every thread resolves its own and its ring cell's column
+// once per strip (a domain column, an i- or j-ghost column with its side's
+// rule, or no cell) and which adds the domain-range tests of partial tiles,
+// the boundary-face writes and the ghost writes of the update.  The two run as
+// concurrent launches.
 #include "cdm_device.cuh"
 #include "cdm_fast.cuh"
 #include "cdm_finish.cuh"
@@ -116,22 +120,103 @@ __global__ void __launch_bounds__(TX * TY, 2) march3d_fast(const Problem* __rest
   int bad = 0;
   // validity bits of α: read for a step's last iteration only (a check iteration or the one past max_iter)
   const bool track_iter = check || iter > C->max_iter;
-  // stage cell (a, b, c): u with its ghost rule, pseudo-time parameters and
-  // update factors (iteration_parameters.jl:2-15 in reciprocal form)
-  auto stage = [&](int a, int b, int c, bool track) -> C3 {
-    C3 r{0.0, 0.0, 0.0, 0.0, 0.0};
-    const int cls = classify(P, a, b, c);
-    if (cls < 0) return r;
-    const int64_t id = fidx(P, a, b, c);
-    double u, src;
-    if (cls == 6) {
-      u = uin[id];
-      src = alpha_from_u ? u : P.u_prev[id];
-    } else {
-      u = ghost_value(P, uin, cls, a, b, c);
-      src = alpha_from_u ? u : ghost_value(P, P.u_prev, cls, a, b, c);
+  // raw loads of a cell of plane c (u and uⁿ from the cell the ghost rules
+  // read, ρ of the cell itself), issued a plane ahead of stage_pre; mode: 0
+  // copy, 1 negate, 2 constant (the value already in u and up), 3 no cell (a
+  // corner ghost or a position outside the ghost layer: staged as zeros)
+  struct Pre3 {
+    double u, rho, up;
+    int mode;
+  };
+  const int64_t plane_sz = (int64_t)P.nx * P.ny;
+  const int64_t own_col = fidx(P, oa, ob, 0);
+  const int64_t ring_col = rx >= 0 ? fidx(P, ra, rb, 0) : own_col;
+  // (i, j) source of a cell's column, fixed for the strip: kind 0 a domain
+  // column (the k-ghost rule of each plane applies), 1 / 2 / 3 a first-layer i-
+  // or j-ghost column whose side's rule copies / negates the column at `off`
+  // or is the side's constant (boundary_operators.jl), 4 neither; the side
+  // sits in bits 3 and up.  Interior tiles have domain columns only.
+  struct ColSrc {
+    int64_t off;
+    int code;
+  };
+  auto col_src = [&](int a, int b) -> ColSrc {
+    ColSrc r{0, 0};
+    if (!EDGE) return r;
+    const bool ia = a >= 0 && a < ni, ib = b >= 0 && b < nj;
+    if (ia && ib) return r;
+    int side = -1;
+    if (ib && (a == -1 || a == ni)) side = a < 0 ? 0 : 1;
+    else if (ia && (b == -1 || b == nj)) side = b < 0 ? 2 : 3;
+    r.code = 4;
+    if (side < 0) return r;
+    const int rule = P.rule[side];
+    if (rule == GR_DIRICHLET) {
+      r.code = 3 | (side << 3);
+      return r;
     }
-    const double rho = P.rho[id];
+    const bool lo = (side & 1) == 0;
+    const int n = side < 2 ? ni : nj;
+    const int pos = rule == GR_NONE ? (lo ? -1 : n) : rule == GR_PERIODIC ? (lo ? n - 1 : 0) : (lo ? 0 : n - 1);
+    r.off = side < 2 ? fidx(P, pos, b, 0) : fidx(P, a, pos, 0);
+    r.code = rule == GR_NEGSYM ? 2 : 1;
+    return r;
+  };
+  const ColSrc own_src = col_src(oa, ob);
+  const ColSrc ring_src = rx >= 0 ? col_src(ra, rb) : ColSrc{0, 4};
+  // k-ghost rule of plane c (block-uniform): source plane, 1 negate, 2 constant
+  auto kplane = [&](int c, int& cs, int& mode, double& cv) {
+    cs = c;
+    mode = 0;
+    cv = 0.0;
+    if (c >= 0 && c < nk) return;
+    const int side = c < 0 ? 4 : 5;
+    const int rule = P.rule[side];
+    const bool lo = side == 4;
+    if (rule == GR_DIRICHLET) {
+      mode = 2;
+      cv = P.val[side];
+    } else if (rule == GR_PERIODIC) {
+      cs = lo ? nk - 1 : 0;
+    } else if (rule != GR_NONE) {
+      cs = lo ? 0 : nk - 1;
+      mode = rule == GR_NEGSYM ? 1 : 0;
+    }
+  };
+  auto load_cell = [&](const ColSrc& cd, int64_t col, int c, int cs, int kmode, double kcv, Pre3& L) {
+    const int kind = cd.code & 7;
+    if (kind == 0) {
+      L.mode = kmode;
+      L.rho = P.rho[col + plane_sz * c];
+      L.u = kmode == 2 ? kcv : uin[col + plane_sz * cs];
+      L.up = (!alpha_from_u && kmode != 2) ? P.u_prev[col + plane_sz * cs] : kcv;
+    } else if (kind == 4 || c < 0 || c >= nk) {
+      L.mode = 3;
+    } else {
+      L.mode = kind == 3 ? 2 : kind - 1;
+      const double val = kind == 3 ? P.val[cd.code >> 3] : 0.0;
+      L.rho = P.rho[col + plane_sz * c];
+      L.u = L.mode == 2 ? val : uin[cd.off + plane_sz * c];
+      L.up = (!alpha_from_u && L.mode != 2) ? P.u_prev[cd.off + plane_sz * c] : val;
+    }
+  };
+  // the loads of plane c; `mode` returns the plane's k rule (the mode of every
+  // cell of an interior tile)
+  auto prefetch = [&](int c, Pre3& own, Pre3& rg, int& mode) {
+    int cs;
+    double cv;
+    kplane(c, cs, mode, cv);
+    load_cell(own_src, own_col, c, cs, mode, cv, own);
+    if (rx >= 0) load_cell(ring_src, ring_col, c, cs, mode, cv, rg);
+  };
+  // the diffusivity, pseudo-time parameters and update factors from raw loads
+  // (iteration_parameters.jl:2-15 in reciprocal form)
+  auto stage_pre = [&](const Pre3& L, int mode, bool track) -> C3 {
+    C3 r{0.0, 0.0, 0.0, 0.0, 0.0};
+    if (EDGE && mode == 3) return r;
+    const double u = mode == 1 ? -L.u : L.u;
+    const double src = alpha_from_u ? u : (mode == 1 ? -L.up : L.up);
+    const double rho = L.rho;
     const double kap = isfinite(src) ? k0c * pow_fast(fabs(src), kmode, km, khalf, kn) : 0.0;
     const double rc = rho * cp;
     const double inva = rc * rcp_nr(kap);
@@ -168,85 +253,6 @@ __global__ void __launch_bounds__(TX * TY, 2) march3d_fast(const Problem* __rest
     }
     return r;
   };
-  // interior tiles: raw loads of the cells of plane c (u from the cell the
-  // k-ghost rule reads, ρ of the cell itself), issued a plane ahead of stage_pre
-  struct Pre3 {
-    double u, rho, up;
-  };
-  const int64_t plane_sz = (int64_t)P.nx * P.ny;
-  const int64_t own_col = fidx(P, oa, ob, 0);
-  const int64_t ring_col = rx >= 0 ? fidx(P, ra, rb, 0) : own_col;
-  // k-ghost rule of plane c (block-uniform): source plane, 1 negate, 2 constant
-  auto kplane = [&](int c, int& cs, int& mode, double& cv) {
-    cs = c;
-    mode = 0;
-    cv = 0.0;
-    if (c >= 0 && c < nk) return;
-    const int side = c < 0 ? 4 : 5;
-    const int rule = P.rule[side];
-    const bool lo = side == 4;
-    if (rule == GR_DIRICHLET) {
-      mode = 2;
-      cv = P.val[side];
-    } else if (rule == GR_PERIODIC) {
-      cs = lo ? nk - 1 : 0;
-    } else if (rule != GR_NONE) {
-      cs = lo ? 0 : nk - 1;
-      mode = rule == GR_NEGSYM ? 1 : 0;
-    }
-  };
-  auto prefetch = [&](int c, Pre3& own, Pre3& rg, int& mode, double& cv) {
-    int cs;
-    kplane(c, cs, mode, cv);
-    const int64_t po = plane_sz * c, ps = plane_sz * cs;
-    own.rho = P.rho[own_col + po];
-    own.u = mode == 2 ? cv : uin[own_col + ps];
-    own.up = (!alpha_from_u && mode != 2) ? P.u_prev[own_col + ps] : cv;
-    if (rx >= 0) {
-      rg.rho = P.rho[ring_col + po];
-      rg.u = mode == 2 ? cv : uin[ring_col + ps];
-      rg.up = (!alpha_from_u && mode != 2) ? P.u_prev[ring_col + ps] : cv;
-    }
-  };
-  // the diffusivity, pseudo-time parameters and update factors from raw loads
-  auto stage_pre = [&](const Pre3& L, int mode, bool track) -> C3 {
-    C3 r{0.0, 0.0, 0.0, 0.0, 0.0};
-    const double u = mode == 1 ? -L.u : L.u;
-    const double src = alpha_from_u ? u : (mode == 1 ? -L.up : L.up);
-    const double rho = L.rho;
-    const double kap = isfinite(src) ? k0c * pow_fast(fabs(src), kmode, km, khalf, kn) : 0.0;
-    const double rc = rho * cp;
-    const double inva = rc * rcp_nr(kap);
-    const double Re = kPi + sqrt(kPi * kPi + LLdt * rho * inva);
-    r.u = u;
-    if (HARM) {
-      const double VA = VpL * inva;
-      const double dRe = dt * Re;
-      const double D = dRe + VA;
-      const bool fin = isfinite(D);
-      const double iD = rcp_pos(fin ? D : 1.0);
-      r.g = fin ? dRe * iD : 1.0;
-      r.f = fin ? VA * dt * iD : 0.0;
-      r.ia = inva;
-      r.it = VpoL * Re;
-    } else {
-      const double iRe = rcp_nr(Re);
-      double dtau = VpL * inva * iRe;
-      double th = LoVp * iRe;
-      dtau = isfinite(dtau) ? dtau : 0.0;
-      th = isfinite(th) ? th : 0.0;
-      const double idd = rcp_nr(dt + dtau);
-      r.g = dt * idd;
-      r.f = dtau * dt * idd;
-      r.ia = kap * rcp_nr(rc);
-      r.it = th;
-    }
-    if (track && track_iter) {
-      if (!(isfinite(kap) && isfinite(rc) && rc != 0.0)) bad |= 1;
-      if (kap != 0.0 && ((kap < 0.0) != (rc < 0.0))) bad |= 2;
-    }
-    return r;
-  };
   auto publish = [&](int s, const C3& own, const C3& rg) {
     sm.U[s][oy][ox] = own.u;
     sm.IA[s][oy][ox] = own.ia;
@@ -257,35 +263,21 @@ __global__ void __launch_bounds__(TX * TY, 2) march3d_fast(const Problem* __rest
       sm.IT[s][ry][rx] = rg.it;
     }
   };
-  // stage plane c into cell slot s from loads prefetched earlier (interior tiles)
+  // stage plane c into cell slot s from loads prefetched earlier; `mode` is the
+  // plane's k rule, every cell's mode on interior tiles
   auto stage_plane_pre = [&](int c, int s, const Pre3& own_l, const Pre3& rg_l, int mode) -> C3 {
     const bool inz = c >= k0 && c < k1;
-    const C3 own = stage_pre(own_l, mode, inz || c == -1 || c == nk);
-    const C3 rg = rx >= 0 ? stage_pre(rg_l, mode, inz) : C3{0.0, 0.0, 0.0, 0.0, 0.0};
+    const C3 own = stage_pre(own_l, EDGE ? own_l.mode : mode, inz || c == -1 || c == nk);
+    const C3 rg = rx >= 0 ? stage_pre(rg_l, EDGE ? rg_l.mode : mode, inz) : C3{0.0, 0.0, 0.0, 0.0, 0.0};
     publish(s, own, rg);
     return own;
   };
   // stage plane c into cell slot s: the own cell (returned) and the ring cell
   auto stage_plane = [&](int c, int s) -> C3 {
-    if (!EDGE) {
-      Pre3 lo, lr;
-      int mode;
-      double cv;
-      prefetch(c, lo, lr, mode, cv);
-      return stage_plane_pre(c, s, lo, lr, mode);
-    }
-    const bool inz = c >= k0 && c < k1;
-    const C3 own = stage(oa, ob, c, inz || c == -1 || c == nk);
-    sm.U[s][oy][ox] = own.u;
-    sm.IA[s][oy][ox] = own.ia;
-    sm.IT[s][oy][ox] = own.it;
-    if (rx >= 0) {
-      const C3 rg = stage(ra, rb, c, inz);
-      sm.U[s][ry][rx] = rg.u;
-      sm.IA[s][ry][rx] = rg.ia;
-      sm.IT[s][ry][rx] = rg.it;
-    }
-    return own;
+    Pre3 lo, lr;
+    int mode;
+    prefetch(c, lo, lr, mode);
+    return stage_plane_pre(c, s, lo, lr, mode);
   };
   auto flux = [&](double ia0, double ia1, double it0, double it1, double du, double qold, double& qp) -> double {
     if (HARM) {
@@ -474,24 +466,19 @@ __global__ void __launch_bounds__(TX * TY, 2) march3d_fast(const Problem* __rest
   load_faces(k0 + 1, k0, true, qa);  // used by the first plane of the loop
   __syncthreads();
 
-  // interior tiles: the stage loads of plane k0 + 1, for the first loop iteration
-  Pre3 p_own{0.0, 0.0, 0.0}, p_rg{0.0, 0.0, 0.0};
+  // the stage loads of plane k0 + 1, for the first loop iteration
+  Pre3 p_own{0.0, 0.0, 0.0, 3}, p_rg{0.0, 0.0, 0.0, 3};
   int p_mode = 0;
-  double p_cv = 0.0;
-  if (!EDGE) prefetch(k0 + 1, p_own, p_rg, p_mode, p_cv);
+  prefetch(k0 + 1, p_own, p_rg, p_mode);
 
   double local = 0.0;
   bool local_nan = false;
   for (int z = k0; z < k1; ++z) {
     // old fluxes of the next plane's faces, one plane ahead of their use
     if (z + 1 < k1) load_faces(z + 2, z + 1, true, qb);
-    C3 nxt;
-    if (EDGE) {
-      nxt = stage_plane(z + 1, s_p);
-    } else {
-      nxt = stage_plane_pre(z + 1, s_p, p_own, p_rg, p_mode);
-      if (z + 1 < k1) prefetch(z + 2, p_own, p_rg, p_mode, p_cv);
-    }
+    // stage plane z + 1 from its loads, then issue those of plane z + 2
+    const C3 nxt = stage_plane_pre(z + 1, s_p, p_own, p_rg, p_mode);
+    if (z + 1 < k1) prefetch(z + 2, p_own, p_rg, p_mode);
     __syncthreads();
     // own cell's coefficients: their loads overlap the face computations
     double cf[9], up = 0.0, S = 0.0;
