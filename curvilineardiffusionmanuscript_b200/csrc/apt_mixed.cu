@@ -957,7 +957,10 @@ __global__ void __launch_bounds__(NT3, 3) mixed_sweep3d(const Problem* __restric
                                                         const int2* __restrict__ items) {
   __shared__ MixSmem3 sm;
   const int2 item = items[blockIdx.x];
-  const Problem& P = probs[item.x];
+  // one descriptor copy serves the whole strip (see stage_problem)
+  __shared__ __align__(16) Problem sP;
+  stage_problem<NT3>(sP, probs + item.x);
+  const Problem& P = sP;
   Ctrl* C = P.ctrl;
   if (ld_cg_int(&C->inner_done) || ld_cg_int(&C->done)) return;
   const int kk = ld_cg_int(&C->inner_iter) + 1;  // inner iteration of this cycle

@@ -90,10 +90,11 @@ struct Problem {
 };
 
 // Copy of a problem descriptor into shared memory by the whole block, ending
-// with a barrier.  The 3D plane march reads the descriptor's sizes, scalars
-// and array pointers throughout its loop; from shared memory those reads are
-// short-latency loads instead of L1 round trips (its register budget does not
-// hold all of them), and one copy serves a whole strip.  The 2D wavefront
+// with a barrier.  The 3D plane marches (FP64 and the FP32 correction sweep)
+// read the descriptor's sizes, scalars and array pointers throughout their
+// loops; from shared memory those reads are short-latency loads instead of L1
+// round trips (their register budgets do not hold all of them), and one copy
+// serves a whole strip.  The 2D wavefront
 // kernel changes problem at every ticket and keeps reading the descriptor
 // from global memory: there the copy's latency, exposed once per ticket, cost
 // more than it saved.  The descriptor is constant during a launch.

@@ -754,14 +754,19 @@ int Engine::run_iterations(const cdm_step_opts* o, int predicted, double t_start
   }
 }
 
+// the shortest strip of the tail re-tiling: a strip's iteration costs the march
+// of its rows plus two staged ring rows, one after the other, so with the GPU
+// underfilled shorter strips finish an iteration sooner despite the ring rows
+constexpr int kTailMinRows = 4;
+
 // Wavefront schedule, once most problems of a batch have converged: the
 // strips of the problems still iterating no longer fill the GPU, and an
 // iteration of each costs the march of one whole strip.  Halve the strip
-// height of those problems (down to 8 rows) until their strips number at least
-// twice the blocks the launch keeps resident, and drop converged problems from
-// the ticket list.  Tiling changes no result under the max norm (the partials
-// of a problem reduce by max), so this applies between launches only.  The
-// step after restores the tuned tiling.
+// height of those problems (down to kTailMinRows rows) until their strips
+// number at least twice the blocks the launch keeps resident, and drop
+// converged problems from the ticket list.  Tiling changes no result under the
+// max norm (the partials of a problem reduce by max), so this applies between
+// launches only.  The step after restores the tuned tiling.
 int Engine::retile_tail() {
   const int nprob = (int)ps.size();
   const TileShape ts = tile_shape(ndim, variant);
@@ -773,7 +778,7 @@ int Engine::retile_tail() {
       strips += ps[p].ntiles;
       h = std::max(h, ps[p].strip_h);
     }
-  if (strips >= target || h <= 8) return CDM_OK;
+  if (strips >= target || h <= kTailMinRows) return CDM_OK;
   auto count = [&](int hh) {
     long long n = 0;
     for (int p = 0; p < nprob; ++p)
@@ -781,7 +786,7 @@ int Engine::retile_tail() {
     return n;
   };
   int hn = h;
-  while (hn > 8 && count(hn) < target) hn = std::max(8, hn / 2);
+  while (hn > kTailMinRows && count(hn) < target) hn = std::max(kTailMinRows, hn / 2);
   std::vector<int2> items;
   for (int p = 0; p < nprob; ++p) {
     if (h_ctrl[p].done) continue;
