@@ -939,8 +939,10 @@ __global__ void __launch_bounds__(R3NT) mixed_restart3d(const Problem* __restric
 }
 
 // FP32 correction sweep in 3D: the plane-marching layout of apt_march3d.cu
-// (32 x 8 column, two staged planes, three i/j face planes, two k face planes)
-// with the cells and faces of the 2D increment form above.
+// (32 x 8 column, two staged planes, three i/j face planes, two k face planes,
+// the loads that stage plane z + 2 issued while plane z is updated, column
+// ghost rules resolved once per strip and the k rule once per plane) with the
+// cells and faces of the 2D increment form above.
 constexpr int X3 = 32, Y3 = 8, NT3 = X3 * Y3, RX3 = X3 + 2, RY3 = Y3 + 2;
 constexpr int NRING3 = RX3 * RY3 - NT3;
 
@@ -1005,19 +1007,95 @@ __global__ void __launch_bounds__(NT3, 3) mixed_sweep3d(const Problem* __restric
   }
   const int ra = i0 + rx - 1, rb = j0 + ry - 1;
 
-  // cell (a, b, c): correction with its ghost rule, base state and diffusivity
-  // at the cell itself (the restart writes first-layer ghosts), increments
-  auto stage = [&](int a, int b, int c) -> MCell {
+  // Raw loads of a cell of plane c — the correction from the cell its ghost
+  // rules read, base state, base diffusivity and ρ at the cell itself (the
+  // restart writes first-layer ghosts) — issued a plane ahead of stage_pre.
+  // mode: 0 copy, 1 negate, 2 constant ghost (zero correction), 3 no cell (a
+  // corner ghost or a position outside the ghost layer: staged as zeros).
+  struct PreM {
+    float d, ub, ab, rh;
+    int mode;
+  };
+  const int64_t plane_sz = (int64_t)P.nx * P.ny;
+  const int64_t own_col = fidx(P, oa, ob, 0);
+  const int64_t ring_col = rx >= 0 ? fidx(P, ra, rb, 0) : own_col;
+  // (i, j) source of a cell's column, fixed for the strip: kind 0 a domain
+  // column (the k-ghost rule of each plane applies), 1 / 2 / 3 a first-layer
+  // i- or j-ghost column whose side's rule copies / negates the column at `off`
+  // or is a constant, 4 neither (boundary_operators.jl)
+  struct ColSrc {
+    int64_t off;
+    int kind;
+  };
+  auto col_src = [&](int a, int b) -> ColSrc {
+    ColSrc r{0, 0};
+    const bool ia = a >= 0 && a < ni, ib = b >= 0 && b < nj;
+    if (ia && ib) return r;
+    int side = -1;
+    if (ib && (a == -1 || a == ni)) side = a < 0 ? 0 : 1;
+    else if (ia && (b == -1 || b == nj)) side = b < 0 ? 2 : 3;
+    r.kind = 4;
+    if (side < 0) return r;
+    const int rule = P.rule[side];
+    if (rule == GR_DIRICHLET) {
+      r.kind = 3;
+      return r;
+    }
+    const bool lo = (side & 1) == 0;
+    const int n = side < 2 ? ni : nj;
+    const int pos = rule == GR_NONE ? (lo ? -1 : n) : rule == GR_PERIODIC ? (lo ? n - 1 : 0) : (lo ? 0 : n - 1);
+    r.off = side < 2 ? fidx(P, pos, b, 0) : fidx(P, a, pos, 0);
+    r.kind = rule == GR_NEGSYM ? 2 : 1;
+    return r;
+  };
+  const ColSrc own_src = col_src(oa, ob);
+  const ColSrc ring_src = rx >= 0 ? col_src(ra, rb) : ColSrc{0, 4};
+  // k-ghost rule of plane c (block-uniform): source plane, mode 1 negate, 2 constant
+  auto kplane = [&](int c, int& cs, int& mode) {
+    cs = c;
+    mode = 0;
+    if (c >= 0 && c < nk) return;
+    const int side = c < 0 ? 4 : 5;
+    const int rule = P.rule[side];
+    const bool lo = side == 4;
+    if (rule == GR_DIRICHLET) mode = 2;
+    else if (rule == GR_PERIODIC) cs = lo ? nk - 1 : 0;
+    else if (rule != GR_NONE) {
+      cs = lo ? 0 : nk - 1;
+      mode = rule == GR_NEGSYM ? 1 : 0;
+    }
+  };
+  auto load_cell = [&](const ColSrc& cd, int64_t col, int c, int cs, int kmode, PreM& L) {
+    if (cd.kind == 4 || (cd.kind != 0 && (c < 0 || c >= nk))) {
+      L.mode = 3;
+      return;
+    }
+    const int64_t o = col + plane_sz * c;
+    L.ub = ub[o];
+    L.ab = abv[o];
+    L.rh = rho[o];
+    if (cd.kind == 0) {
+      L.mode = kmode;
+      L.d = kmode == 2 ? 0.f : din[col + plane_sz * cs];
+    } else {
+      L.mode = cd.kind == 3 ? 2 : cd.kind - 1;
+      L.d = L.mode == 2 ? 0.f : din[cd.off + plane_sz * c];
+    }
+  };
+  auto prefetch = [&](int c, PreM& own, PreM& rg) {
+    int cs, mode;
+    kplane(c, cs, mode);
+    load_cell(own_src, own_col, c, cs, mode, own);
+    if (rx >= 0) load_cell(ring_src, ring_col, c, cs, mode, rg);
+  };
+  // the cell's increments from its raw loads
+  auto stage_pre = [&](const PreM& L) -> MCell {
     MCell r{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    bool cst, neg;
-    double val;
-    const int64_t so = ghost_src3(P, a, b, c, cst, neg, val);
-    if (so == -2) return r;
-    const int64_t o = fidx(P, a, b, c);
-    r.d = cst ? 0.f : (neg ? -din[so] : din[so]);
-    r.ub = ub[o];
-    r.ab = abv[o];
-    const float rh = rho[o];
+    if (L.mode == 3) return r;
+    r.d = L.mode == 1 ? -L.d : L.d;
+    r.ub = L.ub;
+    r.ab = L.ab;
+    const float rh = L.rh;
     float da = 0.f;
     if (kmode != 0) {
       const float x = r.d * rcp_a(r.ub);
@@ -1036,15 +1114,16 @@ __global__ void __launch_bounds__(NT3, 3) mixed_sweep3d(const Problem* __restric
     }
     return r;
   };
-  auto stage_plane = [&](int c, int s) -> MCell {
-    const MCell own = stage(oa, ob, c);
+  // stage plane c into cell slot s from its loads: the own cell (returned) and the ring cell
+  auto stage_plane_pre = [&](int s, const PreM& own_l, const PreM& rg_l) -> MCell {
+    const MCell own = stage_pre(own_l);
     sm.D[s][oy][ox] = own.d;
     sm.UB[s][oy][ox] = own.ub;
     sm.AB[s][oy][ox] = own.ab;
     sm.DA[s][oy][ox] = own.da;
     sm.IT[s][oy][ox] = own.it;
     if (rx >= 0) {
-      const MCell rg = stage(ra, rb, c);
+      const MCell rg = stage_pre(rg_l);
       sm.D[s][ry][rx] = rg.d;
       sm.UB[s][ry][rx] = rg.ub;
       sm.AB[s][ry][rx] = rg.ab;
@@ -1052,6 +1131,11 @@ __global__ void __launch_bounds__(NT3, 3) mixed_sweep3d(const Problem* __restric
       sm.IT[s][ry][rx] = rg.it;
     }
     return own;
+  };
+  auto stage_plane = [&](int c, int s) -> MCell {
+    PreM lo{0.f, 0.f, 0.f, 0.f, 3}, lr{0.f, 0.f, 0.f, 0.f, 3};
+    prefetch(c, lo, lr);
+    return stage_plane_pre(s, lo, lr);
   };
   // new flux correction between cells (s0, y0, x0) and (s1, y1, x1), and its undamped part
   auto face = [&](int s0, int y0, int x0, int s1, int y1, int x1, float eold, float& dqp) -> float {
@@ -1221,11 +1305,16 @@ __global__ void __launch_bounds__(NT3, 3) mixed_sweep3d(const Problem* __restric
   faces(k0, 1, f_0, 0, 0, 0, 0, false, eb);
   load_faces(k0 + 1, k0, true, ea);
   __syncthreads();
+  // the stage loads of plane k0 + 1, for the first loop iteration
+  PreM p_own{0.f, 0.f, 0.f, 0.f, 3}, p_rg{0.f, 0.f, 0.f, 0.f, 3};
+  prefetch(k0 + 1, p_own, p_rg);
   float local = 0.f;
   bool nan = false;
   for (int z = k0; z < k1; ++z) {
     if (z + 1 < k1) load_faces(z + 2, z + 1, true, eb);
-    const MCell nxt = stage_plane(z + 1, s_p);
+    // stage plane z + 1 from its loads, then issue those of plane z + 2
+    const MCell nxt = stage_plane_pre(s_p, p_own, p_rg);
+    if (z + 1 < k1) prefetch(z + 2, p_own, p_rg);
     __syncthreads();
     float cf[9], R = 0.f;
     const int64_t id = fidx(P, oa, ob, z);
