@@ -453,7 +453,7 @@ def traffic_per_cell_iter(nd, workload, mixed):
     return None
 
 
-def time_single(pr, precision, steps, warmup, stream, net=None, rtol=None):
+def time_single(pr, precision, steps, warmup, stream, net=None, rtol=None, max_iter=100000):
     """Seconds per time step of one problem (CUDA events on the solver's stream).
     With a guess network the steps after the first start from its prediction;
     the prediction and the plain-start probe are inside the timed step.  `rtol`
@@ -478,8 +478,7 @@ def time_single(pr, precision, steps, warmup, stream, net=None, rtol=None):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             st, _ = step(g, pr.mesh, T, pr.rho, pr.cp, pr.kappa, pr.dt, rtol=pr.rtol if rtol is None else rtol,
-                         atol=pr.atol, max_iter=100000,
-                         guess=guess)
+                         atol=pr.atol, max_iter=max_iter, guess=guess)
             e1.record(stream)
             torch.cuda.synchronize()
             t += pr.dt
@@ -544,7 +543,7 @@ def compare_block(args, stream):
                               ("learned_mixed", "mixed", net)):
             try:
                 a[key] = time_single(build_single("multigauss1024", dev)[0], prec, args.compare_steps, 2, stream,
-                                     net=nn, rtol=0.0)
+                                     net=nn, rtol=0.0, max_iter=20000)
             except RuntimeError as err:  # a step that does not reach the absolute test is reported, not fatal
                 a[key] = {"unavailable": str(err)[:200]}
         if "s_per_step" in a["fp64"] and "s_per_step" in a["learned_mixed"]:
