@@ -338,8 +338,17 @@ def run_ours(args, ws, rank, local):
     rhos = [pr.rho for pr in probs]
     cps, kaps, dts = full([pr.cp for pr in probs]), full([pr.kappa for pr in probs]), full([pr.dt for pr in probs])
     kw = dict(rtol=probs[0].rtol, atol=probs[0].atol, max_iter=100000)
+
+    def one_step(T_list, R_list):
+        st, _ = sb.step(full(T_list), full(R_list), cps, kaps, dts, **kw)
+        return st, sb.batch.profile()
+
     # kernel variant, strip height and iteration block timed on this rank's batch
-    # (set-up, outside the timed region)
+    # (set-up, outside the timed region), from the state after one time step:
+    # the first step of a problem checks its residual at every iteration
+    # (PseudoTransientSolver.jl:206-208, last_err_check = 0), the later ones on
+    # the schedule its previous step sets
+    one_step(Ts, rhos)
     if args.tuning:
         sb.batch.set_tuning(*[int(v) for v in args.tuning.split(",")])
         tuning = sb.batch.tuning()
@@ -347,10 +356,6 @@ def run_ours(args, ws, rank, local):
         cand = sb.batch.autotune(Ts, rhos, [pr.cp for pr in probs], [pr.kappa for pr in probs],
                                  [pr.dt for pr in probs], **kw)
         tuning = dict(candidate=cand, **sb.batch.tuning())
-
-    def one_step(T_list, R_list):
-        st, _ = sb.step(full(T_list), full(R_list), cps, kaps, dts, **kw)
-        return st, sb.batch.profile()
 
     for _ in range(args.warmup):
         one_step(Ts, rhos)

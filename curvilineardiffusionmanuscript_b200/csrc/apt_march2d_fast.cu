@@ -55,6 +55,7 @@ struct FastSmem {
   int flag;
   int ticket;
   int wok;
+  int item;
 };
 
 struct Cell {
@@ -442,19 +443,36 @@ __global__ void __launch_bounds__(TX, 6) march2d_fast_inner(const Problem* __res
   }
 }
 
-// Wavefront schedule: one persistent launch runs K pseudo-iterations of every
-// problem.  Ticket t = k·nitems + i stands for iteration k of the launch on
-// item i (a problem's strips together; bit 30 of the tile index marks a
-// boundary strip).  A block holding ticket t with k > 0 waits until its
-// problem has finished iteration k − 1 of the launch (wave_count[p] >= k);
-// only the blocks holding the problem's tickets of iteration k − 1, all below
-// t, can bring that about.  Tickets are taken in order by running blocks, so
-// the lowest unfinished ticket never waits and the schedule cannot deadlock.
-// A problem starts its next iteration as soon as its own strips are done,
-// instead of when the slowest strip of the whole batch is.  Every wait is
-// bounded (about 2 s); a wait that runs out sets counters[3], after which
-// every block of the launch leaves without work and the host reports the step
-// as failed.
+// Wavefront schedule: one persistent launch runs up to K pseudo-iterations of
+// every problem.  The launch is K rounds; in each round a problem takes part
+// or not, and a problem that takes part contributes one ticket per strip (a
+// problem's strips together; bit 30 of the tile index marks a boundary strip).
+// Tickets are numbered round by round, problems in order within a round: a
+// job is (problem, its j-th iteration of the launch) and covers that
+// problem's strips.  A block holding a ticket of job (p, j) with j > 0 waits
+// until p has finished j iterations of the launch (wave_count[p] >= j); only
+// the blocks holding p's tickets of earlier rounds, all below this ticket, can
+// bring that about.  Tickets are taken in order by running blocks, so the
+// lowest unfinished ticket never waits and the schedule cannot deadlock.  A
+// problem starts its next iteration as soon as its own strips are done.
+//
+// Pacing: the iteration counts of a batch's problems differ by an order of
+// magnitude, and with every problem in every round the fast problems finish
+// first and leave the slow ones to run their last iterations on a GPU they no
+// longer fill.  The plan kernel gives problem p
+//   K_p = ceil(K · rem_p / max_q rem_q)   (1 <= K_p <= K)
+// rounds of the launch, rem_p being the iterations left to its expected count
+// (the previous step's, Ctrl::est_iter), spread evenly over the K rounds
+// (round floor((j + ½)·K/K_p) for its j-th iteration), so that every round
+// mixes all problems and they converge together.  A problem without an
+// estimate, or past it, takes every round; so does every problem when no
+// problem has one (the first step), which is the unpaced schedule.  Pacing
+// reorders iterations of independent problems only: every problem runs the
+// same iterations on the same data as without it.
+//
+// Every wait is bounded (about 2 s); a wait that runs out sets counters[3],
+// after which every block of the launch leaves without work and the host
+// reports the step as failed.
 __device__ __forceinline__ int ld_acquire_int(const int* p) {
   int v;
   asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -495,40 +513,131 @@ cudaError_t launch_wave_wait_probe(const int* count, unsigned int* err, double l
   return cudaGetLastError();
 }
 
-// launch prologue: problems already done pass every wait; the ticket restarts
-__global__ void march2d_wave_init(const Problem* __restrict__ probs, int nprob, int* wave_count,
-                                  unsigned int* counters) {
-  for (int p = threadIdx.x; p < nprob; p += blockDim.x)
-    wave_count[p] = ld_cg_int(&probs[p].ctrl->done) ? kWaveDone : 0;
-  if (threadIdx.x == 0) counters[2] = 0u;
+constexpr int kPlanThreads = 256;
+
+// block-wide inclusive sum of v (kPlanThreads threads); returns the block total in *tot
+__device__ __forceinline__ long long plan_scan(long long v, long long* s_w, long long* tot) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long w = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += w;
+  }
+  if (lane == 31) s_w[warp] = v;
+  __syncthreads();
+  long long base = 0, all = 0;
+#pragma unroll
+  for (int w = 0; w < kPlanThreads / 32; ++w) {
+    const long long x = s_w[w];
+    if (w < warp) base += x;
+    all += x;
+  }
+  __syncthreads();
+  *tot = all;
+  return v + base;
+}
+
+// Launch prologue (one block): wave counts (problems already done pass every
+// wait), the launch's jobs in ticket order and the ticket counter's restart.
+__global__ void __launch_bounds__(kPlanThreads) march2d_wave_plan(const Problem* __restrict__ probs, int nprob,
+                                                                  int K, int pace, int* wave_count,
+                                                                  unsigned int* counters, WavePlan W) {
+  __shared__ long long s_w[kPlanThreads / 32];
+  __shared__ int s_max[kPlanThreads / 32];
+  const int tid = threadIdx.x;
+  // the largest number of iterations a problem is expected to have left
+  int rmax = 0;
+  for (int p = tid; p < nprob; p += kPlanThreads) {
+    const Ctrl* C = probs[p].ctrl;
+    const int done = ld_cg_int(&C->done);
+    wave_count[p] = done ? kWaveDone : 0;
+    if (!done && pace) rmax = max(rmax, ld_cg_int(&C->est_iter) - ld_cg_int(&C->iter));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) rmax = max(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+  if ((tid & 31) == 0) s_max[tid >> 5] = rmax;
+  __syncthreads();
+  rmax = 0;
+  for (int w = 0; w < kPlanThreads / 32; ++w) rmax = max(rmax, s_max[w]);
+  // each problem's rounds
+  for (int p = tid; p < nprob; p += kPlanThreads) {
+    const Ctrl* C = probs[p].ctrl;
+    unsigned long long m = 0ull;
+    if (!ld_cg_int(&C->done) && probs[p].item0 >= 0) {
+      const int rem = ld_cg_int(&C->est_iter) - ld_cg_int(&C->iter);
+      int kp = K;
+      if (pace && rmax > 0 && rem > 0) kp = min(K, max(1, (int)(((long long)K * rem + rmax - 1) / rmax)));
+      for (int j = 0; j < kp; ++j) m |= 1ull << ((2 * j + 1) * K / (2 * kp));
+    }
+    W.mask[p] = m;
+  }
+  __syncthreads();
+  // jobs round by round, problems in order within a round
+  int jobs = 0, tickets = 0;
+  for (int r = 0; r < K; ++r) {
+    for (int base = 0; base < nprob; base += kPlanThreads) {
+      const int p = base + tid;
+      unsigned long long m = 0ull;
+      int nt = 0;
+      if (p < nprob) {
+        m = W.mask[p];
+        if ((m >> r) & 1ull) nt = probs[p].ntiles;
+      }
+      const int part = ((m >> r) & 1ull) ? 1 : 0;
+      long long tot;
+      const long long inc = plan_scan(((long long)part << 40) | (long long)nt, s_w, &tot);
+      if (part) {
+        const long long ex = inc - (((long long)part << 40) | (long long)nt);
+        const int J = jobs + (int)(ex >> 40);
+        W.tb[J] = tickets + (int)(ex & ((1ll << 40) - 1));
+        W.pj[J] = make_int2(p, __popcll(m & ((1ull << r) - 1ull)));
+      }
+      jobs += (int)(tot >> 40);
+      tickets += (int)(tot & ((1ll << 40) - 1));
+    }
+  }
+  if (tid == 0) {
+    W.tb[jobs] = tickets;
+    W.head[0] = jobs;
+    W.head[1] = tickets;
+    counters[2] = 0u;
+  }
 }
 
 // 640 threads per SM at the register budget of 5 blocks of 128 (96 registers)
 template <int TX, bool HARM>
 __global__ void __launch_bounds__(TX, 640 / TX) march2d_fast_wave(const Problem* __restrict__ probs,
-                                                           const int2* __restrict__ items, int nitems, int K,
+                                                           const int2* __restrict__ items, WavePlan W,
                                                            unsigned int* counters, int* wave_count) {
   __shared__ FastSmem<TX> sm;
-  const int total = K * nitems;
+  const int total = W.head[1], njobs = W.head[0];
   while (true) {
-    // thread 0 takes the ticket and waits for the problem's previous iteration
+    // thread 0 takes the ticket, finds its job and waits for the problem's
+    // previous iteration of the launch
     if (threadIdx.x == 0) {
       const int t = ld_cg_int((const int*)&counters[3]) ? total : (int)atomicAdd(&counters[2], 1u);
-      int ok = 1;
-      if (t < total && t >= nitems) {
-        const int k = t / nitems;
-        ok = wave_wait(&wave_count[items[t - k * nitems].x], k, &counters[3]);
+      int ok = 1, item = 0;
+      if (t < total) {
+        int lo = 0, hi = njobs - 1;  // the last job starting at or before t
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (__ldg(&W.tb[mid]) <= t) lo = mid;
+          else hi = mid - 1;
+        }
+        const int2 pj = __ldg(&W.pj[lo]);
+        item = probs[pj.x].item0 + (t - __ldg(&W.tb[lo]));
+        if (pj.y > 0) ok = wave_wait(&wave_count[pj.x], pj.y, &counters[3]);
       }
       sm.ticket = t;
       sm.wok = ok;
+      sm.item = item;
     }
     __syncthreads();
     const int t = sm.ticket, ok = sm.wok;
+    const int2 item = items[sm.item];
     __syncthreads();
     if (t >= total) break;
     if (!ok) continue;
-    const int k = t / nitems, i = t - k * nitems;
-    const int2 item = items[i];
     const Problem& P = probs[item.x];
     Ctrl* C = P.ctrl;
     if (ld_cg_int(&C->done)) continue;
@@ -560,25 +669,27 @@ int march2d_wave_slots(int tx, int harmonic) {
 }
 
 template <int TX, bool HARM>
-static cudaError_t launch_wave(const Problem* probs, int nprob, const int2* items, int nitems, int K,
-                               unsigned int* counters, int* wave_count, cudaStream_t s) {
+static cudaError_t launch_wave(const Problem* probs, int nprob, const int2* items, int nitems, int K, int pace,
+                               unsigned int* counters, int* wave_count, const WavePlan& W, cudaStream_t s) {
   const long long slots = wave_slots<TX, HARM>();
   const long long total = (long long)K * nitems;
   const int grid = (int)(total < slots ? total : slots);
-  march2d_wave_init<<<1, 256, 0, s>>>(probs, nprob, wave_count, counters);
-  march2d_fast_wave<TX, HARM><<<grid, TX, 0, s>>>(probs, items, nitems, K, counters, wave_count);
+  march2d_wave_plan<<<1, kPlanThreads, 0, s>>>(probs, nprob, K, pace, wave_count, counters, W);
+  march2d_fast_wave<TX, HARM><<<grid, TX, 0, s>>>(probs, items, W, counters, wave_count);
   return cudaGetLastError();
 }
 
 cudaError_t launch_march2d_wave(int tx, int harmonic, const Problem* probs, int nprob, const int2* items,
-                                int nitems, int K, unsigned int* counters, int* wave_count, cudaStream_t s) {
+                                int nitems, int K, int pace, unsigned int* counters, int* wave_count,
+                                const WavePlan& W, cudaStream_t s) {
   if (nitems <= 0 || K <= 0) return cudaSuccess;
-  if ((long long)K * nitems >= (1ll << 31)) return cudaErrorInvalidValue;
+  if (K > kWaveMaxRounds || (long long)K * nitems >= (1ll << 31) || (long long)K * nprob > W.cap)
+    return cudaErrorInvalidValue;
   if (tx == 64)
-    return harmonic ? launch_wave<64, true>(probs, nprob, items, nitems, K, counters, wave_count, s)
-                    : launch_wave<64, false>(probs, nprob, items, nitems, K, counters, wave_count, s);
-  return harmonic ? launch_wave<128, true>(probs, nprob, items, nitems, K, counters, wave_count, s)
-                  : launch_wave<128, false>(probs, nprob, items, nitems, K, counters, wave_count, s);
+    return harmonic ? launch_wave<64, true>(probs, nprob, items, nitems, K, pace, counters, wave_count, W, s)
+                    : launch_wave<64, false>(probs, nprob, items, nitems, K, pace, counters, wave_count, W, s);
+  return harmonic ? launch_wave<128, true>(probs, nprob, items, nitems, K, pace, counters, wave_count, W, s)
+                  : launch_wave<128, false>(probs, nprob, items, nitems, K, pace, counters, wave_count, W, s);
 }
 
 // Is tile `tile` of a problem free of domain-boundary logic (no ghost column,

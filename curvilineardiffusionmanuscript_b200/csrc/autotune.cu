@@ -30,7 +30,7 @@ constexpr int kStripH[] = {8, 16, 32, 64};
 constexpr int kBlock[] = {4, 8, 16};
 constexpr int kNumBlock = 3;
 constexpr int kWaveH[] = {16, 32, 64};
-constexpr int kWaveBlock[] = {8, 16, 32};
+constexpr int kWaveBlock[] = {16, 32, 64};
 // candidates 0..11: marching kernel, strip height kStripH[c / 3], block kBlock[c % 3];
 // 12..17 (2D FP64): tile kernels (variants 2, 3: 32x16 and 32x8 tiles, every row of a
 // tile at once, for grids too small to hide a strip's serial march), block kBlock[c % 3];

@@ -52,6 +52,9 @@ struct Ctrl {
   int restart_nan;
   int inner_stall;      // inner checks since the last new best
   double inner_best;    // best max|r| of the cycle
+  // wavefront schedule: the iteration count this step is expected to take
+  // (the previous step's, last_err_check); 0 when unknown
+  int est_iter;
 };
 
 // Kernel-facing description of one problem (one mesh, one step! call).
@@ -64,6 +67,8 @@ struct Problem {
   int subcycle;                     // subcycle_conductivity
   int kmode, km, khalf;             // conductivity exponent decomposition
   int qpar;                         // ping-pong index of q holding the state
+  int item0;                        // wavefront schedule: index of the problem's first strip in the
+                                    // item list, -1 when it has none
   int rule[6];
   double val[6];
   double dt, cp, k0, kn, L, LL, Vpdtau, VpL;

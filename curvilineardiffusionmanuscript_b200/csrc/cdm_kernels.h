@@ -37,14 +37,27 @@ cudaError_t launch_march2d_fast(int variant, int harmonic, const Problem* probs,
 // kernel), and no ghost row only (the FP64 row-marching kernels' branch-free body)
 bool march_tile_interior(int ni, int nj, int tiles_i, int strip_h, int tx, int tile);
 bool march_tile_no_ghost_rows(int nj, int tiles_i, int strip_h, int tile);
-// the same kernel on the wavefront schedule: K pseudo-iterations of every problem in one
-// persistent launch, each problem's next iteration starting when its own strips are done.
-// items: each problem's strips together, boundary strips with bit 30 of the tile set.
-// counters[2] is the launch's ticket, counters[3] a flag set when a bounded dependency
-// wait ran out (left set; clear it before the next step); wave_count holds nprob ints.
+// the same kernel on the wavefront schedule: up to K pseudo-iterations of every problem
+// in one persistent launch of K rounds, each problem's next iteration starting when its
+// own strips are done.  items: each problem's strips together from Problem::item0,
+// boundary strips with bit 30 of the tile set.  pace = 1 spreads the iterations a
+// problem is expected to have left (Ctrl::est_iter) evenly over the rounds; pace = 0
+// (or no estimates) puts every problem in every round.  counters[2] is the launch's
+// ticket, counters[3] a flag set when a bounded dependency wait ran out (left set; clear
+// it before the next step); wave_count holds nprob ints; W holds the launch's jobs
+// (written by the launch's prologue, room for cap >= K * nprob jobs).
 // tx: threads per block (128 or 64; tx - 2 owned columns)
+constexpr int kWaveMaxRounds = 64;
+struct WavePlan {
+  int* head;                 // [0] jobs, [1] tickets of the launch
+  int* tb;                   // cap + 1: first ticket of each job, in ticket order
+  int2* pj;                  // cap: (problem, its iteration of the launch) of each job
+  unsigned long long* mask;  // nprob: the rounds each problem takes part in
+  long long cap;
+};
 cudaError_t launch_march2d_wave(int tx, int harmonic, const Problem* probs, int nprob, const int2* items,
-                                int nitems, int K, unsigned int* counters, int* wave_count, cudaStream_t s);
+                                int nitems, int K, int pace, unsigned int* counters, int* wave_count,
+                                const WavePlan& W, cudaStream_t s);
 // blocks one wavefront launch of tx-thread blocks keeps resident on the current device
 int march2d_wave_slots(int tx, int harmonic);
 // one block whose thread 0 runs the wavefront's dependency wait on *count (which

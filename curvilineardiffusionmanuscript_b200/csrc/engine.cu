@@ -118,6 +118,10 @@ Engine::~Engine() {
   dfree(d_flags);
   dfree(d_counters);
   dfree(d_wave);
+  dfree(wave_plan.head);
+  dfree(wave_plan.tb);
+  dfree(wave_plan.pj);
+  dfree(wave_plan.mask);
   dfree(d_red);
   dfree(d_redout);
   dfree(d_jobs);
@@ -382,6 +386,12 @@ int Engine::init(int nprob, const cdm_mesh_desc* meshes, const cdm_bc* bcs, cons
   CDM_CK(dalloc(&d_flags, (size_t)nprob));
   CDM_CK(dalloc(&d_counters, (size_t)4));
   CDM_CK(dalloc(&d_wave, (size_t)nprob));
+  wave_plan.cap = (long long)kWaveMaxRounds * nprob;
+  CDM_CK(dalloc(&wave_plan.head, (size_t)2));
+  CDM_CK(dalloc(&wave_plan.tb, (size_t)wave_plan.cap + 1));
+  CDM_CK(dalloc(&wave_plan.pj, (size_t)wave_plan.cap));
+  CDM_CK(dalloc(&wave_plan.mask, (size_t)nprob));
+  if (const char* e = std::getenv("CDM_WAVE_PACE")) wave_pace = std::atoi(e) != 0 ? 1 : 0;
   CDM_CK(cudaMallocHost((void**)&h_wave_err, sizeof(unsigned int)));
   *h_wave_err = 0u;
   CDM_CK(dalloc(&d_red, (size_t)4 * 1024));
@@ -459,6 +469,11 @@ int Engine::build_items() {
   // which have finished by the time they are reached, and boundary strips are
   // tagged in bit 30 of the tile index.
   if (ts.march == 3) {
+    int first = 0;
+    for (ProbState& s : ps) {
+      s.item0 = first;
+      first += s.ntiles;
+    }
     for (int2& it : items) {
       const ProbState& s = ps[it.x];
       if (!march_tile_no_ghost_rows(s.nj, s.tiles_i, s.strip_h, it.y)) it.y |= 1 << 30;
@@ -661,7 +676,7 @@ double Engine::collect_profile_ms() {
 cudaError_t Engine::launch_iters(int K) {
   if (tile_shape(ndim, variant).march == 3)
     return launch_march2d_wave(tile_shape(ndim, variant).tx, mean == CDM_MEAN_HARMONIC, d_probs, (int)ps.size(),
-                               d_items, nitems, K, d_counters, d_wave, stream);
+                               d_items, nitems, K, wave_pace, d_counters, d_wave, wave_plan, stream);
   cudaError_t le = cudaSuccess;
   for (int k = 0; k < K && le == cudaSuccess; ++k)
     le = launch_sweep_fp64(ndim, variant, precision == CDM_PREC_FP64_EXACT || tz_active, mean == CDM_MEAN_HARMONIC,
@@ -789,14 +804,19 @@ int Engine::retile_tail() {
   while (hn > kTailMinRows && count(hn) < target) hn = std::max(kTailMinRows, hn / 2);
   std::vector<int2> items;
   for (int p = 0; p < nprob; ++p) {
-    if (h_ctrl[p].done) continue;
+    if (h_ctrl[p].done) {
+      ps[p].item0 = hp[p].item0 = -1;
+      continue;
+    }
     ProbState& s = ps[p];
     s.strip_h = std::min(hn, s.nj);
     s.tiles_j = (s.nj + s.strip_h - 1) / s.strip_h;
     s.ntiles = s.tiles_i * s.tiles_j;
+    s.item0 = (int)items.size();
     hp[p].strip_h = s.strip_h;
     hp[p].tiles_j = s.tiles_j;
     hp[p].ntiles = s.ntiles;
+    hp[p].item0 = s.item0;
     for (int t = 0; t < s.ntiles; ++t) {
       int2 it = make_int2(p, t);
       if (!march_tile_no_ghost_rows(s.nj, s.tiles_i, s.strip_h, t)) it.y |= 1 << 30;
@@ -1015,6 +1035,7 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
     P.tiles_k = s.tiles_k;
     P.ntiles = s.ntiles;
     P.strip_h = s.strip_h;
+    P.item0 = s.item0;
     P.mean = mean;
     P.subcycle = o.subcycle_conductivity ? 1 : 0;
     kappa_decompose(kappa[p].n, P.kmode, P.km, P.khalf);
@@ -1090,6 +1111,7 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
     C.abs = 2 * o.atol;
     C.nfull = (double)s.nfull;
     C.sqrtN = std::sqrt((double)s.nfull);
+    C.est_iter = wave_pace ? last : 0;
     predicted = std::min(predicted, o.check_every > 0 ? 0 : std::max(0, C.min_err_check - 1));
   }
   CDM_CK(cudaMemcpyAsync(d_probs, hp.data(), sizeof(Problem) * nprob, cudaMemcpyHostToDevice, stream));

@@ -36,6 +36,7 @@ struct ProbState {
   double val[6] = {0, 0, 0, 0, 0, 0};
   int bc_kind[6] = {0, 0, 0, 0, 0, 0};
   int tiles_i = 1, tiles_j = 1, tiles_k = 1, ntiles = 1, strip_h = 1;
+  int item0 = -1;  // wavefront schedule: first strip in the item list (-1: none)
   // device buffers owned by the engine
   double* u[2] = {nullptr, nullptr};
   double* q[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
@@ -92,6 +93,8 @@ struct Engine {
   unsigned int* d_counters = nullptr;  // [0, 1] tile tickets of the persistent sweep; [2] wavefront
                                        // ticket, [3] wavefront wait-expired flag
   int* d_wave = nullptr;               // wavefront schedule: per problem, iterations done in the launch
+  WavePlan wave_plan{};                // wavefront schedule: the launch's jobs (device, written per launch)
+  int wave_pace = 1;                   // pace problems by their expected iteration counts (CDM_WAVE_PACE=0: off)
   unsigned int* h_wave_err = nullptr;  // pinned mirror of d_counters[3]
   int n_edge = 0;                      // items [0, n_edge) touch a domain boundary
   cudaStream_t side_stream = nullptr;  // boundary strips run here, concurrently

@@ -309,7 +309,7 @@ int cdm_batch_step(cdm_batch* b, double* const* T, const double* const* rho, con
  * host polls), candidate index 3·index(h) + index(K); for 2D FP64 also the
  * tile kernels (32x16 and 32x8 tiles) x K, indices 12..17, and for the
  * reciprocal form the wavefront schedule with 128-thread blocks (variant 4) and
- * with 64-thread blocks (variant 5), each with h ∈ {16, 32, 64} x K ∈ {8, 16, 32},
+ * with 64-thread blocks (variant 5), each with h ∈ {16, 32, 64} x K ∈ {16, 32, 64},
  * indices 18 + 9·(variant − 4) + 3·index(h) + index(K); for 3D FP64 (reciprocal
  * form) the plane march on 32x8 column tiles (indices 0..11) and on 16x16 column
  * tiles (variant 3, indices 12 + 3·index(h) + index(K)) — from the given inputs
@@ -337,6 +337,59 @@ int cdm_batch_tuning(const cdm_batch* b, int* variant, int* strip_h, int* iter_b
  * iter_block in [1, 64]. */
 int cdm_batch_set_tuning(cdm_batch* b, int variant, int strip_h, int iter_block);
 int cdm_batch_get_profile(const cdm_batch* b, cdm_profile* out);
+
+/* ---- implicit comparator ------------------------------------------------
+ * The reference's implicit scheme: backward Euler in the conservative
+ * curvilinear form with the diffusivity taken at Tⁿ, one sparse linear system
+ * per time step solved by a Krylov method.  2D, Neumann, Dirichlet and periodic
+ * sides (FixedNegSymmetryBC has no matrix rows in the reference; CDM_BAD_INPUT).
+ * The system covers the domain plus one halo layer; the reference's GMRES +
+ * ILU(0) is replaced by Jacobi-preconditioned BiCGSTAB with the same stopping
+ * rule on the true residual, ||b - A x||_2 <= atol + rtol ||b - A x0||_2. */
+typedef struct cdm_implicit cdm_implicit; /* opaque handle */
+
+/* keyword arguments of nonlinear_thermal_conduction_step!(::ImplicitScheme)
+ * (nonlinear_thermal_conduction.jl:4-16), _iterative_solve!
+ * (ImplictSolver.jl:249-259) and next_dt (timestep_control.jl:33-42) */
+typedef struct cdm_implicit_opts {
+  double atol, rtol;             /* 1e-9, 1e-9                                   */
+  int max_iter;                  /* Krylov iterations, 0 = 2 x rows (Krylov.jl)  */
+  int enforce_positivity;        /* 1: cutoff of the solution                    */
+  int apply_density_bc;          /* 1: the boundary rules applied to rho too      */
+  double ndt_tol;                /* 1e-3                                          */
+  double maximum_u_change;       /* 0.05                                          */
+  double timestep_growth_factor; /* 1.1                                           */
+  int mem;                       /* enum cdm_mem of T and rho                     */
+} cdm_implicit_opts;
+
+void cdm_implicit_opts_default(cdm_implicit_opts* opts);
+/* ImplicitScheme(mesh, bcs; mean, backend)  (ImplictSolver.jl:49-160); reads
+ * mesh.cell_J, edge_J[0..1] and edge_hat[f][{0,1,3,4}] (the J-scaled ξ̂ and η̂
+ * face metrics), cfg->mean and cfg->device (precision is not used) */
+int cdm_implicit_create(const cdm_mesh_desc* mesh, const cdm_bc* bcs /* 4 */, const cdm_apt_config* cfg,
+                        cdm_implicit** out);
+int cdm_implicit_destroy(cdm_implicit* h);
+/* scheme.source_term (ImplictSolver.jl:28): a full-size array, the domain and
+ * its first halo layer are used */
+int cdm_implicit_set_source(cdm_implicit* h, const double* S, int mem);
+/* nonlinear_thermal_conduction_step!(scheme, mesh, T, ρ, cₚ, κ, Δt; ...)
+ * (nonlinear_thermal_conduction.jl:4-48) with solve! = _iterative_solve!
+ * (ImplictSolver.jl:249-330): applybcs! on T (and rho into a library copy:
+ * the caller's rho is not modified), α = |κ/(ρcₚ)|, validate_scalar, assemble!,
+ * Krylov solve (from zero on the first call, from the previous solution
+ * after), cutoff, next_dt; T is overwritten on the domain and its first halo
+ * layer.  stats: niter (BiCGSTAB iterations, two products with A each),
+ * rel_err = abs_err = the final ||b - A x||_2 (the reference returns the
+ * Krylov residual for both), status; the energy fields are 0. */
+int cdm_implicit_step(cdm_implicit* h, double* T, const double* rho, double cp, cdm_kappa kappa, double dt,
+                      const cdm_implicit_opts* opts, cdm_stats* stats, double* next_dt);
+/* the system of the last step (no reference counterpart; for checks): A as 9
+ * arrays of (ni+2)(nj+2) values, entry e = 3(dj+1) + (di+1) at offset (di, dj)
+ * (offsets2d, inner_operators.jl:19-21) on interior rows (0 on boundary rows,
+ * whose constraint rows are the ones init_matrix.jl builds), and b */
+int cdm_implicit_get_system(cdm_implicit* h, double* A, double* b);
+/* device time of the last Krylov solve (CUDA events), products with A, rows */
+int cdm_implicit_get_profile(const cdm_implicit* h, double* solve_ms, int64_t* spmv, int64_t* rows);
 
 /* ---- allocation-free end-of-step reductions ------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device

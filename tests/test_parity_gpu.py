@@ -339,6 +339,21 @@ def test_wavefront_schedule_equals_per_iteration_launches(K):
     assert all(torch.equal(a, b) for a, b in zip(T0, T1))
 
 
+@pytest.mark.parametrize("K", [8, 32])
+def test_paced_wavefront_equals_unpaced(K, monkeypatch):
+    """From the second step on, the wavefront schedule spreads each problem's
+    expected remaining iterations over the launch's rounds (pacing); it only
+    reorders iterations of independent problems, so fields and iteration counts
+    equal those of the unpaced schedule (CDM_WAVE_PACE=0) bit for bit."""
+    probs = problems.batch_2d(nprob=12, nmin=20, nmax=300, seed=5)
+    (i1, T1), = _run_tunings(probs, [(5, 16, K)], nsteps=4)
+    monkeypatch.setenv("CDM_WAVE_PACE", "0")
+    (i0, T0), = _run_tunings(probs, [(5, 16, K)], nsteps=4)
+    assert len({n for step in i0[1:] for n in step}) > 3
+    assert i0 == i1
+    assert all(torch.equal(a, b) for a, b in zip(T0, T1))
+
+
 def test_wavefront_boundary_conditions_sources_and_one_problem():
     bcs = [[DirichletBC(1.5), NeumannBC(), PeriodicBC(), PeriodicBC()],
            [FixedNegSymmetryBC(), NeumannBC(), NeumannBC(), DirichletBC(2.0)],
@@ -373,7 +388,7 @@ def test_fast_batch_autotune_includes_the_wavefront():
     if c >= 18:
         t = c - 18
         assert b.tuning() == {"variant": 4 + t // 9, "strip_h": [16, 32, 64][(t % 9) // 3],
-                              "iter_block": [8, 16, 32][t % 3]}
+                              "iter_block": [16, 32, 64][t % 3]}
     b.close()
 
 
