@@ -505,6 +505,45 @@ def time_single(pr, precision, steps, warmup, stream, net=None, rtol=None, max_i
     return out
 
 
+# algorithmic bytes per row of one BiCGSTAB iteration of the implicit solve: the
+# nine stencil entries twice (two products with A) and the vectors its five
+# kernels read and write (p, p̂, v, s, ŝ, t, x, r, r̂, D⁻¹), 43 doubles
+IMPLICIT_BYTES_PER_ROW_ITER = 43 * 8
+
+
+def time_implicit(pr, steps, warmup, stream):
+    """Seconds per time step of the reference's implicit comparator (backward
+    Euler, Krylov solve to atol = rtol = 1e-9 as _iterative_solve! defaults)
+    on one problem, CUDA events around each step's library call."""
+    import torch
+    from curvilineardiffusionmanuscript_b200.solver import ImplicitScheme
+    g = ImplicitScheme(pr.mesh, pr.bcs, stream=stream.cuda_stream)
+    try:
+        T = pr.T0.clone()
+        times, iters, res, gbs = [], [], [], []
+        for k in range(warmup + steps):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st, _ = g.step(pr.mesh, T, pr.rho, pr.cp, pr.kappa, pr.dt)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if k >= warmup:
+                pf = g.profile()
+                times.append(e0.elapsed_time(e1) / 1e3)
+                iters.append(st["niter"])
+                res.append(st["abs_err"])
+                if pf["solve_ms"] > 0:
+                    gbs.append(IMPLICIT_BYTES_PER_ROW_ITER * pf["rows"] * st["niter"] / (pf["solve_ms"] / 1e3) / 1e9)
+        return {"s_per_step": statistics.median(times), "krylov_iters": statistics.mean(iters),
+                "final_residual_2norm": statistics.mean(res), "tol": "atol = rtol = 1e-9 (2-norm)",
+                "solver": "BiCGSTAB, Jacobi preconditioner on the right",
+                "solve_GBs": statistics.mean(gbs) if gbs else None,
+                "bytes_per_row_iter": IMPLICIT_BYTES_PER_ROW_ITER}
+    finally:
+        g.close()
+
+
 def train_guess(n, nseeds, nsteps, train_steps):
     """Guess network trained on APT trajectories of the multi-Gaussian problem
     (seeds disjoint from the timed problem's)."""
@@ -534,6 +573,9 @@ def compare_block(args, stream):
     for prec in ("fp64", "mixed"):
         w[prec] = time_single(build_single("multigauss1024", dev)[0], prec, args.compare_steps, 2, stream)
     w["speedup_mixed_vs_fp64"] = w["fp64"]["s_per_step"] / w["mixed"]["s_per_step"]
+    # the manuscript's comparison: the reference's implicit scheme on the same problem
+    w["implicit_krylov"] = time_implicit(build_single("multigauss1024", dev)[0], args.compare_steps, 2, stream)
+    w["implicit_s_per_step_over_fp64"] = w["implicit_krylov"]["s_per_step"] / w["fp64"]["s_per_step"]
     if DEFAULT_CHECKPOINT.exists():
         net = learned.GuessNet(seed=0)
         net.load(DEFAULT_CHECKPOINT)

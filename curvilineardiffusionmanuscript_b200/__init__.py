@@ -6,8 +6,8 @@ The solver runs in hand-written CUDA for sm_100a behind the C ABI of
 Julia interface on top of it.
 """
 from .mesh import CurvilinearMesh, wavy_mesh_2d, wavy_mesh_3d, uniform_mesh_2d, mesh_from_nodes_2d  # noqa: F401
-from .solver import (APTError, DirichletBC, FixedNegSymmetryBC, NeumannBC, PeriodicBC,  # noqa: F401
-                     PowerLawConductivity, PseudoTransientBatch, PseudoTransientSolver,
+from .solver import (APTError, DirichletBC, FixedNegSymmetryBC, ImplicitScheme, NeumannBC,  # noqa: F401
+                     PeriodicBC, PowerLawConductivity, PseudoTransientBatch, PseudoTransientSolver,
                      nonlinear_thermal_conduction_step, step)
 
 __version__ = "0.1.0"

@@ -82,6 +82,13 @@ class Profile(C.Structure):
                 ("cell_iters", C.c_int64), ("fp32_cell_iters", C.c_int64), ("fp64_cell_evals", C.c_int64)]
 
 
+class ImplicitOpts(C.Structure):
+    """cdm_implicit_opts (include/cdm_apt.h)."""
+    _fields_ = [("atol", C.c_double), ("rtol", C.c_double), ("max_iter", C.c_int), ("enforce_positivity", C.c_int),
+                ("apply_density_bc", C.c_int), ("ndt_tol", C.c_double), ("maximum_u_change", C.c_double),
+                ("timestep_growth_factor", C.c_double), ("mem", C.c_int)]
+
+
 class NetBatch(C.Structure):
     """cdm_net_batch (include/cdm_net.h)."""
     _fields_ = [
@@ -129,6 +136,14 @@ SIGNATURES = {
     "cdm_apt_get_profile": (C.c_int, [C.c_void_p, C.POINTER(Profile)]),
     "cdm_batch_get_profile": (C.c_int, [C.c_void_p, C.POINTER(Profile)]),
     "cdm_step_reductions_noalloc": (C.c_int, [C.c_int] * 5 + [C.c_void_p] * 5 + [C.c_double] * 5 + [PD, C.c_void_p]),
+    "cdm_implicit_opts_default": (None, [C.POINTER(ImplicitOpts)]),
+    "cdm_implicit_create": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(BC), C.POINTER(Config), C.POINTER(C.c_void_p)]),
+    "cdm_implicit_destroy": (C.c_int, [C.c_void_p]),
+    "cdm_implicit_set_source": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "cdm_implicit_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, Kappa, C.c_double,
+                                    C.POINTER(ImplicitOpts), C.POINTER(Stats), PD]),
+    "cdm_implicit_get_system": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "cdm_implicit_get_profile": (C.c_int, [C.c_void_p, PD, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "cdm_net_create": (C.c_int, [C.c_int, C.c_uint64, C.c_void_p, C.POINTER(C.c_void_p)]),
     "cdm_net_destroy": (C.c_int, [C.c_void_p]),
     "cdm_net_num_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),

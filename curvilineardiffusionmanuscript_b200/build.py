@@ -37,6 +37,7 @@ UNITS = {
     "net_kernels.cu": [],
     "net_conv_tc.cu": [],
     "net.cu": [],
+    "implicit.cu": ["-fmad=false"],
 }
 
 

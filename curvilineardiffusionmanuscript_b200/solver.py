@@ -301,11 +301,100 @@ def step(solver: PseudoTransientSolver, mesh, T, rho, cp: float, kappa: PowerLaw
 
 
 def nonlinear_thermal_conduction_step(solver, mesh, T, rho, cp, kappa, dt, *, show_convergence=True, **kwargs):
-    """nonlinear_thermal_conduction_step! for the PT solver (nonlinear_thermal_conduction.jl:51-72)."""
+    """nonlinear_thermal_conduction_step! for the PT solver (nonlinear_thermal_conduction.jl:51-72)
+    and, given an :class:`ImplicitScheme`, for the implicit scheme (:4-48)."""
+    if isinstance(solver, ImplicitScheme):
+        stats, next_dt = solver.step(mesh, T, rho, cp, kappa, dt, **kwargs)
+        if show_convergence:
+            print("\tKrylov stats: L2: %.1e, iterations: %i" % (stats["abs_err"], stats["niter"]))
+        return stats, next_dt
     stats, next_dt = step(solver, mesh, T, rho, cp, kappa, dt, **kwargs)
     if show_convergence:
         print("\trel error: %.3e, abs err: %.3e, %i" % (stats["rel_err"], stats["abs_err"], stats["niter"]))
     return stats, next_dt
+
+
+# --------------------------------------------------------------- implicit scheme
+_IMPLICIT_KW = {"atol": float, "rtol": float, "max_iter": int, "enforce_positivity": int,
+                "apply_density_bc": int, "maximum_u_change": float, "timestep_growth_factor": float}
+
+
+class ImplicitScheme:
+    """ImplicitScheme(mesh, bcs; mean=:harmonic) — the reference's implicit
+    comparator (src/implicit/ImplictSolver.jl:49-160) on one B200: backward
+    Euler with the diffusivity at Tⁿ, one linear system per step solved by a
+    Krylov method to ||b - A x|| <= atol + rtol ||b - A x0||."""
+
+    def __init__(self, mesh: CurvilinearMesh, bcs, mean: str = "harmonic", device: int = 0,
+                 stream: Optional[int] = None):
+        self._lib = L.load()
+        self.mesh = mesh
+        self.bcs = bc_list(bcs)
+        cfg = L.default_config()
+        cfg.mean = L.CDM_MEAN_HARMONIC if mean == "harmonic" else L.CDM_MEAN_ARITHMETIC
+        cfg.device = device
+        cfg.stream = stream
+        desc, keep = mesh_desc(mesh)
+        h = C.c_void_p()
+        rc = self._lib.cdm_implicit_create(C.byref(desc), _bcs_c(self.bcs, mesh.ndim), C.byref(cfg), C.byref(h))
+        del keep
+        if rc != L.CDM_OK:
+            raise APTError(rc, L.last_error())
+        self._h = h
+        self.rows = (mesh.ni + 2) * (mesh.nj + 2)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.cdm_implicit_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_source(self, S):
+        S = S.contiguous() if isinstance(S, torch.Tensor) else np.ascontiguousarray(S, dtype=np.float64)
+        rc = self._lib.cdm_implicit_set_source(self._h, _ptr(S), _mem(S))
+        if rc != L.CDM_OK:
+            raise APTError(rc, L.last_error())
+
+    def step(self, mesh, T, rho, cp: float, kappa: PowerLawConductivity, dt: float, **kwargs):
+        """One implicit time step; T is updated in place -> (stats, next_dt)."""
+        o = L.ImplicitOpts()
+        self._lib.cdm_implicit_opts_default(C.byref(o))
+        for k, v in kwargs.items():
+            if k in _IMPLICIT_KW:
+                setattr(o, k, _IMPLICIT_KW[k](v))
+            elif k == "tol":
+                o.ndt_tol = float(v)
+        o.mem = _mem(T)
+        if _mem(rho) != o.mem:
+            raise ValueError("T and rho must live in the same memory space")
+        st = L.Stats()
+        ndt = C.c_double(0.0)
+        rc = self._lib.cdm_implicit_step(self._h, _ptr(T), _ptr(rho), float(cp), kappa.as_c(), float(dt),
+                                         C.byref(o), C.byref(st), C.byref(ndt))
+        stats = stats_dict(st)
+        if rc != L.CDM_OK:
+            raise APTError(rc, L.last_error(), stats)
+        return stats, ndt.value
+
+    def system(self):
+        """(A, b) of the last step: A as (9, nj+2, ni+2) stencil entries, b as (nj+2, ni+2)."""
+        n2, n1 = self.mesh.nj + 2, self.mesh.ni + 2
+        A = np.zeros((9, n2, n1))
+        b = np.zeros((n2, n1))
+        rc = self._lib.cdm_implicit_get_system(self._h, A.ctypes.data, b.ctypes.data)
+        if rc != L.CDM_OK:
+            raise APTError(rc, L.last_error())
+        return A, b
+
+    def profile(self) -> dict:
+        ms, spmv, rows = C.c_double(0.0), C.c_int64(0), C.c_int64(0)
+        self._lib.cdm_implicit_get_profile(self._h, C.byref(ms), C.byref(spmv), C.byref(rows))
+        return {"solve_ms": ms.value, "spmv": spmv.value, "rows": rows.value}
 
 
 def advance(solver: PseudoTransientSolver, mesh, T, rho, cp: float, kappa: PowerLawConductivity, dt: float,

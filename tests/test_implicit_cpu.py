@@ -1,0 +1,78 @@
+"""CPU checks of the implicit-scheme oracle (oracle/implicit_oracle.py), the
+checker of the library's implicit comparator: known answers of the
+conservative curvilinear stencil (stencils.jl:14-40, edge_terms.jl:31-87)."""
+import numpy as np
+
+from helpers import small_case_2d
+from oracle.implicit_oracle import ImplicitOracle
+from curvilineardiffusionmanuscript_b200.mesh import wavy_mesh_2d
+from curvilineardiffusionmanuscript_b200.solver import DirichletBC, NeumannBC, PeriodicBC
+
+
+def _assemble(pr, dt=None):
+    o = ImplicitOracle(pr.mesh, pr.bcs)
+    T, rho = pr.T0.numpy().copy(), pr.rho.numpy().copy()
+    from oracle.oracle import applybcs
+    m = pr.mesh
+    applybcs(2, m.ni, m.nj, 1, m.nhalo, pr.bcs, T)
+    applybcs(2, m.ni, m.nj, 1, m.nhalo, pr.bcs, rho)
+    A, b, c, alpha = o.assemble(T, rho, pr.cp, pr.kappa.k0, pr.kappa.n, dt or pr.dt)
+    return o, A, b, c, alpha
+
+
+def test_stencil_rows_sum_to_the_cell_volume():
+    """The conservative form: every flux term appears with both signs, so an
+    interior row applied to a constant field gives J (wavy mesh, κ = T³)."""
+    pr = small_case_2d(ni=31, nj=23, amp=0.07)
+    o, A, b, c, _ = _assemble(pr, dt=1e-3)
+    J = o._r2(pr.mesh.cell_J)[1:-1, 1:-1]
+    rows = c[:, 1:-1, 1:-1].sum(axis=0)
+    assert np.max(np.abs(rows - J) / J) < 1e-11
+    # boundary rows: Neumann constraints annihilate constants too
+    y = (A @ np.ones(o.N)).reshape(o.n2, o.n1)
+    assert np.allclose(y[0, 1:-1], 0.0) and np.allclose(y[1:-1, 0], 0.0)
+
+
+def test_uniform_mesh_gives_the_five_point_operator():
+    """Rectilinear h x h cells, constant α: no cross terms, neighbour entries
+    -αΔt, diagonal J + 4αΔt."""
+    n = 12
+    m = wavy_mesh_2d(n, n, amp=0.0)
+    x, y = m.centroids
+    import torch
+    from curvilineardiffusionmanuscript_b200 import problems
+    from curvilineardiffusionmanuscript_b200.solver import PowerLawConductivity
+    T0 = (1.0 + 0.0 * x).contiguous()
+    pr = problems.Problem("u", m, [NeumannBC()] * 4, T0, torch.ones_like(T0), 1.0, PowerLawConductivity(2.0, 0.0),
+                          1e-3, 1)
+    o, A, b, c, alpha = _assemble(pr)
+    I = (slice(1, -1), slice(1, -1))
+    h2 = (1.0 / n) ** 2
+    for e in (0, 2, 6, 8):
+        assert np.max(np.abs(c[e][I])) < 1e-17
+    for e in (1, 3, 5, 7):
+        assert np.allclose(c[e][I], -2.0 * 1e-3, rtol=1e-12)
+    assert np.allclose(c[4][I], h2 + 8.0 * 1e-3, rtol=1e-12)
+    assert np.allclose(b.reshape(o.n2, o.n1)[I], h2, rtol=1e-12)
+
+
+def test_boundary_rows_follow_the_side_kinds():
+    pr = small_case_2d(ni=9, nj=7, bcs=[DirichletBC(1.5), DirichletBC(0.5), PeriodicBC(), PeriodicBC()])
+    o, A, b, c, _ = _assemble(pr)
+    b2 = b.reshape(o.n2, o.n1)
+    assert np.all(b2[:, 0] == 1.5) and np.all(b2[:, -1] == 0.5)  # ilo/ihi first, corners included
+    assert np.all(b2[0, 1:-1] == 0.0) and np.all(b2[-1, 1:-1] == 0.0)
+    A = A.tocsr()
+    r = 0 * o.n1 + 3  # jlo row, i = 3: periodic partner (3, nj) with -1
+    assert A[r, r] == 1.0 and A[r, (o.n2 - 2) * o.n1 + 3] == -1.0 and A[r].nnz == 2
+    r = 4 * o.n1  # ilo row (Dirichlet): the diagonal only
+    assert A[r].nnz == 1 and A[r, r] == 1.0
+
+
+def test_small_time_step_returns_the_input():
+    pr = small_case_2d(ni=16, nj=16)
+    o = ImplicitOracle(pr.mesh, pr.bcs)
+    T = pr.T0.numpy().copy()
+    o.step(T, pr.rho.numpy(), pr.cp, pr.kappa.k0, pr.kappa.n, 1e-16)
+    d = o._r2(T)[1:-1, 1:-1] - o._r2(pr.T0.numpy())[1:-1, 1:-1]
+    assert np.max(np.abs(d)) < 1e-8
