@@ -27,8 +27,9 @@
 //
 // Every Krylov scalar is reduced on the device (per-block partials, the last
 // block of a launch sums them in a fixed order, so results do not depend on
-// timing) and the stopping rule is evaluated there; the host polls every
-// kPollIters iterations.
+// timing) and the stopping rule is evaluated there; kPollIters iterations
+// (five kernels each, which return at once after the rule has stopped the
+// solve) are replayed from one CUDA graph between host polls.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -49,7 +50,7 @@ namespace cdm {
 namespace imp {
 
 constexpr int NT = 256;
-constexpr int kPollIters = 8;
+constexpr int kPollIters = 16;
 
 // Krylov state on the device
 struct KState {
@@ -549,6 +550,7 @@ struct Implicit {
   double last_solve_ms = 0.0;
   int64_t last_spmv = 0;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaGraphExec_t iters_graph = nullptr;  // kPollIters BiCGSTAB iterations
   ~Implicit();
 };
 
@@ -604,6 +606,7 @@ Implicit::~Implicit() {
   if (ev_caller) cudaEventDestroy(ev_caller);
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
+  if (iters_graph) cudaGraphExecDestroy(iters_graph);
   if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -900,15 +903,26 @@ extern "C" int cdm_implicit_step(cdm_implicit* h, double* T, const double* rho, 
       rc = read_state(s, timeout_s - (seconds_now() - t_start));
       continue;
     }
-    for (int k = 0; k < imp::kPollIters; ++k) {
-      imp::k_p<<<s.grid, imp::NT, 0, s.stream>>>(g, V);
-      imp::k_v<<<s.grid, imp::NT, 0, s.stream>>>(g, V);
-      imp::k_s<<<s.grid, imp::NT, 0, s.stream>>>(g, V);
-      imp::k_t<<<s.grid, imp::NT, 0, s.stream>>>(g, V);
-      imp::k_x<<<s.grid, imp::NT, 0, s.stream>>>(g, V);
+    if (!s.iters_graph) {  // the kernels' arguments are fixed for the handle's life
+      cudaGraph_t graph;
+      CDM_CK(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal));
+      for (int k = 0; k < imp::kPollIters; ++k) {
+        imp::k_p<<<s.grid, imp::NT, 0, s.stream>>>(g, V);
+        imp::k_v<<<s.grid, imp::NT, 0, s.stream>>>(g, V);
+        imp::k_s<<<s.grid, imp::NT, 0, s.stream>>>(g, V);
+        imp::k_t<<<s.grid, imp::NT, 0, s.stream>>>(g, V);
+        imp::k_x<<<s.grid, imp::NT, 0, s.stream>>>(g, V);
+      }
+      const cudaError_t le = cudaGetLastError();
+      const cudaError_t ce = cudaStreamEndCapture(s.stream, &graph);
+      CDM_CK(le);
+      CDM_CK(ce);
+      const cudaError_t ie = cudaGraphInstantiate(&s.iters_graph, graph, 0);
+      cudaGraphDestroy(graph);
+      CDM_CK(ie);
     }
+    CDM_CK(cudaGraphLaunch(s.iters_graph, s.stream));
     fresh = false;
-    CDM_CK(cudaGetLastError());
     rc = read_state(s, timeout_s - (seconds_now() - t_start));
     if (rc == CDM_OK && seconds_now() - t_start > timeout_s) {
       set_error("step exceeded its wall-clock limit");
