@@ -26,6 +26,7 @@ step one time step of every sampled problem after the warm-up steps; the
                   [--precision fp64|fp64_exact|mixed] [--tuning V,H,K]
   python bench.py --compare [--workload W]     seconds per time step, FP64 vs mixed (vs learned)
   python bench.py --net-timing N               guess network: training step and N^2 prediction
+  python bench.py --implicit N                 the implicit comparator, s/timestep on the N^2 multi-Gaussian
 
 Without --tuning the kernel variant, strip height and iteration block are
 chosen by the library's autotuner before the warm-up (outside the timed
@@ -75,6 +76,8 @@ def parse():
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the per-time-step FP64 / mixed / learned comparison of the default line")
     ap.add_argument("--compare-steps", type=int, default=3)
+    ap.add_argument("--implicit", type=int, default=0, metavar="N",
+                    help="time the implicit comparator on the N^2 multi-Gaussian problem (--steps, --warmup)")
     return ap.parse_args()
 
 
@@ -668,8 +671,27 @@ def run_net_timing(args):
     print(json.dumps(out), flush=True)
 
 
+def run_implicit(args):
+    """Seconds per time step of the implicit comparator on the N² multi-Gaussian
+    problem (κ = T³, seed 0), one JSON line."""
+    import torch
+    from curvilineardiffusionmanuscript_b200 import problems
+    dev = torch.device("cuda", 0)
+    pr = problems.multi_gaussian_2d(args.implicit, seed=0, device=dev)
+    r = time_implicit(pr, args.steps, args.warmup, torch.cuda.current_stream(dev))
+    r.update(n=args.implicit, rows=(args.implicit + 2) ** 2)
+    peak, kind = measured_peak()
+    if r["solve_GBs"]:
+        r["roofline"] = {"bound": "hbm", "achieved": r["solve_GBs"], "peak": peak, "unit": "GB/s",
+                         "frac": r["solve_GBs"] / peak, "peak_kind": kind}
+    print(json.dumps({"implicit": r}), flush=True)
+
+
 def main():
     args = parse()
+    if args.implicit:
+        run_implicit(args)
+        return
     if args.net_timing:
         run_net_timing(args)
         return
