@@ -97,27 +97,6 @@ __device__ __forceinline__ long long partner(const Geo& g, int i2, int j2, long 
   return -1;
 }
 
-// (A x)[r]
-__device__ __forceinline__ double spmv_row(const Geo& g, const double* __restrict__ A, const double* x,
-                                           long long r) {
-  const int i2 = (int)(r % g.n1), j2 = (int)(r / g.n1);
-  if (i2 > 0 && i2 < g.n1 - 1 && j2 > 0 && j2 < g.n2 - 1) {
-    const long long N = g.N, n1 = g.n1;
-    double y = A[4 * N + r] * x[r];
-    y = fma(A[0 * N + r], x[r - n1 - 1], y);
-    y = fma(A[1 * N + r], x[r - n1], y);
-    y = fma(A[2 * N + r], x[r - n1 + 1], y);
-    y = fma(A[3 * N + r], x[r - 1], y);
-    y = fma(A[5 * N + r], x[r + 1], y);
-    y = fma(A[6 * N + r], x[r + n1 - 1], y);
-    y = fma(A[7 * N + r], x[r + n1], y);
-    y = fma(A[8 * N + r], x[r + n1 + 1], y);
-    return y;
-  }
-  const long long c = partner(g, i2, j2, r);
-  return c >= 0 ? x[r] - x[c] : x[r];
-}
-
 // ------------------------------------------------------------ block reductions
 template <int K>
 __device__ __forceinline__ void block_sum(double (&v)[K], double* s_red) {
@@ -295,6 +274,54 @@ struct Vecs {
   KState* ks;
 };
 
+// The iteration kernels keep several rows' loads in flight per thread: rows
+// r0 + k·stride (k < U) are loaded first, then combined and stored, with
+// 32-bit row arithmetic (the diffusion region has fewer than 2^31 rows).
+constexpr int U = 4;   // rows per thread and loop trip, streaming kernels
+constexpr int US = 2;  // the same for the products with A (19 loads per row)
+
+__device__ __forceinline__ void row_pos(const Geo& g, int r, int& i2, int& j2) {
+  j2 = (int)((unsigned)r / (unsigned)g.n1);
+  i2 = r - j2 * g.n1;
+}
+
+// the 9 stencil loads of row r (interior) or its constraint row
+struct RowProd {
+  double a[9], x[9];
+  bool inner;
+  long long c;
+};
+
+__device__ __forceinline__ void load_row(const Geo& g, const double* __restrict__ A, const double* x, int r,
+                                         RowProd& q) {
+  int i2, j2;
+  row_pos(g, r, i2, j2);
+  q.inner = i2 > 0 && i2 < g.n1 - 1 && j2 > 0 && j2 < g.n2 - 1;
+  if (q.inner) {
+    const long long N = g.N;
+    const int n1 = g.n1;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      const int di = e % 3 - 1, dj = e / 3 - 1;
+      q.a[e] = __ldg(&A[e * N + r]);
+      q.x[e] = x[r + di + dj * n1];
+    }
+  } else {
+    q.c = partner(g, i2, j2, r);
+    q.x[4] = x[r];
+    q.x[0] = q.c >= 0 ? x[q.c] : 0.0;
+  }
+}
+
+__device__ __forceinline__ double row_value(const RowProd& q) {
+  if (!q.inner) return q.c >= 0 ? q.x[4] - q.x[0] : q.x[4];
+  double y = q.a[4] * q.x[4];
+#pragma unroll
+  for (int e = 0; e < 9; ++e)
+    if (e != 4) y = fma(q.a[e], q.x[e], y);
+  return y;
+}
+
 // r = b - A x; r̂ = r; p = v = 0 and the scalars of a fresh Krylov cycle.
 // first = 1: also ||r0||, the stopping tolerance and the iteration count;
 // otherwise (restart or the final check) done = (||r|| <= tol)
@@ -302,8 +329,11 @@ __global__ void __launch_bounds__(NT) k_restart(Geo g, Vecs V, int first, double
   __shared__ double s_red[2 * NT / 32];
   __shared__ int s_last;
   double acc[1] = {0.0};
-  for (long long r = blockIdx.x * (long long)NT + threadIdx.x; r < g.N; r += (long long)gridDim.x * NT) {
-    const double rr = V.b[r] - spmv_row(g, V.A, V.x, r);
+  const int N = (int)g.N;
+  for (int r = blockIdx.x * NT + threadIdx.x; r < N; r += gridDim.x * NT) {
+    RowProd q;
+    load_row(g, V.A, V.x, r, q);
+    const double rr = V.b[r] - row_value(q);
     V.r[r] = rr;
     V.rh[r] = rr;
     V.p[r] = 0.0;
@@ -340,10 +370,33 @@ __global__ void __launch_bounds__(NT) k_p(Geo g, Vecs V) {
   const KState* K = V.ks;
   if (K->done) return;
   const double beta = (K->rho1 / K->rho0) * (K->alpha / K->omega), om = K->omega;
-  for (long long r = blockIdx.x * (long long)NT + threadIdx.x; r < g.N; r += (long long)gridDim.x * NT) {
-    const double p = V.r[r] + beta * (V.p[r] - om * V.v[r]);
-    V.p[r] = p;
-    V.ph[r] = V.dinv[r] * p;
+  const int N = (int)g.N, stride = gridDim.x * NT;
+  const double* __restrict__ R = V.r;
+  const double* __restrict__ D = V.dinv;
+  const double* __restrict__ Vv = V.v;
+  double* __restrict__ P = V.p;
+  double* __restrict__ Ph = V.ph;
+  for (int r0 = blockIdx.x * NT + threadIdx.x; r0 < N; r0 += U * stride) {
+    double rr[U], pp[U], vv[U], dd[U];
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      const int r = r0 + k * stride;
+      if (r < N) {
+        rr[k] = R[r];
+        pp[k] = P[r];
+        vv[k] = Vv[r];
+        dd[k] = __ldg(&D[r]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      const int r = r0 + k * stride;
+      if (r < N) {
+        const double p = rr[k] + beta * (pp[k] - om * vv[k]);
+        P[r] = p;
+        Ph[r] = dd[k] * p;
+      }
+    }
   }
 }
 
@@ -354,10 +407,27 @@ __global__ void __launch_bounds__(NT) k_v(Geo g, Vecs V) {
   KState* K = V.ks;
   if (K->done) return;
   double acc[1] = {0.0};
-  for (long long r = blockIdx.x * (long long)NT + threadIdx.x; r < g.N; r += (long long)gridDim.x * NT) {
-    const double v = spmv_row(g, V.A, V.ph, r);
-    V.v[r] = v;
-    acc[0] = fma(V.rh[r], v, acc[0]);
+  const int N = (int)g.N, stride = gridDim.x * NT;
+  for (int r0 = blockIdx.x * NT + threadIdx.x; r0 < N; r0 += US * stride) {
+    RowProd q[US];
+    double h[US];
+#pragma unroll
+    for (int k = 0; k < US; ++k) {
+      const int r = r0 + k * stride;
+      if (r < N) {
+        load_row(g, V.A, V.ph, r, q[k]);
+        h[k] = V.rh[r];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < US; ++k) {
+      const int r = r0 + k * stride;
+      if (r < N) {
+        const double v = row_value(q[k]);
+        V.v[r] = v;
+        acc[0] = fma(h[k], v, acc[0]);
+      }
+    }
   }
   double out[1];
   if (!grid_sum<1>(acc, V.part, &K->arrive[1], s_red, &s_last, out)) return;
@@ -376,10 +446,32 @@ __global__ void __launch_bounds__(NT) k_s(Geo g, Vecs V) {
   const KState* K = V.ks;
   if (K->done) return;
   const double al = K->alpha;
-  for (long long r = blockIdx.x * (long long)NT + threadIdx.x; r < g.N; r += (long long)gridDim.x * NT) {
-    const double s = V.r[r] - al * V.v[r];
-    V.s[r] = s;
-    V.sh[r] = V.dinv[r] * s;
+  const int N = (int)g.N, stride = gridDim.x * NT;
+  const double* __restrict__ R = V.r;
+  const double* __restrict__ Vv = V.v;
+  const double* __restrict__ D = V.dinv;
+  double* __restrict__ S = V.s;
+  double* __restrict__ Sh = V.sh;
+  for (int r0 = blockIdx.x * NT + threadIdx.x; r0 < N; r0 += U * stride) {
+    double rr[U], vv[U], dd[U];
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      const int r = r0 + k * stride;
+      if (r < N) {
+        rr[k] = R[r];
+        vv[k] = Vv[r];
+        dd[k] = __ldg(&D[r]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      const int r = r0 + k * stride;
+      if (r < N) {
+        const double sv = rr[k] - al * vv[k];
+        S[r] = sv;
+        Sh[r] = dd[k] * sv;
+      }
+    }
   }
 }
 
@@ -390,11 +482,28 @@ __global__ void __launch_bounds__(NT) k_t(Geo g, Vecs V) {
   KState* K = V.ks;
   if (K->done) return;
   double acc[2] = {0.0, 0.0};
-  for (long long r = blockIdx.x * (long long)NT + threadIdx.x; r < g.N; r += (long long)gridDim.x * NT) {
-    const double t = spmv_row(g, V.A, V.sh, r);
-    V.t[r] = t;
-    acc[0] = fma(t, V.s[r], acc[0]);
-    acc[1] = fma(t, t, acc[1]);
+  const int N = (int)g.N, stride = gridDim.x * NT;
+  for (int r0 = blockIdx.x * NT + threadIdx.x; r0 < N; r0 += US * stride) {
+    RowProd q[US];
+    double sv[US];
+#pragma unroll
+    for (int k = 0; k < US; ++k) {
+      const int r = r0 + k * stride;
+      if (r < N) {
+        load_row(g, V.A, V.sh, r, q[k]);
+        sv[k] = V.s[r];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < US; ++k) {
+      const int r = r0 + k * stride;
+      if (r < N) {
+        const double t = row_value(q[k]);
+        V.t[r] = t;
+        acc[0] = fma(t, sv[k], acc[0]);
+        acc[1] = fma(t, t, acc[1]);
+      }
+    }
   }
   double out[2];
   if (!grid_sum<2>(acc, V.part, &K->arrive[2], s_red, &s_last, out)) return;
@@ -412,12 +521,39 @@ __global__ void __launch_bounds__(NT) k_x(Geo g, Vecs V) {
   if (K->done) return;
   const double al = K->alpha, om = K->omega;
   double acc[2] = {0.0, 0.0};
-  for (long long r = blockIdx.x * (long long)NT + threadIdx.x; r < g.N; r += (long long)gridDim.x * NT) {
-    V.x[r] = V.x[r] + al * V.ph[r] + om * V.sh[r];
-    const double rr = V.s[r] - om * V.t[r];
-    V.r[r] = rr;
-    acc[0] = fma(V.rh[r], rr, acc[0]);
-    acc[1] = fma(rr, rr, acc[1]);
+  const int N = (int)g.N, stride = gridDim.x * NT;
+  double* __restrict__ X = V.x;
+  double* __restrict__ R = V.r;
+  const double* __restrict__ Ph = V.ph;
+  const double* __restrict__ Sh = V.sh;
+  const double* __restrict__ S = V.s;
+  const double* __restrict__ T = V.t;
+  const double* __restrict__ Rh = V.rh;
+  for (int r0 = blockIdx.x * NT + threadIdx.x; r0 < N; r0 += U * stride) {
+    double xx[U], ph[U], sh[U], ss[U], tt[U], rh[U];
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      const int r = r0 + k * stride;
+      if (r < N) {
+        xx[k] = X[r];
+        ph[k] = Ph[r];
+        sh[k] = Sh[r];
+        ss[k] = S[r];
+        tt[k] = T[r];
+        rh[k] = Rh[r];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      const int r = r0 + k * stride;
+      if (r < N) {
+        X[r] = xx[k] + al * ph[k] + om * sh[k];
+        const double rr = ss[k] - om * tt[k];
+        R[r] = rr;
+        acc[0] = fma(rh[k], rr, acc[0]);
+        acc[1] = fma(rr, rr, acc[1]);
+      }
+    }
   }
   double out[2];
   if (!grid_sum<2>(acc, V.part, &K->arrive[3], s_red, &s_last, out)) return;
@@ -752,6 +888,10 @@ extern "C" int cdm_implicit_create(const cdm_mesh_desc* mesh, const cdm_bc* bcs,
   }
   if (mesh->ni < 1 || mesh->nj < 1 || mesh->nhalo < 1) {
     set_error("mesh sizes must be >= 1 and nhalo >= 1");
+    return CDM_BAD_INPUT;
+  }
+  if ((long long)(mesh->ni + 2) * (mesh->nj + 2) >= (1ll << 31)) {
+    set_error("the implicit system takes fewer than 2^31 rows");
     return CDM_BAD_INPUT;
   }
   for (int l = 0; l < 4; ++l)
