@@ -509,9 +509,9 @@ def time_single(pr, precision, steps, warmup, stream, net=None, rtol=None, max_i
 
 
 # algorithmic bytes per row of one BiCGSTAB iteration of the implicit solve: the
-# nine stencil entries twice (two products with A) and the vectors its five
-# kernels read and write (p, p̂, v, s, ŝ, t, x, r, r̂, D⁻¹), 43 doubles
-IMPLICIT_BYTES_PER_ROW_ITER = 43 * 8
+# stored stencil entries twice (two products with A; 9 in 2D, 19 in 3D) and the
+# 25 vector reads and writes of its five kernels (p, p̂, v, s, ŝ, t, x, r, r̂, D⁻¹)
+IMPLICIT_BYTES_PER_ROW_ITER = {2: (2 * 9 + 25) * 8, 3: (2 * 19 + 25) * 8}
 
 
 def time_implicit(pr, steps, warmup, stream):
@@ -537,12 +537,13 @@ def time_implicit(pr, steps, warmup, stream):
                 iters.append(st["niter"])
                 res.append(st["abs_err"])
                 if pf["solve_ms"] > 0:
-                    gbs.append(IMPLICIT_BYTES_PER_ROW_ITER * pf["rows"] * st["niter"] / (pf["solve_ms"] / 1e3) / 1e9)
+                    gbs.append(IMPLICIT_BYTES_PER_ROW_ITER[pr.mesh.ndim] * pf["rows"] * st["niter"]
+                               / (pf["solve_ms"] / 1e3) / 1e9)
         return {"s_per_step": statistics.median(times), "krylov_iters": statistics.mean(iters),
                 "final_residual_2norm": statistics.mean(res), "tol": "atol = rtol = 1e-9 (2-norm)",
                 "solver": "BiCGSTAB, Jacobi preconditioner on the right",
                 "solve_GBs": statistics.mean(gbs) if gbs else None,
-                "bytes_per_row_iter": IMPLICIT_BYTES_PER_ROW_ITER}
+                "bytes_per_row_iter": IMPLICIT_BYTES_PER_ROW_ITER[pr.mesh.ndim]}
     finally:
         g.close()
 

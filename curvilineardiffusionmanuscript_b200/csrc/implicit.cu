@@ -64,36 +64,57 @@ enum { KS_OK = 0, KS_MAX_ITER = 1, KS_NONFINITE = 2 };
 enum { CONV_NO = 0, CONV_TOL = 1, CONV_BREAKDOWN = 2 };
 
 struct Geo {
-  int ni, nj, nh, nx;  // domain, halo layers, full row length of the mesh arrays
-  int n1, n2;          // diffusion region (ni + 2) x (nj + 2)
+  int nd;                  // 2 or 3
+  int ni, nj, nk, nh;      // domain cells (nk = 1 in 2D), halo layers of the mesh arrays
+  int nx, ny;              // full row and column lengths of the mesh arrays
+  int n1, n2, n3;          // diffusion region (n3 = 1 in 2D)
   long long N;
-  int kind[4];         // side kinds (cdm_bc_kind): ilo, ihi, jlo, jhi
-  double val[4];       // Dirichlet values
-  int rule[4];         // ghost rules of applybcs! (GhostRule, folded per side)
+  int kind[6];             // side kinds (cdm_bc_kind): ilo, ihi, jlo, jhi, klo, khi
+  double val[6];           // Dirichlet values
+  int rule[6];             // ghost rules of applybcs! (GhostRule, folded per side)
 };
 
-__device__ __forceinline__ long long mesh_index(const Geo& g, int i2, int j2) {
-  return (long long)(i2 - 1 + g.nh) + (long long)g.nx * (long long)(j2 - 1 + g.nh);
+__device__ __forceinline__ void row_pos(const Geo& g, int r, int& i2, int& j2, int& k2) {
+  const unsigned plane = (unsigned)g.n1 * (unsigned)g.n2;
+  k2 = (int)((unsigned)r / plane);
+  const int rem = r - k2 * (int)plane;
+  j2 = (int)((unsigned)rem / (unsigned)g.n1);
+  i2 = rem - j2 * g.n1;
+}
+
+__device__ __forceinline__ long long mesh_index(const Geo& g, int i2, int j2, int k2) {
+  const long long kz = g.nd == 3 ? (long long)(k2 - 1 + g.nh) : 0;
+  return (long long)(i2 - 1 + g.nh) + (long long)g.nx * ((long long)(j2 - 1 + g.nh) + (long long)g.ny * kz);
+}
+
+// number of region-2 coordinates on the region's boundary (0: interior row)
+__device__ __forceinline__ int on_boundary(const Geo& g, int i2, int j2, int k2) {
+  return (i2 == 0 || i2 == g.n1 - 1) + (j2 == 0 || j2 == g.n2 - 1) + (g.nd == 3 && (k2 == 0 || k2 == g.n3 - 1));
 }
 
 // the column of the one off-diagonal entry of a boundary row, -1 for none
-// (init_matrix.jl:69-167: corners and Dirichlet rows have the diagonal only)
-__device__ __forceinline__ long long partner(const Geo& g, int i2, int j2, long long r) {
-  const bool ib = i2 == 0 || i2 == g.n1 - 1, jb = j2 == 0 || j2 == g.n2 - 1;
-  if (ib && jb) return -1;
-  if (i2 == 0) {
-    if (g.kind[0] == CDM_BC_NEUMANN) return r + 1;
-    if (g.kind[0] == CDM_BC_PERIODIC) return (long long)(g.n1 - 2) + (long long)j2 * g.n1;
-  } else if (i2 == g.n1 - 1) {
-    if (g.kind[1] == CDM_BC_NEUMANN) return r - 1;
-    if (g.kind[1] == CDM_BC_PERIODIC) return 1 + (long long)j2 * g.n1;
-  } else if (j2 == 0) {
-    if (g.kind[2] == CDM_BC_NEUMANN) return r + g.n1;
-    if (g.kind[2] == CDM_BC_PERIODIC) return (long long)i2 + (long long)(g.n2 - 2) * g.n1;
-  } else if (j2 == g.n2 - 1) {
-    if (g.kind[3] == CDM_BC_NEUMANN) return r - g.n1;
-    if (g.kind[3] == CDM_BC_PERIODIC) return (long long)i2 + (long long)g.n1;
+// (init_matrix.jl:69-167, :252-390: a side's rows over the interior range of
+// the other axes; Dirichlet rows, edges and corners have the diagonal only)
+__device__ __forceinline__ long long partner(const Geo& g, int i2, int j2, int k2, long long r) {
+  if (on_boundary(g, i2, j2, k2) != 1) return -1;
+  int side, n;
+  long long st;
+  if (i2 == 0 || i2 == g.n1 - 1) {
+    side = i2 == 0 ? 0 : 1;
+    st = 1;
+    n = g.n1;
+  } else if (j2 == 0 || j2 == g.n2 - 1) {
+    side = j2 == 0 ? 2 : 3;
+    st = g.n1;
+    n = g.n2;
+  } else {
+    side = k2 == 0 ? 4 : 5;
+    st = (long long)g.n1 * g.n2;
+    n = g.n3;
   }
+  const bool lo = (side & 1) == 0;
+  if (g.kind[side] == CDM_BC_NEUMANN) return lo ? r + st : r - st;
+  if (g.kind[side] == CDM_BC_PERIODIC) return lo ? r + (long long)(n - 2) * st : r - (long long)(n - 2) * st;
   return -1;
 }
 
@@ -152,54 +173,65 @@ __device__ bool grid_sum(double (&v)[K], double* part, unsigned int* arrive, dou
 // --------------------------------------------------------------- set-up work
 // applybcs! (boundary_operators.jl:26-263) on a full mesh array, every side in
 // one launch: a side writes only its own ghost slab (the other axes over the
-// domain, corners never written) and reads only domain cells, so the sides do
-// not depend on one another.  blockIdx.y = side.
+// domain, edges and corners never written) and reads only domain cells, so
+// the sides do not depend on one another.  blockIdx.y = side.
 __global__ void ghost_fill(Geo g, double* u) {
   const int side = blockIdx.y, axis = side >> 1;
   const bool lo = (side & 1) == 0;
-  const int len = axis == 0 ? g.nj : g.ni;
   const int rule = g.rule[side];
-  const int nh = g.nh, ni = g.ni, nj = g.nj, nx = g.nx;
-  auto at = [&](int p, int a) -> long long {  // p along the axis (full coordinates), a the domain position
-    return axis == 0 ? (long long)p + (long long)nx * (a + nh) : (long long)(a + nh) + (long long)nx * p;
-  };
-  const int dlo = nh, dhi = nh + (axis == 0 ? ni : nj) - 1;
-  const int nfull = (axis == 0 ? ni : nj) + 2 * nh;
-  for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < len; a += gridDim.x * blockDim.x) {
+  const int nh = g.nh;
+  const int dims[3] = {g.ni, g.nj, g.nk};
+  const int e0 = axis == 0 ? g.nj : g.ni;                       // first other axis (domain extent)
+  const int e1 = axis == 2 ? g.nj : (g.nd == 3 ? g.nk : 1);     // second other axis
+  const long long sx = 1, sy = g.nx, sz = (long long)g.nx * g.ny;
+  const long long sa = axis == 0 ? sx : axis == 1 ? sy : sz;    // stride along the axis
+  const long long s0 = axis == 0 ? sy : sx;
+  const long long s1 = axis == 2 ? sy : sz;
+  const int k0 = g.nd == 3 ? nh : 0;                            // full offset of the second other axis (2D: z = 0)
+  const int dlo = nh, dhi = nh + dims[axis] - 1, nfull = dims[axis] + 2 * nh;
+  const long long len = (long long)e0 * e1;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < len; q += (long long)gridDim.x * blockDim.x) {
+    const int a0 = (int)(q % e0), a1 = (int)(q / e0);
+    const long long base = (long long)(a0 + nh) * s0 + (long long)(a1 + (axis == 2 ? nh : k0)) * s1;
+    auto at = [&](int p) { return base + (long long)p * sa; };
     if (rule == GR_NEUMANN) {
-      if (lo) u[at(dlo - 1, a)] = u[at(dlo, a)];
-      else u[at(dhi + 1, a)] = u[at(dhi, a)];
-    } else if (rule == GR_DIRICHLET) {  // 2D: every halo layer (:137-155)
-      if (lo)
-        for (int p = 0; p < dlo; ++p) u[at(p, a)] = g.val[side];
-      else
-        for (int p = dhi + 1; p < nfull; ++p) u[at(p, a)] = g.val[side];
+      if (lo) u[at(dlo - 1)] = u[at(dlo)];
+      else u[at(dhi + 1)] = u[at(dhi)];
+    } else if (rule == GR_DIRICHLET) {
+      if (g.nd == 2) {  // every halo layer (:137-155)
+        if (lo)
+          for (int p = 0; p < dlo; ++p) u[at(p)] = g.val[side];
+        else
+          for (int p = dhi + 1; p < nfull; ++p) u[at(p)] = g.val[side];
+      } else {  // one layer (:178-200)
+        u[at(lo ? dlo - 1 : dhi + 1)] = g.val[side];
+      }
     } else if (rule == GR_PERIODIC) {
-      if (lo) u[at(dlo - 1, a)] = u[at(dhi, a)];
-      else u[at(dhi + 1, a)] = u[at(dlo, a)];
+      if (lo) u[at(dlo - 1)] = u[at(dhi)];
+      else u[at(dhi + 1)] = u[at(dlo)];
     } else if (rule == GR_NEGSYM) {
-      if (lo) u[at(dlo - 1, a)] = -u[at(dlo, a)];
-      else u[at(dhi + 1, a)] = -u[at(dhi, a)];
+      if (lo) u[at(dlo - 1)] = -u[at(dlo)];
+      else u[at(dhi + 1)] = -u[at(dhi)];
     }
   }
 }
 
 // update_conductivity! with scalar cp (conductivity.jl:93-104) over the
 // diffusion region; flags a non-finite diffusivity on the domain and its first
-// halo layer without the corners (validate_scalar, validity_checks.jl:1-43)
+// halo layer without edges and corners (validate_scalar, validity_checks.jl:1-43)
 __global__ void diffusivity_kernel(Geo g, const double* __restrict__ T, const double* __restrict__ rho,
                                    double cp, double k0, int kmode, int km, int khalf, double kn,
                                    double* __restrict__ alpha, int* bad) {
-  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < g.N;
-       r += (long long)gridDim.x * blockDim.x) {
-    const int i2 = (int)(r % g.n1), j2 = (int)(r / g.n1);
-    const long long m = mesh_index(g, i2, j2);
+  const int N = (int)g.N;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < N; r += gridDim.x * blockDim.x) {
+    int i2, j2, k2;
+    row_pos(g, r, i2, j2, k2);
+    const long long m = mesh_index(g, i2, j2, k2);
     const double t = T[m];
     const double kap = isfinite(t) ? k0 * pow_model(fabs(t), kmode, km, khalf, kn) : 0.0;
     const double a = fabs(kap / (rho[m] * cp));
     alpha[r] = a;
-    const bool corner = (i2 == 0 || i2 == g.n1 - 1) && (j2 == 0 || j2 == g.n2 - 1);
-    if (!corner && !isfinite(a)) atomicOr(bad, 1);
+    if (on_boundary(g, i2, j2, k2) < 2 && !isfinite(a)) atomicOr(bad, 1);
   }
 }
 
@@ -208,9 +240,15 @@ __device__ __forceinline__ double face_mean_ref(int mean, double a, double b) {
 }
 
 struct EdgeMetrics {
-  const double* J[2];     // edge_metrics.{i+1/2, j+1/2}.J
-  const double* hat[2][4];  // ξ̂.x₁, ξ̂.x₂, η̂.x₁, η̂.x₂ of each face family
+  const double* J[3];       // edge_metrics.{i+1/2, j+1/2, k+1/2}.J
+  const double* hat[3][9];  // {ξ̂, η̂, ζ̂}.{x₁, x₂, x₃} of each face family, [3a + c]
 };
+
+// bc_operator (inner_operators.jl:188-236): ilo, ihi, jlo, jhi, klo, khi in that order
+__device__ __forceinline__ double bc_rhs(const Geo& g, int i2, int j2, int k2) {
+  const int side = i2 == 0 ? 0 : i2 == g.n1 - 1 ? 1 : j2 == 0 ? 2 : j2 == g.n2 - 1 ? 3 : k2 == 0 ? 4 : 5;
+  return g.kind[side] == CDM_BC_DIRICHLET ? g.val[side] : 0.0;
+}
 
 // _assembly_kernel_2d (inner_operators.jl:62-105): interior rows get the
 // stencil of stencils.jl:14-40 built from conservative_edge_terms
@@ -221,17 +259,15 @@ __global__ void assemble_kernel(Geo g, int mean, double dt, const double* __rest
                                 const double* __restrict__ cellJ, EdgeMetrics em, double* __restrict__ A,
                                 double* __restrict__ b, double* __restrict__ dinv) {
   const long long N = g.N;
-  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N; r += (long long)gridDim.x * blockDim.x) {
-    const int i2 = (int)(r % g.n1), j2 = (int)(r / g.n1);
-    const bool onbc = i2 == 0 || i2 == g.n1 - 1 || j2 == 0 || j2 == g.n2 - 1;
-    if (onbc) {
-      // bc_operator (inner_operators.jl:188-211): ilo, ihi, jlo, jhi in that order
-      const int side = i2 == 0 ? 0 : i2 == g.n1 - 1 ? 1 : j2 == 0 ? 2 : 3;
-      b[r] = g.kind[side] == CDM_BC_DIRICHLET ? g.val[side] : 0.0;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < (int)N; r += gridDim.x * blockDim.x) {
+    int i2, j2, k2;
+    row_pos(g, r, i2, j2, k2);
+    if (on_boundary(g, i2, j2, k2)) {
+      b[r] = bc_rhs(g, i2, j2, k2);
       dinv[r] = 1.0;
       continue;
     }
-    const long long m = mesh_index(g, i2, j2);
+    const long long m = mesh_index(g, i2, j2, k2);
     const long long mi = m - 1, mj = m - g.nx;  // cells whose +1/2 faces are this cell's -1/2 faces
     const double ac = alpha[r];
     const double a_ip = face_mean_ref(mean, ac, alpha[r + 1]);
@@ -239,16 +275,17 @@ __global__ void assemble_kernel(Geo g, int mean, double dt, const double* __rest
     const double a_jp = face_mean_ref(mean, ac, alpha[r + g.n1]);
     const double a_jm = face_mean_ref(mean, ac, alpha[r - g.n1]);
     const double Jip = em.J[0][m], Jim = em.J[0][mi], Jjp = em.J[1][m], Jjm = em.J[1][mj];
-    double xx = em.hat[0][0][m], xy = em.hat[0][1][m], ex = em.hat[0][2][m], ey = em.hat[0][3][m];
+    // ξ̂.x₁ = [0], ξ̂.x₂ = [1], η̂.x₁ = [3], η̂.x₂ = [4]
+    double xx = em.hat[0][0][m], xy = em.hat[0][1][m], ex = em.hat[0][3][m], ey = em.hat[0][4][m];
     const double a_xi2_ip = a_ip * (xx * xx + xy * xy) / Jip;
     const double a_xieta_ip = a_ip * (xx * ex + xy * ey) / (4.0 * Jip);
-    xx = em.hat[0][0][mi], xy = em.hat[0][1][mi], ex = em.hat[0][2][mi], ey = em.hat[0][3][mi];
+    xx = em.hat[0][0][mi], xy = em.hat[0][1][mi], ex = em.hat[0][3][mi], ey = em.hat[0][4][mi];
     const double a_xi2_im = a_im * (xx * xx + xy * xy) / Jim;
     const double a_xieta_im = a_im * (xx * ex + xy * ey) / (4.0 * Jim);
-    xx = em.hat[1][0][m], xy = em.hat[1][1][m], ex = em.hat[1][2][m], ey = em.hat[1][3][m];
+    xx = em.hat[1][0][m], xy = em.hat[1][1][m], ex = em.hat[1][3][m], ey = em.hat[1][4][m];
     const double a_eta2_jp = a_jp * (ex * ex + ey * ey) / Jjp;
     const double a_etaxi_jp = a_jp * (xx * ex + xy * ey) / (4.0 * Jjp);
-    xx = em.hat[1][0][mj], xy = em.hat[1][1][mj], ex = em.hat[1][2][mj], ey = em.hat[1][3][mj];
+    xx = em.hat[1][0][mj], xy = em.hat[1][1][mj], ex = em.hat[1][3][mj], ey = em.hat[1][4][mj];
     const double a_eta2_jm = a_jm * (ex * ex + ey * ey) / Jjm;
     const double a_etaxi_jm = a_jm * (xx * ex + xy * ey) / (4.0 * Jjm);
     const double Jc = cellJ[m];
@@ -267,6 +304,105 @@ __global__ void assemble_kernel(Geo g, int mean, double dt, const double* __rest
   }
 }
 
+// the 18 conservative edge terms of one face (edge_terms.jl:235-257): the
+// face's J and J-scaled metric vectors ξ̂, η̂, ζ̂ at full index m of family f
+struct Face3 {
+  double J, v[3][3];
+};
+__device__ __forceinline__ Face3 face3(const EdgeMetrics& em, int f, long long m) {
+  Face3 F;
+  F.J = em.J[f][m];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) F.v[a][c] = em.hat[f][3 * a + c][m];
+  return F;
+}
+__device__ __forceinline__ double dot3(const double* u, const double* v) {
+  return u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+}
+
+// _assembly_kernel_3d (inner_operators.jl:107-160): the 19 non-zero entries of
+// stencils.jl:42-137 (the eight corner entries are zero), stored in slot order
+__global__ void assemble_kernel3(Geo g, int mean, double dt, const double* __restrict__ alpha,
+                                 const double* __restrict__ T, const double* __restrict__ S,
+                                 const double* __restrict__ cellJ, EdgeMetrics em, double* __restrict__ A,
+                                 double* __restrict__ b, double* __restrict__ dinv) {
+  const long long N = g.N;
+  const int n1 = g.n1, n12 = g.n1 * g.n2;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < (int)N; r += gridDim.x * blockDim.x) {
+    int i2, j2, k2;
+    row_pos(g, r, i2, j2, k2);
+    if (on_boundary(g, i2, j2, k2)) {
+      b[r] = bc_rhs(g, i2, j2, k2);
+      dinv[r] = 1.0;
+      continue;
+    }
+    const long long m = mesh_index(g, i2, j2, k2);
+    const long long sxy = (long long)g.nx * g.ny;
+    const double ac = alpha[r];
+    const double a_ip = face_mean_ref(mean, ac, alpha[r + 1]);
+    const double a_im = face_mean_ref(mean, ac, alpha[r - 1]);
+    const double a_jp = face_mean_ref(mean, ac, alpha[r + n1]);
+    const double a_jm = face_mean_ref(mean, ac, alpha[r - n1]);
+    const double a_kp = face_mean_ref(mean, ac, alpha[r + n12]);
+    const double a_km = face_mean_ref(mean, ac, alpha[r - n12]);
+    double xi2_ip, xieta_ip, xizeta_ip, xi2_im, xieta_im, xizeta_im;
+    double eta2_jp, etaxi_jp, etazeta_jp, eta2_jm, etaxi_jm, etazeta_jm;
+    double zeta2_kp, zetaxi_kp, zetaeta_kp, zeta2_km, zetaxi_km, zetaeta_km;
+    {
+      Face3 F = face3(em, 0, m);
+      xi2_ip = a_ip * dot3(F.v[0], F.v[0]) / F.J;
+      xieta_ip = a_ip * dot3(F.v[0], F.v[1]) / (4.0 * F.J);
+      xizeta_ip = a_ip * dot3(F.v[0], F.v[2]) / (4.0 * F.J);
+      F = face3(em, 0, m - 1);
+      xi2_im = a_im * dot3(F.v[0], F.v[0]) / F.J;
+      xieta_im = a_im * dot3(F.v[0], F.v[1]) / (4.0 * F.J);
+      xizeta_im = a_im * dot3(F.v[0], F.v[2]) / (4.0 * F.J);
+      F = face3(em, 1, m);
+      eta2_jp = a_jp * dot3(F.v[1], F.v[1]) / F.J;
+      etaxi_jp = a_jp * dot3(F.v[0], F.v[1]) / (4.0 * F.J);
+      etazeta_jp = a_jp * dot3(F.v[1], F.v[2]) / (4.0 * F.J);
+      F = face3(em, 1, m - g.nx);
+      eta2_jm = a_jm * dot3(F.v[1], F.v[1]) / F.J;
+      etaxi_jm = a_jm * dot3(F.v[0], F.v[1]) / (4.0 * F.J);
+      etazeta_jm = a_jm * dot3(F.v[1], F.v[2]) / (4.0 * F.J);
+      F = face3(em, 2, m);
+      zeta2_kp = a_kp * dot3(F.v[2], F.v[2]) / F.J;
+      zetaxi_kp = a_kp * dot3(F.v[2], F.v[0]) / (4.0 * F.J);
+      zetaeta_kp = a_kp * dot3(F.v[2], F.v[1]) / (4.0 * F.J);
+      F = face3(em, 2, m - sxy);
+      zeta2_km = a_km * dot3(F.v[2], F.v[2]) / F.J;
+      zetaxi_km = a_km * dot3(F.v[2], F.v[0]) / (4.0 * F.J);
+      zetaeta_km = a_km * dot3(F.v[2], F.v[1]) / (4.0 * F.J);
+    }
+    const double Jc = cellJ[m];
+    const double diag = Jc + (zeta2_kp + zeta2_km + eta2_jp + eta2_jm + xi2_ip + xi2_im) * dt;
+    // compact entries, slot order (slots 1 3 4 5 7 9 10 11 12 13 14 15 16 17 19 21 22 23 25)
+    A[0 * N + r] = (-zetaeta_km - etazeta_jm) * dt;                                  // (0,-1,-1)
+    A[1 * N + r] = (-zetaxi_km - xizeta_im) * dt;                                    // (-1,0,-1)
+    A[2 * N + r] = (-zeta2_km + xizeta_ip - xizeta_im + etazeta_jp - etazeta_jm) * dt;  // (0,0,-1)
+    A[3 * N + r] = (zetaxi_km + xizeta_ip) * dt;                                     // (1,0,-1)
+    A[4 * N + r] = (zetaeta_km + etazeta_jp) * dt;                                   // (0,1,-1)
+    A[5 * N + r] = (-etaxi_jm - xieta_im) * dt;                                      // (-1,-1,0)
+    A[6 * N + r] = (-eta2_jm + xieta_ip - xieta_im + zetaeta_kp - zetaeta_km) * dt;  // (0,-1,0)
+    A[7 * N + r] = (etaxi_jm + xieta_ip) * dt;                                       // (1,-1,0)
+    A[8 * N + r] = (-xi2_im + etaxi_jp - etaxi_jm + zetaxi_kp - zetaxi_km) * dt;     // (-1,0,0)
+    A[9 * N + r] = diag;                                                             // (0,0,0)
+    A[10 * N + r] = (-xi2_ip - etaxi_jp + etaxi_jm - zetaxi_kp + zetaxi_km) * dt;    // (1,0,0)
+    A[11 * N + r] = (etaxi_jp + xieta_im) * dt;                                      // (-1,1,0)
+    A[12 * N + r] = (-eta2_jp - xieta_ip + xieta_im - zetaeta_kp + zetaeta_km) * dt; // (0,1,0)
+    A[13 * N + r] = (-etaxi_jp - xieta_ip) * dt;                                     // (1,1,0)
+    A[14 * N + r] = (zetaeta_kp + etazeta_jm) * dt;                                  // (0,-1,1)
+    A[15 * N + r] = (zetaxi_kp + xizeta_im) * dt;                                    // (-1,0,1)
+    A[16 * N + r] = (-zeta2_kp - xizeta_ip + xizeta_im - etazeta_jp + etazeta_jm) * dt;  // (0,0,1)
+    A[17 * N + r] = (-zetaxi_kp - xizeta_ip) * dt;                                   // (1,0,1)
+    A[18 * N + r] = (-zetaeta_kp - etazeta_jp) * dt;                                 // (0,1,1)
+    b[r] = (S[r] * dt + T[m]) * Jc;
+    dinv[r] = 1.0 / diag;
+  }
+}
+
 // ------------------------------------------------------------- BiCGSTAB
 struct Vecs {
   double *x, *r, *rh, *p, *ph, *v, *s, *sh, *t, *b, *dinv, *part;
@@ -275,64 +411,73 @@ struct Vecs {
 };
 
 // The iteration kernels keep several rows' loads in flight per thread: rows
-// r0 + k·stride (k < U) are loaded first, then combined and stored, with
-// 32-bit row arithmetic (the diffusion region has fewer than 2^31 rows).
-constexpr int U = 4;   // rows per thread and loop trip, streaming kernels
-constexpr int US = 2;  // the same for the products with A (19 loads per row)
+// r0 + k·stride (k < U; the products with A two rows in 2D, one in 3D) are
+// loaded first, then combined and stored, with 32-bit row arithmetic (the
+// diffusion region has fewer than 2^31 rows).
+constexpr int U = 4;  // rows per thread and loop trip, streaming kernels
 
-__device__ __forceinline__ void row_pos(const Geo& g, int r, int& i2, int& j2) {
-  j2 = (int)((unsigned)r / (unsigned)g.n1);
-  i2 = r - j2 * g.n1;
-}
-
-// the 9 stencil loads of row r (interior) or its constraint row
+// one row's product with A: the stored entries of an interior row (9 in 2D,
+// the 19 non-corner entries in 3D, slot order), or its constraint row
+template <int ND>
 struct RowProd {
-  double a[9], x[9];
+  static constexpr int NE = ND == 2 ? 9 : 19;
+  static constexpr int CENTER = ND == 2 ? 4 : 9;
+  double a[NE], x[NE];
   bool inner;
   long long c;
 };
 
+template <int ND>
 __device__ __forceinline__ void load_row(const Geo& g, const double* __restrict__ A, const double* x, int r,
-                                         RowProd& q) {
-  int i2, j2;
-  row_pos(g, r, i2, j2);
-  q.inner = i2 > 0 && i2 < g.n1 - 1 && j2 > 0 && j2 < g.n2 - 1;
+                                         RowProd<ND>& q) {
+  int i2, j2, k2;
+  row_pos(g, r, i2, j2, k2);
+  q.inner = on_boundary(g, i2, j2, k2) == 0;
   if (q.inner) {
     const long long N = g.N;
-    const int n1 = g.n1;
+    const int n1 = g.n1, n12 = g.n1 * g.n2;
+    int e = 0;
 #pragma unroll
-    for (int e = 0; e < 9; ++e) {
-      const int di = e % 3 - 1, dj = e / 3 - 1;
-      q.a[e] = __ldg(&A[e * N + r]);
-      q.x[e] = x[r + di + dj * n1];
-    }
+    for (int dk = (ND == 3 ? -1 : 0); dk <= (ND == 3 ? 1 : 0); ++dk)
+#pragma unroll
+      for (int dj = -1; dj <= 1; ++dj)
+#pragma unroll
+        for (int di = -1; di <= 1; ++di) {
+          if (ND == 3 && di != 0 && dj != 0 && dk != 0) continue;  // corner entries are zero
+          q.a[e] = __ldg(&A[e * N + r]);
+          q.x[e] = x[r + di + dj * n1 + dk * n12];
+          ++e;
+        }
   } else {
-    q.c = partner(g, i2, j2, r);
-    q.x[4] = x[r];
+    q.c = partner(g, i2, j2, k2, r);
+    q.x[RowProd<ND>::CENTER] = x[r];
     q.x[0] = q.c >= 0 ? x[q.c] : 0.0;
   }
 }
 
-__device__ __forceinline__ double row_value(const RowProd& q) {
-  if (!q.inner) return q.c >= 0 ? q.x[4] - q.x[0] : q.x[4];
-  double y = q.a[4] * q.x[4];
+template <int ND>
+__device__ __forceinline__ double row_value(const RowProd<ND>& q) {
+  constexpr int C = RowProd<ND>::CENTER;
+  if (!q.inner) return q.c >= 0 ? q.x[C] - q.x[0] : q.x[C];
+  double y = q.a[C] * q.x[C];
 #pragma unroll
-  for (int e = 0; e < 9; ++e)
-    if (e != 4) y = fma(q.a[e], q.x[e], y);
+  for (int e = 0; e < RowProd<ND>::NE; ++e)
+    if (e != C) y = fma(q.a[e], q.x[e], y);
   return y;
 }
 
 // r = b - A x; r̂ = r; p = v = 0 and the scalars of a fresh Krylov cycle.
 // first = 1: also ||r0||, the stopping tolerance and the iteration count;
 // otherwise (restart or the final check) done = (||r|| <= tol)
+template <int ND>
 __global__ void __launch_bounds__(NT) k_restart(Geo g, Vecs V, int first, double atol, double rtol, int max_iter) {
   __shared__ double s_red[2 * NT / 32];
   __shared__ int s_last;
   double acc[1] = {0.0};
   const int N = (int)g.N;
   for (int r = blockIdx.x * NT + threadIdx.x; r < N; r += gridDim.x * NT) {
-    RowProd q;
-    load_row(g, V.A, V.x, r, q);
+    RowProd<ND> q;
+    load_row<ND>(g, V.A, V.x, r, q);
     const double rr = V.b[r] - row_value(q);
     V.r[r] = rr;
     V.rh[r] = rr;
@@ -401,7 +546,9 @@ __global__ void __launch_bounds__(NT) k_p(Geo g, Vecs V) {
 }
 
 // v = A p̂; α = ρ / (r̂ · v)
+template <int ND>
 __global__ void __launch_bounds__(NT) k_v(Geo g, Vecs V) {
+  constexpr int US = ND == 2 ? 2 : 1;  // rows in flight per thread (9 or 19 loads each)
   __shared__ double s_red[2 * NT / 32];
   __shared__ int s_last;
   KState* K = V.ks;
@@ -409,13 +556,13 @@ __global__ void __launch_bounds__(NT) k_v(Geo g, Vecs V) {
   double acc[1] = {0.0};
   const int N = (int)g.N, stride = gridDim.x * NT;
   for (int r0 = blockIdx.x * NT + threadIdx.x; r0 < N; r0 += US * stride) {
-    RowProd q[US];
+    RowProd<ND> q[US];
     double h[US];
 #pragma unroll
     for (int k = 0; k < US; ++k) {
       const int r = r0 + k * stride;
       if (r < N) {
-        load_row(g, V.A, V.ph, r, q[k]);
+        load_row<ND>(g, V.A, V.ph, r, q[k]);
         h[k] = V.rh[r];
       }
     }
@@ -476,7 +623,9 @@ __global__ void __launch_bounds__(NT) k_s(Geo g, Vecs V) {
 }
 
 // t = A ŝ; ω = (t · s) / (t · t)
+template <int ND>
 __global__ void __launch_bounds__(NT) k_t(Geo g, Vecs V) {
+  constexpr int US = ND == 2 ? 2 : 1;
   __shared__ double s_red[2 * NT / 32];
   __shared__ int s_last;
   KState* K = V.ks;
@@ -484,13 +633,13 @@ __global__ void __launch_bounds__(NT) k_t(Geo g, Vecs V) {
   double acc[2] = {0.0, 0.0};
   const int N = (int)g.N, stride = gridDim.x * NT;
   for (int r0 = blockIdx.x * NT + threadIdx.x; r0 < N; r0 += US * stride) {
-    RowProd q[US];
+    RowProd<ND> q[US];
     double sv[US];
 #pragma unroll
     for (int k = 0; k < US; ++k) {
       const int r = r0 + k * stride;
       if (r < N) {
-        load_row(g, V.A, V.sh, r, q[k]);
+        load_row<ND>(g, V.A, V.sh, r, q[k]);
         sv[k] = V.s[r];
       }
     }
@@ -594,7 +743,9 @@ __global__ void __launch_bounds__(NT) k_post1(Geo g, double* x, const double* __
       const double a = x[r];
       x[r] = isfinite(a) ? 0.5 * (fabs(a) + a) : 0.0;
     }
-    const double u = T[mesh_index(g, (int)(r % g.n1), (int)(r / g.n1))];
+    int i2, j2, k2;
+    row_pos(g, (int)r, i2, j2, k2);
+    const double u = T[mesh_index(g, i2, j2, k2)];
     if (u != u) nan = true;
     m = fmax(m, u);
   }
@@ -632,7 +783,9 @@ __global__ void __launch_bounds__(NT) k_post2(Geo g, const double* __restrict__ 
   const double u0 = K->umax * ndt_tol;
   double m = -INFINITY;
   for (long long r = blockIdx.x * (long long)NT + threadIdx.x; r < g.N; r += (long long)gridDim.x * NT) {
-    const long long mi = mesh_index(g, (int)(r % g.n1), (int)(r / g.n1));
+    int i2, j2, k2;
+    row_pos(g, (int)r, i2, j2, k2);
+    const long long mi = mesh_index(g, i2, j2, k2);
     const double a = x[r], b = T[mi];
     const double d = fabs(a - b) / (a + u0);
     m = fmax(m, isfinite(d) ? d : 0.0);  // δ * isfinite(δ), false a strong zero
@@ -669,7 +822,9 @@ struct Implicit {
   int64_t nfull = 0;
   // device arrays: mesh inputs (full mesh layout)
   double* cellJ = nullptr;
-  double* edge[2][5] = {{nullptr}};  // J, ξ̂.x₁, ξ̂.x₂, η̂.x₁, η̂.x₂ per face family
+  double* edgeJ[3] = {nullptr, nullptr, nullptr};  // face J per family
+  double* edgehat[3][9] = {{nullptr}};              // J-scaled face metrics [3a + c] (2D: those read)
+  int nent = 9;                                     // stored stencil entries per row (3D: 19)
   double* T = nullptr;               // full mesh layout work copies
   double* rho = nullptr;
   // diffusion region
@@ -731,7 +886,9 @@ Implicit::~Implicit() {
   double* bufs[] = {cellJ, T, rho, A, alpha, S, x, r, rh, p, ph, v, s, sh, t, b, dinv, part};
   for (double* q : bufs)
     if (q) cudaFree(q);
-  for (auto& f : edge)
+  for (double* q : edgeJ)
+    if (q) cudaFree(q);
+  for (auto& f : edgehat)
     for (double* q : f)
       if (q) cudaFree(q);
   if (ks) cudaFree(ks);
@@ -782,36 +939,51 @@ int implicit_init(Implicit& s, const cdm_mesh_desc* mesh, const cdm_bc* bcs, con
     s.own_stream = true;
   }
   imp::Geo& g = s.g;
+  const int nd = mesh->ndim;
+  g.nd = nd;
   g.ni = mesh->ni;
   g.nj = mesh->nj;
+  g.nk = nd == 3 ? mesh->nk : 1;
   g.nh = mesh->nhalo;
   g.nx = mesh->ni + 2 * mesh->nhalo;
+  g.ny = mesh->nj + 2 * mesh->nhalo;
   g.n1 = mesh->ni + 2;
   g.n2 = mesh->nj + 2;
-  g.N = (long long)g.n1 * g.n2;
+  g.n3 = nd == 3 ? mesh->nk + 2 : 1;
+  g.N = (long long)g.n1 * g.n2 * g.n3;
   double gval[6] = {0, 0, 0, 0, 0, 0};
   int grule[6] = {0, 0, 0, 0, 0, 0};
-  if (resolve_ghost_rules(2, bcs, grule, gval) != CDM_OK) {
+  if (resolve_ghost_rules(nd, bcs, grule, gval) != CDM_OK) {
     set_error("invalid boundary condition kind");
     return CDM_BAD_INPUT;
   }
-  for (int l = 0; l < 4; ++l) {
+  for (int l = 0; l < 2 * nd; ++l) {
     g.kind[l] = bcs[l].kind;
     g.rule[l] = grule[l];
     g.val[l] = bcs[l].kind == CDM_BC_DIRICHLET ? bcs[l].value : 0.0;
   }
-  s.nfull = (int64_t)g.nx * (mesh->nj + 2 * mesh->nhalo);
+  s.nent = nd == 3 ? 19 : 9;
+  s.nfull = (int64_t)g.nx * g.ny * (nd == 3 ? mesh->nk + 2 * mesh->nhalo : 1);
   const size_t nf = (size_t)s.nfull, N = (size_t)g.N;
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, s.device);
   const long long need = (g.N + imp::NT - 1) / imp::NT;
   s.grid = (int)std::min<long long>(need, (long long)nsm * 8);
+  const cudaMemcpyKind kind = mesh->mem == CDM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   CDM_CK(zalloc(&s.cellJ, nf));
-  for (int f = 0; f < 2; ++f)
-    for (int q = 0; q < 5; ++q) CDM_CK(zalloc(&s.edge[f][q], nf));
+  CDM_CK(cudaMemcpy(s.cellJ, mesh->cell_J, nf * sizeof(double), kind));
+  for (int f = 0; f < nd; ++f) {
+    CDM_CK(zalloc(&s.edgeJ[f], nf));
+    CDM_CK(cudaMemcpy(s.edgeJ[f], mesh->edge_J[f], nf * sizeof(double), kind));
+    for (int a = 0; a < nd; ++a)
+      for (int c = 0; c < nd; ++c) {
+        CDM_CK(zalloc(&s.edgehat[f][3 * a + c], nf));
+        CDM_CK(cudaMemcpy(s.edgehat[f][3 * a + c], mesh->edge_hat[f][3 * a + c], nf * sizeof(double), kind));
+      }
+  }
   CDM_CK(zalloc(&s.T, nf));
   CDM_CK(zalloc(&s.rho, nf));
-  CDM_CK(zalloc(&s.A, 9 * N));
+  CDM_CK(zalloc(&s.A, (size_t)s.nent * N));
   double** vecs[] = {&s.alpha, &s.S, &s.x, &s.r, &s.rh, &s.p, &s.ph, &s.v, &s.s, &s.sh, &s.t, &s.b, &s.dinv};
   for (double** q : vecs) CDM_CK(zalloc(q, N));
   CDM_CK(zalloc(&s.part, (size_t)2 * s.grid));
@@ -823,14 +995,6 @@ int implicit_init(Implicit& s, const cdm_mesh_desc* mesh, const cdm_bc* bcs, con
   CDM_CK(cudaEventCreateWithFlags(&s.ev_caller, cudaEventDisableTiming));
   CDM_CK(cudaEventCreate(&s.e0));
   CDM_CK(cudaEventCreate(&s.e1));
-  const cudaMemcpyKind kind = mesh->mem == CDM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  const int hat_k[4] = {0, 1, 3, 4};  // ξ̂.x₁, ξ̂.x₂, η̂.x₁, η̂.x₂
-  CDM_CK(cudaMemcpy(s.cellJ, mesh->cell_J, nf * sizeof(double), kind));
-  for (int f = 0; f < 2; ++f) {
-    CDM_CK(cudaMemcpy(s.edge[f][0], mesh->edge_J[f], nf * sizeof(double), kind));
-    for (int q = 0; q < 4; ++q)
-      CDM_CK(cudaMemcpy(s.edge[f][1 + q], mesh->edge_hat[f][hat_k[q]], nf * sizeof(double), kind));
-  }
   return CDM_OK;
 }
 
@@ -882,39 +1046,46 @@ extern "C" int cdm_implicit_create(const cdm_mesh_desc* mesh, const cdm_bc* bcs,
     return CDM_BAD_INPUT;
   }
   *out = nullptr;
-  if (mesh->ndim != 2) {
-    set_error("the implicit scheme is built for 2D meshes");
+  const int nd = mesh->ndim;
+  if (nd != 2 && nd != 3) {
+    set_error("the implicit scheme takes 2D and 3D meshes");
     return CDM_BAD_INPUT;
   }
-  if (mesh->ni < 1 || mesh->nj < 1 || mesh->nhalo < 1) {
+  if (mesh->ni < 1 || mesh->nj < 1 || (nd == 3 && mesh->nk < 1) || mesh->nhalo < 1) {
     set_error("mesh sizes must be >= 1 and nhalo >= 1");
     return CDM_BAD_INPUT;
   }
-  if ((long long)(mesh->ni + 2) * (mesh->nj + 2) >= (1ll << 31)) {
+  if ((long long)(mesh->ni + 2) * (mesh->nj + 2) * (nd == 3 ? mesh->nk + 2 : 1) >= (1ll << 31)) {
     set_error("the implicit system takes fewer than 2^31 rows");
     return CDM_BAD_INPUT;
   }
-  for (int l = 0; l < 4; ++l)
+  for (int l = 0; l < 2 * nd; ++l)
     if (bcs[l].kind == CDM_BC_NEG_SYMMETRY || bcs[l].kind < CDM_BC_NEUMANN || bcs[l].kind > CDM_BC_NEG_SYMMETRY) {
       set_error("the implicit scheme takes Neumann, Dirichlet and periodic sides (init_matrix.jl)");
       return CDM_BAD_INPUT;
     }
+  // init_matrix.jl:7-12 and :184-192 (in 3D the test covers the i and j sides only)
   for (int a = 0; a < 2; ++a)
     if ((bcs[2 * a].kind == CDM_BC_PERIODIC) != (bcs[2 * a + 1].kind == CDM_BC_PERIODIC)) {
-      set_error("Inconsistent periodic boundary conditions");  // init_matrix.jl:7-12
+      set_error("Inconsistent periodic boundary conditions");
       return CDM_BAD_INPUT;
     }
-  if (!mesh->cell_J || !mesh->edge_J[0] || !mesh->edge_J[1]) {
-    set_error("the implicit scheme needs cell_J and the i/j face J");
+  if (!mesh->cell_J) {
+    set_error("the implicit scheme needs cell_J");
     return CDM_BAD_INPUT;
   }
-  const int hat_k[4] = {0, 1, 3, 4};
-  for (int f = 0; f < 2; ++f)
-    for (int k : hat_k)
-      if (!mesh->edge_hat[f][k]) {
-        set_error("the implicit scheme needs the face metrics xi_hat and eta_hat (x1, x2) of both face families");
-        return CDM_BAD_INPUT;
-      }
+  for (int f = 0; f < nd; ++f) {
+    if (!mesh->edge_J[f]) {
+      set_error("the implicit scheme needs the face J of every face family");
+      return CDM_BAD_INPUT;
+    }
+    for (int a = 0; a < nd; ++a)
+      for (int c = 0; c < nd; ++c)
+        if (!mesh->edge_hat[f][3 * a + c]) {
+          set_error("the implicit scheme needs the J-scaled face metrics of every face family");
+          return CDM_BAD_INPUT;
+        }
+  }
   cdm_apt_config c;
   cdm_apt_config_default(&c);
   if (cfg) c = *cfg;
@@ -946,12 +1117,17 @@ extern "C" int cdm_implicit_set_source(cdm_implicit* h, const double* S, int mem
   }
   Implicit& s = h->s;
   CDM_CK(cudaSetDevice(s.device));
-  // the diffusion region of a full mesh array, one row of n1 values per j
+  // the diffusion region of a full mesh array: n1 values per row, n2 rows per plane, n3 planes
   const imp::Geo& g = s.g;
   if (mem == CDM_MEM_DEVICE) CDM_CK(fence(s));
-  CDM_CK(cudaMemcpy2DAsync(s.S, (size_t)g.n1 * sizeof(double), S + (g.nh - 1) + (int64_t)g.nx * (g.nh - 1),
-                           (size_t)g.nx * sizeof(double), (size_t)g.n1 * sizeof(double), (size_t)g.n2,
-                           mem == CDM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s.stream));
+  const int64_t plane = (int64_t)g.nx * g.ny;
+  for (int k2 = 0; k2 < g.n3; ++k2) {
+    const int64_t kz = g.nd == 3 ? (int64_t)(k2 - 1 + g.nh) : 0;
+    const double* src = S + (g.nh - 1) + (int64_t)g.nx * (g.nh - 1) + kz * plane;
+    CDM_CK(cudaMemcpy2DAsync(s.S + (int64_t)k2 * g.n1 * g.n2, (size_t)g.n1 * sizeof(double), src,
+                             (size_t)g.nx * sizeof(double), (size_t)g.n1 * sizeof(double), (size_t)g.n2,
+                             mem == CDM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s.stream));
+  }
   CDM_CK(cudaStreamSynchronize(s.stream));
   return CDM_OK;
 }
@@ -981,7 +1157,8 @@ extern "C" int cdm_implicit_step(cdm_implicit* h, double* T, const double* rho, 
   // applybcs! on T and, with apply_density_bc, on rho (nonlinear_thermal_conduction.jl:19-23)
   CDM_CK(stage(s.T, T, s.nfull, o.mem, s.stream));
   CDM_CK(stage(s.rho, rho, s.nfull, o.mem, s.stream));
-  const dim3 gg((unsigned)std::max(1, std::min(64, (std::max(g.ni, g.nj) + 255) / 256)), 4);
+  const long long slab = std::max<long long>({(long long)g.nj * g.nk, (long long)g.ni * g.nk, (long long)g.ni * g.nj});
+  const dim3 gg((unsigned)std::max<long long>(1, std::min<long long>(256, (slab + 255) / 256)), 2 * g.nd);
   imp::ghost_fill<<<gg, 256, 0, s.stream>>>(g, s.T);
   if (o.apply_density_bc) imp::ghost_fill<<<gg, 256, 0, s.stream>>>(g, s.rho);
   // update_conductivity! and validate_scalar (:25-33)
@@ -999,13 +1176,17 @@ extern "C" int cdm_implicit_step(cdm_implicit* h, double* T, const double* rho, 
   imp::diffusivity_kernel<<<s.grid, imp::NT, 0, s.stream>>>(g, s.T, s.rho, cp, kappa.k0, kmode, km, khalf,
                                                             kappa.n, s.alpha, s.d_bad);
   imp::EdgeMetrics em;
-  for (int f = 0; f < 2; ++f) {
-    em.J[f] = s.edge[f][0];
-    for (int q = 0; q < 4; ++q) em.hat[f][q] = s.edge[f][1 + q];
+  for (int f = 0; f < 3; ++f) {
+    em.J[f] = s.edgeJ[f];
+    for (int q = 0; q < 9; ++q) em.hat[f][q] = s.edgehat[f][q];
   }
-  // assemble! (matrix_assembly.jl:5-31)
-  imp::assemble_kernel<<<s.grid, imp::NT, 0, s.stream>>>(g, s.mean, dt, s.alpha, s.T, s.S, s.cellJ, em, s.A, s.b,
-                                                         s.dinv);
+  // assemble! (matrix_assembly.jl:5-59)
+  if (g.nd == 2)
+    imp::assemble_kernel<<<s.grid, imp::NT, 0, s.stream>>>(g, s.mean, dt, s.alpha, s.T, s.S, s.cellJ, em, s.A,
+                                                           s.b, s.dinv);
+  else
+    imp::assemble_kernel3<<<s.grid, imp::NT, 0, s.stream>>>(g, s.mean, dt, s.alpha, s.T, s.S, s.cellJ, em, s.A,
+                                                            s.b, s.dinv);
   CDM_CK(cudaGetLastError());
   CDM_CK(cudaMemcpyAsync(s.h_bad, s.d_bad, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
   CDM_CK(cudaEventRecord(s.ev, s.stream));
@@ -1020,7 +1201,11 @@ extern "C" int cdm_implicit_step(cdm_implicit* h, double* T, const double* rho, 
   const int max_iter = o.max_iter > 0 ? o.max_iter : (int)std::min<long long>(2 * g.N, 1 << 30);
   imp::Vecs V = vecs_of(s);
   CDM_CK(cudaEventRecord(s.e0, s.stream));
-  imp::k_restart<<<s.grid, imp::NT, 0, s.stream>>>(g, V, 1, o.atol, o.rtol, max_iter);
+  auto restart = [&](int first) {
+    if (g.nd == 2) imp::k_restart<2><<<s.grid, imp::NT, 0, s.stream>>>(g, V, first, o.atol, o.rtol, max_iter);
+    else imp::k_restart<3><<<s.grid, imp::NT, 0, s.stream>>>(g, V, first, o.atol, o.rtol, max_iter);
+  };
+  restart(1);
   CDM_CK(cudaGetLastError());
   rc = read_state(s, timeout_s - (seconds_now() - t_start));
   bool fresh = true;  // r holds the true residual b - A x (just computed)
@@ -1037,7 +1222,7 @@ extern "C" int cdm_implicit_step(cdm_implicit* h, double* T, const double* rho, 
         stats->niter = K.iter;
         return stats->status = CDM_NONFINITE;
       }
-      imp::k_restart<<<s.grid, imp::NT, 0, s.stream>>>(g, V, 0, o.atol, o.rtol, max_iter);
+      restart(0);
       CDM_CK(cudaGetLastError());
       fresh = true;
       rc = read_state(s, timeout_s - (seconds_now() - t_start));
@@ -1048,9 +1233,11 @@ extern "C" int cdm_implicit_step(cdm_implicit* h, double* T, const double* rho, 
       CDM_CK(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal));
       for (int k = 0; k < imp::kPollIters; ++k) {
         imp::k_p<<<s.grid, imp::NT, 0, s.stream>>>(g, V);
-        imp::k_v<<<s.grid, imp::NT, 0, s.stream>>>(g, V);
+        if (g.nd == 2) imp::k_v<2><<<s.grid, imp::NT, 0, s.stream>>>(g, V);
+        else imp::k_v<3><<<s.grid, imp::NT, 0, s.stream>>>(g, V);
         imp::k_s<<<s.grid, imp::NT, 0, s.stream>>>(g, V);
-        imp::k_t<<<s.grid, imp::NT, 0, s.stream>>>(g, V);
+        if (g.nd == 2) imp::k_t<2><<<s.grid, imp::NT, 0, s.stream>>>(g, V);
+        else imp::k_t<3><<<s.grid, imp::NT, 0, s.stream>>>(g, V);
         imp::k_x<<<s.grid, imp::NT, 0, s.stream>>>(g, V);
       }
       const cudaError_t le = cudaGetLastError();
@@ -1114,7 +1301,21 @@ extern "C" int cdm_implicit_get_system(cdm_implicit* h, double* A, double* b) {
   Implicit& s = h->s;
   CDM_CK(cudaSetDevice(s.device));
   const size_t N = (size_t)s.g.N;
-  CDM_CK(cudaMemcpyAsync(A, s.A, 9 * N * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+  if (s.g.nd == 2) {
+    CDM_CK(cudaMemcpyAsync(A, s.A, 9 * N * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+  } else {  // the 19 stored entries into their slots of 27, the corner slots zero
+    int e = 0;
+    for (int slot = 0; slot < 27; ++slot) {
+      const int di = slot % 3 - 1, dj = (slot / 3) % 3 - 1, dk = slot / 9 - 1;
+      if (di != 0 && dj != 0 && dk != 0) {
+        std::memset(A + (size_t)slot * N, 0, N * sizeof(double));
+        continue;
+      }
+      CDM_CK(cudaMemcpyAsync(A + (size_t)slot * N, s.A + (size_t)e * N, N * sizeof(double), cudaMemcpyDeviceToHost,
+                             s.stream));
+      ++e;
+    }
+  }
   CDM_CK(cudaMemcpyAsync(b, s.b, N * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
   CDM_CK(cudaStreamSynchronize(s.stream));
   return CDM_OK;

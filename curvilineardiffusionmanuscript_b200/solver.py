@@ -341,7 +341,8 @@ class ImplicitScheme:
         if rc != L.CDM_OK:
             raise APTError(rc, L.last_error())
         self._h = h
-        self.rows = (mesh.ni + 2) * (mesh.nj + 2)
+        self.shape = ((mesh.nk + 2,) if mesh.ndim == 3 else ()) + (mesh.nj + 2, mesh.ni + 2)
+        self.rows = int(np.prod(self.shape))
 
     def close(self):
         if getattr(self, "_h", None):
@@ -382,10 +383,10 @@ class ImplicitScheme:
         return stats, ndt.value
 
     def system(self):
-        """(A, b) of the last step: A as (9, nj+2, ni+2) stencil entries, b as (nj+2, ni+2)."""
-        n2, n1 = self.mesh.nj + 2, self.mesh.ni + 2
-        A = np.zeros((9, n2, n1))
-        b = np.zeros((n2, n1))
+        """(A, b) of the last step: A as 9 (2D) or 27 (3D) stencil entries over the
+        region ([nk+2,] nj+2, ni+2), b over the region."""
+        A = np.zeros((9 if self.mesh.ndim == 2 else 27,) + self.shape)
+        b = np.zeros(self.shape)
         rc = self._lib.cdm_implicit_get_system(self._h, A.ctypes.data, b.ctypes.data)
         if rc != L.CDM_OK:
             raise APTError(rc, L.last_error())

@@ -341,8 +341,9 @@ int cdm_batch_get_profile(const cdm_batch* b, cdm_profile* out);
 /* ---- implicit comparator ------------------------------------------------
  * The reference's implicit scheme: backward Euler in the conservative
  * curvilinear form with the diffusivity taken at Tⁿ, one sparse linear system
- * per time step solved by a Krylov method.  2D, Neumann, Dirichlet and periodic
- * sides (FixedNegSymmetryBC has no matrix rows in the reference; CDM_BAD_INPUT).
+ * per time step solved by a Krylov method.  2D (9-point) and 3D (27-point
+ * stencil, 19 non-zero entries); Neumann, Dirichlet and periodic sides
+ * (FixedNegSymmetryBC has no matrix rows in the reference; CDM_BAD_INPUT).
  * The system covers the domain plus one halo layer; the reference's GMRES +
  * ILU(0) is replaced by Jacobi-preconditioned BiCGSTAB with the same stopping
  * rule on the true residual, ||b - A x||_2 <= atol + rtol ||b - A x0||_2. */
@@ -364,9 +365,9 @@ typedef struct cdm_implicit_opts {
 
 void cdm_implicit_opts_default(cdm_implicit_opts* opts);
 /* ImplicitScheme(mesh, bcs; mean, backend)  (ImplictSolver.jl:49-160); reads
- * mesh.cell_J, edge_J[0..1] and edge_hat[f][{0,1,3,4}] (the J-scaled ξ̂ and η̂
- * face metrics), cfg->mean and cfg->device (precision is not used) */
-int cdm_implicit_create(const cdm_mesh_desc* mesh, const cdm_bc* bcs /* 4 */, const cdm_apt_config* cfg,
+ * mesh.cell_J, edge_J[f] and edge_hat[f][3a + c] (the J-scaled face metrics)
+ * for f, a, c < ndim, cfg->mean and cfg->device (precision is not used) */
+int cdm_implicit_create(const cdm_mesh_desc* mesh, const cdm_bc* bcs /* 2 ndim */, const cdm_apt_config* cfg,
                         cdm_implicit** out);
 int cdm_implicit_destroy(cdm_implicit* h);
 /* scheme.source_term (ImplictSolver.jl:28): a full-size array, the domain and
@@ -384,8 +385,9 @@ int cdm_implicit_set_source(cdm_implicit* h, const double* S, int mem);
 int cdm_implicit_step(cdm_implicit* h, double* T, const double* rho, double cp, cdm_kappa kappa, double dt,
                       const cdm_implicit_opts* opts, cdm_stats* stats, double* next_dt);
 /* the system of the last step (no reference counterpart; for checks): A as 9
- * arrays of (ni+2)(nj+2) values, entry e = 3(dj+1) + (di+1) at offset (di, dj)
- * (offsets2d, inner_operators.jl:19-21) on interior rows (0 on boundary rows,
+ * (2D) or 27 (3D) arrays of rows = (ni+2)(nj+2)[(nk+2)] values, entry
+ * e = (di+1) + 3(dj+1) [+ 9(dk+1)] at offset (di, dj[, dk]) (offsets2d /
+ * offsets3d, inner_operators.jl:19-49) on interior rows (0 on boundary rows,
  * whose constraint rows are the ones init_matrix.jl builds), and b */
 int cdm_implicit_get_system(cdm_implicit* h, double* A, double* b);
 /* device time of the last Krylov solve (CUDA events), products with A, rows */

@@ -8,10 +8,10 @@ What it restates (paths inside the reference project):
 * the matrix pattern and its boundary rows        src/implicit/init_matrix.jl:1-170
   (diagonal 1 on every row; Neumann / periodic sides add -1 at the interior /
   opposite cell on the side's rows without the corners; Dirichlet adds nothing)
-* assemble!, _assembly_kernel_2d                  src/implicit/matrix_assembly.jl:5-31,
-                                                  src/implicit/inner_operators.jl:62-105
-* edge_diffusivity, conservative_edge_terms       inner_operators.jl:265-280, src/edge_terms.jl:31-87
-* stencil_2d                                      src/implicit/stencils.jl:14-40
+* assemble!, _assembly_kernel_2d / _3d           src/implicit/matrix_assembly.jl:5-59,
+                                                  src/implicit/inner_operators.jl:62-160
+* edge_diffusivity, conservative_edge_terms       inner_operators.jl:254-280, src/edge_terms.jl:31-87, :146-263
+* stencil_2d, stencil_3d                          src/implicit/stencils.jl:14-40, :42-137
 * bc_operator / bc_rhs_coefficient                inner_operators.jl:188-211,
                                                   src/boundary_conditions/boundary_operators.jl:271-273
 * update_conductivity! (scalar cp)                src/conductivity.jl:13-31, :93-104
@@ -36,8 +36,10 @@ import scipy.sparse.linalg as spla
 from oracle.oracle import applybcs
 
 NEUMANN, DIRICHLET, PERIODIC, NEG_SYMMETRY = 0, 1, 2, 3
-# stencil entries in the order of stencils.jl:35 (offsets2d, inner_operators.jl:19-21)
+# stencil entries in the order of stencils.jl:35 and :108-136 (offsets2d / offsets3d,
+# inner_operators.jl:19-49): i fastest, then j, then k
 OFFSETS_2D = [(-1, -1), (0, -1), (1, -1), (-1, 0), (0, 0), (1, 0), (-1, 1), (0, 1), (1, 1)]
+OFFSETS_3D = [(di, dj, dk) for dk in (-1, 0, 1) for dj in (-1, 0, 1) for di in (-1, 0, 1)]
 
 
 def pow_model(x, n):
@@ -72,36 +74,45 @@ def _mean(mean, a, b):
 
 
 class ImplicitOracle:
-    """ImplicitScheme + nonlinear_thermal_conduction_step! on one 2D mesh (nhalo >= 1).
+    """ImplicitScheme + nonlinear_thermal_conduction_step! on one 2D or 3D mesh (nhalo >= 1).
 
     The diffusion problem covers the domain and one halo layer (region 2 of
     ImplictSolver.jl:77-98); rows are numbered column-major over it."""
 
     def __init__(self, mesh, bcs, mean="harmonic"):
-        assert mesh.ndim == 2, "the implicit oracle restates the 2D scheme"
         self.mesh = mesh
+        self.nd = mesh.ndim
         self.bcs = list(bcs.values()) if isinstance(bcs, dict) else list(bcs)
         self.kinds = [b.kind for b in self.bcs]
         self.vals = [float(getattr(b, "value", 0.0)) for b in self.bcs]
+        # init_matrix.jl:7-12 and :184-192 (in 3D the k sides are not part of the test)
         for lo, hi in ((0, 1), (2, 3)):
             if (self.kinds[lo] == PERIODIC) != (self.kinds[hi] == PERIODIC):
-                raise ValueError("Inconsistent periodic boundary conditions")  # init_matrix.jl:7-12
+                raise ValueError("Inconsistent periodic boundary conditions")
         if NEG_SYMMETRY in self.kinds:
             raise ValueError("the implicit scheme has no FixedNegSymmetryBC rows")
         self.mean = mean
         m = mesh
-        self.n1, self.n2 = m.ni + 2, m.nj + 2
-        self.N = self.n1 * self.n2
         h = m.nhalo
-        # region 2 inside the mesh arrays
-        self.sl = (slice(h - 1, h + m.nj + 1), slice(h - 1, h + m.ni + 1))  # [j, i] on (ny, nx) views
-        self.source = np.zeros((self.n2, self.n1))
-        self.x = None  # Krylov warm start (the previous solution)
+        self.n1, self.n2 = m.ni + 2, m.nj + 2
+        self.n3 = m.nk + 2 if self.nd == 3 else 1
+        self.N = self.n1 * self.n2 * self.n3
+        # region 2 inside the mesh arrays ([k,] j, i views)
+        self.sl = (slice(h - 1, h + m.nj + 1), slice(h - 1, h + m.ni + 1))
+        if self.nd == 3:
+            self.sl = (slice(h - 1, h + m.nk + 1),) + self.sl
+        self.shape = (self.n3, self.n2, self.n1) if self.nd == 3 else (self.n2, self.n1)
+        self.source = np.zeros(self.shape)
+        self.x = None
+
+    def _full_shape(self):
+        m, h = self.mesh, self.mesh.nhalo
+        fs = (m.nj + 2 * h, m.ni + 2 * h)
+        return ((m.nk + 2 * h),) + fs if self.nd == 3 else fs
 
     def _r2(self, a):
-        """Region 2 of a full mesh array, as a (nj+2, ni+2) [j, i] view."""
-        m = self.mesh
-        a = np.asarray(a, dtype=np.float64).reshape(m.nj + 2 * m.nhalo, m.ni + 2 * m.nhalo)
+        """Region 2 of a full mesh array, as a ([nk+2,] nj+2, ni+2) view."""
+        a = np.asarray(a, dtype=np.float64).reshape(self._full_shape())
         return a[self.sl]
 
     def set_source(self, S):
@@ -109,17 +120,40 @@ class ImplicitOracle:
 
     # ---------------------------------------------------------------- assembly
     def assemble(self, T, rho, cp, k0, n, dt):
-        """A (scipy CSR), b, the 9 stencil coefficients of the interior rows
-        (9, nj+2, ni+2; zero elsewhere) and alpha, for temperatures T and
-        densities rho already carrying their boundary conditions."""
+        """A (scipy CSR), b, the stencil coefficients of the interior rows
+        (9 or 27, region-2 shape; zero elsewhere) and alpha, for T and rho
+        already carrying their boundary conditions."""
         m = self.mesh
         Tr, rr = self._r2(T), self._r2(rho)
         with np.errstate(divide="ignore", invalid="ignore"):
             alpha = np.abs(kappa(k0, n, Tr) / (rr * cp))
         J = self._r2(m.cell_J)
-        eJ = [self._r2(m.edge_J[f]) for f in range(2)]
+        nf = self.nd
+        eJ = [self._r2(m.edge_J[f]) for f in range(nf)]
         eh = [[self._r2(m.edge_hat[f][k]) if m.edge_hat[f][k] is not None else None for k in range(9)]
-              for f in range(2)]
+              for f in range(nf)]
+        c = self._stencil2(alpha, J, eJ, eh, dt) if self.nd == 2 else self._stencil3(alpha, J, eJ, eh, dt)
+        I = (slice(1, -1),) * self.nd
+        b = np.zeros(self.shape)
+        b[I] = (self.source[I] * dt + Tr[I]) * J[I]
+        rhs = [0.0 if k != DIRICHLET else v for k, v in zip(self.kinds, self.vals)]
+        # bc_operator priority ilo, ihi, jlo, jhi[, klo, khi]: later assignments win here
+        if self.nd == 3:
+            b[-1, :, :] = rhs[5]
+            b[0, :, :] = rhs[4]
+            b[:, -1, :] = rhs[3]
+            b[:, 0, :] = rhs[2]
+            b[:, :, -1] = rhs[1]
+            b[:, :, 0] = rhs[0]
+        else:
+            b[-1, :] = rhs[3]
+            b[0, :] = rhs[2]
+            b[:, -1] = rhs[1]
+            b[:, 0] = rhs[0]
+        A = self._matrix(c)
+        return A, b.ravel(), c, alpha
+
+    def _stencil2(self, alpha, J, eJ, eh, dt):
         I = slice(1, -1)
         a_c = alpha[I, I]
         a_ip = _mean(self.mean, a_c, alpha[I, 2:])
@@ -162,46 +196,108 @@ class ImplicitOracle:
         c[3][I, I] = (a_etaxi_jp - a_etaxi_jm - a_xi2_im) * dt   # i-1, j
         c[7][I, I] = (-a_eta2_jp - a_xieta_ip + a_xieta_im) * dt  # i, j+1
         c[1][I, I] = (-a_eta2_jm + a_xieta_ip - a_xieta_im) * dt  # i, j-1
-        # right-hand side: (S dt + u) J inside, bc_operator on the boundary rows
-        b = np.zeros((self.n2, self.n1))
-        b[I, I] = (self.source[I, I] * dt + Tr[I, I]) * Jc
-        rhs = [0.0 if k != DIRICHLET else v for k, v in zip(self.kinds, self.vals)]
-        # priority of bc_operator: ilo, ihi, jlo, jhi (later assignments first here)
-        b[-1, :] = rhs[3]
-        b[0, :] = rhs[2]
-        b[:, -1] = rhs[1]
-        b[:, 0] = rhs[0]
-        A = self._matrix(c)
-        return A, b.ravel(), c, alpha
+        return c
+
+    def _stencil3(self, alpha, J, eJ, eh, dt):
+        I = slice(1, -1)
+        C3 = (I, I, I)
+        a_c = alpha[C3]
+        sh = {"c": C3, "i": (I, I, slice(None, -2)), "j": (I, slice(None, -2), I), "k": (slice(None, -2), I, I)}
+        a = {"ip": _mean(self.mean, a_c, alpha[I, I, 2:]), "im": _mean(self.mean, a_c, alpha[I, I, :-2]),
+             "jp": _mean(self.mean, a_c, alpha[I, 2:, I]), "jm": _mean(self.mean, a_c, alpha[I, :-2, I]),
+             "kp": _mean(self.mean, a_c, alpha[2:, I, I]), "km": _mean(self.mean, a_c, alpha[:-2, I, I])}
+
+        def face(f, where):
+            """J and the three J-scaled metric vectors (ξ̂, η̂, ζ̂) of a face (edge_terms.jl:158-233)."""
+            s = sh[where]
+            vec = [[eh[f][3 * v + cc][s] for cc in range(3)] for v in range(3)]
+            return eJ[f][s], vec
+
+        def dot(u, v):
+            return u[0] * v[0] + u[1] * v[1] + u[2] * v[2]
+
+        t = {}
+        for name, f, where in (("ip", 0, "c"), ("im", 0, "i"), ("jp", 1, "c"), ("jm", 1, "j"), ("kp", 2, "c"),
+                               ("km", 2, "k")):
+            Jf, (xi, eta, zeta) = face(f, where)
+            al = a[name]
+            if f == 0:  # edge_terms.jl:235-243
+                t["xi2_" + name] = al * dot(xi, xi) / Jf
+                t["xieta_" + name] = al * dot(xi, eta) / (4.0 * Jf)
+                t["xizeta_" + name] = al * dot(xi, zeta) / (4.0 * Jf)
+            elif f == 1:  # :245-250
+                t["eta2_" + name] = al * dot(eta, eta) / Jf
+                t["etaxi_" + name] = al * dot(xi, eta) / (4.0 * Jf)
+                t["etazeta_" + name] = al * dot(eta, zeta) / (4.0 * Jf)
+            else:  # :252-257
+                t["zeta2_" + name] = al * dot(zeta, zeta) / Jf
+                t["zetaxi_" + name] = al * dot(zeta, xi) / (4.0 * Jf)
+                t["zetaeta_" + name] = al * dot(zeta, eta) / (4.0 * Jf)
+        T = t
+        c = np.zeros((27, self.n3, self.n2, self.n1))
+        slot = lambda di, dj, dk: (di + 1) + 3 * (dj + 1) + 9 * (dk + 1)
+        # stencils.jl:84-106
+        c[slot(0, -1, -1)][C3] = (-T["zetaeta_km"] - T["etazeta_jm"]) * dt
+        c[slot(-1, 0, -1)][C3] = (-T["zetaxi_km"] - T["xizeta_im"]) * dt
+        c[slot(1, 0, -1)][C3] = (T["zetaxi_km"] + T["xizeta_ip"]) * dt
+        c[slot(0, 1, -1)][C3] = (T["zetaeta_km"] + T["etazeta_jp"]) * dt
+        c[slot(-1, -1, 0)][C3] = (-T["etaxi_jm"] - T["xieta_im"]) * dt
+        c[slot(1, -1, 0)][C3] = (T["etaxi_jm"] + T["xieta_ip"]) * dt
+        c[slot(-1, 1, 0)][C3] = (T["etaxi_jp"] + T["xieta_im"]) * dt
+        c[slot(1, 1, 0)][C3] = (-T["etaxi_jp"] - T["xieta_ip"]) * dt
+        c[slot(0, -1, 1)][C3] = (T["zetaeta_kp"] + T["etazeta_jm"]) * dt
+        c[slot(-1, 0, 1)][C3] = (T["zetaxi_kp"] + T["xizeta_im"]) * dt
+        c[slot(1, 0, 1)][C3] = (-T["zetaxi_kp"] - T["xizeta_ip"]) * dt
+        c[slot(0, 1, 1)][C3] = (-T["zetaeta_kp"] - T["etazeta_jp"]) * dt
+        c[slot(0, 0, 0)][C3] = J[C3] + (T["zeta2_kp"] + T["zeta2_km"] + T["eta2_jp"] + T["eta2_jm"] + T["xi2_ip"]
+                                        + T["xi2_im"]) * dt
+        c[slot(1, 0, 0)][C3] = (-T["xi2_ip"] - T["etaxi_jp"] + T["etaxi_jm"] - T["zetaxi_kp"] + T["zetaxi_km"]) * dt
+        c[slot(-1, 0, 0)][C3] = (-T["xi2_im"] + T["etaxi_jp"] - T["etaxi_jm"] + T["zetaxi_kp"] - T["zetaxi_km"]) * dt
+        c[slot(0, 1, 0)][C3] = (-T["eta2_jp"] - T["xieta_ip"] + T["xieta_im"] - T["zetaeta_kp"] + T["zetaeta_km"]) * dt
+        c[slot(0, -1, 0)][C3] = (-T["eta2_jm"] + T["xieta_ip"] - T["xieta_im"] + T["zetaeta_kp"] - T["zetaeta_km"]) * dt
+        c[slot(0, 0, 1)][C3] = (-T["zeta2_kp"] - T["xizeta_ip"] + T["xizeta_im"] - T["etazeta_jp"]
+                                + T["etazeta_jm"]) * dt
+        c[slot(0, 0, -1)][C3] = (-T["zeta2_km"] + T["xizeta_ip"] - T["xizeta_im"] + T["etazeta_jp"]
+                                 - T["etazeta_jm"]) * dt
+        return c
 
     def _matrix(self, c):
-        n1, n2 = self.n1, self.n2
-        idx = np.arange(self.N).reshape(n2, n1)
-        rows, cols, vals = [idx.ravel()], [idx.ravel()], [np.ones(self.N)]
-        inner = idx[1:-1, 1:-1].ravel()
-        for s, (di, dj) in enumerate(OFFSETS_2D):
-            if (di, dj) == (0, 0):
+        idx = np.arange(self.N).reshape(self.shape)
+        offs = OFFSETS_2D if self.nd == 2 else OFFSETS_3D
+        strides = (1, self.n1, self.n1 * self.n2)
+        inner_sl = (slice(1, -1),) * self.nd
+        inner = idx[inner_sl].ravel()
+        rows, cols, vals = [], [], []
+        diag = np.ones(self.N)
+        for s, off in enumerate(offs):
+            if all(o == 0 for o in off):
+                diag[inner] = c[s][inner_sl].ravel()
                 continue
             rows.append(inner)
-            cols.append(inner + di + dj * n1)
-            vals.append(c[s][1:-1, 1:-1].ravel())
-        diag = np.ones(self.N)
-        diag[inner] = c[4][1:-1, 1:-1].ravel()
-        vals[0] = diag
-        # boundary rows (init_matrix.jl:69-167), corners excluded
-        jj = np.arange(1, n2 - 1)
-        ii = np.arange(1, n1 - 1)
-        sides = [
-            (self.kinds[0], idx[jj, 0], idx[jj, 1], idx[jj, n1 - 2]),
-            (self.kinds[1], idx[jj, n1 - 1], idx[jj, n1 - 2], idx[jj, 1]),
-            (self.kinds[2], idx[0, ii], idx[1, ii], idx[n2 - 2, ii]),
-            (self.kinds[3], idx[n2 - 1, ii], idx[n2 - 2, ii], idx[1, ii]),
-        ]
-        for kind, r, neumann_col, periodic_col in sides:
+            cols.append(inner + sum(o * st for o, st in zip(off, strides)))
+            vals.append(c[s][inner_sl].ravel())
+        rows.insert(0, idx.ravel())
+        cols.insert(0, idx.ravel())
+        vals.insert(0, diag)
+        # boundary rows (init_matrix.jl:69-167, :252-390): every side over the
+        # interior range of the other axes (edges and corners: the diagonal only)
+        n = (self.n1, self.n2, self.n3)[:self.nd]
+        for side in range(2 * self.nd):
+            axis, lo = side // 2, side % 2 == 0
+            kind = self.kinds[side]
+            if kind not in (NEUMANN, PERIODIC):
+                continue
+            # region-2 coordinates of the side's rows, arrays indexed [k, j, i] -> reverse axis
+            sel = [slice(1, -1)] * self.nd
+            ax = self.nd - 1 - axis
+            sel[ax] = 0 if lo else -1
+            r = idx[tuple(sel)].ravel()
+            st = strides[axis]
             if kind == NEUMANN:
-                rows.append(r), cols.append(neumann_col), vals.append(-np.ones(len(r)))
-            elif kind == PERIODIC:
-                rows.append(r), cols.append(periodic_col), vals.append(-np.ones(len(r)))
+                col = r + st if lo else r - st
+            else:  # periodic: the cell next to the opposite side's ghost
+                col = r + (n[axis] - 2) * st if lo else r - (n[axis] - 2) * st
+            rows.append(r), cols.append(col), vals.append(-np.ones(len(r)))
         return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
                              shape=(self.N, self.N))
 
@@ -212,12 +308,13 @@ class ImplicitOracle:
         in place over region 2; returns (stats, next_dt, A, b, c) with c the
         stencil entries of the interior rows (9, nj+2, ni+2)."""
         m = self.mesh
-        applybcs(2, m.ni, m.nj, 1, m.nhalo, self.bcs, T)
+        nk = m.nk if self.nd == 3 else 1
+        applybcs(self.nd, m.ni, m.nj, nk, m.nhalo, self.bcs, T)
         rho = rho.copy()
         if apply_density_bc:
-            applybcs(2, m.ni, m.nj, 1, m.nhalo, self.bcs, rho)
+            applybcs(self.nd, m.ni, m.nj, nk, m.nhalo, self.bcs, rho)
         A, b, c, alpha = self.assemble(T, rho, cp, k0, n, dt)
-        dom = alpha[1:-1, 1:-1]
+        dom = alpha[(slice(1, -1),) * self.nd]
         if not np.all(np.isfinite(dom)):
             raise ValueError("invalid diffusivity")
         x = spla.spsolve(A.tocsc(), b)
@@ -233,7 +330,7 @@ class ImplicitOracle:
         d = np.where(np.isfinite(d), d, 0.0) * 1.0
         mr = d.max()
         ndt = min(dt * np.sqrt(abs(maximum_u_change / mr)), timestep_growth_factor * dt)
-        self._r2(T)[...] = x.reshape(self.n2, self.n1)
+        self._r2(T)[...] = x.reshape(self.shape)
         self.x = x
         return {"abs_err": resid, "rel_err": resid}, ndt, A, b, c
 

@@ -14,8 +14,9 @@ def _assemble(pr, dt=None):
     T, rho = pr.T0.numpy().copy(), pr.rho.numpy().copy()
     from oracle.oracle import applybcs
     m = pr.mesh
-    applybcs(2, m.ni, m.nj, 1, m.nhalo, pr.bcs, T)
-    applybcs(2, m.ni, m.nj, 1, m.nhalo, pr.bcs, rho)
+    nk = m.nk if m.ndim == 3 else 1
+    applybcs(m.ndim, m.ni, m.nj, nk, m.nhalo, pr.bcs, T)
+    applybcs(m.ndim, m.ni, m.nj, nk, m.nhalo, pr.bcs, rho)
     A, b, c, alpha = o.assemble(T, rho, pr.cp, pr.kappa.k0, pr.kappa.n, dt or pr.dt)
     return o, A, b, c, alpha
 
@@ -76,3 +77,35 @@ def test_small_time_step_returns_the_input():
     o.step(T, pr.rho.numpy(), pr.cp, pr.kappa.k0, pr.kappa.n, 1e-16)
     d = o._r2(T)[1:-1, 1:-1] - o._r2(pr.T0.numpy())[1:-1, 1:-1]
     assert np.max(np.abs(d)) < 1e-8
+
+
+def test_3d_rows_sum_to_the_cell_volume_and_uniform_seven_point():
+    from helpers import small_case_3d
+    from curvilineardiffusionmanuscript_b200.mesh import wavy_mesh_3d
+    pr = small_case_3d(n=(9, 8, 7), amp=0.06)
+    o, A, b, c, _ = _assemble(pr, dt=1e-3)
+    I = (slice(1, -1),) * 3
+    J = o._r2(pr.mesh.cell_J)[I]
+    assert np.max(np.abs(c[(slice(None),) + I].sum(axis=0) - J) / J) < 1e-11
+    corners = [s for s in range(27) if s in (0, 2, 6, 8, 18, 20, 24, 26)]
+    assert all(np.all(c[s] == 0.0) for s in corners)  # stencils.jl:75-82
+    # uniform mesh, constant α: the seven-point operator
+    import torch
+    from curvilineardiffusionmanuscript_b200 import problems
+    from curvilineardiffusionmanuscript_b200.solver import PowerLawConductivity
+    n = 6
+    m = wavy_mesh_3d(n, n, n, amp=0.0, nhalo=1)
+    T0 = torch.ones_like(m.cell_J).contiguous()
+    pru = problems.Problem("u3", m, [NeumannBC()] * 6, T0, torch.ones_like(T0), 1.0,
+                           PowerLawConductivity(2.0, 0.0), 1e-3, 1)
+    o, A, b, c, _ = _assemble(pru)
+    h3 = (1.0 / n) ** 3
+    h = 1.0 / n
+    face = [4, 10, 12, 14, 16, 22]
+    for s in range(27):
+        if s == 13:
+            assert np.allclose(c[s][I], h3 + 6 * 2.0 * h * 1e-3, rtol=1e-12)
+        elif s in face:
+            assert np.allclose(c[s][I], -2.0 * h * 1e-3, rtol=1e-12)
+        else:
+            assert np.max(np.abs(c[s][I])) < 1e-17

@@ -64,7 +64,8 @@ def test_trajectory_follows_the_oracle():
 
 
 def _assert_system(r):
-    assert np.array_equal(r["Ag"][:, 1:-1, 1:-1], r["c"][:, 1:-1, 1:-1])
+    inner = (slice(None),) + (slice(1, -1),) * (r["Ag"].ndim - 1)
+    assert np.array_equal(r["Ag"][inner], r["c"][inner])
     assert np.array_equal(r["bg"].ravel(), r["b"])
 
 
@@ -148,3 +149,18 @@ def test_invalid_inputs():
     with pytest.raises(APTError) as ei:
         g.step(pr.mesh, T, pr.rho.numpy(), pr.cp, pr.kappa, pr.dt)
     assert ei.value.status in (2, 3)
+
+
+@pytest.mark.parametrize("bcs", [
+    None,
+    [DirichletBC(1.5), NeumannBC(), PeriodicBC(), PeriodicBC(), NeumannBC(), DirichletBC(3.0)],
+])
+def test_3d_assembly_bit_exact_and_tight_solution(bcs):
+    from helpers import small_case_3d
+    pr = small_case_3d(n=(13, 11, 9), amp=0.05, kn=2.5, bcs=bcs)
+    _, _, out = _pair(pr, nsteps=2, **TIGHT)
+    for r in out:
+        _assert_system(r)
+        T3 = lambda T: np.asarray(T).reshape(pr.mesh.nk + 2, pr.mesh.nj + 2, pr.mesh.ni + 2)
+        assert rel_l2(T3(r["Tg"]), T3(r["To"])) <= 1e-10
+        assert abs(r["ndg"] - r["ndo"]) <= 1e-8 * abs(r["ndo"])
