@@ -572,31 +572,32 @@ __global__ void __launch_bounds__(kPlanThreads) march2d_wave_plan(const Problem*
     W.mask[p] = m;
   }
   __syncthreads();
-  // jobs round by round, problems in order within a round
-  int jobs = 0, tickets = 0;
-  for (int r = 0; r < K; ++r) {
-    for (int base = 0; base < nprob; base += kPlanThreads) {
-      const int p = base + tid;
-      unsigned long long m = 0ull;
-      int nt = 0;
-      if (p < nprob) {
-        m = W.mask[p];
-        if ((m >> r) & 1ull) nt = probs[p].ntiles;
-      }
-      const int part = ((m >> r) & 1ull) ? 1 : 0;
-      long long tot;
-      const long long inc = plan_scan(((long long)part << 40) | (long long)nt, s_w, &tot);
-      if (part) {
-        const long long ex = inc - (((long long)part << 40) | (long long)nt);
-        const int J = jobs + (int)(ex >> 40);
-        W.tb[J] = tickets + (int)(ex & ((1ll << 40) - 1));
-        W.pj[J] = make_int2(p, __popcll(m & ((1ull << r) - 1ull)));
-      }
-      jobs += (int)(tot >> 40);
-      tickets += (int)(tot & ((1ll << 40) - 1));
+  // jobs round by round, problems in order within a round: the (round,
+  // problem) pairs q = r·nprob + p in ticket order, each thread a contiguous
+  // run of them, one block scan for every thread's first job and ticket
+  const int total = K * nprob;
+  const int per = (total + kPlanThreads - 1) / kPlanThreads;
+  const int q0 = min(total, tid * per), q1 = min(total, q0 + per);
+  long long mine = 0;
+  for (int q = q0; q < q1; ++q) {
+    const int r = q / nprob, p = q - r * nprob;
+    if ((W.mask[p] >> r) & 1ull) mine += (1ll << 40) | (long long)probs[p].ntiles;
+  }
+  long long tot;
+  const long long ex = plan_scan(mine, s_w, &tot) - mine;
+  int J = (int)(ex >> 40), tk = (int)(ex & ((1ll << 40) - 1));
+  for (int q = q0; q < q1; ++q) {
+    const int r = q / nprob, p = q - r * nprob;
+    const unsigned long long m = W.mask[p];
+    if ((m >> r) & 1ull) {
+      W.tb[J] = tk;
+      W.pj[J] = make_int2(p, __popcll(m & ((1ull << r) - 1ull)));
+      ++J;
+      tk += probs[p].ntiles;
     }
   }
   if (tid == 0) {
+    const int jobs = (int)(tot >> 40), tickets = (int)(tot & ((1ll << 40) - 1));
     W.tb[jobs] = tickets;
     W.head[0] = jobs;
     W.head[1] = tickets;
