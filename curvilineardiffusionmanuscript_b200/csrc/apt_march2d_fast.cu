@@ -46,11 +46,19 @@ using fastmath::pow_fast;
 using fastmath::rcp_nr;
 using fastmath::rcp_pos;
 
+// the row's divergence coefficients, uⁿ and the source, copied into shared
+// memory a row ahead by asynchronous copies (each thread its own column): their
+// loads then overlap a whole row instead of the row's face computations, and
+// hold no registers while in flight
+constexpr bool kCoAsync = true;
+constexpr int kCoVals = 7;
+
 template <int TX>
 struct FastSmem {
   double U[3][TX], IA[3][TX], IT[3][TX];  // u, α⁻¹ (or α), θ⁻¹ (or θ) for the i-1 neighbour
   double QX[3][TX], PX[3][TX];           // new damped / undamped i+1/2 fluxes
   double QY[2][TX], PY[2][TX];           // new damped / undamped j+1/2 fluxes
+  double CO[kCoAsync ? 2 : 1][kCoVals][TX];  // g11, g22, c12, α, β, uⁿ, S of rows j, j+1
   double red[TX / 32];
   int flag;
   int ticket;
@@ -61,6 +69,13 @@ struct FastSmem {
 struct Cell {
   double u, ia, it, g, f;
 };
+
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 }  // namespace
 
@@ -314,10 +329,31 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
   double rqx_m = qx_m, rqx_0 = qx_0, rpx_m = px_m, rpx_0 = px_0, rqy_m = qy_m, rpy_m = py_m;
   double g0 = c0.g, f0 = c0.f;  // update factors of row j; its u, α⁻¹, θ⁻¹ are read from shared memory
 
+  // coefficients of row r into buffer r & 1 (owners only; every thread commits a group)
+  auto fetch_co = [&](int r) {
+    if (owner) {
+      const int o = col + nx * (r + nh);
+      const int b = r & 1;
+      cp_async8(&sm.CO[b][0][tid], G11 + o);
+      cp_async8(&sm.CO[b][1][tid], G22 + o);
+      cp_async8(&sm.CO[b][2][tid], C12 + o);
+      cp_async8(&sm.CO[b][3][tid], CA + o);
+      cp_async8(&sm.CO[b][4][tid], CB + o);
+      cp_async8(&sm.CO[b][5][tid], uprev + o);
+      cp_async8(&sm.CO[b][6][tid], Sg + o);
+    }
+    cp_async_commit();
+  };
+  if (kCoAsync) fetch_co(j0);
+
   double local = 0.0;
   bool local_nan = false;
   for (int j = j0; j < j1; ++j) {
     const int o = col + nx * (j + nh);
+    if (kCoAsync) {
+      if (j + 1 < j1) fetch_co(j + 1);
+      else cp_async_commit();  // an empty group: the wait below still covers row j
+    }
     const Cell cp1 = stage(j + 1, Ln);
     const double lqx = Ln.qx, lqy = Ln.qy;  // old fluxes of row j + 1, used below
     if (j + 1 < j1) prefetch(j + 2, Ln);
@@ -325,7 +361,7 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
     __syncthreads();
     // the row's coefficients: their loads overlap the face computations
     double g11 = 0, g22 = 0, c12 = 0, ca = 0, cbv = 0, up = 0, S = 0;
-    if (owner) {
+    if (!kCoAsync && owner) {
       g11 = G11[o];
       g22 = G22[o];
       c12 = C12[o];
@@ -345,6 +381,19 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
       sm.PY[y_0][tid] = py_0n;
     }
     __syncthreads();
+    if (kCoAsync) {
+      cp_async_wait1();  // this thread's copies of row j have landed
+      if (owner) {
+        const int b = j & 1;
+        g11 = sm.CO[b][0][tid];
+        g22 = sm.CO[b][1][tid];
+        c12 = sm.CO[b][2][tid];
+        ca = sm.CO[b][3][tid];
+        cbv = sm.CO[b][4][tid];
+        up = sm.CO[b][5][tid];
+        S = sm.CO[b][6][tid];
+      }
+    }
     if (owner) {
       const int x = tid;
       const double dq = g11 * (rqx_0 - sm.QX[s_0][x - 1]) + g22 * (qy_0n - rqy_m) +
