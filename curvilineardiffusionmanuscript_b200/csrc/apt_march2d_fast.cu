@@ -49,16 +49,18 @@ using fastmath::rcp_pos;
 // the row's divergence coefficients, uⁿ and the source, copied into shared
 // memory a row ahead by asynchronous copies (each thread its own column): their
 // loads then overlap a whole row instead of the row's face computations, and
-// hold no registers while in flight
-constexpr bool kCoAsync = true;
+// hold no registers while in flight.  The wavefront kernel (CO = true) does
+// this; the per-iteration kernels keep plain loads: their 6 blocks of 128
+// threads per SM would not fit the buffer's shared memory
 constexpr int kCoVals = 7;
+constexpr int kCoBuf = 2;  // rows in flight + 1: the copies of row j + kCoBuf - 1 are issued at row j
 
-template <int TX>
+template <int TX, bool CO = false>
 struct FastSmem {
   double U[3][TX], IA[3][TX], IT[3][TX];  // u, α⁻¹ (or α), θ⁻¹ (or θ) for the i-1 neighbour
   double QX[3][TX], PX[3][TX];           // new damped / undamped i+1/2 fluxes
   double QY[2][TX], PY[2][TX];           // new damped / undamped j+1/2 fluxes
-  double CO[kCoAsync ? 2 : 1][kCoVals][TX];  // g11, g22, c12, α, β, uⁿ, S of rows j, j+1
+  double CO_[CO ? kCoBuf : 1][kCoVals][CO ? TX : 1];  // g11, g22, c12, α, β, uⁿ, S of the next rows
   double red[TX / 32];
   int flag;
   int ticket;
@@ -70,12 +72,7 @@ struct Cell {
   double u, ia, it, g, f;
 };
 
-__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
 
 }  // namespace
 
@@ -84,7 +81,8 @@ __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_g
 // L2 only (no read-only-path or L1 copies of another block's writes).
 template <int TX, bool EDGE, bool HARM, bool WAVE = false>
 __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, int iter, bool check,
-                                          FastSmem<TX>& sm, int* wave_count = nullptr) {
+                                          FastSmem<TX, WAVE>& sm, int* wave_count = nullptr) {
+  constexpr bool kCoAsync = WAVE;
   constexpr int OW = TX - 2;
   const int tid = threadIdx.x;
   const int cb = tile % P.tiles_i, sj = tile / P.tiles_i;
@@ -329,31 +327,29 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
   double rqx_m = qx_m, rqx_0 = qx_0, rpx_m = px_m, rpx_0 = px_0, rqy_m = qy_m, rpy_m = py_m;
   double g0 = c0.g, f0 = c0.f;  // update factors of row j; its u, α⁻¹, θ⁻¹ are read from shared memory
 
-  // coefficients of row r into buffer r & 1 (owners only; every thread commits a group)
+  // coefficients of row r into buffer r mod kCoBuf (owners only; every thread commits a group)
   auto fetch_co = [&](int r) {
-    if (owner) {
+    if (owner && r < j1) {
       const int o = col + nx * (r + nh);
-      const int b = r & 1;
-      cp_async8(&sm.CO[b][0][tid], G11 + o);
-      cp_async8(&sm.CO[b][1][tid], G22 + o);
-      cp_async8(&sm.CO[b][2][tid], C12 + o);
-      cp_async8(&sm.CO[b][3][tid], CA + o);
-      cp_async8(&sm.CO[b][4][tid], CB + o);
-      cp_async8(&sm.CO[b][5][tid], uprev + o);
-      cp_async8(&sm.CO[b][6][tid], Sg + o);
+      const int b = r % kCoBuf;
+      cp_async8(&sm.CO_[b][0][tid], G11 + o);
+      cp_async8(&sm.CO_[b][1][tid], G22 + o);
+      cp_async8(&sm.CO_[b][2][tid], C12 + o);
+      cp_async8(&sm.CO_[b][3][tid], CA + o);
+      cp_async8(&sm.CO_[b][4][tid], CB + o);
+      cp_async8(&sm.CO_[b][5][tid], uprev + o);
+      cp_async8(&sm.CO_[b][6][tid], Sg + o);
     }
     cp_async_commit();
   };
-  if (kCoAsync) fetch_co(j0);
+  if (kCoAsync)
+    for (int r = j0; r < j0 + kCoBuf - 1; ++r) fetch_co(r);
 
   double local = 0.0;
   bool local_nan = false;
   for (int j = j0; j < j1; ++j) {
     const int o = col + nx * (j + nh);
-    if (kCoAsync) {
-      if (j + 1 < j1) fetch_co(j + 1);
-      else cp_async_commit();  // an empty group: the wait below still covers row j
-    }
+    if (kCoAsync) fetch_co(j + kCoBuf - 1);  // past the strip: an empty group, so the wait below covers row j
     const Cell cp1 = stage(j + 1, Ln);
     const double lqx = Ln.qx, lqy = Ln.qy;  // old fluxes of row j + 1, used below
     if (j + 1 < j1) prefetch(j + 2, Ln);
@@ -382,16 +378,16 @@ __device__ __forceinline__ void fast_body(const Problem& P, Ctrl* C, int tile, i
     }
     __syncthreads();
     if (kCoAsync) {
-      cp_async_wait1();  // this thread's copies of row j have landed
+      cp_async_wait<kCoBuf - 1>();  // this thread's copies of row j have landed
       if (owner) {
-        const int b = j & 1;
-        g11 = sm.CO[b][0][tid];
-        g22 = sm.CO[b][1][tid];
-        c12 = sm.CO[b][2][tid];
-        ca = sm.CO[b][3][tid];
-        cbv = sm.CO[b][4][tid];
-        up = sm.CO[b][5][tid];
-        S = sm.CO[b][6][tid];
+        const int b = j % kCoBuf;
+        g11 = sm.CO_[b][0][tid];
+        g22 = sm.CO_[b][1][tid];
+        c12 = sm.CO_[b][2][tid];
+        ca = sm.CO_[b][3][tid];
+        cbv = sm.CO_[b][4][tid];
+        up = sm.CO_[b][5][tid];
+        S = sm.CO_[b][6][tid];
       }
     }
     if (owner) {
@@ -659,7 +655,7 @@ template <int TX, bool HARM>
 __global__ void __launch_bounds__(TX, 640 / TX) march2d_fast_wave(const Problem* __restrict__ probs,
                                                            const int2* __restrict__ items, WavePlan W,
                                                            unsigned int* counters, int* wave_count) {
-  __shared__ FastSmem<TX> sm;
+  __shared__ FastSmem<TX, true> sm;
   const int total = W.head[1], njobs = W.head[0];
   while (true) {
     // thread 0 takes the ticket, finds its job and waits for the problem's

@@ -112,6 +112,16 @@ __device__ __forceinline__ void stage_problem(Problem& dst, const Problem* __res
   __syncthreads();
 }
 
+// asynchronous 8-byte copy global -> shared memory (cp.async, L1-allocating:
+// for arrays no block writes during the launch), its group commit and wait
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 __host__ __device__ inline int64_t fidx(const Problem& P, int a, int b, int c = 0) {
   // domain coordinates (a, b, c) -> full-array offset
   return (int64_t)(a + P.nh) + (int64_t)P.nx * ((int64_t)(b + P.nh) + (int64_t)P.ny * (int64_t)(c + (P.ndim == 3 ? P.nh : 0)));
