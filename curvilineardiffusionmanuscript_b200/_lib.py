@@ -20,7 +20,7 @@ CDM_BC_NEUMANN, CDM_BC_DIRICHLET, CDM_BC_PERIODIC, CDM_BC_NEG_SYMMETRY = range(4
 CDM_MEAN_HARMONIC, CDM_MEAN_ARITHMETIC = 0, 1
 CDM_NORM_MAX, CDM_NORM_RMS = 0, 1
 CDM_PREC_FP64, CDM_PREC_MIXED, CDM_PREC_FP64_EXACT = 0, 1, 2
-CDM_GUESS_PREV, CDM_GUESS_USER, CDM_GUESS_LEARNED = 0, 1, 2
+CDM_GUESS_PREV, CDM_GUESS_USER, CDM_GUESS_LEARNED, CDM_GUESS_EXTRAPOLATE = 0, 1, 2, 3
 
 PD = C.POINTER(C.c_double)
 

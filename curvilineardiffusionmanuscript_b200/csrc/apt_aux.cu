@@ -368,6 +368,18 @@ cudaError_t launch_clamp(double* u, int64_t n, int positivity, int cutoff, cudaS
   return cudaGetLastError();
 }
 
+// extrapolated start: out = 2a - b (a = Tⁿ, b = Tⁿ⁻¹) over the full array
+__global__ void extrapolate_kernel(double* __restrict__ out, const double* __restrict__ a,
+                                   const double* __restrict__ b, int64_t n) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+    out[e] = 2.0 * a[e] - b[e];
+}
+
+cudaError_t launch_extrapolate(double* out, const double* a, const double* b, int64_t n, cudaStream_t s) {
+  extrapolate_kernel<<<grid_for(n, 256), 256, 0, s>>>(out, a, b, n);
+  return cudaGetLastError();
+}
+
 int step_reduction_blocks(int64_t nfull) {
   int64_t nb = (nfull + kRedThreads - 1) / kRedThreads;
   if (nb > kRedBlocks) nb = kRedBlocks;

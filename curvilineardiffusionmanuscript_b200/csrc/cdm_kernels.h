@@ -115,6 +115,9 @@ cudaError_t launch_dirichlet_fill(const Problem& P, double* u, cudaStream_t s);
 // enforce_positivity / cutoff! over the full array (PseudoTransientSolver.jl:323-368)
 cudaError_t launch_clamp(double* u, int64_t n, int positivity, int cutoff, cudaStream_t s);
 
+// extrapolated start of a step: out = 2·Tⁿ − Tⁿ⁻¹ over the full array
+cudaError_t launch_extrapolate(double* out, const double* Tn, const double* Tnm1, int64_t n, cudaStream_t s);
+
 // next_dt reductions (timestep_control.jl:33-73) and the energy balance.
 // out[0] = max(u_prev) (NaN-propagating), out[1] = max relative change,
 // out[2] = sum rho*cp*T*J (T = u_prev) over the domain, out[3] = same for u,

@@ -855,6 +855,19 @@ int Engine::learned_guess(int p, const cdm_kappa& kappa) {
   return 1;
 }
 
+// Linear extrapolation of this step's solution from the last two steps,
+// 2Tⁿ − Tⁿ⁻¹ (the part of the learned guess the network corrects): 1 when
+// s.guess holds it, 0 when the step starts from Tⁿ (no previous step), -1 on
+// a CUDA error.  No reference counterpart (the reference starts from Tⁿ).
+int Engine::extrapolated_guess(int p) {
+  ProbState& s = ps[p];
+  if (!s.has_hist) return 0;
+  if (!s.guess && dalloc(&s.guess, (size_t)s.nfull) != cudaSuccess) return -1;
+  if (launch_extrapolate(s.guess, s.u_prev, s.t_hist, s.nfull, stream) != cudaSuccess) return -1;
+  prof.other_launches += 1;
+  return 1;
+}
+
 // A guessed start is stopped where the plain start would stop: the relative
 // criterion (:297) divides by the residual norm that the plain start (u = Tⁿ)
 // reaches at its first check.  One FP64 iteration from Tⁿ gives that norm;
@@ -1010,6 +1023,11 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
       const int lg = learned_guess(p, kappa[p]);
       if (lg < 0) return lg == -1 ? CDM_CUDA_ERROR : -lg;
       if (lg == 1) init = s.guess;
+    } else if (o.guess == CDM_GUESS_EXTRAPOLATE) {
+      keep_hist = true;
+      const int lg = extrapolated_guess(p);
+      if (lg < 0) return CDM_CUDA_ERROR;
+      if (lg == 1) init = s.guess;
     }
     inits[p] = init;
     guessed[p] = init != s.u_prev;
@@ -1154,8 +1172,8 @@ int Engine::step(double* const* T, const double* const* rho, const double* cp, c
       continue;
     }
     s.last_err_check = C.iter;
-    // Tⁿ becomes the previous step of the next call's learned guess
-    if (guess_net) {
+    // Tⁿ becomes the previous step of the next call's learned or extrapolated guess
+    if (guess_net || keep_hist) {
       if (!s.t_hist) CDM_CK(dalloc(&s.t_hist, (size_t)s.nfull));
       CDM_CK(cudaMemcpyAsync(s.t_hist, s.u_prev, (size_t)s.nfull * sizeof(double), cudaMemcpyDeviceToDevice,
                              stream));
@@ -1439,7 +1457,7 @@ int cdm_apt_set_guess_net(cdm_apt* h, cdm_net* net, double log_jmean) {
   if (!h) return CDM_BAD_INPUT;
   h->e.guess_net = net;
   h->e.log_jmean = log_jmean;
-  if (!net)
+  if (!net && !h->e.keep_hist)
     for (auto& s : h->e.ps) s.has_hist = 0;
   return CDM_OK;
 }

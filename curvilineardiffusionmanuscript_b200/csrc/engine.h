@@ -152,6 +152,8 @@ struct Engine {
   int mixed_alloc();
   int step_mixed(const cdm_step_opts* o, double t_start, double timeout_s);
   int learned_guess(int p, const cdm_kappa& kappa);
+  int extrapolated_guess(int p);
+  bool keep_hist = false;  // a step asked for the extrapolated start: keep Tⁿ for the next one
   int autotune(double* const* T, const double* const* rho, const double* cp, const cdm_kappa* kappa,
                const double* dt, const cdm_step_opts* opts, const char* cache_path, int* chosen);
   int probe_plain_norm(const std::vector<int>& guessed, const std::vector<const double*>& init, double t_start,

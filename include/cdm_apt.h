@@ -84,7 +84,10 @@ enum cdm_precision {
 enum cdm_guess {
   CDM_GUESS_PREV = 0,   /* u = T^n, as PseudoTransientSolver.jl:229                */
   CDM_GUESS_USER = 1,   /* u = array given by cdm_apt_set_guess                    */
-  CDM_GUESS_LEARNED = 2 /* u = T^n + network(T^n, T^{n-1}, kappa, J) (learned guess) */
+  CDM_GUESS_LEARNED = 2, /* u = T^n + network(T^n, T^{n-1}, kappa, J) (learned guess) */
+  CDM_GUESS_EXTRAPOLATE = 3 /* u = 2 T^n - T^{n-1}, the previous call's T^n kept by the
+                               handle (the first call starts from T^n); no counterpart in
+                               the reference, which starts from T^n (PseudoTransientSolver.jl:229) */
 };
 
 /* conductivity model: replaces the Julia closure kappa(rho, T) of the drivers,

@@ -178,3 +178,35 @@ def test_trained_guess_gain_over_the_plain_start():
         assert e_tr <= 0.5 * e_un, (e_tr, e_un)
     print(f"pseudo-iterations of steps 2..6: plain {total_plain}, learned {total_learned}")
     assert total_learned < total_plain, (total_learned, total_plain)
+
+
+def test_extrapolated_start_matches_the_user_guess_and_the_plain_solution():
+    """CDM_GUESS_EXTRAPOLATE starts step n+1 from 2Tⁿ − Tⁿ⁻¹ (the first step
+    from Tⁿ): bit for bit the run of a user guess computed the same way, and
+    within the stopping tolerance of the plain start's solution."""
+    pr = small_problem(128)(901)
+    kw = dict(rtol=1e-8, atol=1e-8, max_iter=100000, check_every=4)
+
+    def run(mode):
+        g = PseudoTransientSolver(pr.mesh, pr.bcs)
+        T, prev, its = pr.T0.clone(), None, []
+        for k in range(4):
+            guess = L.CDM_GUESS_PREV
+            if mode == "extrap":
+                guess = L.CDM_GUESS_EXTRAPOLATE
+            elif mode == "user" and prev is not None:
+                g.set_guess((2.0 * T - prev).contiguous())
+                guess = L.CDM_GUESS_USER
+            cur = T.clone()
+            st, _ = step(g, pr.mesh, T, pr.rho, pr.cp, pr.kappa, pr.dt, guess=guess, **kw)
+            prev = cur
+            its.append(st["niter"])
+        g.close()
+        return T, its
+
+    Te, ie = run("extrap")
+    Tu, iu = run("user")
+    Tp, ip = run("plain")
+    assert ie == iu and torch.equal(Te, Tu)
+    assert ie[0] == ip[0]
+    assert rel_l2(Te.cpu().numpy(), Tp.cpu().numpy()) <= 1e-6
