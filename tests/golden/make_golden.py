@@ -15,6 +15,7 @@ sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "tests"))
 
 from helpers import small_case_2d, small_case_3d  # noqa: E402
+from oracle.implicit_oracle import ImplicitOracle  # noqa: E402
 from oracle.oracle import OracleSolver  # noqa: E402
 from curvilineardiffusionmanuscript_b200.solver import DirichletBC, PeriodicBC, NeumannBC, FixedNegSymmetryBC  # noqa: E402
 
@@ -48,9 +49,38 @@ def run_case(name, spec, nsteps=3):
     return dict(T=T, q=q, last=last, cache=o.metric_cache(), **{k: np.array(v) for k, v in out.items()})
 
 
+# the implicit scheme's oracle: two steps of a 2D and a 3D case (stencil entries,
+# right-hand side and solution of every step)
+IMPLICIT_CASES = {
+    "implicit2d": dict(dim=2, kw=dict(ni=14, nj=11, bcs=[DirichletBC(1.5), NeumannBC(), PeriodicBC(), PeriodicBC()],
+                                      source=True)),
+    "implicit3d": dict(dim=3, kw=dict(n=(7, 6, 5))),
+}
+
+
+def run_implicit(name, spec, nsteps=2):
+    pr = small_case_2d(**spec["kw"]) if spec["dim"] == 2 else small_case_3d(**spec["kw"])
+    o = ImplicitOracle(pr.mesh, pr.bcs)
+    if pr.source is not None:
+        o.set_source(pr.source.numpy())
+    T = pr.T0.numpy().copy()
+    out = {"c": [], "b": [], "T": [], "next_dt": []}
+    for _ in range(nsteps):
+        _, ndt, A, b, c = o.step(T, pr.rho.numpy(), pr.cp, pr.kappa.k0, pr.kappa.n, pr.dt)
+        out["c"].append(c)
+        out["b"].append(b)
+        out["T"].append(T.copy())
+        out["next_dt"].append(ndt)
+    return {k: np.array(v) for k, v in out.items()}
+
+
 if __name__ == "__main__":
     here = Path(__file__).resolve().parent
     for name, spec in CASES.items():
         res = run_case(name, spec)
         np.savez_compressed(here / f"{name}.npz", **res)
         print(name, res["niter"], res["T"].shape)
+    for name, spec in IMPLICIT_CASES.items():
+        res = run_implicit(name, spec)
+        np.savez_compressed(here / f"{name}.npz", **res)
+        print(name, res["c"].shape, res["next_dt"])

@@ -109,3 +109,23 @@ def test_3d_rows_sum_to_the_cell_volume_and_uniform_seven_point():
             assert np.allclose(c[s][I], -2.0 * h * 1e-3, rtol=1e-12)
         else:
             assert np.max(np.abs(c[s][I])) < 1e-17
+
+
+def test_oracle_matches_its_golden_fixtures():
+    """The implicit oracle's stencil entries, right-hand sides and solutions of
+    two steps (tests/golden/make_golden.py) against regressions: the entries and
+    b bit for bit, the direct solutions to rounding."""
+    import sys
+    from pathlib import Path
+    here = Path(__file__).resolve().parent / "golden"
+    sys.path.insert(0, str(here))
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", here / "make_golden.py")
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    for name, sp in mg.IMPLICIT_CASES.items():
+        ref = np.load(here / f"{name}.npz")
+        res = mg.run_implicit(name, sp)
+        assert np.array_equal(res["c"], ref["c"]) and np.array_equal(res["b"], ref["b"]), name
+        assert np.max(np.abs(res["T"] - ref["T"])) <= 1e-12 * np.max(np.abs(ref["T"])), name
+        assert np.allclose(res["next_dt"], ref["next_dt"], rtol=1e-10), name
