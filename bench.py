@@ -27,6 +27,7 @@ step one time step of every sampled problem after the warm-up steps; the
   python bench.py --compare [--workload W]     seconds per time step, FP64 vs mixed (vs learned)
   python bench.py --net-timing N               guess network: training step and N^2 prediction
   python bench.py --implicit N                 the implicit comparator, s/timestep on the N^2 multi-Gaussian
+  python bench.py --implicit3d N               the same on the N^3 Gaussian pulse
 
 Without --tuning the kernel variant, strip height and iteration block are
 chosen by the library's autotuner before the warm-up (outside the timed
@@ -78,6 +79,8 @@ def parse():
     ap.add_argument("--compare-steps", type=int, default=3)
     ap.add_argument("--implicit", type=int, default=0, metavar="N",
                     help="time the implicit comparator on the N^2 multi-Gaussian problem (--steps, --warmup)")
+    ap.add_argument("--implicit3d", type=int, default=0, metavar="N",
+                    help="the same on the N^3 Gaussian pulse (kappa = T^2.5)")
     return ap.parse_args()
 
 
@@ -690,13 +693,18 @@ def run_net_timing(args):
 
 def run_implicit(args):
     """Seconds per time step of the implicit comparator on the N² multi-Gaussian
-    problem (κ = T³, seed 0), one JSON line."""
+    problem (κ = T³, seed 0) or the N³ Gaussian pulse (κ = T^2.5), one JSON line."""
     import torch
     from curvilineardiffusionmanuscript_b200 import problems
     dev = torch.device("cuda", 0)
-    pr = problems.multi_gaussian_2d(args.implicit, seed=0, device=dev)
+    if args.implicit3d:
+        n, nd = args.implicit3d, 3
+        pr = problems.gaussian_3d(n, device=dev)
+    else:
+        n, nd = args.implicit, 2
+        pr = problems.multi_gaussian_2d(n, seed=0, device=dev)
     r = time_implicit(pr, args.steps, args.warmup, torch.cuda.current_stream(dev))
-    r.update(n=args.implicit, rows=(args.implicit + 2) ** 2)
+    r.update(n=n, ndim=nd, rows=(n + 2) ** nd)
     peak, kind = measured_peak()
     if r["solve_GBs"]:
         r["roofline"] = {"bound": "hbm", "achieved": r["solve_GBs"], "peak": peak, "unit": "GB/s",
@@ -706,7 +714,7 @@ def run_implicit(args):
 
 def main():
     args = parse()
-    if args.implicit:
+    if args.implicit or args.implicit3d:
         run_implicit(args)
         return
     if args.net_timing:
