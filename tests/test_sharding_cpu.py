@@ -212,3 +212,25 @@ def test_sharded_batch_from_factory_builds_only_local_problems():
     assert sorted(res[0][1] + res[1][1]) == list(range(7))
     for rank, local, built, niters in res:
         assert built == local and niters == sizes
+
+
+def test_batch_weights_follow_the_expected_iterations():
+    """The bench's LPT weights: expected iterations grow with the side and, at
+    the batch's larger sides, with the conductivity exponent; on 8 seeded
+    batches over 8 ranks the weighted assignment carries less spread of
+    expected work than the assignment by cells alone."""
+    from curvilineardiffusionmanuscript_b200 import problems as P
+    from curvilineardiffusionmanuscript_b200.sharding import lpt_assign
+    e = P.batch_expected_iterations
+    assert e({"n": 512, "kn": 3.0}) > e({"n": 256, "kn": 3.0}) > e({"n": 64, "kn": 3.0})
+    assert e({"n": 400, "kn": 3.0}) > e({"n": 400, "kn": 1.0}) > e({"n": 400, "kn": 0.0})
+    params = [q for r in range(8) for q in P.batch_2d_params(256, seed=P.BATCH_SEED + r)]
+    cells = [q["n"] ** 2 for q in params]
+    work = [c * e(q) for c, q in zip(cells, params)]
+
+    def spread(assign):
+        loads = [sum(work[i] for i in a) for a in assign]
+        return max(loads) / (sum(loads) / len(loads))
+
+    assert spread(lpt_assign(work, 8)) < spread(lpt_assign(cells, 8))
+    assert spread(lpt_assign(work, 8)) < 1.01
