@@ -129,3 +129,26 @@ def test_oracle_matches_its_golden_fixtures():
         assert np.array_equal(res["c"], ref["c"]) and np.array_equal(res["b"], ref["b"]), name
         assert np.max(np.abs(res["T"] - ref["T"])) <= 1e-12 * np.max(np.abs(ref["T"])), name
         assert np.allclose(res["next_dt"], ref["next_dt"], rtol=1e-10), name
+
+
+def test_3d_boundary_rows_follow_the_side_kinds():
+    """init_matrix.jl:252-390: each side's rows over the interior range of the
+    other two axes; Neumann and periodic rows pair with the interior / opposite
+    cell, Dirichlet rows and edge or corner rows keep the diagonal only."""
+    from helpers import small_case_3d
+    bcs = [DirichletBC(1.5), NeumannBC(), NeumannBC(), NeumannBC(), PeriodicBC(), PeriodicBC()]
+    pr = small_case_3d(n=(5, 4, 6), bcs=bcs)
+    o, A, b, c, _ = _assemble(pr)
+    A = A.tocsr()
+    n1, n2, n3 = o.n1, o.n2, o.n3
+    rid = lambda i, j, k: i + n1 * (j + n2 * k)
+    r = rid(0, 2, 3)  # ilo, Dirichlet: the diagonal only, b = 1.5
+    assert A[r].nnz == 1 and A[r, r] == 1.0 and b[r] == 1.5
+    r = rid(n1 - 1, 2, 3)  # ihi, Neumann: -1 at the interior neighbour
+    assert A[r].nnz == 2 and A[r, rid(n1 - 2, 2, 3)] == -1.0 and b[r] == 0.0
+    r = rid(2, 1, 0)  # klo, periodic: -1 at (i, j, khi - 1)
+    assert A[r].nnz == 2 and A[r, rid(2, 1, n3 - 2)] == -1.0
+    r = rid(2, 1, n3 - 1)  # khi, periodic: -1 at (i, j, klo + 1)
+    assert A[r].nnz == 2 and A[r, rid(2, 1, 1)] == -1.0
+    r = rid(0, 0, 2)  # an edge (ilo and jlo): the diagonal only, bc_operator takes ilo first
+    assert A[r].nnz == 1 and b[r] == 1.5
